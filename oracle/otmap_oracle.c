@@ -25,8 +25,9 @@
 #define VID(i, j) ((j) + (i) * (n + 1))
 #define FID(i, j) ((j) + (i) * n)
 
-static double dmin(double a, double b) { return a < b ? a : b; }
-static double dmax(double a, double b) { return a > b ? a : b; }
+/* std::min / std::max semantics (NaN in the second argument yields the first) */
+static double dmin(double a, double b) { return b < a ? b : a; }
+static double dmax(double a, double b) { return a < b ? b : a; }
 
 /* ------------------------------------------------------------------------- */
 /* otsolver_2dgrid.cpp:47-63 */
