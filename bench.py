@@ -1,0 +1,411 @@
+#!/usr/bin/env python
+"""Throughput of 1024^2 grid transport solves on B200 (residual <= 1e-7).
+
+One step = one batch of `--batch` independent 1024x1024 solves of the single-large-
+solve workload (6 random filled disks / convex polygons, value 1 on background
+1e-3, Gaussian blur sigma = 5 px, normalised to mean 1; seeded synthetic data),
+solved together by the library's batched engine; value = solves/s over all ranks.
+Multi-GPU runs are weak-scaled: every rank solves its own batch, no collective on
+the data path (instances are independent).
+
+Fields beyond the base contract:
+  e2e           the same metric through the public C ABI with host (pinned) inputs
+                and outputs, host<->device copies inside the timed region
+  plain         solves/s of the plain single-instance form: the same densities
+                solved one call at a time
+  roofline      dominant kernel: algorithmic bytes (or flops) / its CUDA-event time
+  cpu_baseline  the reference library (compiled from its own sources) timed on this
+                host: one full 1024^2 solve on one core, rank 0 at N=1 only
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "1024^2 OT solves/s at residual<=1e-7"
+UNIT = "solves/s"
+N_GRID = 1024
+THRESHOLD = 1e-7
+SIGMA_PX = 5.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--batch", type=int, default=8)
+    p.add_argument("--n", type=int, default=N_GRID)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations timed per step")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def densities(n, count, first_seed):
+    from otmap_b200 import workloads as W
+
+    return [W.to_cells(W.blurred_shapes(n, first_seed + k, sigma_px=SIGMA_PX)) for k in range(count)]
+
+
+def config(args, world, extra=None):
+    c = {"workload": f"{args.n}x{args.n} blurred shapes (6 disks/convex polygons, sigma 5 px, floor 1e-3), "
+                     f"threshold {THRESHOLD:g}, batch {args.batch} per GPU",
+         "grid": args.n, "batch_per_gpu": args.batch, "global_batch": args.batch * world,
+         "threshold": THRESHOLD, "parallelism": f"independent instances x{world}"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if parts[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+# algorithmic traffic per cell for one launch of each stencil kernel (FP64 arrays
+# read + written once each; halos, L2 hits and scalars not counted)
+STENCIL_ARRAYS = {"beta": 5, "coeffs": 5, "update": 5}
+
+
+def roofline(prof, stats, ns, peaks):
+    """Dominant kernel of the profiled launches: achieved algorithmic rate / measured peak."""
+    if not prof:
+        return None
+    name, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
+    cells_iter = sum(st.iterations * n * n for st, n in zip(stats, ns))
+    if name in STENCIL_ARRAYS:
+        alg = STENCIL_ARRAYS[name] * 8 * cells_iter
+        return {"kernel": name, "bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peaks.get("hbm_gbs"),
+                "unit": "GB/s", "frac": (alg / (ms / 1e3) / 1e9) / peaks.get("hbm_gbs", 1.0),
+                "launches": cnt, "avg_launch_us": ms * 1e3 / max(cnt, 1), "alg_bytes_per_cell": STENCIL_ARRAYS[name] * 8,
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}
+    if name == "dct_gemm":
+        flops = sum(st.iterations * 4 * 2.0 * n ** 3 for st, n in zip(stats, ns))
+        tf = flops / (ms / 1e3) / 1e12
+        return {"kernel": name, "bound": "fp64", "achieved": tf, "unit": "TFLOP/s", "peak": None, "frac": None,
+                "launches": cnt, "avg_launch_us": ms * 1e3 / max(cnt, 1), "traffic": None,
+                "note": "FP64 CUDA-core GEMM form of the cosine transform (8 n^3 flop per Poisson solve)"}
+    return {"kernel": name, "launches": cnt, "total_ms": ms}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        d["source"] = "measured"
+        return d
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from otmap_b200 import native as N
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    ctx = N.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+    n, B = args.n, args.batch
+    ns = [n] * B
+    host = densities(n, B, 1000 * rank)
+    dev_in = [torch.from_numpy(d).cuda() for d in host]
+    V = (n + 1) ** 2
+    dev_out = [torch.empty((V, 2), dtype=torch.float64, device="cuda") for _ in range(B)]
+    opt = N.default_options()
+    opt.threshold = THRESHOLD
+    stats = (N.SolveStatsC * B)()
+    ns_c = (C.c_int * B)(*ns)
+
+    def solve_batch(inp, out):
+        dp = (C.c_void_p * B)(*[x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data for x in inp])
+        fp = (C.c_void_p * B)(*[x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data for x in out])
+        N.check(N.lib().otm_solve_batch(ctx.handle, B, ns_c, dp, C.byref(opt), fp, None, stats))
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    def timed(inp, out, steps, profile=False):
+        ctx.profile(-1)
+        ctx.profile(1 if profile else 0)
+        total = 0.0
+        launches0 = ctx.launch_count()
+        barrier()
+        torch.cuda.synchronize()
+        for _ in range(steps):
+            flush.fill_(1.0)  # L2 flush between steps (outside the events)
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            solve_batch(inp, out)
+            b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        torch.cuda.synchronize()
+        barrier()
+        launches = ctx.launch_count() - launches0
+        prof = ctx.profile_totals() if profile else None
+        ctx.profile(0)
+        return total, launches, prof
+
+    for k in range(B):
+        ctx.init(n)
+    for _ in range(args.warmup):
+        solve_batch(dev_in, dev_out)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    clocks.start()
+    t_ms, launches, prof = timed(dev_in, dev_out, args.steps, profile=True)
+    clk = clocks.stop()
+
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_ms = float(t.item())
+    ms_step = t_ms / args.steps
+    value = B * world / (ms_step / 1e3)
+    st_list = [stats[k] for k in range(B)]
+    iters = [s.iterations for s in st_list]
+    resid = [s.residual for s in st_list]
+
+    e2e = None
+    if not args.no_e2e:
+        h_in = [torch.from_numpy(d).pin_memory() for d in host]
+        h_out = [torch.empty((V, 2), dtype=torch.float64).pin_memory() for _ in range(B)]
+        e_ms, _, _ = timed(h_in, h_out, args.steps)
+        if world > 1:
+            import torch.distributed as dist
+
+            t = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        e2e = {"value": B * world / (e_ms / args.steps / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": B * n * n * 8, "d2h_bytes_per_step": B * V * 2 * 8}
+
+    plain = None
+    if not args.no_plain:
+        # the plain single-instance form: one otm_solve call per density
+        tot = 0.0
+        torch.cuda.synchronize()
+        for k in range(B):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            N.check(N.lib().otm_solve(ctx.handle, n, C.c_void_p(dev_in[k].data_ptr()), C.byref(opt),
+                                      C.c_void_p(dev_out[k].data_ptr()), None, None))
+            b.record(stream)
+            b.synchronize()
+            tot += a.elapsed_time(b)
+        plain = {"value": B / (tot / 1e3), "unit": UNIT, "form": "one otm_solve call per density, same kernels"}
+
+    peaks = load_peaks()
+    roof = roofline(prof, st_list, ns, peaks)
+    if roof is not None:
+        roof["peak_source"] = roof.get("peak_source", peaks.get("source"))
+    kernels = {k: {"ms": v[0], "launches": v[1]} for k, v in (prof or {}).items()}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(host[0], n)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
+                "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
+                "iterations": iters, "final_residual_max": max(resid), "gpu_launches": launches,
+                "e2e": e2e, "plain": plain, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "cpu_baseline": cpu}
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    ctx.close()
+
+
+def cpu_baseline(density_cells, n):
+    """The reference (oracle/_ref, compiled from the reference sources) on one host core."""
+    from oracle import ref
+
+    if not ref.available():
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "unavailable: oracle/_ref not built"}
+    s = ref.RefSolver()
+    t_init = s.init(n)
+    m = s.solve(density_cells, threshold=THRESHOLD)
+    return {"value": 1.0 / m.seconds, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"one full {n}^2 solve of the rank-0 instance 0 density ({m.iterations} iterations, "
+                      f"residual {m.residual:.3g}); solve {m.seconds:.2f} s, init (LDLT factorisation, "
+                      f"cached per size by the reference) {t_init:.2f} s excluded",
+            "init_seconds": t_init, "solve_seconds": m.seconds}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the reference's own CPU code path on all host cores
+
+
+def _ref_worker(args_tuple):
+    n, seeds, sample_iters, steps, warmup = args_tuple
+    sys.path.insert(0, ROOT)
+    from oracle import ref
+
+    from otmap_b200 import workloads as W
+
+    dens = [W.to_cells(W.blurred_shapes(n, s, sigma_px=SIGMA_PX)) for s in seeds]
+    s = ref.RefSolver()
+    s.init(n)
+    full = []
+    for d in dens:  # one full solve per density: iteration count and full-solve time
+        m = s.solve(d, threshold=THRESHOLD)
+        full.append((m.iterations, m.seconds))
+    per_step = []
+    for k in range(warmup + steps):
+        t0 = time.perf_counter()
+        for d in dens:
+            s.solve(d, threshold=THRESHOLD, max_iter=sample_iters)
+        dt = time.perf_counter() - t0
+        if k >= warmup:
+            per_step.append(dt)
+    return full, per_step
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+
+    n, B = args.n, args.batch
+    total = B * world
+    seeds = [1000 * r + k for r in range(world) for k in range(B)]
+    cores = len(os.sched_getaffinity(0))
+    P = max(1, min(cores, total))
+    groups = [seeds[p::P] for p in range(P)]
+    ctxm = mp.get_context("spawn")
+    with ctxm.Pool(P) as pool:
+        res = pool.map(_ref_worker, [(n, g, args.sample_iters, args.steps, 1) for g in groups])
+    # per process: estimated full-solve time of its densities per step = sample time
+    # scaled by (full iterations / sampled iterations)
+    step_est = []
+    for k in range(args.steps):
+        worst = 0.0
+        for (full, per_step), g in zip(res, groups):
+            scale = sum(min(it, 10 ** 9) for it, _ in full) / (args.sample_iters * len(full))
+            worst = max(worst, per_step[k] * scale)
+        step_est.append(worst)
+    ms_step = 1e3 * statistics.mean(step_est)
+    value = total / (ms_step / 1e3)
+    full_times = [t for full, _ in res for _, t in full]
+    its = [it for full, _ in res for it, _ in full]
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
+            "config": config(args, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": "reference",
+                             "sample": f"{total} densities over {P} processes of the reference library "
+                                       f"(oracle/_ref, Eigen SimplicialLDLT); each step times "
+                                       f"{args.sample_iters} iterations per density and scales to the full "
+                                       f"iteration counts {its} measured by one full solve each "
+                                       f"(mean full solve {statistics.mean(full_times):.2f} s); init excluded"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,161 @@
+/* otmap_b200 -- C ABI of the B200 (sm_100a) grid optimal-transport solver.
+ *
+ * One shared library (libotmap_b200.so) holds the CUDA kernels and these entry
+ * points. They take plain pointers and sizes only; every pointer argument may be
+ * host memory or device memory of the context's GPU (the library checks which and
+ * copies host buffers through the context's stream). There is no CPU fallback: a
+ * context cannot be created without a CUDA device.
+ *
+ * Each entry point replaces one piece of the reference otmap library
+ * (ggael/otmap, otlib/), cited as file:line:
+ *
+ *   otm_init              GridBasedTransportSolver::init           otsolver_2dgrid.h:55, otsolver_2dgrid.cpp:75-104
+ *   otm_solve             GridBasedTransportSolver::solve          otsolver_2dgrid.h:58, otsolver_2dgrid.cpp:106-245
+ *   otm_solve_batch       (many independent solve() calls)         apps/common/generic_tasks.cpp:57-68
+ *   otm_map_create        TransportMap::TransportMap               transport_map.h:33-35, transport_map.cpp:30-34
+ *   otm_map_init_inverse  TransportMap::init_inverse               transport_map.h:41, transport_map.cpp:36-43
+ *   otm_map_inverse       apply_inverse_map / TransportMap::inv    transport_map.h:44,66-68, transport_map.cpp:50-128
+ *   otm_rasterize         rasterize_image (both overloads)         utils/rasterizer.h:21-22, utils/rasterizer.cpp:188-308
+ *
+ * Buffer conventions (identical to the reference's in-memory layouts):
+ *   n        grid size, N = n*n cells, V = (n+1)*(n+1) vertices
+ *   cells    double[N], face index f = j + i*n with i the x cell index and j the
+ *            y cell index (otsolver_2dgrid.h:90); a column-major n x n image
+ *            (rows = y) flattened, as generic_tasks.cpp:67 passes vec(MatrixXd)
+ *   vertices double[2*V] AoS (x, y), vertex v = j + i*(n+1) at (i/n, j/n) on the
+ *            origin grid (otsolver_2dgrid.h:91, utils/mesh_utils.cpp:90-122);
+ *            face f's corners are (i,j), (i+1,j), (i+1,j+1), (i,j+1)
+ *   points   double[2*P] AoS
+ *   images   double[rows*cols] row-major [y][x]
+ *
+ * Errors: every entry point returns an otm_status; negative values are errors
+ * (nothing written to outputs), zero is success. otm_last_error() describes the
+ * most recent error of the calling thread.
+ */
+#ifndef OTMAP_B200_H
+#define OTMAP_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OTM_ABI_VERSION 1
+
+typedef enum {
+  OTM_OK = 0,
+  OTM_ERR_BAD_ARG = -1,     /* invalid size, null pointer, unknown option */
+  OTM_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  OTM_ERR_NO_DEVICE = -3,   /* no usable CUDA device */
+  OTM_ERR_TIMEOUT = -4,     /* a bounded device-side wait gave up */
+  OTM_ERR_NOT_INIT = -5     /* otm_solve before otm_init for that size */
+} otm_status;
+
+/* Per-solve outcome codes reported in otm_solve_stats.outcome. The reference has
+ * no error channel: solve() returns a map whatever happens (otsolver_2dgrid.cpp:244). */
+typedef enum {
+  OTM_CONVERGED = 0,      /* residual <= threshold */
+  OTM_MAX_ITER = 1,       /* stopped at max_iter with residual > threshold */
+  OTM_SMALL_STEP = 2,     /* stopped because |d_hat| <= 2*DBL_MIN (otsolver_2dgrid.cpp:182) */
+  OTM_NONFINITE = 3       /* residual became NaN/Inf (the loop condition then fails, as in the reference) */
+} otm_outcome;
+
+/* otmap::BetaOpt (otsolver_2dgrid.h:33-35) */
+typedef enum { OTM_BETA_ZERO = 0, OTM_BETA_CONJUGATE_JACOBIAN = 1 } otm_beta;
+
+/* otmap::SolverOptions (otsolver_2dgrid.h:37-43). otm_default_options() fills the
+ * reference defaults: ConjugateJacobian, 1000, 1e-7, DBL_MAX. */
+typedef struct {
+  int beta;          /* otm_beta */
+  int max_iter;
+  double threshold;  /* stop when sum(r^2)/e^2 <= threshold */
+  double max_ratio;  /* density max/min clamp (otsolver_2dgrid.cpp:57-63) */
+} otm_solver_options;
+
+/* What one solve did. */
+typedef struct {
+  int iterations;
+  int outcome;           /* otm_outcome */
+  double residual;       /* final sum(r^2)/e^2 as the reference reports it (line-search value) */
+  double linf;           /* max(r)/e^2 of the final residual vector (otsolver_2dgrid.cpp:236) */
+  double initial_residual;
+} otm_solve_stats;
+
+typedef struct otm_context otm_context; /* one GPU, one CUDA stream, cached per-size tables */
+typedef struct otm_map otm_map;         /* a transport map resident on the GPU */
+
+const char* otm_last_error(void);
+int otm_abi_version(void);
+void otm_default_options(otm_solver_options* opt);
+
+/* Creates a context on CUDA device `device` (its own non-blocking stream). */
+int otm_create(int device, otm_context** ctx);
+int otm_destroy(otm_context* ctx);
+
+/* GridBasedTransportSolver::init (otsolver_2dgrid.cpp:75-104): prepares the size-n
+ * tables (cosine basis, eigenvalues) and checks on the GPU that the reference's
+ * assembled pseudo-Laplacian (otsolver_2dgrid.cpp:284-311) is diagonalised by that
+ * basis before the cosine-transform Poisson solve is used. Cached per n. */
+int otm_init(otm_context* ctx, int n);
+
+/* GridBasedTransportSolver::solve (otsolver_2dgrid.cpp:106-245).
+ *   density   cells, the raw input density (normalised here as the reference does)
+ *   opt       NULL = reference defaults
+ *   fwd_xy    vertices out: the forward mesh (origin grid + vertex gradients)
+ *   adjusted  cells out, optional: the adjusted density the map carries
+ *   stats     optional */
+int otm_solve(otm_context* ctx, int n, const double* density, const otm_solver_options* opt,
+              double* fwd_xy, double* adjusted, otm_solve_stats* stats);
+
+/* `count` independent solves of possibly different sizes, run together on the GPU
+ * (each with its own convergence test). Arrays of `count` entries; entries of
+ * `adjusted` and `stats` may be NULL as a whole. */
+int otm_solve_batch(otm_context* ctx, int count, const int* n, const double* const* density,
+                    const otm_solver_options* opt, double* const* fwd_xy, double* const* adjusted,
+                    otm_solve_stats* stats);
+
+/* TransportMap(origin, fwd, density) (transport_map.cpp:30-34): copies the forward
+ * mesh vertices and the per-cell density to the GPU. The origin mesh is the regular
+ * (n+1)^2 grid. */
+int otm_map_create(otm_context* ctx, int n, const double* fwd_xy, const double* density, otm_map** map);
+int otm_map_destroy(otm_map* map);
+/* Builds the point-location structure (done lazily by otm_map_inverse otherwise). */
+int otm_map_init_inverse(otm_map* map);
+
+/* apply_inverse_map (transport_map.cpp:105-128): each point, clamped to [0,1]^2, is
+ * located in the forward mesh; the result is the bilinear interpolation of the
+ * origin grid at the located face (transport_map.cpp:50-102, same hit-selection
+ * rule). points are overwritten in place.
+ *   face   optional int[P]: the chosen face index, -1 where no face contains the point
+ *          (the point is then set to NaN; the reference reads an empty hit list there)
+ *   nhits  optional int[P]: how many faces contain the point
+ *   missing optional: number of points with no face */
+int otm_map_inverse(otm_map* map, double* points, long count, int* face, int* nhits, long* missing);
+
+/* rasterize_image (utils/rasterizer.cpp:188-308), PerFace mode on the quad mesh of
+ * an (n+1)^2 grid whose vertex positions are `xy`: each pixel whose centre lies in a
+ * face (bilinear coordinates in [0,1]) gets float(1/N) * density[f] / |area f|, the
+ * highest face index winning as in the reference's sequential loop. density NULL =
+ * unit density (rasterizer.cpp:305-308). img receives rows*cols doubles. */
+int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
+                  double* img);
+
+/* ---- instrumentation (no counterpart in the reference, which times its phases
+ * with BenchTimer, otsolver_2dgrid.cpp:153-217) ---- */
+
+/* The context's CUDA stream (a cudaStream_t), for callers that record their own
+ * events around otm_* calls; every otm_* call has finished on it when it returns. */
+int otm_stream(otm_context* ctx, void** stream);
+/* Kernels this context has launched since it was created. */
+long otm_launch_count(otm_context* ctx);
+/* enable = 1 / 0 turns per-kernel CUDA-event timing on / off; -1 resets the totals. */
+int otm_profile(otm_context* ctx, int enable);
+/* Reads entry `index` of the per-kernel totals: kernel name, total ms, launches.
+ * Returns 0 past the last entry. */
+int otm_profile_entry(otm_context* ctx, int index, const char** name, double* ms, long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,167 @@
+// Context management, host/device copies and error reporting of the C ABI.
+
+#include <cfloat>
+#include <cstring>
+#include <string>
+
+#include "context.h"
+
+namespace otm {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+void make_current(otm_context* ctx) { OTM_CUDA(cudaSetDevice(ctx->device)); }
+
+void copy_in(otm_context* ctx, void* dst, const void* src, size_t bytes) {
+  if (!bytes) return;
+  OTM_CUDA(cudaMemcpyAsync(dst, src, bytes, is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                           ctx->stream));
+}
+
+void copy_out(otm_context* ctx, void* dst, const void* src, size_t bytes) {
+  if (!bytes) return;
+  OTM_CUDA(cudaMemcpyAsync(dst, src, bytes, is_device_ptr(dst) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                           ctx->stream));
+}
+
+int Profiler::id(const char* name) {
+  for (size_t k = 0; k < names.size(); ++k)
+    if (std::strcmp(names[k], name) == 0) return (int)k;
+  names.push_back(name);
+  ms.push_back(0.0);
+  count.push_back(0);
+  return (int)names.size() - 1;
+}
+
+cudaEvent_t Profiler::get() {
+  if (!pool.empty()) {
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  OTM_CUDA(cudaEventCreate(&e));
+  return e;
+}
+
+void Profiler::flush() {
+  for (auto& r : pending) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, r.a, r.b) == cudaSuccess) {
+      ms[r.name] += t;
+      count[r.name] += 1;
+    } else {
+      cudaGetLastError();
+    }
+    pool.push_back(r.a);
+    pool.push_back(r.b);
+  }
+  pending.clear();
+}
+
+Profiler::~Profiler() {
+  for (auto& r : pending) {
+    pool.push_back(r.a);
+    pool.push_back(r.b);
+  }
+  for (auto e : pool) cudaEventDestroy(e);
+}
+
+}  // namespace otm
+
+using namespace otm;
+
+extern "C" const char* otm_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int otm_abi_version(void) { return OTM_ABI_VERSION; }
+
+extern "C" void otm_default_options(otm_solver_options* opt) {
+  if (!opt) return;
+  opt->beta = OTM_BETA_CONJUGATE_JACOBIAN;
+  opt->max_iter = 1000;
+  opt->threshold = 1e-7;
+  opt->max_ratio = DBL_MAX;
+}
+
+extern "C" int otm_create(int device, otm_context** out) {
+  if (!out) {
+    set_error("otm_create: null output pointer");
+    return OTM_ERR_BAD_ARG;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("otm_create: no CUDA device");
+    return OTM_ERR_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) {
+    set_error("otm_create: device index out of range");
+    return OTM_ERR_BAD_ARG;
+  }
+  return guarded([&] {
+    auto* ctx = new otm_context;
+    ctx->device = device;
+    try {
+      OTM_CUDA(cudaSetDevice(device));
+      OTM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+      OTM_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+    } catch (...) {
+      delete ctx;
+      throw;
+    }
+    *out = ctx;
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_destroy(otm_context* ctx) {
+  if (!ctx) return OTM_OK;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  cudaStream_t st = ctx->stream;
+  delete ctx;
+  if (st) cudaStreamDestroy(st);
+  return OTM_OK;
+}
+
+extern "C" int otm_stream(otm_context* ctx, void** stream) {
+  if (!ctx || !stream) {
+    set_error("otm_stream: null argument");
+    return OTM_ERR_BAD_ARG;
+  }
+  *stream = (void*)ctx->stream;
+  return OTM_OK;
+}
+
+extern "C" long otm_launch_count(otm_context* ctx) { return ctx ? ctx->launches : 0; }
+
+extern "C" int otm_profile(otm_context* ctx, int enable) {
+  if (!ctx) {
+    set_error("otm_profile: null context");
+    return OTM_ERR_BAD_ARG;
+  }
+  return guarded([&] {
+    make_current(ctx);
+    OTM_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->prof.flush();
+    if (enable < 0) {  // reset the totals
+      for (auto& m : ctx->prof.ms) m = 0.0;
+      for (auto& c : ctx->prof.count) c = 0;
+    } else {
+      ctx->prof.on = enable != 0;
+    }
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_profile_entry(otm_context* ctx, int index, const char** name, double* ms, long* launches) {
+  if (!ctx) return 0;
+  if (index < 0 || index >= (int)ctx->prof.names.size()) return 0;
+  if (name) *name = ctx->prof.names[index];
+  if (ms) *ms = ctx->prof.ms[index];
+  if (launches) *launches = ctx->prof.count[index];
+  return 1;
+}

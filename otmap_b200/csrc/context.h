@@ -1,0 +1,153 @@
+// Host-side state behind the opaque otm_context / otm_map handles.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "common.cuh"
+#include "otmap_b200.h"
+
+namespace otm {
+
+// Owning device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // Grows (never shrinks) to at least `b` bytes; contents are not preserved.
+  void reserve(size_t b);
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+// Per grid size: the orthonormal DCT-II basis and cos(pi k / n), built by otm_init.
+struct SizeTables {
+  int n = 0;
+  DevBuf C;     // n*n doubles, C[k*n + i]
+  DevBuf cosk;  // n doubles
+  bool dct_ok = false;      // the assembled matrix is diagonalised by C (checked on the GPU)
+  double dct_check_err = 0;  // relative error of that check
+};
+
+struct Inst;  // device instance record (solver.cu)
+
+// Buffers of one batch configuration (the list of grid sizes), reused across calls.
+struct Workspace {
+  std::vector<int> sizes;
+  DevBuf insts;      // Inst[count]
+  DevBuf tile_inst;  // int per stencil tile
+  DevBuf gemm_inst;  // int per GEMM tile
+  DevBuf partials;   // double[total_tiles * 8]
+  DevBuf arena;      // per-instance cell arrays
+  DevBuf host_rec;   // unused placeholder to keep layout stable
+  std::vector<unsigned char> h_insts;  // host mirror of Inst[count]
+  void* h_pinned = nullptr;            // pinned staging for Inst readback
+  size_t h_pinned_bytes = 0;
+  int total_tiles = 0, total_gemm = 0;
+  ~Workspace() {
+    if (h_pinned) cudaFreeHost(h_pinned);
+  }
+};
+
+}  // namespace otm
+
+namespace otm {
+// Per-kernel CUDA-event timing on the context stream (enabled by otm_profile).
+struct Profiler {
+  struct Rec {
+    int name;
+    cudaEvent_t a, b;
+  };
+  bool on = false;
+  std::vector<const char*> names;
+  std::vector<double> ms;
+  std::vector<long> count;
+  std::vector<Rec> pending;
+  std::vector<cudaEvent_t> pool;
+  int id(const char* name);
+  cudaEvent_t get();
+  void flush();  // after a stream sync: fold pending pairs into the totals
+  ~Profiler();
+};
+}  // namespace otm
+
+struct otm_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int num_sms = 0;
+  long launches = 0;  // kernels launched by this context since creation
+  otm::Profiler prof;
+  std::map<int, std::unique_ptr<otm::SizeTables>> tables;
+  otm::Workspace ws;
+  otm::DevBuf staging;  // device staging for host inputs/outputs
+};
+
+struct otm_map {
+  otm_context* ctx = nullptr;
+  int n = 0;
+  otm::DevBuf fwd;      // V*2 doubles
+  otm::DevBuf density;  // N doubles
+  // point-location structure (built lazily)
+  bool located = false;
+  int bins = 0;
+  otm::DevBuf bin_start;  // int[bins*bins + 1]
+  otm::DevBuf bin_faces;  // int[entries]
+  otm::DevBuf face_box;   // double4 per face (min x, min y, max x, max y)
+  otm::DevBuf scratch;
+};
+
+namespace otm {
+// Makes the context's device current; defined in capi.cu.
+void make_current(otm_context* ctx);
+// Copies `bytes` from src (host or device) into dst (device), on the context stream.
+void copy_in(otm_context* ctx, void* dst, const void* src, size_t bytes);
+// Copies `bytes` from src (device) into dst (host or device), on the context stream.
+void copy_out(otm_context* ctx, void* dst, const void* src, size_t bytes);
+
+// Launches `kernel` on the context stream, counting it and (when profiling) bracketing
+// it with CUDA events.
+template <class K, class... Args>
+void launch(otm_context* ctx, const char* name, K kernel, dim3 grid, dim3 block, Args... args) {
+  ctx->launches++;
+  if (ctx->prof.on) {
+    int id = ctx->prof.id(name);
+    cudaEvent_t a = ctx->prof.get(), b = ctx->prof.get();
+    cudaEventRecord(a, ctx->stream);
+    kernel<<<grid, block, 0, ctx->stream>>>(args...);
+    cudaEventRecord(b, ctx->stream);
+    ctx->prof.pending.push_back({id, a, b});
+  } else {
+    kernel<<<grid, block, 0, ctx->stream>>>(args...);
+  }
+}
+
+// Runs an entry point body, mapping exceptions to otm_status codes.
+template <class F>
+int guarded(F&& f) {
+  try {
+    return f();
+  } catch (const BadArg& e) {
+    set_error(e.what);
+    return OTM_ERR_BAD_ARG;
+  } catch (const CudaError& e) {
+    set_error(std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")");
+    return OTM_ERR_CUDA;
+  } catch (const std::exception& e) {
+    set_error(e.what());
+    return OTM_ERR_CUDA;
+  }
+}
+}  // namespace otm

@@ -1,0 +1,918 @@
+// The grid transport solver on the GPU: GridBasedTransportSolver::init/solve of the
+// reference (otlib/otsolver_2dgrid.cpp) as CUDA kernels for sm_100a.
+//
+// One engine serves single and batched solves: every kernel walks a flat list of
+// (instance, tile) work items, reads its instance's state from a device record
+// (Inst) and returns at once when that instance has stopped, so instances of
+// different sizes converge independently inside the same launches.
+//
+// Per iteration (otsolver_2dgrid.cpp:160-220):
+//   k_dct_gemm x4   d_hat = M^+ r_k: orthonormal 2-D DCT-II, divide by the
+//                   eigenvalues of the reference's pseudo-Laplacian, inverse DCT
+//                   (:175-179; the (0,0) mode is dropped = mean-zero projection)
+//   k_beta          |d_hat| (early exit, :182) and the conjugate-Jacobian beta:
+//                   residual at psi - (alpha/2) d_hat (:248-261)
+//   k_coeffs        d = d_hat + beta d_prev, line coefficients a, b per cell and the
+//                   five quartic sums; the last block solves the cubic (:541-595)
+//   k_update        psi += alpha d, r += alpha b + alpha^2 a (:599-605); the last
+//                   block advances the iteration and tests convergence (:160)
+// Stencil kernels stage a (TI+2) x (TJ+2) halo tile of the potential in shared
+// memory, derive the (TI+1) x (TJ+1) vertex gradients there (never stored) and
+// finish with a fixed-order block reduction; the last block of an instance (atomic
+// ticket) reduces the per-tile partials in tile order, so every reduction is
+// run-to-run deterministic. All arithmetic is FP64, compiled without FMA
+// contraction so each cell's operations round as the reference's scalar code does.
+
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+#include "context.h"
+
+namespace otm {
+
+constexpr int TI = 8, TJ = 32, NT = 256;  // stencil tile: TI cells along x (i), TJ along y (j)
+constexpr int HI = TI + 2, HJ = TJ + 2;   // halo tile of cells
+constexpr int VI = TI + 1, VJ = TJ + 1;   // vertex tile
+constexpr int KP = 8;                     // partial sums per tile
+constexpr int GB = 64, GK = 16;           // DCT GEMM tile (GB x GB outputs, GK deep)
+
+// Device record of one solve instance. Buffer pointers are fixed for the life of
+// the workspace; everything below `it` is loop state updated by the kernels.
+struct Inst {
+  int n, tile0, ntiles, gemm0, ngemm;
+  int max_iter, beta_cj, pad0;
+  double threshold, max_ratio;
+  double* psi[2];
+  double* r[3];
+  double* dhat;
+  double* d[2];
+  double* rho;
+  double* t1;
+  double* t2;
+  const double* C;
+  const double* cosk;
+  // loop state
+  int it, active, outcome, use_beta;
+  unsigned int counter, pad1;
+  double residual, residual0, alpha, beta, linf, dnorm;
+  double dens_scale, dens_beta;
+};
+
+__device__ __forceinline__ int clampi(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
+
+// s[(HI) x (HJ)] <- f(cell) over cells (i0-1 .. i0+TI) x (j0-1 .. j0+TJ), indices
+// clamped to the grid. With clamped indices the interior vertex-gradient formula
+// reproduces the reference's boundary rules exactly (otsolver_2dgrid.cpp:405-422):
+// tangential one-sided differences, zero normal component, zero at the corners.
+template <class F>
+__device__ __forceinline__ void load_halo(double* s, int n, int i0, int j0, F f) {
+  for (int idx = threadIdx.x; idx < HI * HJ; idx += NT) {
+    int li = idx / HJ, lj = idx - li * HJ;
+    int gi = clampi(i0 + li - 1, n), gj = clampi(j0 + lj - 1, n);
+    s[idx] = f((size_t)gi * n + gj);
+  }
+}
+
+// Vertex gradients (otsolver_2dgrid.cpp:379-391): vertex (i0+vi, j0+vj) from the
+// four cells around it, 0.5 n ((p10 + p11) - (p00 + p01)) and 0.5 n ((p01 + p11) - (p00 + p10)).
+__device__ __forceinline__ void vertex_grads(const double* s, double* gx, double* gy, double hw) {
+  for (int idx = threadIdx.x; idx < VI * VJ; idx += NT) {
+    int vi = idx / VJ, vj = idx - vi * VJ;
+    double p00 = s[vi * HJ + vj], p01 = s[vi * HJ + vj + 1];
+    double p10 = s[(vi + 1) * HJ + vj], p11 = s[(vi + 1) * HJ + vj + 1];
+    gx[idx] = hw * ((p10 + p11) - (p00 + p01));
+    gy[idx] = hw * ((p01 + p11) - (p00 + p10));
+  }
+}
+
+// Quad area from its corner displacements (otsolver_2dgrid.cpp:425-447).
+__device__ __forceinline__ double cell_area(const double* gx, const double* gy, int ci, int cj, double e) {
+  int v00 = ci * VJ + cj, v10 = (ci + 1) * VJ + cj, v01 = ci * VJ + cj + 1, v11 = (ci + 1) * VJ + cj + 1;
+  return 0.5 * ((gx[v11] - gx[v00] + e) * (gy[v01] - gy[v10] + e) -
+                (gy[v11] - gy[v00] + e) * (gx[v01] - gx[v10] - e));
+}
+
+// r(psi + t dir) = r(psi) + b t + a t^2 (otsolver_2dgrid.cpp:516-537): g = gradients at
+// psi, h = gradients of dir.
+__device__ __forceinline__ void cell_ab(const double* gx, const double* gy, const double* hx, const double* hy,
+                                        int ci, int cj, double e, double& a, double& b) {
+  int v00 = ci * VJ + cj, v10 = (ci + 1) * VJ + cj, v01 = ci * VJ + cj + 1, v11 = (ci + 1) * VJ + cj + 1;
+  double diag0a_x = gx[v11] - gx[v00] + e;
+  double diag0a_y = gy[v11] - gy[v00] + e;
+  double diag0b_x = gx[v01] - gx[v10] - e;
+  double diag0b_y = gy[v01] - gy[v10] + e;
+  double dda_x = hx[v11] - hx[v00];
+  double dda_y = hy[v11] - hy[v00];
+  double ddb_x = hx[v01] - hx[v10];
+  double ddb_y = hy[v01] - hy[v10];
+  a = 0.5 * (dda_x * ddb_y - dda_y * ddb_x);
+  b = 0.5 * (dda_x * diag0b_y - dda_y * diag0b_x + diag0a_x * ddb_y - diag0a_y * ddb_x);
+}
+
+struct TileCoord {
+  int i0, j0, ci, cj, gi, gj;
+  bool inside;
+  size_t f;
+};
+
+__device__ __forceinline__ TileCoord tile_coord(const Inst& I, int block) {
+  TileCoord t;
+  int n = I.n, tl = block - I.tile0, tjn = (n + TJ - 1) / TJ;
+  t.i0 = (tl / tjn) * TI;
+  t.j0 = (tl % tjn) * TJ;
+  t.ci = threadIdx.x / TJ;
+  t.cj = threadIdx.x % TJ;
+  t.gi = t.i0 + t.ci;
+  t.gj = t.j0 + t.cj;
+  t.inside = t.gi < n && t.gj < n;
+  t.f = (size_t)t.gi * n + t.gj;
+  return t;
+}
+
+// Sums partials[tile0 .. tile0+ntiles) (K values each) in tile order.
+template <int K>
+__device__ __forceinline__ void reduce_partials(const double* partials, int tile0, int ntiles, double (&v)[K],
+                                                double* red) {
+#pragma unroll
+  for (int k = 0; k < K; ++k) v[k] = 0.0;
+  for (int t = threadIdx.x; t < ntiles; t += NT)
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] += __ldcg(&partials[(size_t)(tile0 + t) * KP + k]);
+  block_sum<K>(v, red);
+}
+
+__device__ __forceinline__ double reduce_partials_max(const double* partials, int tile0, int ntiles, int k,
+                                                      double* red) {
+  double m = -INFINITY;
+  for (int t = threadIdx.x; t < ntiles; t += NT) m = fmax(m, __ldcg(&partials[(size_t)(tile0 + t) * KP + k]));
+  return block_max(m, red);
+}
+
+__device__ __forceinline__ double reduce_partials_min(const double* partials, int tile0, int ntiles, int k,
+                                                      double* red) {
+  double m = INFINITY;
+  for (int t = threadIdx.x; t < ntiles; t += NT) m = fmin(m, __ldcg(&partials[(size_t)(tile0 + t) * KP + k]));
+  return -block_max(-m, red);
+}
+
+__device__ __forceinline__ double elem_area(int n) { return 1.0 / ((double)n * (double)n); }
+
+// Sets `outcome` for an instance whose loop condition (otsolver_2dgrid.cpp:160) failed.
+__device__ __forceinline__ void stop_outcome(Inst& I) {
+  if (I.residual <= I.threshold)
+    I.outcome = OTM_CONVERGED;
+  else if (!isfinite(I.residual))
+    I.outcome = OTM_NONFINITE;
+  else
+    I.outcome = OTM_MAX_ITER;
+}
+
+// ---------------------------------------------------------------------------
+// Density normalisation (otsolver_2dgrid.cpp:47-63), three passes.
+
+__global__ __launch_bounds__(NT) void k_density_sum(Inst* insts, const int* tile_inst, double* partials) {
+  __shared__ double red[32 * 2];
+  Inst& I = insts[tile_inst[blockIdx.x]];
+  TileCoord t = tile_coord(I, blockIdx.x);
+  double v[1] = {t.inside ? I.rho[t.f] : 0.0};
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) partials[(size_t)blockIdx.x * KP] = v[0];
+  if (last_block(&I.counter, I.ntiles)) {
+    double s[1];
+    reduce_partials<1>(partials, I.tile0, I.ntiles, s, red);
+    if (threadIdx.x == 0) I.dens_scale = s[0] * elem_area(I.n);
+  }
+}
+
+__global__ __launch_bounds__(NT) void k_density_scale(Inst* insts, const int* tile_inst, double* partials) {
+  __shared__ double red[32 * 2];
+  Inst& I = insts[tile_inst[blockIdx.x]];
+  TileCoord t = tile_coord(I, blockIdx.x);
+  double mn = INFINITY, mx = -INFINITY;
+  if (t.inside) {
+    double x = I.rho[t.f] / I.dens_scale;
+    I.rho[t.f] = x;
+    mn = x;
+    mx = x;
+  }
+  mx = block_max(mx, red);
+  mn = -block_max(-mn, red);
+  if (threadIdx.x == 0) {
+    partials[(size_t)blockIdx.x * KP + 0] = mn;
+    partials[(size_t)blockIdx.x * KP + 1] = mx;
+  }
+  if (last_block(&I.counter, I.ntiles)) {
+    double gmn = reduce_partials_min(partials, I.tile0, I.ntiles, 0, red);
+    double gmx = reduce_partials_max(partials, I.tile0, I.ntiles, 1, red);
+    if (threadIdx.x == 0) {
+      double ratio = std_min(I.max_ratio, gmx / gmn);
+      I.dens_beta = std_max(0.0, (ratio * gmn - gmx) / (1.0 - ratio));
+    }
+  }
+}
+
+__global__ __launch_bounds__(NT) void k_density_apply(Inst* insts, const int* tile_inst) {
+  Inst& I = insts[tile_inst[blockIdx.x]];
+  TileCoord t = tile_coord(I, blockIdx.x);
+  if (t.inside) I.rho[t.f] = (I.rho[t.f] + I.dens_beta) / (1.0 + I.dens_beta);
+}
+
+// ---------------------------------------------------------------------------
+// Initial residual at psi = 0 (otsolver_2dgrid.cpp:146).
+
+__global__ __launch_bounds__(NT) void k_residual_init(Inst* insts, const int* tile_inst, double* partials) {
+  __shared__ double s[HI * HJ];
+  __shared__ double gx[VI * VJ], gy[VI * VJ];
+  __shared__ double red[32 * 2];
+  Inst& I = insts[tile_inst[blockIdx.x]];
+  const int n = I.n;
+  const double e = 1.0 / (double)n, ea = elem_area(n);
+  TileCoord t = tile_coord(I, blockIdx.x);
+  const double* psi = I.psi[0];
+  load_halo(s, n, t.i0, t.j0, [&](size_t g) { return psi[g]; });
+  __syncthreads();
+  vertex_grads(s, gx, gy, 0.5 * (double)n);
+  __syncthreads();
+  double v[1] = {0.0};
+  double mx = -INFINITY;
+  if (t.inside) {
+    double r = cell_area(gx, gy, t.ci, t.cj, e) - ea * I.rho[t.f];
+    I.r[0][t.f] = r;
+    v[0] = r * r;
+    mx = r;
+  }
+  block_sum<1>(v, red);
+  mx = block_max(mx, red);
+  if (threadIdx.x == 0) {
+    partials[(size_t)blockIdx.x * KP + 0] = v[0];
+    partials[(size_t)blockIdx.x * KP + 1] = mx;
+  }
+  if (last_block(&I.counter, I.ntiles)) {
+    double sum[1];
+    reduce_partials<1>(partials, I.tile0, I.ntiles, sum, red);
+    double gmx = reduce_partials_max(partials, I.tile0, I.ntiles, 1, red);
+    if (threadIdx.x == 0) {
+      I.residual = sum[0] / ea;
+      I.residual0 = I.residual;
+      I.linf = gmx / ea;
+      I.it = 0;
+      I.alpha = 0.0;
+      I.beta = 0.0;
+      I.use_beta = 0;
+      I.active = (0 < I.max_iter && I.residual > I.threshold) ? 1 : 0;
+      if (!I.active) stop_outcome(I);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Poisson solve as dense products with the cosine basis C (n x n, C[k][i]):
+//   t1 = C r ; t2 = (t1 C^T) / lambda ; t1 = C^T t2 ; d_hat = t1 C
+// lambda_kl = 2 - 2 cos(pi k/n) cos(pi l/n) are the eigenvalues of the reference's
+// assembled matrix (otsolver_2dgrid.cpp:284-311); dropping the (0,0) mode is the
+// mean-zero projection of :179. epi = 2 multiplies by lambda instead (the
+// diagonalisation check at init).
+
+__global__ __launch_bounds__(256) void k_dct_gemm(const Inst* insts, const int* gemm_inst, int stage, int epi) {
+  const Inst& I = insts[gemm_inst[blockIdx.x]];
+  if (!I.active) return;
+  const int n = I.n;
+  const int tl = blockIdx.x - I.gemm0, tn = (n + GB - 1) / GB;
+  const int m0 = (tl / tn) * GB, n0 = (tl % tn) * GB;
+  const double *A, *B;
+  double* D;
+  bool ta, tb;
+  int ep = 0;
+  switch (stage) {
+    case 0: A = I.C; ta = false; B = I.r[I.it % 3]; tb = false; D = I.t1; break;
+    case 1: A = I.t1; ta = false; B = I.C; tb = true; D = I.t2; ep = epi; break;
+    case 2: A = I.C; ta = true; B = I.t2; tb = false; D = I.t1; break;
+    default: A = I.t1; ta = false; B = I.C; tb = false; D = I.dhat; break;
+  }
+  __shared__ double As[GK][GB + 1];
+  __shared__ double Bs[GK][GB + 1];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+  for (int k0 = 0; k0 < n; k0 += GK) {
+    for (int e = threadIdx.x; e < GB * GK; e += 256) {
+      int mm, kk;
+      if (!ta) {
+        mm = e / GK;
+        kk = e - mm * GK;
+      } else {
+        kk = e / GB;
+        mm = e - kk * GB;
+      }
+      int gm = m0 + mm, gk = k0 + kk;
+      double v = 0.0;
+      if (gm < n && gk < n) v = ta ? A[(size_t)gk * n + gm] : A[(size_t)gm * n + gk];
+      As[kk][mm] = v;
+    }
+    for (int e = threadIdx.x; e < GB * GK; e += 256) {
+      int nn, kk;
+      if (!tb) {
+        kk = e / GB;
+        nn = e - kk * GB;
+      } else {
+        nn = e / GK;
+        kk = e - nn * GK;
+      }
+      int gn = n0 + nn, gk = k0 + kk;
+      double v = 0.0;
+      if (gn < n && gk < n) v = tb ? B[(size_t)gn * n + gk] : B[(size_t)gk * n + gn];
+      Bs[kk][nn] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GK; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int gm = m0 + ty * 4 + i;
+    if (gm >= n) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      int gn = n0 + tx * 4 + j;
+      if (gn >= n) continue;
+      double v = acc[i][j];
+      if (ep) {
+        double lam = 2.0 - 2.0 * I.cosk[gm] * I.cosk[gn];
+        if (ep == 1)
+          v = (gm == 0 && gn == 0) ? 0.0 : v / lam;
+        else
+          v = v * lam;
+      }
+      D[(size_t)gm * n + gn] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// |d_hat|, early exit and the conjugate-Jacobian beta (otsolver_2dgrid.cpp:179-200, 248-261).
+
+__global__ __launch_bounds__(NT) void k_beta(Inst* insts, const int* tile_inst, double* partials) {
+  __shared__ double s[HI * HJ];
+  __shared__ double gx[VI * VJ], gy[VI * VJ];
+  __shared__ double red[32 * 3];
+  Inst& I = insts[tile_inst[blockIdx.x]];
+  if (!I.active) return;
+  const int n = I.n, it = I.it;
+  const double e = 1.0 / (double)n, ea = elem_area(n);
+  const bool use_beta = it >= 1 && I.beta_cj;
+  TileCoord t = tile_coord(I, blockIdx.x);
+  double v[3] = {0.0, 0.0, 0.0};
+  if (t.inside) {
+    double dh = I.dhat[t.f];
+    v[0] = dh * dh;
+  }
+  if (use_beta) {
+    const double eps = I.alpha / 2.0;
+    const double* psi = I.psi[it & 1];
+    const double* dh = I.dhat;
+    load_halo(s, n, t.i0, t.j0, [&](size_t g) { return psi[g] - eps * dh[g]; });
+    __syncthreads();
+    vertex_grads(s, gx, gy, 0.5 * (double)n);
+    __syncthreads();
+    if (t.inside) {
+      double reps = cell_area(gx, gy, t.ci, t.cj, e) - ea * I.rho[t.f];
+      double rk = I.r[it % 3][t.f], rkm1 = I.r[(it + 2) % 3][t.f];
+      double jd = rk - rkm1;
+      v[1] = jd * (reps - rk);
+      v[2] = jd * jd;
+    }
+  }
+  block_sum<3>(v, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) partials[(size_t)blockIdx.x * KP + k] = v[k];
+  if (last_block(&I.counter, I.ntiles)) {
+    double sum[3];
+    reduce_partials<3>(partials, I.tile0, I.ntiles, sum, red);
+    if (threadIdx.x == 0) {
+      if (sqrt(sum[0]) <= 2.0 * DBL_MIN) {
+        I.active = 0;
+        I.outcome = OTM_SMALL_STEP;
+      } else {
+        I.use_beta = use_beta ? 1 : 0;
+        if (use_beta) {
+          double eps = I.alpha / 2.0;
+          I.beta = std_max(-1.0, sum[1] / sum[2] / eps * I.alpha);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Exact line search (otsolver_2dgrid.cpp:541-606).
+
+__device__ double cubic_eval(const double c[4], double t) { return ((c[3] * t + c[2]) * t + c[1]) * t + c[0]; }
+__device__ double cubic_deriv(const double c[4], double t) { return (3.0 * c[3] * t + 2.0 * c[2]) * t + c[1]; }
+
+// Real roots of w3 t^3 + w2 t^2 + w1 t + w0: closed form of the depressed cubic
+// (Cardano for one real root, the trigonometric form for three) and two Newton
+// steps; replaces the companion-matrix eigensolver of otsolver_2dgrid.cpp:568-572.
+__device__ int cubic_real_roots(const double w[4], double roots[3]) {
+  double a = w[2] / w[3], b = w[1] / w[3], c = w[0] / w[3];
+  if (!isfinite(a) || !isfinite(b) || !isfinite(c)) return 0;
+  double p = b - a * a / 3.0;
+  double q = 2.0 * a * a * a / 27.0 - a * b / 3.0 + c;
+  double disc = 0.25 * q * q + p * p * p / 27.0;
+  int m;
+  if (disc > 0.0) {
+    double sq = sqrt(disc);
+    double u = cbrt(-0.5 * q + (q <= 0.0 ? sq : -sq));
+    double y = (u != 0.0) ? u - p / (3.0 * u) : 0.0;
+    roots[0] = y - a / 3.0;
+    m = 1;
+  } else {
+    double r = sqrt(std_max(0.0, -p / 3.0));
+    if (r == 0.0) {
+      roots[0] = roots[1] = roots[2] = -a / 3.0;
+    } else {
+      double arg = std_max(-1.0, std_min(1.0, -0.5 * q / (r * r * r)));
+      double phi = acos(arg) / 3.0;
+      for (int k = 0; k < 3; ++k) roots[k] = 2.0 * r * cos(phi - 2.0943951023931954923 * k) - a / 3.0;
+    }
+    m = 3;
+  }
+  double cc[4] = {c, b, a, 1.0};
+  for (int k = 0; k < m; ++k)
+    for (int s = 0; s < 2; ++s) {
+      double f = cubic_eval(cc, roots[k]), df = cubic_deriv(cc, roots[k]);
+      if (df != 0.0 && isfinite(f / df)) roots[k] -= f / df;
+    }
+  return m;
+}
+
+// Among the real stationary points of e(t) = z0 + z1 t + ... + z4 t^4 in [-10, 10] the
+// one with least e(t); else t = 0.5 (otsolver_2dgrid.cpp:575-595).
+__device__ void pick_step(const double z[5], double* alpha, double* emin) {
+  double w[4] = {z[1], 2.0 * z[2], 3.0 * z[3], 4.0 * z[4]};
+  double roots[3];
+  int m = cubic_real_roots(w, roots);
+  bool found = false;
+  double best = 0.0, rmin = 0.0;
+  for (int k = 0; k < m; ++k) {
+    double t = roots[k];
+    if (t >= -10.0 && t <= 10.0) {
+      double r = z[0] + t * (z[1] + t * (z[2] + t * (z[3] + t * z[4])));
+      if (!found || r < rmin) {
+        found = true;
+        best = t;
+        rmin = r;
+      }
+    }
+  }
+  if (!found) {
+    best = 0.5;
+    rmin = z[0] + best * (z[1] + best * (z[2] + best * (z[3] + best * z[4])));
+  }
+  *alpha = best;
+  *emin = rmin;
+}
+
+// d = d_hat + beta d_prev (written), a and b per cell, the quartic's sums; the last
+// block picks the step.
+__global__ __launch_bounds__(NT) void k_coeffs(Inst* insts, const int* tile_inst, double* partials) {
+  __shared__ double sp[HI * HJ], sd[HI * HJ];
+  __shared__ double gx[VI * VJ], gy[VI * VJ], hx[VI * VJ], hy[VI * VJ];
+  __shared__ double red[32 * 6];
+  Inst& I = insts[tile_inst[blockIdx.x]];
+  if (!I.active) return;
+  const int n = I.n, it = I.it;
+  const double e = 1.0 / (double)n, hw = 0.5 * (double)n;
+  TileCoord t = tile_coord(I, blockIdx.x);
+  const bool use_beta = I.use_beta;
+  const double beta = I.beta;
+  const double* dh = I.dhat;
+  const double* dprev = I.d[(it + 1) & 1];
+  double* dnew = I.d[it & 1];
+  const double* psi = I.psi[it & 1];
+  load_halo(sd, n, t.i0, t.j0, [&](size_t g) { return use_beta ? dh[g] + beta * dprev[g] : dh[g]; });
+  load_halo(sp, n, t.i0, t.j0, [&](size_t g) { return psi[g]; });
+  __syncthreads();
+  vertex_grads(sp, gx, gy, hw);
+  vertex_grads(sd, hx, hy, hw);
+  __syncthreads();
+  double v[6] = {0, 0, 0, 0, 0, 0};
+  if (t.inside) {
+    double dv = sd[(t.ci + 1) * HJ + t.cj + 1];
+    dnew[t.f] = dv;
+    double a, b;
+    cell_ab(gx, gy, hx, hy, t.ci, t.cj, e, a, b);
+    double rk = I.r[it % 3][t.f];
+    v[0] = b * rk;
+    v[1] = b * b;
+    v[2] = a * rk;
+    v[3] = a * b;
+    v[4] = a * a;
+    v[5] = dv * dv;
+  }
+  block_sum<6>(v, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 6; ++k) partials[(size_t)blockIdx.x * KP + k] = v[k];
+  if (last_block(&I.counter, I.ntiles)) {
+    double sum[6];
+    reduce_partials<6>(partials, I.tile0, I.ntiles, sum, red);
+    if (threadIdx.x == 0) {
+      const double ea = elem_area(n);
+      double z[5] = {I.residual * ea, 2.0 * sum[0], sum[1] + 2 * sum[2], 2.0 * sum[3], sum[4]};
+      double alpha, rmin;
+      pick_step(z, &alpha, &rmin);
+      I.alpha = alpha;
+      I.residual = rmin / ea;
+      I.dnorm = sqrt(sum[5]);
+    }
+  }
+}
+
+// psi_{k+1} = psi_k + alpha d and r_{k+1} = a alpha^2 + b alpha + r_k; the last block
+// advances the iteration and evaluates the loop condition.
+__global__ __launch_bounds__(NT) void k_update(Inst* insts, const int* tile_inst, double* partials) {
+  __shared__ double sp[HI * HJ], sd[HI * HJ];
+  __shared__ double gx[VI * VJ], gy[VI * VJ], hx[VI * VJ], hy[VI * VJ];
+  __shared__ double red[32 * 2];
+  Inst& I = insts[tile_inst[blockIdx.x]];
+  if (!I.active) return;
+  const int n = I.n, it = I.it;
+  const double e = 1.0 / (double)n, hw = 0.5 * (double)n, alpha = I.alpha;
+  TileCoord t = tile_coord(I, blockIdx.x);
+  const double* d = I.d[it & 1];
+  const double* psi = I.psi[it & 1];
+  load_halo(sd, n, t.i0, t.j0, [&](size_t g) { return d[g]; });
+  load_halo(sp, n, t.i0, t.j0, [&](size_t g) { return psi[g]; });
+  __syncthreads();
+  vertex_grads(sp, gx, gy, hw);
+  vertex_grads(sd, hx, hy, hw);
+  __syncthreads();
+  double mx = -INFINITY;
+  if (t.inside) {
+    double a, b;
+    cell_ab(gx, gy, hx, hy, t.ci, t.cj, e, a, b);
+    double p = sp[(t.ci + 1) * HJ + t.cj + 1], dv = sd[(t.ci + 1) * HJ + t.cj + 1];
+    I.psi[(it + 1) & 1][t.f] = p + alpha * dv;
+    double rn = a * (alpha * alpha) + b * alpha + I.r[it % 3][t.f];
+    I.r[(it + 1) % 3][t.f] = rn;
+    mx = rn;
+  }
+  mx = block_max(mx, red);
+  if (threadIdx.x == 0) partials[(size_t)blockIdx.x * KP] = mx;
+  if (last_block(&I.counter, I.ntiles)) {
+    double gmx = reduce_partials_max(partials, I.tile0, I.ntiles, 0, red);
+    if (threadIdx.x == 0) {
+      I.linf = gmx / elem_area(n);
+      I.it = it + 1;
+      I.active = (I.it < I.max_iter && I.residual > I.threshold) ? 1 : 0;
+      if (!I.active) stop_outcome(I);
+    }
+  }
+}
+
+// Forward mesh: origin grid + exact vertex gradients of the final potential
+// (otsolver_2dgrid.cpp:222-227). One thread per vertex.
+__global__ void k_forward_mesh(const Inst* insts, int q, double* xy) {
+  const Inst& I = insts[q];
+  const int n = I.n;
+  long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long V = (long)(n + 1) * (n + 1);
+  if (v >= V) return;
+  int i = (int)(v / (n + 1)), j = (int)(v % (n + 1));
+  const double* psi = I.psi[I.it & 1];
+  auto P = [&](int a, int b) { return psi[(size_t)clampi(a, n) * n + clampi(b, n)]; };
+  double p00 = P(i - 1, j - 1), p01 = P(i - 1, j), p10 = P(i, j - 1), p11 = P(i, j);
+  double hw = 0.5 * (double)n;
+  double gx = hw * ((p10 + p11) - (p00 + p01));
+  double gy = hw * ((p01 + p11) - (p00 + p10));
+  double dx = 1.0 / (double)n;
+  xy[2 * v] = (double)i * dx + gx;
+  xy[2 * v + 1] = (double)j * dx + gy;
+}
+
+// y = M x, the reference's assembled matrix (otsolver_2dgrid.cpp:284-311), for the
+// diagonalisation check.
+__global__ void k_laplacian_apply(int n, const double* x, double* y) {
+  long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= (long)n * n) return;
+  int i = (int)(f / n), j = (int)(f % n);
+  int i1 = i == 0 ? i : i - 1, j1 = j == 0 ? j : j - 1;
+  int i2 = i == n - 1 ? i : i + 1, j2 = j == n - 1 ? j : j + 1;
+  y[f] = 2.0 * x[f] - 0.5 * (x[(size_t)i1 * n + j1] + x[(size_t)i1 * n + j2] + x[(size_t)i2 * n + j1] +
+                             x[(size_t)i2 * n + j2]);
+}
+
+// ---------------------------------------------------------------------------
+// Host side.
+
+void DevBuf::reserve(size_t b) {
+  if (b <= bytes) return;
+  release();
+  OTM_CUDA(cudaMalloc(&p, b));
+  bytes = b;
+}
+
+static int tiles_of(int n) { return ((n + TI - 1) / TI) * ((n + TJ - 1) / TJ); }
+static int gemm_tiles_of(int n) {
+  int t = (n + GB - 1) / GB;
+  return t * t;
+}
+
+// Lays out (or reuses) the workspace for a list of sizes and returns host copies of
+// the instance records with buffer pointers filled in.
+static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<int>& sizes) {
+  Workspace& ws = ctx->ws;
+  const int count = (int)sizes.size();
+  std::vector<Inst> h(count);
+  size_t cells = 0;
+  int tiles = 0, gemm = 0;
+  for (int q = 0; q < count; ++q) {
+    int n = sizes[q];
+    Inst& I = h[q];
+    std::memset(&I, 0, sizeof(Inst));
+    I.n = n;
+    I.tile0 = tiles;
+    I.ntiles = tiles_of(n);
+    I.gemm0 = gemm;
+    I.ngemm = gemm_tiles_of(n);
+    tiles += I.ntiles;
+    gemm += I.ngemm;
+    // 11 cell arrays per instance, each padded to 32 doubles (256 bytes)
+    cells += 11 * (((size_t)n * n + 31) / 32 * 32);
+  }
+  bool same = ws.sizes == sizes;
+  if (!same) {
+    ws.insts.reserve(sizeof(Inst) * count);
+    ws.tile_inst.reserve(sizeof(int) * tiles);
+    ws.gemm_inst.reserve(sizeof(int) * gemm);
+    ws.partials.reserve(sizeof(double) * KP * (size_t)tiles);
+    ws.arena.reserve(sizeof(double) * cells);
+    std::vector<int> ti(tiles), gi(gemm);
+    for (int q = 0; q < count; ++q) {
+      for (int k = 0; k < h[q].ntiles; ++k) ti[h[q].tile0 + k] = q;
+      for (int k = 0; k < h[q].ngemm; ++k) gi[h[q].gemm0 + k] = q;
+    }
+    OTM_CUDA(cudaMemcpyAsync(ws.tile_inst.p, ti.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, ctx->stream));
+    OTM_CUDA(cudaMemcpyAsync(ws.gemm_inst.p, gi.data(), sizeof(int) * gemm, cudaMemcpyHostToDevice, ctx->stream));
+    OTM_CUDA(cudaStreamSynchronize(ctx->stream));
+    ws.sizes = sizes;
+    ws.total_tiles = tiles;
+    ws.total_gemm = gemm;
+    size_t need = sizeof(Inst) * count;
+    if (ws.h_pinned_bytes < need) {
+      if (ws.h_pinned) cudaFreeHost(ws.h_pinned);
+      ws.h_pinned = nullptr;
+      OTM_CUDA(cudaMallocHost(&ws.h_pinned, need));
+      ws.h_pinned_bytes = need;
+    }
+  }
+  double* base = ws.arena.as<double>();
+  for (int q = 0; q < count; ++q) {
+    Inst& I = h[q];
+    size_t N = (((size_t)I.n * I.n + 31) / 32) * 32;
+    double* arr[11];
+    for (int k = 0; k < 11; ++k) {
+      arr[k] = base;
+      base += N;
+    }
+    I.psi[0] = arr[0];
+    I.psi[1] = arr[1];
+    I.r[0] = arr[2];
+    I.r[1] = arr[3];
+    I.r[2] = arr[4];
+    I.dhat = arr[5];
+    I.d[0] = arr[6];
+    I.d[1] = arr[7];
+    I.rho = arr[8];
+    I.t1 = arr[9];
+    I.t2 = arr[10];
+    SizeTables* T = ctx->tables.at(I.n).get();
+    I.C = T->C.as<double>();
+    I.cosk = T->cosk.as<double>();
+  }
+  return h;
+}
+
+static SizeTables* init_size(otm_context* ctx, int n);
+
+// Runs the whole solve for `count` instances whose raw densities have been copied
+// into their rho buffers. Host-side copies of the final records are returned.
+static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, const otm_solver_options& o) {
+  Workspace& ws = ctx->ws;
+  cudaStream_t st = ctx->stream;
+  const int count = (int)h.size();
+  for (auto& I : h) {
+    I.max_iter = o.max_iter;
+    I.beta_cj = o.beta == OTM_BETA_CONJUGATE_JACOBIAN ? 1 : 0;
+    I.threshold = o.threshold;
+    I.max_ratio = o.max_ratio;
+    size_t N = (size_t)I.n * I.n;
+    OTM_CUDA(cudaMemsetAsync(I.psi[0], 0, N * sizeof(double), st));
+    OTM_CUDA(cudaMemsetAsync(I.d[0], 0, N * sizeof(double), st));
+    OTM_CUDA(cudaMemsetAsync(I.d[1], 0, N * sizeof(double), st));
+    OTM_CUDA(cudaMemsetAsync(I.r[2], 0, N * sizeof(double), st));
+  }
+  Inst* d_insts = ws.insts.as<Inst>();
+  OTM_CUDA(cudaMemcpyAsync(d_insts, h.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice, st));
+  const int* ti = ws.tile_inst.as<int>();
+  const int* gi = ws.gemm_inst.as<int>();
+  double* part = ws.partials.as<double>();
+  const int T = ws.total_tiles, G = ws.total_gemm;
+
+  launch(ctx, "density_sum", k_density_sum, T, NT, d_insts, ti, part);
+  launch(ctx, "density_scale", k_density_scale, T, NT, d_insts, ti, part);
+  launch(ctx, "density_apply", k_density_apply, T, NT, d_insts, ti);
+  launch(ctx, "residual_init", k_residual_init, T, NT, d_insts, ti, part);
+  OTM_CUDA(cudaGetLastError());
+
+  Inst* hp = static_cast<Inst*>(ws.h_pinned);
+  int launched = 0;
+  const int chunk = 4;
+  while (true) {
+    OTM_CUDA(cudaMemcpyAsync(hp, d_insts, sizeof(Inst) * count, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    bool any = false;
+    for (int q = 0; q < count; ++q) any |= hp[q].active != 0;
+    if (!any || launched >= o.max_iter) break;
+    for (int c = 0; c < chunk && launched < o.max_iter; ++c, ++launched) {
+      for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, gi, s, 1);
+      launch(ctx, "beta", k_beta, T, NT, d_insts, ti, part);
+      launch(ctx, "coeffs", k_coeffs, T, NT, d_insts, ti, part);
+      launch(ctx, "update", k_update, T, NT, d_insts, ti, part);
+    }
+    OTM_CUDA(cudaGetLastError());
+  }
+  std::vector<Inst> out(hp, hp + count);
+  return out;
+}
+
+static void fill_stats(const Inst& I, otm_solve_stats* s) {
+  if (!s) return;
+  s->iterations = I.it;
+  s->outcome = I.outcome;
+  s->residual = I.residual;
+  s->linf = I.linf;
+  s->initial_residual = I.residual0;
+}
+
+// Builds the size-n cosine tables and runs the diagonalisation check on the GPU.
+static SizeTables* init_size(otm_context* ctx, int n) {
+  auto it = ctx->tables.find(n);
+  if (it != ctx->tables.end()) return it->second.get();
+  auto T = std::make_unique<SizeTables>();
+  T->n = n;
+  std::vector<double> C((size_t)n * n), ck(n);
+  for (int k = 0; k < n; ++k) {
+    double s = k == 0 ? std::sqrt(1.0 / n) : std::sqrt(2.0 / n);
+    for (int i = 0; i < n; ++i) C[(size_t)k * n + i] = s * std::cos(M_PI * (i + 0.5) * k / n);
+    ck[k] = std::cos(M_PI * k / n);
+  }
+  T->C.reserve(sizeof(double) * C.size());
+  T->cosk.reserve(sizeof(double) * n);
+  cudaStream_t st = ctx->stream;
+  OTM_CUDA(cudaMemcpyAsync(T->C.p, C.data(), sizeof(double) * C.size(), cudaMemcpyHostToDevice, st));
+  OTM_CUDA(cudaMemcpyAsync(T->cosk.p, ck.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
+
+  // Check M x == C^T (lambda o (C X C^T)) C on a random probe (otsolver_2dgrid.cpp:284-311).
+  size_t N = (size_t)n * n;
+  DevBuf buf;
+  buf.reserve(sizeof(double) * N * 5);
+  double* x = buf.as<double>();
+  double* y1 = x + N;
+  double* y2 = x + 2 * N;
+  double* t1 = x + 3 * N;
+  double* t2 = x + 4 * N;
+  std::vector<double> hx(N);
+  std::mt19937_64 rng(12345 + n);
+  std::uniform_real_distribution<double> U(-1.0, 1.0);
+  for (auto& v : hx) v = U(rng);
+  OTM_CUDA(cudaMemcpyAsync(x, hx.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+  k_laplacian_apply<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(n, x, y1);
+  Inst I;
+  std::memset(&I, 0, sizeof(I));
+  I.n = n;
+  I.ngemm = gemm_tiles_of(n);
+  I.r[0] = x;
+  I.dhat = y2;
+  I.t1 = t1;
+  I.t2 = t2;
+  I.C = T->C.as<double>();
+  I.cosk = T->cosk.as<double>();
+  I.active = 1;
+  DevBuf dI, dG;
+  dI.reserve(sizeof(Inst));
+  dG.reserve(sizeof(int) * I.ngemm);
+  std::vector<int> zeros(I.ngemm, 0);
+  OTM_CUDA(cudaMemcpyAsync(dI.p, &I, sizeof(Inst), cudaMemcpyHostToDevice, st));
+  OTM_CUDA(cudaMemcpyAsync(dG.p, zeros.data(), sizeof(int) * I.ngemm, cudaMemcpyHostToDevice, st));
+  for (int s = 0; s < 4; ++s) k_dct_gemm<<<I.ngemm, 256, 0, st>>>(dI.as<Inst>(), dG.as<int>(), s, 2);
+  OTM_CUDA(cudaGetLastError());
+  std::vector<double> h1(N), h2(N);
+  OTM_CUDA(cudaMemcpyAsync(h1.data(), y1, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  OTM_CUDA(cudaMemcpyAsync(h2.data(), y2, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+  OTM_CUDA(cudaStreamSynchronize(st));
+  double err = 0, scale = 0;
+  for (size_t f = 0; f < N; ++f) {
+    err = std::max(err, std::fabs(h1[f] - h2[f]));
+    scale = std::max(scale, std::fabs(h1[f]));
+  }
+  T->dct_check_err = scale > 0 ? err / scale : err;
+  T->dct_ok = T->dct_check_err <= 1e-10;
+  SizeTables* raw = T.get();
+  ctx->tables[n] = std::move(T);
+  return raw;
+}
+
+}  // namespace otm
+
+using namespace otm;
+
+extern "C" int otm_init(otm_context* ctx, int n) {
+  return guarded([&] {
+    if (!ctx) throw BadArg{"otm_init: null context"};
+    if (n < 1 || n > 16384) throw BadArg{"otm_init: grid size must be in [1, 16384]"};
+    make_current(ctx);
+    SizeTables* T = init_size(ctx, n);
+    if (!T->dct_ok)
+      throw BadArg{"otm_init: the cosine basis does not diagonalise the assembled matrix (relative error " +
+                   std::to_string(T->dct_check_err) + ")"};
+    return (int)OTM_OK;
+  });
+}
+
+static void check_opts(const otm_solver_options& o) {
+  if (o.beta != OTM_BETA_ZERO && o.beta != OTM_BETA_CONJUGATE_JACOBIAN) throw BadArg{"unknown beta option"};
+  if (o.max_iter < 0) throw BadArg{"max_iter must be >= 0"};
+}
+
+extern "C" int otm_solve_batch(otm_context* ctx, int count, const int* ns, const double* const* density,
+                               const otm_solver_options* opt, double* const* fwd_xy, double* const* adjusted,
+                               otm_solve_stats* stats) {
+  return guarded([&] {
+    if (!ctx) throw BadArg{"otm_solve_batch: null context"};
+    if (count < 1 || !ns || !density || !fwd_xy) throw BadArg{"otm_solve_batch: bad arguments"};
+    otm_solver_options o;
+    otm_default_options(&o);
+    if (opt) o = *opt;
+    check_opts(o);
+    make_current(ctx);
+    std::vector<int> sizes(ns, ns + count);
+    for (int q = 0; q < count; ++q) {
+      if (sizes[q] < 1 || sizes[q] > 16384) throw BadArg{"otm_solve_batch: grid size out of range"};
+      if (!density[q] || !fwd_xy[q]) throw BadArg{"otm_solve_batch: null buffer"};
+      auto it = ctx->tables.find(sizes[q]);
+      if (it == ctx->tables.end()) {
+        SizeTables* T = init_size(ctx, sizes[q]);
+        if (!T->dct_ok) throw BadArg{"otm_solve_batch: diagonalisation check failed"};
+      }
+    }
+    std::vector<Inst> h = layout_workspace(ctx, sizes);
+    for (int q = 0; q < count; ++q)
+      copy_in(ctx, h[q].rho, density[q], sizeof(double) * (size_t)sizes[q] * sizes[q]);
+    std::vector<Inst> fin = run_solver(ctx, h, o);
+    Inst* d_insts = ctx->ws.insts.as<Inst>();
+    for (int q = 0; q < count; ++q) {
+      int n = sizes[q];
+      size_t V = (size_t)(n + 1) * (n + 1);
+      bool dev = is_device_ptr(fwd_xy[q]);
+      double* dst = fwd_xy[q];
+      if (!dev) {
+        ctx->staging.reserve(sizeof(double) * 2 * V);
+        dst = ctx->staging.as<double>();
+      }
+      launch(ctx, "forward_mesh", k_forward_mesh, (unsigned)((V + 255) / 256), 256, (const Inst*)d_insts, q, dst);
+      OTM_CUDA(cudaGetLastError());
+      if (!dev) copy_out(ctx, fwd_xy[q], dst, sizeof(double) * 2 * V);
+      if (adjusted && adjusted[q]) copy_out(ctx, adjusted[q], h[q].rho, sizeof(double) * (size_t)n * n);
+      if (stats) fill_stats(fin[q], &stats[q]);
+    }
+    OTM_CUDA(cudaStreamSynchronize(ctx->stream));
+    ctx->prof.flush();
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_solve(otm_context* ctx, int n, const double* density, const otm_solver_options* opt,
+                         double* fwd_xy, double* adjusted, otm_solve_stats* stats) {
+  double* adj[1] = {adjusted};
+  double* fwd[1] = {fwd_xy};
+  const double* dens[1] = {density};
+  return otm_solve_batch(ctx, 1, &n, dens, opt, fwd, adjusted ? adj : nullptr, stats);
+}

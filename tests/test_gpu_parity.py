@@ -1,0 +1,136 @@
+"""Parity of the CUDA path (through the C ABI) with the reference's golden vectors
+and the C oracle. Tolerances: vertex positions within 1e-6 of the unit square (the
+FP64 solver), identical iteration counts; point location and rasterization
+bit-exact."""
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def ot():
+    from otmap_b200 import otmap
+
+    return otmap
+
+
+def _solve(ot, g):
+    n = int(g["n"])
+    s = ot.GridBasedTransportSolver()
+    s.set_verbose_level(0)
+    s.init(n)
+    opt = ot.SolverOptions(beta=ot.BetaOpt(int(g["beta_cj"])), max_iter=int(g["max_iter"]),
+                           threshold=float(g["threshold"]), max_ratio=float(g["max_ratio"]))
+    return s.solve(g["density"], opt)
+
+
+@pytest.mark.parametrize("name", golden_names("solve_"))
+def test_solve_matches_reference(name, ot):
+    g = load_golden(name)
+    m = _solve(ot, g)
+    assert m.stats.iterations == int(g["iterations"])
+    np.testing.assert_allclose(m.density(), g["adjusted"], rtol=1e-13, atol=0)
+    assert np.abs(m.fwd_mesh() - g["fwd"]).max() <= POS_TOL
+    if m.stats.iterations:
+        np.testing.assert_allclose(m.stats.residual, float(g["residual"]), rtol=1e-4, atol=1e-14)
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_solve_config1_256_matches_oracle(seed, ot, oracle_port):
+    from otmap_b200 import workloads as W
+
+    n = 256
+    d = W.to_cells(W.gaussian_mixture(n, seed))
+    o = oracle_port.solve(d, n)
+    s = ot.GridBasedTransportSolver()
+    s.set_verbose_level(0)
+    s.init(n)
+    m = s.solve(d)
+    assert m.stats.iterations == o.iterations
+    err = np.abs(m.fwd_mesh() - o.fwd).max()
+    assert err <= POS_TOL, err
+    assert m.stats.residual <= 1e-7
+
+
+def test_batch_matches_individual_solves(ot):
+    from otmap_b200 import workloads as W
+
+    dens = [W.gaussian_mixture(n, 40 + k) for k, n in enumerate([32, 64, 17, 128, 64])]
+    maps = ot.solve_batch(dens)
+    for img, m in zip(dens, maps):
+        n = img.shape[0]
+        s = ot.GridBasedTransportSolver()
+        s.set_verbose_level(0)
+        s.init(n)
+        single = s.solve(W.to_cells(img))
+        assert m.stats.iterations == single.stats.iterations
+        assert np.array_equal(m.fwd_mesh(), single.fwd_mesh())
+
+
+@pytest.mark.parametrize("name", golden_names("inverse_"))
+def test_inverse_bit_exact(name, ot):
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    n = int(g["n"])
+    tm = ot.TransportMap(n, s["fwd"], s["adjusted"])
+    pts = np.ascontiguousarray(g["points"].copy())
+    face = np.zeros(pts.shape[0], dtype=np.int32)
+    nh = np.zeros(pts.shape[0], dtype=np.int32)
+    missing = tm.apply_inverse(pts, face, nh)
+    assert np.array_equal(nh, g["nhits"])
+    assert missing == int((g["nhits"] == 0).sum())
+    one = g["nhits"] == 1
+    assert np.array_equal(face[one], g["faces"][one, 0])
+    assert np.array_equal(pts[one], g["inverse"][one])
+
+
+def test_inverse_random_points_1024_shapes(ot, oracle_port):
+    """Forward mesh of an oracle solve at 128^2; 2^16 random FP32 points; bit-exact
+    against the oracle's restatement of the reference BVH query."""
+    from otmap_b200 import workloads as W
+
+    n = 128
+    d = W.to_cells(W.blurred_shapes(n, 3, sigma_px=1.0))
+    o = oracle_port.solve(d, n, trace=False)
+    pts = W.random_points(1 << 16, 7)
+    pos_o, face_o, nh_o, _ = oracle_port.apply_inverse(o.fwd, o.density, n, pts)
+    tm = ot.TransportMap(n, o.fwd, o.density)
+    p = np.ascontiguousarray(pts.copy())
+    face = np.zeros(p.shape[0], dtype=np.int32)
+    nh = np.zeros(p.shape[0], dtype=np.int32)
+    tm.apply_inverse(p, face, nh)
+    assert np.array_equal(nh, nh_o)
+    one = nh_o == 1
+    assert np.array_equal(face[one], face_o[one])
+    assert np.array_equal(p[one], pos_o[one])
+
+
+@pytest.mark.parametrize("name", golden_names("raster_"))
+def test_raster_bit_exact(name, ot):
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    n = int(g["n"])
+    for key in g:
+        if not key.startswith("img_"):
+            continue
+        tag, size = key[4:].split("_")
+        rows, cols = map(int, size.split("x"))
+        img = np.empty((rows, cols))
+        ot.rasterize_image(s["fwd"], s["adjusted"] if tag == "dens" else None, img, n=n)
+        assert np.array_equal(img, g[key]), key
+
+
+def test_bad_arguments_raise(ot):
+    from otmap_b200 import native
+
+    s = ot.GridBasedTransportSolver()
+    with pytest.raises(native.OtmError):
+        s._ctx.init(0)
+    with pytest.raises(RuntimeError):
+        ot.GridBasedTransportSolver().solve(np.ones(16))
