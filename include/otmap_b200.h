@@ -141,6 +141,30 @@ int otm_map_inverse(otm_map* map, double* points, long count, int* face, int* nh
 int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
                   double* img);
 
+/* ---- allocation-free solve (no counterpart in the reference) ----
+ *
+ * For callers that cannot let a library call cudaMalloc: code that runs while a
+ * stream is being captured into a CUDA graph, hosts whose own allocator owns all
+ * device memory, and latency-critical loops that must stay off the driver's
+ * allocator. otm_solve_noalloc does what otm_solve does for one density but
+ * allocates nothing: its working memory is a fixed 8 MiB array in the library's
+ * device data, which every GPU that loads the library holds until the process
+ * exits. Hence the size limit: n <= OTM_NOALLOC_MAX_N (larger n is rejected with
+ * OTM_ERR_BAD_ARG).
+ *   - Runs on the calling thread's current device, on `stream` (a cudaStream_t;
+ *     NULL = the legacy default stream), and returns when the result is written.
+ *   - Buffers may be host or device memory, as for otm_solve; no context needed.
+ *   - The first call on each device looks up the array's device address and checks
+ *     the cosine basis against the assembled matrix for that n; make that first call
+ *     before any stream capture.
+ *   - All calls on a device share the one array (it keeps the last call's contents;
+ *     each call re-initialises what must start at zero): calls that overlap on the
+ *     GPU -- from two threads, or on two streams -- race and give wrong results.
+ *     Serialise them. */
+#define OTM_NOALLOC_MAX_N 256
+int otm_solve_noalloc(int n, const double* density, const otm_solver_options* opt, double* fwd_xy,
+                      double* adjusted, otm_solve_stats* stats, void* stream);
+
 /* ---- instrumentation (no counterpart in the reference, which times its phases
  * with BenchTimer, otsolver_2dgrid.cpp:153-217) ---- */
 

@@ -26,6 +26,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <vector>
 
@@ -915,4 +916,245 @@ extern "C" int otm_solve(otm_context* ctx, int n, const double* density, const o
   double* fwd[1] = {fwd_xy};
   const double* dens[1] = {density};
   return otm_solve_batch(ctx, 1, &n, dens, opt, fwd, adjusted ? adj : nullptr, stats);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free solve.
+//
+// Some callers cannot let a library call cudaMalloc: code that runs while a stream
+// is being captured into a CUDA graph (an allocation there breaks or is refused by
+// the capture), hosts that hand every byte of device memory to their own allocator
+// and forbid other allocations, and latency-critical loops that must not hit the
+// driver's allocator. otm_solve_noalloc serves them: it runs the same kernels as
+// otm_solve, but its working memory -- instance record, work lists, partial sums,
+// cosine tables and the per-cell arrays -- lives in one file-scope device array of
+// fixed size, so the call allocates nothing. That array is held by every GPU that
+// loads the library until the process exits, which is why it is kept modest: it
+// bounds the grid size to OTM_NOALLOC_MAX_N.
+
+namespace otm {
+
+constexpr size_t kNoallocWords = size_t(1) << 20;  // 8 MiB of doubles
+static __device__ __align__(256) double g_noalloc_scratch[kNoallocWords];
+
+constexpr int kMaxDevices = 64;
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[kMaxDevices];                        // device address of the array, per device
+static unsigned char g_noalloc_checked[kMaxDevices][OTM_NOALLOC_MAX_N + 1];  // diagonalisation verified
+
+// Cosine tables for size n, built on the device (no host staging buffer).
+__global__ void k_noalloc_tables(int n, double* C, double* cosk) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < (long)n * n) {
+    int k = (int)(t / n), i = (int)(t % n);
+    double s = k == 0 ? sqrt(1.0 / n) : sqrt(2.0 / n);
+    C[t] = s * cos(M_PI * (i + 0.5) * k / n);
+  }
+  if (t < n) cosk[t] = cos(M_PI * (double)t / n);
+}
+
+// Deterministic probe vector in [-1, 1) for the diagonalisation check.
+__global__ void k_noalloc_probe(long N, double* x) {
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= N) return;
+  unsigned long long h = (unsigned long long)(t + 1) * 0x9E3779B97F4A7C15ull;
+  h ^= h >> 31;
+  h *= 0xBF58476D1CE4E5B9ull;
+  h ^= h >> 29;
+  x[t] = (double)(h >> 11) * (1.0 / 9007199254740992.0) * 2.0 - 1.0;
+}
+
+// out[0] = max |a - b|, out[1] = max |a| (one block).
+__global__ void k_noalloc_maxdiff(long N, const double* a, const double* b, double* out) {
+  __shared__ double red[32];
+  double d = 0.0, m = 0.0;
+  for (long t = threadIdx.x; t < N; t += blockDim.x) {
+    d = fmax(d, fabs(a[t] - b[t]));
+    m = fmax(m, fabs(a[t]));
+  }
+  d = block_max(d, red);
+  m = block_max(m, red);
+  if (threadIdx.x == 0) {
+    out[0] = d;
+    out[1] = m;
+  }
+}
+
+// Word offsets of everything the solve keeps in the array, for grid size n.
+struct NoallocLayout {
+  size_t inst, tiles, gemm, partials, C, cosk, cells, fwd, check, end;
+  size_t npad;
+};
+
+static size_t up32(size_t w) { return (w + 31) / 32 * 32; }
+
+static NoallocLayout noalloc_layout(int n) {
+  NoallocLayout L;
+  size_t w = 0;
+  L.inst = w;
+  w += up32((sizeof(Inst) + 7) / 8);
+  L.tiles = w;
+  w += up32(((size_t)tiles_of(n) + 1) / 2);
+  L.gemm = w;
+  w += up32(((size_t)gemm_tiles_of(n) + 1) / 2);
+  L.partials = w;
+  w += up32((size_t)tiles_of(n) * KP);
+  L.C = w;
+  w += up32((size_t)n * n);
+  L.cosk = w;
+  w += up32((size_t)n);
+  L.npad = up32((size_t)n * n);
+  L.cells = w;
+  w += 11 * L.npad;
+  L.fwd = w;
+  w += up32(2 * (size_t)(n + 1) * (n + 1));
+  L.check = w;
+  w += 2 * 32;
+  L.end = w;
+  return L;
+}
+
+static double* noalloc_scratch(int dev) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    double* p = nullptr;
+    // with `dev` current: the symbol's address on that device
+    OTM_CUDA(cudaGetSymbolAddress((void**)&p, g_noalloc_scratch));
+    g_noalloc_ptr[dev] = p;
+  }
+  return g_noalloc_ptr[dev];
+}
+
+}  // namespace otm
+
+extern "C" int otm_solve_noalloc(int n, const double* density, const otm_solver_options* opt, double* fwd_xy,
+                                 double* adjusted, otm_solve_stats* stats, void* stream_handle) {
+  return guarded([&] {
+    if (n < 1 || n > OTM_NOALLOC_MAX_N)
+      throw BadArg{"otm_solve_noalloc: grid size " + std::to_string(n) + " exceeds the allocation-free limit of " +
+                   std::to_string(OTM_NOALLOC_MAX_N) + " (use otm_solve)"};
+    if (!density || !fwd_xy) throw BadArg{"otm_solve_noalloc: null buffer"};
+    otm_solver_options o;
+    otm_default_options(&o);
+    if (opt) o = *opt;
+    check_opts(o);
+    int dev = 0;
+    OTM_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) throw BadArg{"otm_solve_noalloc: device ordinal out of range"};
+    cudaStream_t st = static_cast<cudaStream_t>(stream_handle);
+    double* base = noalloc_scratch(dev);
+    const NoallocLayout L = noalloc_layout(n);
+    if (L.end > kNoallocWords) throw BadArg{"otm_solve_noalloc: scratch layout exceeds the static array"};
+
+    const size_t N = (size_t)n * n, V = (size_t)(n + 1) * (n + 1);
+    Inst* d_inst = reinterpret_cast<Inst*>(base + L.inst);
+    int* d_tiles = reinterpret_cast<int*>(base + L.tiles);
+    int* d_gemm = reinterpret_cast<int*>(base + L.gemm);
+    double* part = base + L.partials;
+    double* C = base + L.C;
+    double* cosk = base + L.cosk;
+    double* cells = base + L.cells;
+    const int T = tiles_of(n), G = gemm_tiles_of(n);
+
+    // work lists: every tile belongs to instance 0 (T, G <= 256 for n <= 256)
+    int zeros[256];
+    for (int k = 0; k < 256; ++k) zeros[k] = 0;
+    OTM_CUDA(cudaMemcpyAsync(d_tiles, zeros, sizeof(int) * T, cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(d_gemm, zeros, sizeof(int) * G, cudaMemcpyHostToDevice, st));
+    k_noalloc_tables<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(n, C, cosk);
+
+    Inst I;
+    std::memset(&I, 0, sizeof(I));
+    I.n = n;
+    I.tile0 = 0;
+    I.ntiles = T;
+    I.gemm0 = 0;
+    I.ngemm = G;
+    double* arr[11];
+    for (int k = 0; k < 11; ++k) arr[k] = cells + k * L.npad;
+    I.psi[0] = arr[0];
+    I.psi[1] = arr[1];
+    I.r[0] = arr[2];
+    I.r[1] = arr[3];
+    I.r[2] = arr[4];
+    I.dhat = arr[5];
+    I.d[0] = arr[6];
+    I.d[1] = arr[7];
+    I.rho = arr[8];
+    I.t1 = arr[9];
+    I.t2 = arr[10];
+    I.C = C;
+    I.cosk = cosk;
+
+    // the diagonalisation check, once per device and size, in the same array
+    bool checked;
+    {
+      std::lock_guard<std::mutex> lock(g_noalloc_mu);
+      checked = g_noalloc_checked[dev][n] != 0;
+    }
+    if (!checked) {
+      Inst P = I;
+      P.active = 1;
+      P.r[0] = arr[0];   // probe x
+      P.dhat = arr[2];   // C^T (lambda o (C X C^T)) C
+      k_noalloc_probe<<<(unsigned)((N + 255) / 256), 256, 0, st>>>((long)N, arr[0]);
+      k_laplacian_apply<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(n, arr[0], arr[1]);
+      OTM_CUDA(cudaMemcpyAsync(d_inst, &P, sizeof(Inst), cudaMemcpyHostToDevice, st));
+      for (int s = 0; s < 4; ++s) k_dct_gemm<<<G, 256, 0, st>>>(d_inst, d_gemm, s, 2);
+      k_noalloc_maxdiff<<<1, 256, 0, st>>>((long)N, arr[1], arr[2], base + L.check);
+      double res[2] = {0, 0};
+      OTM_CUDA(cudaMemcpyAsync(res, base + L.check, sizeof(res), cudaMemcpyDeviceToHost, st));
+      OTM_CUDA(cudaStreamSynchronize(st));
+      double rel = res[1] > 0 ? res[0] / res[1] : res[0];
+      if (!(rel <= 1e-10))
+        throw BadArg{"otm_solve_noalloc: the cosine basis does not diagonalise the assembled matrix"};
+      std::lock_guard<std::mutex> lock(g_noalloc_mu);
+      g_noalloc_checked[dev][n] = 1;
+    }
+
+    // state that must start at zero: the initial potential, the directions and the
+    // residual buffer read as r_{k-1} in the first iteration (the record is rewritten)
+    I.max_iter = o.max_iter;
+    I.beta_cj = o.beta == OTM_BETA_CONJUGATE_JACOBIAN ? 1 : 0;
+    I.threshold = o.threshold;
+    I.max_ratio = o.max_ratio;
+    OTM_CUDA(cudaMemsetAsync(I.psi[0], 0, N * sizeof(double), st));
+    OTM_CUDA(cudaMemsetAsync(I.d[0], 0, N * sizeof(double), st));
+    OTM_CUDA(cudaMemsetAsync(I.d[1], 0, N * sizeof(double), st));
+    OTM_CUDA(cudaMemsetAsync(I.r[2], 0, N * sizeof(double), st));
+    OTM_CUDA(cudaMemcpyAsync(d_inst, &I, sizeof(Inst), cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(I.rho, density, N * sizeof(double),
+                             is_device_ptr(density) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, st));
+
+    k_density_sum<<<T, NT, 0, st>>>(d_inst, d_tiles, part);
+    k_density_scale<<<T, NT, 0, st>>>(d_inst, d_tiles, part);
+    k_density_apply<<<T, NT, 0, st>>>(d_inst, d_tiles);
+    k_residual_init<<<T, NT, 0, st>>>(d_inst, d_tiles, part);
+    OTM_CUDA(cudaGetLastError());
+    Inst h;
+    int launched = 0;
+    while (true) {
+      OTM_CUDA(cudaMemcpyAsync(&h, d_inst, sizeof(Inst), cudaMemcpyDeviceToHost, st));
+      OTM_CUDA(cudaStreamSynchronize(st));
+      if (!h.active || launched >= o.max_iter) break;
+      for (int c = 0; c < 4 && launched < o.max_iter; ++c, ++launched) {
+        for (int s = 0; s < 4; ++s) k_dct_gemm<<<G, 256, 0, st>>>(d_inst, d_gemm, s, 1);
+        k_beta<<<T, NT, 0, st>>>(d_inst, d_tiles, part);
+        k_coeffs<<<T, NT, 0, st>>>(d_inst, d_tiles, part);
+        k_update<<<T, NT, 0, st>>>(d_inst, d_tiles, part);
+      }
+      OTM_CUDA(cudaGetLastError());
+    }
+    bool fdev = is_device_ptr(fwd_xy);
+    double* dst = fdev ? fwd_xy : base + L.fwd;
+    k_forward_mesh<<<(unsigned)((V + 255) / 256), 256, 0, st>>>(d_inst, 0, dst);
+    OTM_CUDA(cudaGetLastError());
+    if (!fdev) OTM_CUDA(cudaMemcpyAsync(fwd_xy, dst, sizeof(double) * 2 * V, cudaMemcpyDeviceToHost, st));
+    if (adjusted)
+      OTM_CUDA(cudaMemcpyAsync(adjusted, I.rho, sizeof(double) * N,
+                               is_device_ptr(adjusted) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    fill_stats(h, stats);
+    return (int)OTM_OK;
+  });
 }

@@ -64,6 +64,8 @@ SIGNATURES = {
     "otm_map_inverse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p,
                                   C.POINTER(C.c_long)]),
     "otm_rasterize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "otm_solve_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(SolverOptionsC), C.c_void_p, C.c_void_p,
+                                    C.POINTER(SolveStatsC), C.c_void_p]),
     "otm_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "otm_launch_count": (C.c_long, [C.c_void_p]),
     "otm_profile": (C.c_int, [C.c_void_p, C.c_int]),
