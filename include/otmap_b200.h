@@ -141,6 +141,18 @@ int otm_map_inverse(otm_map* map, double* points, long count, int* face, int* nh
 int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
                   double* img);
 
+/* Context options (no counterpart in the reference).
+ *   OTM_OPT_POISSON: how d_hat = M^+ r is computed.
+ *     OTM_POISSON_AUTO  (default) fast cosine transform for power-of-two n in [8, 4096],
+ *                       dense products otherwise
+ *     OTM_POISSON_DENSE C.X.C^T products with the cosine basis, any n
+ *     OTM_POISSON_FFT   fast transform where possible (same as AUTO) */
+#define OTM_OPT_POISSON 1
+#define OTM_POISSON_AUTO 0
+#define OTM_POISSON_DENSE 1
+#define OTM_POISSON_FFT 2
+int otm_set_option(otm_context* ctx, int key, int value);
+
 /* ---- allocation-free solve (no counterpart in the reference) ----
  *
  * For callers that cannot let a library call cudaMalloc: code that runs while a

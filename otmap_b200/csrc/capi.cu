@@ -165,3 +165,20 @@ extern "C" int otm_profile_entry(otm_context* ctx, int index, const char** name,
   if (launches) *launches = ctx->prof.count[index];
   return 1;
 }
+
+extern "C" int otm_set_option(otm_context* ctx, int key, int value) {
+  if (!ctx) {
+    set_error("otm_set_option: null context");
+    return OTM_ERR_BAD_ARG;
+  }
+  if (key == OTM_OPT_POISSON) {
+    if (value < OTM_POISSON_AUTO || value > OTM_POISSON_FFT) {
+      set_error("otm_set_option: unknown Poisson mode");
+      return OTM_ERR_BAD_ARG;
+    }
+    ctx->poisson_mode = value;
+    return OTM_OK;
+  }
+  set_error("otm_set_option: unknown option");
+  return OTM_ERR_BAD_ARG;
+}

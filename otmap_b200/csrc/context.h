@@ -38,6 +38,8 @@ struct SizeTables {
   int n = 0;
   DevBuf C;     // n*n doubles, C[k*n + i]
   DevBuf cosk;  // n doubles
+  DevBuf tw;    // n/2 double2, exp(-2 pi i k / n) (power-of-two n)
+  DevBuf pt;    // n double2, (cos, sin)(pi k / 2n) (power-of-two n)
   bool dct_ok = false;      // the assembled matrix is diagonalised by C (checked on the GPU)
   double dct_check_err = 0;  // relative error of that check
 };
@@ -49,14 +51,17 @@ struct Workspace {
   std::vector<int> sizes;
   DevBuf insts;      // Inst[count]
   DevBuf tile_inst;  // int per stencil tile
-  DevBuf gemm_inst;  // int per GEMM tile
+  DevBuf gemm_inst;  // int per GEMM tile (instances on the dense-product transform)
+  DevBuf row_inst;   // int per row block of the fast transform
+  DevBuf col_inst;   // int per column block of the fast transform
   DevBuf partials;   // double[total_tiles * 8]
   DevBuf arena;      // per-instance cell arrays
   DevBuf host_rec;   // unused placeholder to keep layout stable
   std::vector<unsigned char> h_insts;  // host mirror of Inst[count]
   void* h_pinned = nullptr;            // pinned staging for Inst readback
   size_t h_pinned_bytes = 0;
-  int total_tiles = 0, total_gemm = 0;
+  int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0;
+  int mode = -1;  // poisson mode the layout was built for
   ~Workspace() {
     if (h_pinned) cudaFreeHost(h_pinned);
   }
@@ -89,6 +94,7 @@ struct otm_context {
   cudaStream_t stream = nullptr;
   int num_sms = 0;
   long launches = 0;  // kernels launched by this context since creation
+  int poisson_mode = 0;  // OTM_POISSON_AUTO / _DENSE / _FFT
   otm::Profiler prof;
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   otm::Workspace ws;
@@ -131,6 +137,22 @@ void launch(otm_context* ctx, const char* name, K kernel, dim3 grid, dim3 block,
     ctx->prof.pending.push_back({id, a, b});
   } else {
     kernel<<<grid, block, 0, ctx->stream>>>(args...);
+  }
+}
+
+// As launch(), with dynamic shared memory.
+template <class K, class... Args>
+void launch_smem(otm_context* ctx, const char* name, K kernel, dim3 grid, dim3 block, size_t smem, Args... args) {
+  ctx->launches++;
+  if (ctx->prof.on) {
+    int id = ctx->prof.id(name);
+    cudaEvent_t a = ctx->prof.get(), b = ctx->prof.get();
+    cudaEventRecord(a, ctx->stream);
+    kernel<<<grid, block, smem, ctx->stream>>>(args...);
+    cudaEventRecord(b, ctx->stream);
+    ctx->prof.pending.push_back({id, a, b});
+  } else {
+    kernel<<<grid, block, smem, ctx->stream>>>(args...);
   }
 }
 

@@ -30,37 +30,9 @@
 #include <random>
 #include <vector>
 
-#include "context.h"
+#include "engine.cuh"
 
 namespace otm {
-
-constexpr int TI = 8, TJ = 32, NT = 256;  // stencil tile: TI cells along x (i), TJ along y (j)
-constexpr int HI = TI + 2, HJ = TJ + 2;   // halo tile of cells
-constexpr int VI = TI + 1, VJ = TJ + 1;   // vertex tile
-constexpr int KP = 8;                     // partial sums per tile
-constexpr int GB = 64, GK = 16;           // DCT GEMM tile (GB x GB outputs, GK deep)
-
-// Device record of one solve instance. Buffer pointers are fixed for the life of
-// the workspace; everything below `it` is loop state updated by the kernels.
-struct Inst {
-  int n, tile0, ntiles, gemm0, ngemm;
-  int max_iter, beta_cj, pad0;
-  double threshold, max_ratio;
-  double* psi[2];
-  double* r[3];
-  double* dhat;
-  double* d[2];
-  double* rho;
-  double* t1;
-  double* t2;
-  const double* C;
-  const double* cosk;
-  // loop state
-  int it, active, outcome, use_beta;
-  unsigned int counter, pad1;
-  double residual, residual0, alpha, beta, linf, dnorm;
-  double dens_scale, dens_beta;
-};
 
 __device__ __forceinline__ int clampi(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
 
@@ -642,7 +614,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
   const int count = (int)sizes.size();
   std::vector<Inst> h(count);
   size_t cells = 0;
-  int tiles = 0, gemm = 0;
+  int tiles = 0, gemm = 0, rows = 0, cols = 0;
   for (int q = 0; q < count; ++q) {
     int n = sizes[q];
     Inst& I = h[q];
@@ -650,31 +622,55 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.n = n;
     I.tile0 = tiles;
     I.ntiles = tiles_of(n);
-    I.gemm0 = gemm;
-    I.ngemm = gemm_tiles_of(n);
     tiles += I.ntiles;
-    gemm += I.ngemm;
+    I.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
+    if (I.fft) {
+      int lines = fft_lines(n);
+      int lg = 0;
+      while ((1 << lg) < n) ++lg;
+      I.logn = lg;
+      I.row0 = rows;
+      I.nrow = n / lines;
+      I.col0 = cols;
+      I.ncol = n / lines;
+      rows += I.nrow;
+      cols += I.ncol;
+    } else {
+      I.gemm0 = gemm;
+      I.ngemm = gemm_tiles_of(n);
+      gemm += I.ngemm;
+    }
     // 11 cell arrays per instance, each padded to 32 doubles (256 bytes)
     cells += 11 * (((size_t)n * n + 31) / 32 * 32);
   }
-  bool same = ws.sizes == sizes;
+  bool same = ws.sizes == sizes && ws.mode == ctx->poisson_mode;
   if (!same) {
     ws.insts.reserve(sizeof(Inst) * count);
     ws.tile_inst.reserve(sizeof(int) * tiles);
-    ws.gemm_inst.reserve(sizeof(int) * gemm);
+    ws.gemm_inst.reserve(sizeof(int) * (gemm > 0 ? gemm : 1));
+    ws.row_inst.reserve(sizeof(int) * (rows > 0 ? rows : 1));
+    ws.col_inst.reserve(sizeof(int) * (cols > 0 ? cols : 1));
     ws.partials.reserve(sizeof(double) * KP * (size_t)tiles);
     ws.arena.reserve(sizeof(double) * cells);
-    std::vector<int> ti(tiles), gi(gemm);
+    std::vector<int> ti(tiles), gi(gemm), ri(rows), ci(cols);
     for (int q = 0; q < count; ++q) {
       for (int k = 0; k < h[q].ntiles; ++k) ti[h[q].tile0 + k] = q;
       for (int k = 0; k < h[q].ngemm; ++k) gi[h[q].gemm0 + k] = q;
+      for (int k = 0; k < h[q].nrow; ++k) ri[h[q].row0 + k] = q;
+      for (int k = 0; k < h[q].ncol; ++k) ci[h[q].col0 + k] = q;
     }
-    OTM_CUDA(cudaMemcpyAsync(ws.tile_inst.p, ti.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, ctx->stream));
-    OTM_CUDA(cudaMemcpyAsync(ws.gemm_inst.p, gi.data(), sizeof(int) * gemm, cudaMemcpyHostToDevice, ctx->stream));
-    OTM_CUDA(cudaStreamSynchronize(ctx->stream));
+    cudaStream_t st = ctx->stream;
+    OTM_CUDA(cudaMemcpyAsync(ws.tile_inst.p, ti.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, st));
+    if (gemm) OTM_CUDA(cudaMemcpyAsync(ws.gemm_inst.p, gi.data(), sizeof(int) * gemm, cudaMemcpyHostToDevice, st));
+    if (rows) OTM_CUDA(cudaMemcpyAsync(ws.row_inst.p, ri.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, st));
+    if (cols) OTM_CUDA(cudaMemcpyAsync(ws.col_inst.p, ci.data(), sizeof(int) * cols, cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
     ws.sizes = sizes;
+    ws.mode = ctx->poisson_mode;
     ws.total_tiles = tiles;
     ws.total_gemm = gemm;
+    ws.total_rows = rows;
+    ws.total_cols = cols;
     size_t need = sizeof(Inst) * count;
     if (ws.h_pinned_bytes < need) {
       if (ws.h_pinned) cudaFreeHost(ws.h_pinned);
@@ -706,6 +702,8 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     SizeTables* T = ctx->tables.at(I.n).get();
     I.C = T->C.as<double>();
     I.cosk = T->cosk.as<double>();
+    I.tw = T->tw.as<double2>();
+    I.pt = T->pt.as<double2>();
   }
   return h;
 }
@@ -753,7 +751,10 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
     for (int q = 0; q < count; ++q) any |= hp[q].active != 0;
     if (!any || launched >= o.max_iter) break;
     for (int c = 0; c < chunk && launched < o.max_iter; ++c, ++launched) {
-      for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, gi, s, 1);
+      if (G > 0)
+        for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, gi, s, 1);
+      if (ws.total_rows > 0)
+        poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), ws.total_rows, ws.col_inst.as<int>(), ws.total_cols);
       launch(ctx, "beta", k_beta, T, NT, d_insts, ti, part);
       launch(ctx, "coeffs", k_coeffs, T, NT, d_insts, ti, part);
       launch(ctx, "update", k_update, T, NT, d_insts, ti, part);
@@ -788,6 +789,16 @@ static SizeTables* init_size(otm_context* ctx, int n) {
   T->C.reserve(sizeof(double) * C.size());
   T->cosk.reserve(sizeof(double) * n);
   cudaStream_t st = ctx->stream;
+  if (fft_eligible(n)) {
+    std::vector<double2> tw(n / 2), pt(n);
+    for (int k = 0; k < n / 2; ++k) tw[k] = make_double2(std::cos(2.0 * M_PI * k / n), -std::sin(2.0 * M_PI * k / n));
+    for (int k = 0; k < n; ++k) pt[k] = make_double2(std::cos(M_PI * k / (2.0 * n)), std::sin(M_PI * k / (2.0 * n)));
+    T->tw.reserve(sizeof(double2) * (n / 2));
+    T->pt.reserve(sizeof(double2) * n);
+    OTM_CUDA(cudaMemcpyAsync(T->tw.p, tw.data(), sizeof(double2) * (n / 2), cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(T->pt.p, pt.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+  }
   OTM_CUDA(cudaMemcpyAsync(T->C.p, C.data(), sizeof(double) * C.size(), cudaMemcpyHostToDevice, st));
   OTM_CUDA(cudaMemcpyAsync(T->cosk.p, ck.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
 

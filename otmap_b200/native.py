@@ -23,6 +23,8 @@ ERR_TIMEOUT = -4
 ERR_NOT_INIT = -5
 
 CONVERGED, MAX_ITER, SMALL_STEP, NONFINITE = 0, 1, 2, 3
+OPT_POISSON = 1
+POISSON_AUTO, POISSON_DENSE, POISSON_FFT = 0, 1, 2
 OUTCOMES = {CONVERGED: "converged", MAX_ITER: "max_iter", SMALL_STEP: "small_step", NONFINITE: "nonfinite"}
 
 _dp = C.POINTER(C.c_double)
@@ -66,6 +68,7 @@ SIGNATURES = {
     "otm_rasterize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "otm_solve_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(SolverOptionsC), C.c_void_p, C.c_void_p,
                                     C.POINTER(SolveStatsC), C.c_void_p]),
+    "otm_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     "otm_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "otm_launch_count": (C.c_long, [C.c_void_p]),
     "otm_profile": (C.c_int, [C.c_void_p, C.c_int]),
@@ -138,6 +141,9 @@ class Context:
 
     def init(self, n: int):
         check(lib().otm_init(self._h, int(n)))
+
+    def set_poisson(self, mode: int):
+        check(lib().otm_set_option(self._h, OPT_POISSON, int(mode)))
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -134,3 +134,41 @@ def test_bad_arguments_raise(ot):
         s._ctx.init(0)
     with pytest.raises(RuntimeError):
         ot.GridBasedTransportSolver().solve(np.ones(16))
+
+
+@pytest.mark.parametrize("n", [8, 16, 64, 128, 512])
+def test_fast_and_dense_transforms_agree(n, ot):
+    """The fast cosine transform (power-of-two n) and the dense products give the same
+    solve: same iterations, positions within 1e-9."""
+    from otmap_b200 import native
+    from otmap_b200 import workloads as W
+
+    d = W.to_cells(W.gaussian_mixture(n, 70 + n))
+    out = {}
+    for mode in (native.POISSON_DENSE, native.POISSON_FFT):
+        ctx = native.Context(0)
+        ctx.set_poisson(mode)
+        s = ot.GridBasedTransportSolver(ctx)
+        s.set_verbose_level(0)
+        s.init(n)
+        out[mode] = s.solve(d)
+    a, b = out[native.POISSON_DENSE], out[native.POISSON_FFT]
+    assert a.stats.iterations == b.stats.iterations
+    assert np.abs(a.fwd_mesh() - b.fwd_mesh()).max() <= 1e-9
+
+
+def test_mixed_batch_uses_both_transforms(ot):
+    """A batch mixing power-of-two and other sizes (fast and dense transforms in the
+    same launches) matches per-instance solves."""
+    from otmap_b200 import workloads as W
+
+    dens = [W.gaussian_mixture(n, 90 + k) for k, n in enumerate([64, 48, 128, 33, 256])]
+    maps = ot.solve_batch(dens)
+    for img, m in zip(dens, maps):
+        n = img.shape[0]
+        s = ot.GridBasedTransportSolver()
+        s.set_verbose_level(0)
+        s.init(n)
+        single = s.solve(W.to_cells(img))
+        assert m.stats.iterations == single.stats.iterations
+        assert np.array_equal(m.fwd_mesh(), single.fwd_mesh())
