@@ -52,6 +52,8 @@ struct Workspace {
   DevBuf insts;      // Inst[count]
   DevBuf tile_inst;  // int per stencil tile
   DevBuf gemm_inst;  // int per GEMM tile (instances on the dense-product transform)
+  DevBuf strip_inst;  // int per sweep block
+  DevBuf sweep_partials;  // double[sweep blocks * SWEEP_SLOTS]
   DevBuf row_inst;   // int per row block of the fast transform
   DevBuf col_inst;   // int per column block of the fast transform
   DevBuf partials;   // double[total_tiles * 8]
@@ -60,7 +62,7 @@ struct Workspace {
   std::vector<unsigned char> h_insts;  // host mirror of Inst[count]
   void* h_pinned = nullptr;            // pinned staging for Inst readback
   size_t h_pinned_bytes = 0;
-  int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0;
+  int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0, total_strips = 0;
   int mode = -1;  // poisson mode the layout was built for
   ~Workspace() {
     if (h_pinned) cudaFreeHost(h_pinned);

@@ -2,6 +2,8 @@
 // transform kernels (poisson.cu).
 #pragma once
 
+#include <cfloat>
+
 #include "context.h"
 
 namespace otm {
@@ -31,6 +33,7 @@ struct Inst {
   const double2* pt;  // (cos, sin)(pi k / (2n)), k < n (fast transform)
   int fft, logn;      // fast transform used (n a power of two) / log2 n
   int row0, nrow, col0, ncol;  // first item and item count in the row / column work lists
+  int strip0, nstrip;          // first block and block count in the strip work list
   // loop state
   int it, active, outcome, use_beta;
   unsigned int counter, pad1;
@@ -39,10 +42,96 @@ struct Inst {
 };
 
 
+// Sets `outcome` for an instance whose loop condition (otsolver_2dgrid.cpp:160) failed.
+__device__ __forceinline__ void stop_outcome(Inst& I) {
+  if (I.residual <= I.threshold)
+    I.outcome = OTM_CONVERGED;
+  else if (!isfinite(I.residual))
+    I.outcome = OTM_NONFINITE;
+  else
+    I.outcome = OTM_MAX_ITER;
+}
+
+// ---------------------------------------------------------------------------
+// Exact line search (otsolver_2dgrid.cpp:541-606).
+
+__device__ __forceinline__ double cubic_eval(const double c[4], double t) { return ((c[3] * t + c[2]) * t + c[1]) * t + c[0]; }
+__device__ __forceinline__ double cubic_deriv(const double c[4], double t) { return (3.0 * c[3] * t + 2.0 * c[2]) * t + c[1]; }
+
+// Real roots of w3 t^3 + w2 t^2 + w1 t + w0: closed form of the depressed cubic
+// (Cardano for one real root, the trigonometric form for three) and two Newton
+// steps; replaces the companion-matrix eigensolver of otsolver_2dgrid.cpp:568-572.
+__device__ __forceinline__ int cubic_real_roots(const double w[4], double roots[3]) {
+  double a = w[2] / w[3], b = w[1] / w[3], c = w[0] / w[3];
+  if (!isfinite(a) || !isfinite(b) || !isfinite(c)) return 0;
+  double p = b - a * a / 3.0;
+  double q = 2.0 * a * a * a / 27.0 - a * b / 3.0 + c;
+  double disc = 0.25 * q * q + p * p * p / 27.0;
+  int m;
+  if (disc > 0.0) {
+    double sq = sqrt(disc);
+    double u = cbrt(-0.5 * q + (q <= 0.0 ? sq : -sq));
+    double y = (u != 0.0) ? u - p / (3.0 * u) : 0.0;
+    roots[0] = y - a / 3.0;
+    m = 1;
+  } else {
+    double r = sqrt(std_max(0.0, -p / 3.0));
+    if (r == 0.0) {
+      roots[0] = roots[1] = roots[2] = -a / 3.0;
+    } else {
+      double arg = std_max(-1.0, std_min(1.0, -0.5 * q / (r * r * r)));
+      double phi = acos(arg) / 3.0;
+      for (int k = 0; k < 3; ++k) roots[k] = 2.0 * r * cos(phi - 2.0943951023931954923 * k) - a / 3.0;
+    }
+    m = 3;
+  }
+  double cc[4] = {c, b, a, 1.0};
+  for (int k = 0; k < m; ++k)
+    for (int s = 0; s < 2; ++s) {
+      double f = cubic_eval(cc, roots[k]), df = cubic_deriv(cc, roots[k]);
+      if (df != 0.0 && isfinite(f / df)) roots[k] -= f / df;
+    }
+  return m;
+}
+
+// Among the real stationary points of e(t) = z0 + z1 t + ... + z4 t^4 in [-10, 10] the
+// one with least e(t); else t = 0.5 (otsolver_2dgrid.cpp:575-595).
+__device__ __forceinline__ void pick_step(const double z[5], double* alpha, double* emin) {
+  double w[4] = {z[1], 2.0 * z[2], 3.0 * z[3], 4.0 * z[4]};
+  double roots[3];
+  int m = cubic_real_roots(w, roots);
+  bool found = false;
+  double best = 0.0, rmin = 0.0;
+  for (int k = 0; k < m; ++k) {
+    double t = roots[k];
+    if (t >= -10.0 && t <= 10.0) {
+      double r = z[0] + t * (z[1] + t * (z[2] + t * (z[3] + t * z[4])));
+      if (!found || r < rmin) {
+        found = true;
+        best = t;
+        rmin = r;
+      }
+    }
+  }
+  if (!found) {
+    best = 0.5;
+    rmin = z[0] + best * (z[1] + best * (z[2] + best * (z[3] + best * z[4])));
+  }
+  *alpha = best;
+  *emin = rmin;
+}
+
+
 // Host launcher of the fast cosine-transform Poisson solve (poisson.cu): d_hat = M^+ r_k
 // for every active instance with fft != 0.
 void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int nrow_items, const int* col_inst,
                  int ncol_items);
+// Two-pass stencil sweep of an iteration (stencil.cu).
+int strip_blocks(int n);
+void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);
+void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);
+constexpr int SWEEP_SLOTS = 32;  // partial-sum slots per sweep block
+
 // Elements staged in shared memory per block of the transform kernels.
 constexpr int FFT_ELEMS = 4096;
 inline int fft_lines(int n) { return n < FFT_ELEMS / n ? n : FFT_ELEMS / n; }

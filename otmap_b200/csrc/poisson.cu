@@ -25,28 +25,62 @@ constexpr int FT = 256;  // threads per block
 
 __device__ __forceinline__ int brev(int m, int logn) { return (int)(__brev((unsigned)m) >> (32 - logn)); }
 
-// In-place radix-2 decimation-in-time FFT of `lines` sequences of length n = 2^logn
-// stored line-major in s, input in bit-reversed order; forward uses exp(-2 pi i k/n),
-// conj the inverse kernel (unnormalised).
+// Shared-memory slot of element `idx` of a line-major staging buffer: one double2 of
+// padding after every 32 keeps bit-reversed scatters and short-stride butterflies
+// free of bank conflicts.
+__device__ __forceinline__ int slot(int idx) { return idx + (idx >> 5); }
+__host__ __device__ constexpr int padded(int elems) { return elems + elems / 32; }
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 w) {
+  return make_double2(fma(a.x, w.x, -a.y * w.y), fma(a.x, w.y, a.y * w.x));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+
+// In-place decimation-in-time FFT of `lines` sequences of length n = 2^logn stored
+// line-major in s (padded slots), input in bit-reversed order; forward uses
+// exp(-2 pi i k/n), conj the inverse kernel (unnormalised). Two radix-2 stages are
+// fused per pass (radix 4, in registers), plus one radix-2 pass when logn is odd.
 __device__ void fft_lines_inplace(double2* s, int logn, int lines, const double2* __restrict__ tw, bool conj) {
-  const int n = 1 << logn, halfn = n >> 1;
-  const int nb = lines * halfn;
-  for (int st = 0; st < logn; ++st) {
-    const int half = 1 << st;
-    const int tsh = logn - 1 - st;
+  const int n = 1 << logn;
+  int st = 0;
+  if (logn & 1) {  // first stage alone: half = 1, twiddle 1
+    const int nb = lines * (n >> 1);
     for (int b = threadIdx.x; b < nb; b += blockDim.x) {
-      const int line = b >> (logn - 1);
-      const int bb = b & (halfn - 1);
+      const int i0 = 2 * b;
+      const double2 a = s[slot(i0)], c = s[slot(i0 + 1)];
+      s[slot(i0)] = cadd(a, c);
+      s[slot(i0 + 1)] = csub(a, c);
+    }
+    __syncthreads();
+    st = 1;
+  }
+  for (; st < logn; st += 2) {
+    const int half = 1 << st;
+    const int nq = lines * (n >> 2);  // radix-4 butterflies
+    for (int b = threadIdx.x; b < nq; b += blockDim.x) {
+      const int line = b >> (logn - 2);
+      const int bb = b & ((n >> 2) - 1);
       const int pos = bb & (half - 1);
-      const int i0 = line * n + ((bb >> st) << (st + 1)) + pos;
-      const int i1 = i0 + half;
-      double2 w = __ldg(&tw[pos << tsh]);
-      if (conj) w.y = -w.y;
-      const double2 a = s[i0], c = s[i1];
-      const double tr = fma(c.x, w.x, -c.y * w.y);
-      const double ti = fma(c.x, w.y, c.y * w.x);
-      s[i0] = make_double2(a.x + tr, a.y + ti);
-      s[i1] = make_double2(a.x - tr, a.y - ti);
+      const int i0 = line * n + ((bb >> st) << (st + 2)) + pos;
+      double2 w1 = __ldg(&tw[pos << (logn - 1 - st)]);
+      double2 w2 = __ldg(&tw[pos << (logn - 2 - st)]);
+      double2 w3 = __ldg(&tw[(pos + half) << (logn - 2 - st)]);
+      if (conj) {
+        w1.y = -w1.y;
+        w2.y = -w2.y;
+        w3.y = -w3.y;
+      }
+      double2 e0 = s[slot(i0)], e1 = s[slot(i0 + half)], e2 = s[slot(i0 + 2 * half)], e3 = s[slot(i0 + 3 * half)];
+      // stage st: (e0, e1) and (e2, e3) with w1
+      double2 t1 = cmul(e1, w1), t3 = cmul(e3, w1);
+      double2 f0 = cadd(e0, t1), f1 = csub(e0, t1), f2 = cadd(e2, t3), f3 = csub(e2, t3);
+      // stage st + 1: (f0, f2) with w2, (f1, f3) with w3
+      double2 u2 = cmul(f2, w2), u3 = cmul(f3, w3);
+      s[slot(i0)] = cadd(f0, u2);
+      s[slot(i0 + 2 * half)] = csub(f0, u2);
+      s[slot(i0 + half)] = cadd(f1, u3);
+      s[slot(i0 + 3 * half)] = csub(f1, u3);
     }
     __syncthreads();
   }
@@ -79,13 +113,13 @@ __global__ __launch_bounds__(FT) void k_fft_rows_fwd(const Inst* insts, const in
   for (int e = threadIdx.x; e < R * n; e += FT) {
     int line = e >> logn, j = e & (n - 1);
     double x = src[(size_t)(i0 + line) * n + j];
-    sm[line * n + brev(makhoul_pos(j, n), logn)] = make_double2(x, 0.0);
+    sm[slot(line * n + brev(makhoul_pos(j, n), logn))] = make_double2(x, 0.0);
   }
   __syncthreads();
   fft_lines_inplace(sm, logn, R, I.tw, false);
   for (int e = threadIdx.x; e < R * n; e += FT) {
     int line = e >> logn, k = e & (n - 1);
-    dst[(size_t)(i0 + line) * n + k] = dct2_post(sm[e], __ldg(&I.pt[k]), dct_scale(k, n));
+    dst[(size_t)(i0 + line) * n + k] = dct2_post(sm[slot(e)], __ldg(&I.pt[k]), dct_scale(k, n));
   }
 }
 
@@ -95,14 +129,14 @@ __global__ __launch_bounds__(FT) void k_fft_cols(const Inst* insts, const int* c
   const Inst& I = insts[col_inst[blockIdx.x]];
   if (!I.active) return;
   const int n = I.n, logn = I.logn, CB = n < FFT_ELEMS / n ? n : FFT_ELEMS / n;
-  double* ybuf = reinterpret_cast<double*>(sm + CB * n);  // CB * n doubles
+  double* ybuf = reinterpret_cast<double*>(sm + padded(CB * n));  // CB * n doubles
   const int l0 = (blockIdx.x - I.col0) * CB;
   double* T = I.t1;
   // load: line c = column l0 + c, sample i = row
   for (int e = threadIdx.x; e < CB * n; e += FT) {
     int i = e / CB, c = e - i * CB;
     double x = T[(size_t)i * n + l0 + c];
-    sm[c * n + brev(makhoul_pos(i, n), logn)] = make_double2(x, 0.0);
+    sm[slot(c * n + brev(makhoul_pos(i, n), logn))] = make_double2(x, 0.0);
   }
   __syncthreads();
   fft_lines_inplace(sm, logn, CB, I.tw, false);
@@ -111,7 +145,7 @@ __global__ __launch_bounds__(FT) void k_fft_cols(const Inst* insts, const int* c
     int c = e >> logn, k = e & (n - 1);
     int l = l0 + c;
     double sk = dct_scale(k, n);
-    double X = dct2_post(sm[e], __ldg(&I.pt[k]), sk);
+    double X = dct2_post(sm[slot(e)], __ldg(&I.pt[k]), sk);
     double lam = 2.0 - 2.0 * I.cosk[k] * I.cosk[l];
     double U = (k == 0 && l == 0) ? 0.0 : X / lam;
     ybuf[e] = sk * U;
@@ -120,14 +154,14 @@ __global__ __launch_bounds__(FT) void k_fft_cols(const Inst* insts, const int* c
   for (int e = threadIdx.x; e < CB * n; e += FT) {
     int c = e >> logn, k = e & (n - 1);
     double a = ybuf[e], b = k == 0 ? 0.0 : ybuf[c * n + (n - k)];
-    sm[c * n + brev(k, logn)] = dct3_pre(k, a, b, __ldg(&I.pt[k]));
+    sm[slot(c * n + brev(k, logn))] = dct3_pre(k, a, b, __ldg(&I.pt[k]));
   }
   __syncthreads();
   fft_lines_inplace(sm, logn, CB, I.tw, true);
   for (int e = threadIdx.x; e < CB * n; e += FT) {
     int i = e / CB, c = e - i * CB;
     int m = (i & 1) ? n - 1 - (i >> 1) : (i >> 1);
-    T[(size_t)i * n + l0 + c] = sm[c * n + m].x;
+    T[(size_t)i * n + l0 + c] = sm[slot(c * n + m)].x;
   }
 }
 
@@ -144,22 +178,22 @@ __global__ __launch_bounds__(FT) void k_fft_rows_inv(const Inst* insts, const in
     const double* row = src + (size_t)(i0 + line) * n;
     double a = dct_scale(k, n) * row[k];
     double b = k == 0 ? 0.0 : dct_scale(n - k, n) * row[n - k];
-    sm[line * n + brev(k, logn)] = dct3_pre(k, a, b, __ldg(&I.pt[k]));
+    sm[slot(line * n + brev(k, logn))] = dct3_pre(k, a, b, __ldg(&I.pt[k]));
   }
   __syncthreads();
   fft_lines_inplace(sm, logn, R, I.tw, true);
   for (int e = threadIdx.x; e < R * n; e += FT) {
     int line = e >> logn, i = e & (n - 1);
     int m = (i & 1) ? n - 1 - (i >> 1) : (i >> 1);
-    dst[(size_t)(i0 + line) * n + i] = sm[line * n + m].x;
+    dst[(size_t)(i0 + line) * n + i] = sm[slot(line * n + m)].x;
   }
 }
 
 void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int nrow_items, const int* col_inst,
                  int ncol_items) {
   static bool attr[64] = {};  // per device ordinal
-  const int smem_rows = FFT_ELEMS * sizeof(double2);
-  const int smem_cols = FFT_ELEMS * (sizeof(double2) + sizeof(double));
+  const int smem_rows = padded(FFT_ELEMS) * sizeof(double2);
+  const int smem_cols = padded(FFT_ELEMS) * sizeof(double2) + FFT_ELEMS * sizeof(double);
   if (ctx->device < 64 && !attr[ctx->device]) {
     OTM_CUDA(cudaFuncSetAttribute(k_fft_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
     OTM_CUDA(cudaFuncSetAttribute(k_fft_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));

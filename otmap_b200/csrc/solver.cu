@@ -133,16 +133,6 @@ __device__ __forceinline__ double reduce_partials_min(const double* partials, in
 
 __device__ __forceinline__ double elem_area(int n) { return 1.0 / ((double)n * (double)n); }
 
-// Sets `outcome` for an instance whose loop condition (otsolver_2dgrid.cpp:160) failed.
-__device__ __forceinline__ void stop_outcome(Inst& I) {
-  if (I.residual <= I.threshold)
-    I.outcome = OTM_CONVERGED;
-  else if (!isfinite(I.residual))
-    I.outcome = OTM_NONFINITE;
-  else
-    I.outcome = OTM_MAX_ITER;
-}
-
 // ---------------------------------------------------------------------------
 // Density normalisation (otsolver_2dgrid.cpp:47-63), three passes.
 
@@ -396,72 +386,6 @@ __global__ __launch_bounds__(NT) void k_beta(Inst* insts, const int* tile_inst, 
 // ---------------------------------------------------------------------------
 // Exact line search (otsolver_2dgrid.cpp:541-606).
 
-__device__ double cubic_eval(const double c[4], double t) { return ((c[3] * t + c[2]) * t + c[1]) * t + c[0]; }
-__device__ double cubic_deriv(const double c[4], double t) { return (3.0 * c[3] * t + 2.0 * c[2]) * t + c[1]; }
-
-// Real roots of w3 t^3 + w2 t^2 + w1 t + w0: closed form of the depressed cubic
-// (Cardano for one real root, the trigonometric form for three) and two Newton
-// steps; replaces the companion-matrix eigensolver of otsolver_2dgrid.cpp:568-572.
-__device__ int cubic_real_roots(const double w[4], double roots[3]) {
-  double a = w[2] / w[3], b = w[1] / w[3], c = w[0] / w[3];
-  if (!isfinite(a) || !isfinite(b) || !isfinite(c)) return 0;
-  double p = b - a * a / 3.0;
-  double q = 2.0 * a * a * a / 27.0 - a * b / 3.0 + c;
-  double disc = 0.25 * q * q + p * p * p / 27.0;
-  int m;
-  if (disc > 0.0) {
-    double sq = sqrt(disc);
-    double u = cbrt(-0.5 * q + (q <= 0.0 ? sq : -sq));
-    double y = (u != 0.0) ? u - p / (3.0 * u) : 0.0;
-    roots[0] = y - a / 3.0;
-    m = 1;
-  } else {
-    double r = sqrt(std_max(0.0, -p / 3.0));
-    if (r == 0.0) {
-      roots[0] = roots[1] = roots[2] = -a / 3.0;
-    } else {
-      double arg = std_max(-1.0, std_min(1.0, -0.5 * q / (r * r * r)));
-      double phi = acos(arg) / 3.0;
-      for (int k = 0; k < 3; ++k) roots[k] = 2.0 * r * cos(phi - 2.0943951023931954923 * k) - a / 3.0;
-    }
-    m = 3;
-  }
-  double cc[4] = {c, b, a, 1.0};
-  for (int k = 0; k < m; ++k)
-    for (int s = 0; s < 2; ++s) {
-      double f = cubic_eval(cc, roots[k]), df = cubic_deriv(cc, roots[k]);
-      if (df != 0.0 && isfinite(f / df)) roots[k] -= f / df;
-    }
-  return m;
-}
-
-// Among the real stationary points of e(t) = z0 + z1 t + ... + z4 t^4 in [-10, 10] the
-// one with least e(t); else t = 0.5 (otsolver_2dgrid.cpp:575-595).
-__device__ void pick_step(const double z[5], double* alpha, double* emin) {
-  double w[4] = {z[1], 2.0 * z[2], 3.0 * z[3], 4.0 * z[4]};
-  double roots[3];
-  int m = cubic_real_roots(w, roots);
-  bool found = false;
-  double best = 0.0, rmin = 0.0;
-  for (int k = 0; k < m; ++k) {
-    double t = roots[k];
-    if (t >= -10.0 && t <= 10.0) {
-      double r = z[0] + t * (z[1] + t * (z[2] + t * (z[3] + t * z[4])));
-      if (!found || r < rmin) {
-        found = true;
-        best = t;
-        rmin = r;
-      }
-    }
-  }
-  if (!found) {
-    best = 0.5;
-    rmin = z[0] + best * (z[1] + best * (z[2] + best * (z[3] + best * z[4])));
-  }
-  *alpha = best;
-  *emin = rmin;
-}
-
 // d = d_hat + beta d_prev (written), a and b per cell, the quartic's sums; the last
 // block picks the step.
 __global__ __launch_bounds__(NT) void k_coeffs(Inst* insts, const int* tile_inst, double* partials) {
@@ -614,7 +538,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
   const int count = (int)sizes.size();
   std::vector<Inst> h(count);
   size_t cells = 0;
-  int tiles = 0, gemm = 0, rows = 0, cols = 0;
+  int tiles = 0, gemm = 0, rows = 0, cols = 0, strips = 0;
   for (int q = 0; q < count; ++q) {
     int n = sizes[q];
     Inst& I = h[q];
@@ -623,6 +547,9 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.tile0 = tiles;
     I.ntiles = tiles_of(n);
     tiles += I.ntiles;
+    I.strip0 = strips;
+    I.nstrip = strip_blocks(n);
+    strips += I.nstrip;
     I.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
     if (I.fft) {
       int lines = fft_lines(n);
@@ -651,16 +578,20 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     ws.row_inst.reserve(sizeof(int) * (rows > 0 ? rows : 1));
     ws.col_inst.reserve(sizeof(int) * (cols > 0 ? cols : 1));
     ws.partials.reserve(sizeof(double) * KP * (size_t)tiles);
+    ws.strip_inst.reserve(sizeof(int) * strips);
+    ws.sweep_partials.reserve(sizeof(double) * SWEEP_SLOTS * (size_t)strips);
     ws.arena.reserve(sizeof(double) * cells);
-    std::vector<int> ti(tiles), gi(gemm), ri(rows), ci(cols);
+    std::vector<int> ti(tiles), gi(gemm), ri(rows), ci(cols), si(strips);
     for (int q = 0; q < count; ++q) {
       for (int k = 0; k < h[q].ntiles; ++k) ti[h[q].tile0 + k] = q;
+      for (int k = 0; k < h[q].nstrip; ++k) si[h[q].strip0 + k] = q;
       for (int k = 0; k < h[q].ngemm; ++k) gi[h[q].gemm0 + k] = q;
       for (int k = 0; k < h[q].nrow; ++k) ri[h[q].row0 + k] = q;
       for (int k = 0; k < h[q].ncol; ++k) ci[h[q].col0 + k] = q;
     }
     cudaStream_t st = ctx->stream;
     OTM_CUDA(cudaMemcpyAsync(ws.tile_inst.p, ti.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(ws.strip_inst.p, si.data(), sizeof(int) * strips, cudaMemcpyHostToDevice, st));
     if (gemm) OTM_CUDA(cudaMemcpyAsync(ws.gemm_inst.p, gi.data(), sizeof(int) * gemm, cudaMemcpyHostToDevice, st));
     if (rows) OTM_CUDA(cudaMemcpyAsync(ws.row_inst.p, ri.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, st));
     if (cols) OTM_CUDA(cudaMemcpyAsync(ws.col_inst.p, ci.data(), sizeof(int) * cols, cudaMemcpyHostToDevice, st));
@@ -671,6 +602,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     ws.total_gemm = gemm;
     ws.total_rows = rows;
     ws.total_cols = cols;
+    ws.total_strips = strips;
     size_t need = sizeof(Inst) * count;
     if (ws.h_pinned_bytes < need) {
       if (ws.h_pinned) cudaFreeHost(ws.h_pinned);
@@ -755,9 +687,8 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
         for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, gi, s, 1);
       if (ws.total_rows > 0)
         poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), ws.total_rows, ws.col_inst.as<int>(), ws.total_cols);
-      launch(ctx, "beta", k_beta, T, NT, d_insts, ti, part);
-      launch(ctx, "coeffs", k_coeffs, T, NT, d_insts, ti, part);
-      launch(ctx, "update", k_update, T, NT, d_insts, ti, part);
+      sweep_sums(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
+      sweep_update(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
     }
     OTM_CUDA(cudaGetLastError());
   }
