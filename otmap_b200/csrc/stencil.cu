@@ -14,9 +14,11 @@
 //                  block advances the iteration and tests the loop condition (:160).
 //
 // Geometry: one warp owns a strip of 32 consecutive columns (j, contiguous in memory)
-// and SR rows; it walks down the rows keeping two rows of the fields and of their
-// vertex gradients in registers. Left/right neighbours come from warp shuffles, the
-// strip's two halo columns from two extra loads. A block is 8 strips side by side.
+// and SR rows and walks down it. Grid rows are prefetched asynchronously (cp.async)
+// into a per-warp ring of RD rows in shared memory, so RD-2 rows per warp are in
+// flight while it computes; the previous vertex-gradient row is kept in registers. The
+// strip's two halo columns are staged with the row; neighbours come from the ring. A
+// block is SWARPS strips side by side.
 // Per cell the arithmetic is the reference's, in FP64, without FMA contraction.
 
 #include "engine.cuh"
@@ -24,10 +26,13 @@
 namespace otm {
 
 constexpr int SW = 32;        // strip width (one warp)
-constexpr int SR = 16;        // strip height (rows per warp)
-constexpr int SWARPS = 8;     // strips per block
+constexpr int SR = 32;        // strip height (rows per warp)
+constexpr int SWARPS = 4;     // strips per block
 constexpr int ST = SW * SWARPS;
 constexpr int KA = SWEEP_SLOTS;  // partial-sum slots per block
+constexpr int RD = 8;         // rows in the per-warp prefetch ring (RD - 3 in flight beyond the two in use)
+
+__device__ __forceinline__ int clampn(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
 
 struct Row {   // one field on one grid row around the lane's column j
   double c;    // column j
@@ -35,25 +40,62 @@ struct Row {   // one field on one grid row around the lane's column j
   double rh;   // lane 31: column j0 + 32
 };
 
+// ---- per-warp asynchronous row prefetch (cp.async, 8-byte copies) ----
+// A stage holds one grid row of the strip for every field: stencil fields take 34
+// slots (columns j0-1 .. j0+32, clamped), pointwise fields 32 (columns j0 .. j0+31).
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+template <int NS, int NP>
+struct Ring {
+  static constexpr int STAGE = NS * 34 + NP * 32;
+  double* buf;  // RD * STAGE doubles (this warp's)
+  const double* sf[NS > 0 ? NS : 1];
+  const double* pf[NP > 0 ? NP : 1];
+  int n, j0, lane, rows_end;  // rows beyond rows_end are not fetched
+
+  __device__ __forceinline__ double* stage(int row) { return buf + ((row + 2 * RD) % RD) * STAGE; }
+
+  // Queues the copies of grid row `row` (clamped) and commits them as one group.
+  __device__ __forceinline__ void issue(int row) {
+    if (row <= rows_end) {
+      double* st = stage(row);
+      const size_t base = (size_t)clampn(row, n) * n;
+      const size_t cj = base + clampn(j0 + lane, n);
+#pragma unroll
+      for (int k = 0; k < NS; ++k) {
+        double* d = st + k * 34;
+        cp_async8(d + 1 + lane, sf[k] + cj);
+        if (lane == 0) cp_async8(d, sf[k] + base + clampn(j0 - 1, n));
+        if (lane == 31) cp_async8(d + 33, sf[k] + base + clampn(j0 + 32, n));
+      }
+#pragma unroll
+      for (int k = 0; k < NP; ++k) cp_async8(st + NS * 34 + k * 32 + lane, pf[k] + cj);
+    }
+    cp_async_commit();
+  }
+  __device__ __forceinline__ Row row_of(int row, int k) {
+    const double* d = stage(row) + k * 34;
+    Row r;
+    r.c = d[1 + lane];
+    r.l = d[lane];
+    r.rh = d[33];
+    return r;
+  }
+  __device__ __forceinline__ double point(int row, int k) { return stage(row)[NS * 34 + k * 32 + lane]; }
+};
+
 struct VG {    // vertex gradients (v, j) and (v, j + 1)
   double gx, gy, gxr, gyr;
 };
-
-__device__ __forceinline__ int clampn(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
-
-template <class F>
-__device__ __forceinline__ Row load_row(F f, int row, int j0, int lane, int n) {
-  Row r;
-  const size_t base = (size_t)clampn(row, n) * n;
-  r.c = f(base + clampn(j0 + lane, n));
-  double halo = 0.0;
-  if (lane == 0) halo = f(base + clampn(j0 - 1, n));
-  if (lane == 31) halo = f(base + clampn(j0 + 32, n));
-  double up = __shfl_up_sync(0xffffffffu, r.c, 1);
-  r.l = lane == 0 ? halo : up;
-  r.rh = halo;
-  return r;
-}
 
 // Vertex gradients of vertex row v from cell rows a = v-1 and b = v
 // (otsolver_2dgrid.cpp:379-391 with clamped cells = boundary rules :405-422).
@@ -145,6 +187,7 @@ enum {
 };
 
 __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip_inst, double* partials) {
+  extern __shared__ double ring_smem[];
   __shared__ double red[32 * S_COUNT];
   Inst& I = insts[strip_inst[blockIdx.x]];
   if (!I.active) return;
@@ -152,38 +195,41 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
   const double e = 1.0 / (double)n, hw = 0.5 * (double)n;
   const StripCoord sc = strip_coord(I, blockIdx.x);
   const int j = sc.j0 + sc.lane;
-  const double* psi = I.psi[it & 1];
-  const double* dh = I.dhat;
-  const double* dp = I.d[(it + 1) & 1];
-  const double* rk = I.r[it % 3];
-  const double* rkm1 = I.r[(it + 2) % 3];
   double acc[S_COUNT];
 #pragma unroll
   for (int k = 0; k < S_COUNT; ++k) acc[k] = 0.0;
-  const bool active_strip = sc.i0 < n;
-  if (active_strip) {
-    auto P = [&](size_t g) { return psi[g]; };
-    auto H = [&](size_t g) { return dh[g]; };
-    auto Q = [&](size_t g) { return dp[g]; };
-    Row pa = load_row(P, sc.i0 - 1, sc.j0, sc.lane, n), ha = load_row(H, sc.i0 - 1, sc.j0, sc.lane, n),
-        qa = load_row(Q, sc.i0 - 1, sc.j0, sc.lane, n);
-    Row pb = load_row(P, sc.i0, sc.j0, sc.lane, n), hb = load_row(H, sc.i0, sc.j0, sc.lane, n),
-        qb = load_row(Q, sc.i0, sc.j0, sc.lane, n);
-    VG gp = vgrad(pa, pb, hw, sc.lane), gh = vgrad(ha, hb, hw, sc.lane), gq = vgrad(qa, qb, hw, sc.lane);
-    for (int c = sc.i0; c < sc.i0 + SR && c < n; ++c) {
-      // vertex row c + 1 from cell rows c and c + 1
-      Row pn = load_row(P, c + 1, sc.j0, sc.lane, n), hn = load_row(H, c + 1, sc.j0, sc.lane, n),
-          qn = load_row(Q, c + 1, sc.j0, sc.lane, n);
-      VG gp2 = vgrad(pb, pn, hw, sc.lane), gh2 = vgrad(hb, hn, hw, sc.lane), gq2 = vgrad(qb, qn, hw, sc.lane);
-      if (j < n) {
-        const size_t f = (size_t)c * n + j;
-        Diag G = diag(gp, gp2), Hd = diag(gh, gh2), Qd = diag(gq, gq2);
+  if (sc.i0 < n) {
+    Ring<3, 2> R;
+    R.buf = ring_smem + sc.warp * RD * Ring<3, 2>::STAGE;
+    R.sf[0] = I.psi[it & 1];
+    R.sf[1] = I.dhat;
+    R.sf[2] = I.d[(it + 1) & 1];
+    R.pf[0] = I.r[it % 3];
+    R.pf[1] = I.r[(it + 2) % 3];
+    R.n = n;
+    R.j0 = sc.j0;
+    R.lane = sc.lane;
+    const int last = min(sc.i0 + SR, n);  // cell rows i0 .. last-1; grid rows i0-1 .. last
+    R.rows_end = last;
+#pragma unroll
+    for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
+    VG gp, gh, gq;
+    for (int row = sc.i0; row <= last; ++row) {
+      cp_async_wait<RD - 3>();
+      __syncwarp();
+      // vertex row `row` from grid rows row-1 and row
+      VG np = vgrad(R.row_of(row - 1, 0), R.row_of(row, 0), hw, sc.lane);
+      VG nh = vgrad(R.row_of(row - 1, 1), R.row_of(row, 1), hw, sc.lane);
+      VG nq = vgrad(R.row_of(row - 1, 2), R.row_of(row, 2), hw, sc.lane);
+      if (row > sc.i0 && j < n) {
+        const int c = row - 1;
+        Diag G = diag(gp, np), Hd = diag(gh, nh), Qd = diag(gq, nq);
         double a11, b1, a22, b2;
         line_ab(G, Hd, e, a11, b1);
         line_ab(G, Qd, e, a22, b2);
         double a12 = 0.5 * (Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx);
-        double r = rk[f], jd = r - rkm1[f];
-        double hv = hb.c, qv = qb.c;
+        double r = R.point(c, 0), jd = r - R.point(c, 1);
+        double hv = R.row_of(c, 1).c, qv = R.row_of(c, 2).c;
         acc[S_HH] += hv * hv;
         acc[S_HQ] += hv * qv;
         acc[S_QQ] += qv * qv;
@@ -211,13 +257,13 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
         acc[S_A12A22] += a12 * a22;
         acc[S_A22A22] += a22 * a22;
       }
-      pb = pn;
-      hb = hn;
-      qb = qn;
-      gp = gp2;
-      gh = gh2;
-      gq = gq2;
+      gp = np;
+      gh = nh;
+      gq = nq;
+      __syncwarp();
+      R.issue(row - 2 + RD);  // refill the stage of grid row row-2, no longer needed
     }
+    cp_async_wait<0>();
   }
   write_partials<S_COUNT>(acc, red, partials, blockIdx.x);
   if (last_block(&I.counter, I.nstrip)) {
@@ -256,6 +302,7 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
 }
 
 __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* strip_inst, double* partials) {
+  extern __shared__ double ring_smem[];
   __shared__ double red[32];
   Inst& I = insts[strip_inst[blockIdx.x]];
   if (!I.active) return;
@@ -265,38 +312,60 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
   const double beta = I.beta;
   const StripCoord sc = strip_coord(I, blockIdx.x);
   const int j = sc.j0 + sc.lane;
-  const double* psi = I.psi[it & 1];
-  const double* dh = I.dhat;
-  const double* dp = I.d[(it + 1) & 1];
-  const double* rk = I.r[it % 3];
   double* dnew = I.d[it & 1];
   double* psin = I.psi[(it + 1) & 1];
   double* rn = I.r[(it + 1) % 3];
   double mx = -INFINITY;
   if (sc.i0 < n) {
-    auto P = [&](size_t g) { return psi[g]; };
-    auto D = [&](size_t g) { return use_beta ? dh[g] + beta * dp[g] : dh[g]; };
-    Row pa = load_row(P, sc.i0 - 1, sc.j0, sc.lane, n), da = load_row(D, sc.i0 - 1, sc.j0, sc.lane, n);
-    Row pb = load_row(P, sc.i0, sc.j0, sc.lane, n), db = load_row(D, sc.i0, sc.j0, sc.lane, n);
-    VG gp = vgrad(pa, pb, hw, sc.lane), gd = vgrad(da, db, hw, sc.lane);
-    for (int c = sc.i0; c < sc.i0 + SR && c < n; ++c) {
-      Row pn = load_row(P, c + 1, sc.j0, sc.lane, n), dn = load_row(D, c + 1, sc.j0, sc.lane, n);
-      VG gp2 = vgrad(pb, pn, hw, sc.lane), gd2 = vgrad(db, dn, hw, sc.lane);
-      if (j < n) {
+    Ring<3, 1> R;
+    R.buf = ring_smem + sc.warp * RD * Ring<3, 1>::STAGE;
+    R.sf[0] = I.psi[it & 1];
+    R.sf[1] = I.dhat;
+    R.sf[2] = I.d[(it + 1) & 1];
+    R.pf[0] = I.r[it % 3];
+    R.n = n;
+    R.j0 = sc.j0;
+    R.lane = sc.lane;
+    const int last = min(sc.i0 + SR, n);
+    R.rows_end = last;
+#pragma unroll
+    for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
+    // d = d_hat + beta d_prev, formed from the staged rows exactly as the reference
+    // forms the vector d before its gradients (otsolver_2dgrid.cpp:199)
+    auto drow = [&](int row) {
+      Row h = R.row_of(row, 1);
+      if (!use_beta) return h;
+      Row q = R.row_of(row, 2);
+      Row d;
+      d.c = h.c + beta * q.c;
+      d.l = h.l + beta * q.l;
+      d.rh = h.rh + beta * q.rh;
+      return d;
+    };
+    VG gp, gd;
+    for (int row = sc.i0; row <= last; ++row) {
+      cp_async_wait<RD - 3>();
+      __syncwarp();
+      Row pc = R.row_of(row - 1, 0), dc = drow(row - 1);
+      VG np = vgrad(pc, R.row_of(row, 0), hw, sc.lane);
+      VG nd = vgrad(dc, drow(row), hw, sc.lane);
+      if (row > sc.i0 && j < n) {
+        const int c = row - 1;
         const size_t f = (size_t)c * n + j;
         double a, b;
-        line_ab(diag(gp, gp2), diag(gd, gd2), e, a, b);
-        dnew[f] = db.c;
-        psin[f] = pb.c + alpha * db.c;
-        double r = a * (alpha * alpha) + b * alpha + rk[f];
+        line_ab(diag(gp, np), diag(gd, nd), e, a, b);
+        dnew[f] = dc.c;
+        psin[f] = pc.c + alpha * dc.c;
+        double r = a * (alpha * alpha) + b * alpha + R.point(c, 0);
         rn[f] = r;
         mx = fmax(mx, r);
       }
-      pb = pn;
-      db = dn;
-      gp = gp2;
-      gd = gd2;
+      gp = np;
+      gd = nd;
+      __syncwarp();
+      R.issue(row - 2 + RD);
     }
+    cp_async_wait<0>();
   }
   mx = block_max(mx, red);
   if (threadIdx.x == 0) partials[(size_t)blockIdx.x * KA] = mx;
@@ -319,12 +388,26 @@ int strip_blocks(int n) {
   return (strips + SWARPS - 1) / SWARPS;
 }
 
+static void sweep_attrs(int device) {
+  static bool done[64] = {};
+  if (device < 64 && done[device]) return;
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(SWARPS * RD * Ring<3, 2>::STAGE * sizeof(double))));
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(SWARPS * RD * Ring<3, 1>::STAGE * sizeof(double))));
+  if (device < 64) done[device] = true;
+}
+
 void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials) {
-  launch(ctx, "sweep_sums", k_sweep_sums, nblocks, ST, d_insts, strip_inst, partials);
+  sweep_attrs(ctx->device);
+  launch_smem(ctx, "sweep_sums", k_sweep_sums, nblocks, ST, SWARPS * RD * Ring<3, 2>::STAGE * sizeof(double),
+              d_insts, strip_inst, partials);
 }
 
 void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials) {
-  launch(ctx, "sweep_update", k_sweep_update, nblocks, ST, d_insts, strip_inst, partials);
+  sweep_attrs(ctx->device);
+  launch_smem(ctx, "sweep_update", k_sweep_update, nblocks, ST, SWARPS * RD * Ring<3, 1>::STAGE * sizeof(double),
+              d_insts, strip_inst, partials);
 }
 
 }  // namespace otm
