@@ -64,6 +64,10 @@ struct Workspace {
   size_t h_pinned_bytes = 0;
   int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0, total_strips = 0;
   int mode = -1;  // poisson mode the layout was built for
+  struct Segment {  // instances of one size on one transform kernel family
+    int n, reg, roff, rcnt, coff, ccnt;
+  };
+  std::vector<Segment> segments;
   ~Workspace() {
     if (h_pinned) cudaFreeHost(h_pinned);
   }

@@ -124,8 +124,13 @@ __device__ __forceinline__ void pick_step(const double z[5], double* alpha, doub
 
 // Host launcher of the fast cosine-transform Poisson solve (poisson.cu): d_hat = M^+ r_k
 // for every active instance with fft != 0.
-void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int nrow_items, const int* col_inst,
-                 int ncol_items);
+void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int roff, int nrow_items,
+                 const int* col_inst, int coff, int ncol_items);
+// Register-resident variant for n in {64, ..., 1024} (dct_reg.cu).
+bool dct_reg_supported(int n);
+int dct_reg_lines_per_block(int n);
+void dct_reg_run(otm_context* ctx, int n, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,
+                 int coff, int ccnt);
 // Two-pass stencil sweep of an iteration (stencil.cu).
 int strip_blocks(int n);
 void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);

@@ -102,12 +102,13 @@ __device__ __forceinline__ double2 dct3_pre(int k, double a, double b, double2 p
   return make_double2(0.5 * fma(a, pt.x, b * pt.y), 0.5 * fma(a, pt.y, -b * pt.x));
 }
 
-__global__ __launch_bounds__(FT) void k_fft_rows_fwd(const Inst* insts, const int* row_inst) {
+__global__ __launch_bounds__(FT) void k_fft_rows_fwd(const Inst* insts, const int* row_inst, int seg) {
   extern __shared__ double2 sm[];
-  const Inst& I = insts[row_inst[blockIdx.x]];
+  const int item = seg + blockIdx.x;
+  const Inst& I = insts[row_inst[item]];
   if (!I.active) return;
   const int n = I.n, logn = I.logn, R = n < FFT_ELEMS / n ? n : FFT_ELEMS / n;
-  const int i0 = (blockIdx.x - I.row0) * R;
+  const int i0 = (item - I.row0) * R;
   const double* src = I.r[I.it % 3];
   double* dst = I.t1;
   for (int e = threadIdx.x; e < R * n; e += FT) {
@@ -124,13 +125,14 @@ __global__ __launch_bounds__(FT) void k_fft_rows_fwd(const Inst* insts, const in
 }
 
 // In place on t1: a block of CB = FFT_ELEMS / n columns (all n rows).
-__global__ __launch_bounds__(FT) void k_fft_cols(const Inst* insts, const int* col_inst) {
+__global__ __launch_bounds__(FT) void k_fft_cols(const Inst* insts, const int* col_inst, int seg) {
   extern __shared__ double2 sm[];
-  const Inst& I = insts[col_inst[blockIdx.x]];
+  const int item = seg + blockIdx.x;
+  const Inst& I = insts[col_inst[item]];
   if (!I.active) return;
   const int n = I.n, logn = I.logn, CB = n < FFT_ELEMS / n ? n : FFT_ELEMS / n;
   double* ybuf = reinterpret_cast<double*>(sm + padded(CB * n));  // CB * n doubles
-  const int l0 = (blockIdx.x - I.col0) * CB;
+  const int l0 = (item - I.col0) * CB;
   double* T = I.t1;
   // load: line c = column l0 + c, sample i = row
   for (int e = threadIdx.x; e < CB * n; e += FT) {
@@ -165,12 +167,13 @@ __global__ __launch_bounds__(FT) void k_fft_cols(const Inst* insts, const int* c
   }
 }
 
-__global__ __launch_bounds__(FT) void k_fft_rows_inv(const Inst* insts, const int* row_inst) {
+__global__ __launch_bounds__(FT) void k_fft_rows_inv(const Inst* insts, const int* row_inst, int seg) {
   extern __shared__ double2 sm[];
-  const Inst& I = insts[row_inst[blockIdx.x]];
+  const int item = seg + blockIdx.x;
+  const Inst& I = insts[row_inst[item]];
   if (!I.active) return;
   const int n = I.n, logn = I.logn, R = n < FFT_ELEMS / n ? n : FFT_ELEMS / n;
-  const int i0 = (blockIdx.x - I.row0) * R;
+  const int i0 = (item - I.row0) * R;
   const double* src = I.t1;
   double* dst = I.dhat;
   for (int e = threadIdx.x; e < R * n; e += FT) {
@@ -189,8 +192,8 @@ __global__ __launch_bounds__(FT) void k_fft_rows_inv(const Inst* insts, const in
   }
 }
 
-void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int nrow_items, const int* col_inst,
-                 int ncol_items) {
+void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int roff, int nrow_items,
+                 const int* col_inst, int coff, int ncol_items) {
   static bool attr[64] = {};  // per device ordinal
   const int smem_rows = padded(FFT_ELEMS) * sizeof(double2);
   const int smem_cols = padded(FFT_ELEMS) * sizeof(double2) + FFT_ELEMS * sizeof(double);
@@ -201,9 +204,9 @@ void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int nrow_
     attr[ctx->device] = true;
   }
   if (nrow_items <= 0) return;
-  launch_smem(ctx, "fft_rows_fwd", k_fft_rows_fwd, nrow_items, FT, smem_rows, (const Inst*)d_insts, row_inst);
-  launch_smem(ctx, "fft_cols", k_fft_cols, ncol_items, FT, smem_cols, (const Inst*)d_insts, col_inst);
-  launch_smem(ctx, "fft_rows_inv", k_fft_rows_inv, nrow_items, FT, smem_rows, (const Inst*)d_insts, row_inst);
+  launch_smem(ctx, "fft_rows_fwd", k_fft_rows_fwd, nrow_items, FT, smem_rows, (const Inst*)d_insts, row_inst, roff);
+  launch_smem(ctx, "fft_cols", k_fft_cols, ncol_items, FT, smem_cols, (const Inst*)d_insts, col_inst, coff);
+  launch_smem(ctx, "fft_rows_inv", k_fft_rows_inv, nrow_items, FT, smem_rows, (const Inst*)d_insts, row_inst, roff);
 }
 
 }  // namespace otm

@@ -25,6 +25,7 @@
 
 #include <cfloat>
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <random>
@@ -552,16 +553,9 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     strips += I.nstrip;
     I.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
     if (I.fft) {
-      int lines = fft_lines(n);
       int lg = 0;
       while ((1 << lg) < n) ++lg;
       I.logn = lg;
-      I.row0 = rows;
-      I.nrow = n / lines;
-      I.col0 = cols;
-      I.ncol = n / lines;
-      rows += I.nrow;
-      cols += I.ncol;
     } else {
       I.gemm0 = gemm;
       I.ngemm = gemm_tiles_of(n);
@@ -569,6 +563,30 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     }
     // 11 cell arrays per instance, each padded to 32 doubles (256 bytes)
     cells += 11 * (((size_t)n * n + 31) / 32 * 32);
+  }
+  // fast-transform work lists, grouped into one segment per (kernel family, size)
+  std::vector<Workspace::Segment> segs;
+  {
+    std::vector<int> order;
+    for (int q = 0; q < count; ++q)
+      if (h[q].fft) order.push_back(q);
+    auto key = [&](int q) { return std::make_pair(dct_reg_supported(h[q].n) ? 1 : 0, h[q].n); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
+    for (size_t k = 0; k < order.size(); ++k) {
+      Inst& I = h[order[k]];
+      const int reg = dct_reg_supported(I.n) ? 1 : 0;
+      const int per = reg ? dct_reg_lines_per_block(I.n) : fft_lines(I.n);
+      if (segs.empty() || segs.back().n != I.n || segs.back().reg != reg)
+        segs.push_back({I.n, reg, rows, 0, cols, 0});
+      I.row0 = rows;
+      I.nrow = I.n / per;
+      I.col0 = cols;
+      I.ncol = I.n / per;
+      rows += I.nrow;
+      cols += I.ncol;
+      segs.back().rcnt += I.nrow;
+      segs.back().ccnt += I.ncol;
+    }
   }
   bool same = ws.sizes == sizes && ws.mode == ctx->poisson_mode;
   if (!same) {
@@ -603,6 +621,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     ws.total_rows = rows;
     ws.total_cols = cols;
     ws.total_strips = strips;
+    ws.segments = segs;
     size_t need = sizeof(Inst) * count;
     if (ws.h_pinned_bytes < need) {
       if (ws.h_pinned) cudaFreeHost(ws.h_pinned);
@@ -685,8 +704,14 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
     for (int c = 0; c < chunk && launched < o.max_iter; ++c, ++launched) {
       if (G > 0)
         for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, gi, s, 1);
-      if (ws.total_rows > 0)
-        poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), ws.total_rows, ws.col_inst.as<int>(), ws.total_cols);
+      for (const auto& sg : ws.segments) {
+        if (sg.reg)
+          dct_reg_run(ctx, sg.n, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff,
+                      sg.ccnt);
+        else
+          poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff,
+                      sg.ccnt);
+      }
       sweep_sums(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
       sweep_update(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
     }
