@@ -78,9 +78,10 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[N], const double2* __restri
 
 // Steps 1-4 for one line. `in(m1)` gives lane t's input sample m = N2*m1 + t; `out(k, X)`
 // receives X_k on lane k1 = k % N1 (only lanes t < N1 call it). buf is this line's
-// N1 x (N2 + 1) shared buffer.
+// N1 x (N2 + 1) shared buffer of doubles (the transpose moves real and imaginary
+// parts in two rounds).
 template <int N1, int N2, class In, class Out>
-__device__ __forceinline__ void fft_line(int t, double2* buf, const double2* __restrict__ tw, bool conj, In in,
+__device__ __forceinline__ void fft_line(int t, double* buf, const double2* __restrict__ tw, bool conj, In in,
                                          Out out) {
   constexpr int n = N1 * N2;
   double2 v[N1];
@@ -90,13 +91,28 @@ __device__ __forceinline__ void fft_line(int t, double2* buf, const double2* __r
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
     const int k1 = rbrev<N1>(r);
-    buf[k1 * (N2 + 1) + t] = k1 == 0 ? v[r] : cmul(v[r], twid(tw, t * k1, n, conj));
+    if (k1 != 0) v[r] = cmul(v[r], twid(tw, t * k1, n, conj));
   }
-  __syncwarp();
-  if (t < N1) {
-    double2 u[N2];
+  // transpose through shared memory, real parts then imaginary parts
+  double2 u[N2];
 #pragma unroll
-    for (int m2 = 0; m2 < N2; ++m2) u[m2] = buf[t * (N2 + 1) + m2];
+  for (int part = 0; part < 2; ++part) {
+#pragma unroll
+    for (int r = 0; r < N1; ++r) buf[rbrev<N1>(r) * (N2 + 1) + t] = part ? v[r].y : v[r].x;
+    __syncwarp();
+    if (t < N1) {
+#pragma unroll
+      for (int m2 = 0; m2 < N2; ++m2) {
+        const double x = buf[t * (N2 + 1) + m2];
+        if (part)
+          u[m2].y = x;
+        else
+          u[m2].x = x;
+      }
+    }
+    __syncwarp();
+  }
+  if (t < N1) {
     fft_reg<N2>(u, tw, n, conj);
 #pragma unroll
     for (int r = 0; r < N2; ++r) out(t + N1 * rbrev<N2>(r), u[r]);
@@ -115,15 +131,15 @@ __device__ __forceinline__ double2 pre3(int k, double a, double b, double2 pt) {
 }
 
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32) void k_dct_rows_fwd(const Inst* insts, const int* row_inst, int seg) {
+__global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_fwd(const Inst* insts, const int* row_inst, int seg) {
   constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
-  extern __shared__ double2 sbuf[];
+  extern __shared__ double sbuf[];
   const int item = seg + blockIdx.x;
   const Inst& I = insts[row_inst[item]];
   if (!I.active) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
   const int row = (item - I.row0) * LPB + warp * LPW + sub;
-  double2* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
+  double* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
   const double* x = I.r[I.it % 3] + (size_t)row * n;
   double* y = I.t1 + (size_t)row * n;
   const double2* tw = I.tw;
@@ -134,15 +150,15 @@ __global__ __launch_bounds__(RW * 32) void k_dct_rows_fwd(const Inst* insts, con
 }
 
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32) void k_dct_rows_inv(const Inst* insts, const int* row_inst, int seg) {
+__global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_inv(const Inst* insts, const int* row_inst, int seg) {
   constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
-  extern __shared__ double2 sbuf[];
+  extern __shared__ double sbuf[];
   const int item = seg + blockIdx.x;
   const Inst& I = insts[row_inst[item]];
   if (!I.active) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
   const int row = (item - I.row0) * LPB + warp * LPW + sub;
-  double2* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
+  double* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
   const double* X = I.t1 + (size_t)row * n;
   double* x = I.dhat + (size_t)row * n;
   const double2* tw = I.tw;
@@ -160,17 +176,17 @@ __global__ __launch_bounds__(RW * 32) void k_dct_rows_inv(const Inst* insts, con
 
 // CB columns per block; the tile holds them (n rows x (CB + 1) doubles).
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32) void k_dct_cols(const Inst* insts, const int* col_inst, int seg) {
+__global__ __launch_bounds__(RW * 32, 2) void k_dct_cols(const Inst* insts, const int* col_inst, int seg) {
   constexpr int n = N1 * N2, LPW = 32 / N2, CB = RW * LPW, TS = CB + 1;
-  extern __shared__ double2 sbuf[];
-  double* tile = reinterpret_cast<double*>(sbuf + CB * N1 * (N2 + 1));
+  extern __shared__ double sbuf[];
+  double* tile = sbuf + CB * N1 * (N2 + 1);
   const int item = seg + blockIdx.x;
   const Inst& I = insts[col_inst[item]];
   if (!I.active) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
   const int c = warp * LPW + sub;  // this line's column within the block
   const int l0 = (item - I.col0) * CB;
-  double2* buf = sbuf + c * N1 * (N2 + 1);
+  double* buf = sbuf + c * N1 * (N2 + 1);
   double* T = I.t1;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
@@ -192,17 +208,16 @@ __global__ __launch_bounds__(RW * 32) void k_dct_cols(const Inst* insts, const i
         tile[k * TS + c] = sk * U;  // column c only: this line's step-1 reads are done
       });
   __syncthreads();
-  // inverse DCT-III along the column
-  double2 w[N1];
-#pragma unroll
-  for (int m1 = 0; m1 < N1; ++m1) {
-    const int k = N2 * m1 + t;
-    const double a = tile[k * TS + c], b = k == 0 ? 0.0 : tile[(n - k) * TS + c];
-    w[m1] = pre3(k, a, b, __ldg(&pt[k]));
-  }
-  __syncthreads();
+  __syncwarp();
+  // inverse DCT-III along the column: step 1 reads this column's s_k U_k from the tile;
+  // its outputs overwrite the column only after every lane of the line is past step 1
   fft_line<N1, N2>(
-      t, buf, tw, true, [&](int m1) { return w[m1]; },
+      t, buf, tw, true,
+      [&](int m1) {
+        const int k = N2 * m1 + t;
+        const double a = tile[k * TS + c], b = k == 0 ? 0.0 : tile[(n - k) * TS + c];
+        return pre3(k, a, b, __ldg(&pt[k]));
+      },
       [&](int m, double2 v) { tile[makhoul_src(m, n) * TS + c] = v.x; });
   __syncthreads();
   for (int e = threadIdx.x; e < n * CB; e += RW * 32) {
@@ -214,7 +229,7 @@ __global__ __launch_bounds__(RW * 32) void k_dct_cols(const Inst* insts, const i
 template <int N1, int N2>
 struct RegDct {
   static constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
-  static size_t rows_smem() { return sizeof(double2) * LPB * N1 * (N2 + 1); }
+  static size_t rows_smem() { return sizeof(double) * LPB * N1 * (N2 + 1); }
   static size_t cols_smem() { return rows_smem() + sizeof(double) * n * (LPB + 1); }
   static void attrs() {
     OTM_CUDA(cudaFuncSetAttribute(k_dct_rows_fwd<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -230,32 +230,32 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
         double a12 = 0.5 * (Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx);
         double r = R.point(c, 0), jd = r - R.point(c, 1);
         double hv = R.row_of(c, 1).c, qv = R.row_of(c, 2).c;
-        acc[S_HH] += hv * hv;
-        acc[S_HQ] += hv * qv;
-        acc[S_QQ] += qv * qv;
-        acc[S_JB] += jd * b1;
-        acc[S_JA] += jd * a11;
-        acc[S_JJ] += jd * jd;
-        acc[S_B1R] += b1 * r;
-        acc[S_B2R] += b2 * r;
-        acc[S_B1B1] += b1 * b1;
-        acc[S_B1B2] += b1 * b2;
-        acc[S_B2B2] += b2 * b2;
-        acc[S_A11R] += a11 * r;
-        acc[S_A12R] += a12 * r;
-        acc[S_A22R] += a22 * r;
-        acc[S_A11B1] += a11 * b1;
-        acc[S_A11B2] += a11 * b2;
-        acc[S_A12B1] += a12 * b1;
-        acc[S_A12B2] += a12 * b2;
-        acc[S_A22B1] += a22 * b1;
-        acc[S_A22B2] += a22 * b2;
-        acc[S_A11A11] += a11 * a11;
-        acc[S_A11A12] += a11 * a12;
-        acc[S_A12A12] += a12 * a12;
-        acc[S_A11A22] += a11 * a22;
-        acc[S_A12A22] += a12 * a22;
-        acc[S_A22A22] += a22 * a22;
+        acc[S_HH] = fma(hv, hv, acc[S_HH]);
+        acc[S_HQ] = fma(hv, qv, acc[S_HQ]);
+        acc[S_QQ] = fma(qv, qv, acc[S_QQ]);
+        acc[S_JB] = fma(jd, b1, acc[S_JB]);
+        acc[S_JA] = fma(jd, a11, acc[S_JA]);
+        acc[S_JJ] = fma(jd, jd, acc[S_JJ]);
+        acc[S_B1R] = fma(b1, r, acc[S_B1R]);
+        acc[S_B2R] = fma(b2, r, acc[S_B2R]);
+        acc[S_B1B1] = fma(b1, b1, acc[S_B1B1]);
+        acc[S_B1B2] = fma(b1, b2, acc[S_B1B2]);
+        acc[S_B2B2] = fma(b2, b2, acc[S_B2B2]);
+        acc[S_A11R] = fma(a11, r, acc[S_A11R]);
+        acc[S_A12R] = fma(a12, r, acc[S_A12R]);
+        acc[S_A22R] = fma(a22, r, acc[S_A22R]);
+        acc[S_A11B1] = fma(a11, b1, acc[S_A11B1]);
+        acc[S_A11B2] = fma(a11, b2, acc[S_A11B2]);
+        acc[S_A12B1] = fma(a12, b1, acc[S_A12B1]);
+        acc[S_A12B2] = fma(a12, b2, acc[S_A12B2]);
+        acc[S_A22B1] = fma(a22, b1, acc[S_A22B1]);
+        acc[S_A22B2] = fma(a22, b2, acc[S_A22B2]);
+        acc[S_A11A11] = fma(a11, a11, acc[S_A11A11]);
+        acc[S_A11A12] = fma(a11, a12, acc[S_A11A12]);
+        acc[S_A12A12] = fma(a12, a12, acc[S_A12A12]);
+        acc[S_A11A22] = fma(a11, a22, acc[S_A11A22]);
+        acc[S_A12A22] = fma(a12, a22, acc[S_A12A22]);
+        acc[S_A22A22] = fma(a22, a22, acc[S_A22A22]);
       }
       gp = np;
       gh = nh;
