@@ -129,30 +129,55 @@ class Clocks:
                 "reasons": sorted(reasons)}
 
 
-# algorithmic traffic per cell for one launch of each stencil kernel (FP64 arrays
-# read + written once each; halos, L2 hits and scalars not counted)
-STENCIL_ARRAYS = {"beta": 5, "coeffs": 5, "update": 5}
+# Algorithmic bytes per cell moved by one launch of each iteration kernel (FP64 arrays
+# read + written once each; halos, L2 hits and scalars not counted):
+#   sweep_sums    reads psi, d_hat, d_prev, r_k, r_{k-1}                    5 x 8 B
+#   sweep_update  reads psi, d_hat, d_prev, r_k; writes d, psi', r'          7 x 8 B
+#   dct_* / fft_* one pass of the cosine transform: reads + writes a line    2 x 8 B
+# Every active instance runs each kernel once per iteration, so the cells a kernel
+# touched over the timed steps are sum over instances of iterations x n^2 (x steps).
+ALG_BYTES_PER_CELL = {"sweep_sums": 40, "sweep_update": 56, "dct_rows_fwd": 16, "dct_cols": 16, "dct_rows_inv": 16,
+                      "fft_rows_fwd": 16, "fft_cols": 16, "fft_rows_inv": 16}
 
 
-def roofline(prof, stats, ns, peaks):
-    """Dominant kernel of the profiled launches: achieved algorithmic rate / measured peak."""
+def load_traffic():
+    """DRAM bytes per cell per launch measured by ncu (profiles/traffic_per_cell.json)."""
+    p = os.path.join(ROOT, "profiles", "traffic_per_cell.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return {}
+
+
+def kernel_rates(prof, cell_iters, peaks):
+    """Achieved algorithmic bandwidth of every profiled iteration kernel."""
+    out = {}
+    for name, (ms, cnt) in (prof or {}).items():
+        rec = {"ms": ms, "launches": cnt, "avg_launch_us": 1e3 * ms / max(cnt, 1)}
+        if name in ALG_BYTES_PER_CELL and ms > 0:
+            gbs = ALG_BYTES_PER_CELL[name] * cell_iters / (ms / 1e3) / 1e9
+            rec.update({"achieved_gbs": gbs, "frac_of_hbm": gbs / peaks["hbm_gbs"]})
+        out[name] = rec
+    return out
+
+
+def roofline(prof, cell_iters, steps, peaks):
+    """Dominant kernel: algorithmic bytes per launch / its average CUDA-event launch time."""
     if not prof:
         return None
     name, (ms, cnt) = max(prof.items(), key=lambda kv: kv[1][0])
-    cells_iter = sum(st.iterations * n * n for st, n in zip(stats, ns))
-    if name in STENCIL_ARRAYS:
-        alg = STENCIL_ARRAYS[name] * 8 * cells_iter
-        return {"kernel": name, "bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peaks.get("hbm_gbs"),
-                "unit": "GB/s", "frac": (alg / (ms / 1e3) / 1e9) / peaks.get("hbm_gbs", 1.0),
-                "launches": cnt, "avg_launch_us": ms * 1e3 / max(cnt, 1), "alg_bytes_per_cell": STENCIL_ARRAYS[name] * 8,
-                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)", "traffic": None}
-    if name == "dct_gemm":
-        flops = sum(st.iterations * 4 * 2.0 * n ** 3 for st, n in zip(stats, ns))
-        tf = flops / (ms / 1e3) / 1e12
-        return {"kernel": name, "bound": "fp64", "achieved": tf, "unit": "TFLOP/s", "peak": None, "frac": None,
-                "launches": cnt, "avg_launch_us": ms * 1e3 / max(cnt, 1), "traffic": None,
-                "note": "FP64 CUDA-core GEMM form of the cosine transform (8 n^3 flop per Poisson solve)"}
-    return {"kernel": name, "launches": cnt, "total_ms": ms}
+    if name not in ALG_BYTES_PER_CELL:
+        return {"kernel": name, "launches": cnt, "total_ms": ms, "bound": None}
+    per_launch_bytes = ALG_BYTES_PER_CELL[name] * cell_iters / cnt
+    avg_s = ms / 1e3 / cnt
+    achieved = per_launch_bytes / avg_s / 1e9
+    traffic = load_traffic().get(name)
+    cells_per_launch = cell_iters / cnt
+    return {"kernel": name, "bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"],
+            "traffic": traffic * cells_per_launch if traffic is not None else None,
+            "alg_bytes_per_launch": per_launch_bytes, "avg_launch_us": avg_s * 1e6, "launches": cnt,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (%s)" % peaks.get("source", "measured"),
+            "traffic_source": "profiles/traffic_per_cell.json (ncu dram__bytes_read+write per cell, scaled)"}
 
 
 def load_peaks():
@@ -285,10 +310,9 @@ def run_ours(args):
         plain = {"value": B / (tot / 1e3), "unit": UNIT, "form": "one otm_solve call per density, same kernels"}
 
     peaks = load_peaks()
-    roof = roofline(prof, st_list, ns, peaks)
-    if roof is not None:
-        roof["peak_source"] = roof.get("peak_source", peaks.get("source"))
-    kernels = {k: {"ms": v[0], "launches": v[1]} for k, v in (prof or {}).items()}
+    cell_iters = args.steps * sum(st.iterations * nn * nn for st, nn in zip(st_list, ns))
+    roof = roofline(prof, cell_iters, args.steps, peaks)
+    kernels = kernel_rates(prof, cell_iters, peaks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
