@@ -141,6 +141,37 @@ int otm_map_inverse(otm_map* map, double* points, long count, int* face, int* nh
 int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
                   double* img);
 
+/* ---- implicit adjoint (no counterpart in the reference, which has no derivatives) ----
+ *
+ * Gradient of a loss of the forward mesh with respect to the raw input density, for a
+ * map produced by otm_solve on that density. With F(psi, rho~) = A(psi) - e^2 rho~ the
+ * converged residual (otsolver_2dgrid.cpp:449-465), dL/drho~ = e^2 lambda where
+ * J^T lambda = G^T dL/dfwd (J = dA/dpsi, G the vertex-gradient operator, both applied
+ * matrix-free on the GPU), chained through the normalisation of
+ * otsolver_2dgrid.cpp:53-55 (the max_ratio clamp must be inactive).
+ *   OTM_ADJOINT_ONE_STEP  lambda = -M^+ G^T dL/dfwd: one cosine-transform Poisson solve
+ *                         (M the reference's pseudo-Laplacian, J = -M at psi = 0)
+ *   OTM_ADJOINT_KRYLOV    Richardson iteration on J^T preconditioned by -M^+ until the
+ *                         relative residual is <= tol (or max_iter iterations) */
+#define OTM_ADJOINT_ONE_STEP 0
+#define OTM_ADJOINT_KRYLOV 1
+typedef struct {
+  int mode;
+  double tol;
+  int max_iter;
+} otm_adjoint_options;
+typedef struct {
+  int iterations;            /* Poisson solves used */
+  double relative_residual;  /* |G^T q - J^T lambda| / |G^T q| (Krylov mode; -1 in one-step mode) */
+} otm_adjoint_stats;
+void otm_default_adjoint_options(otm_adjoint_options* opt); /* Krylov, tol 1e-10, 100 iterations */
+/*   density    cells: the raw density given to otm_solve
+ *   fwd_xy     vertices: the forward mesh otm_solve returned
+ *   grad_fwd   vertices: dL/dfwd (x, y per vertex)
+ *   grad_density cells out: dL/ddensity */
+int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fwd_xy, const double* grad_fwd,
+                const otm_adjoint_options* opt, double* grad_density, otm_adjoint_stats* stats);
+
 /* Context options (no counterpart in the reference).
  *   OTM_OPT_POISSON: how d_hat = M^+ r is computed.
  *     OTM_POISSON_AUTO  (default) fast cosine transform for power-of-two n in [8, 4096],

@@ -1,0 +1,323 @@
+// Implicit adjoint of a converged transport map with respect to its input density.
+//
+// The reference has no derivative; this follows from its equations. The solve drives
+// the area residual F(psi, rho~) = A(psi) - e^2 rho~ to zero (otsolver_2dgrid.cpp:449-465)
+// where A(psi) is the area of each quad of the grid displaced by the vertex gradients
+// g = G psi (otsolver_2dgrid.cpp:362-447) and rho~ = adjust(rho) (otsolver_2dgrid.cpp:47-63).
+// For a loss L(fwd) of the forward mesh fwd = grid + g, with q = dL/dfwd (per vertex):
+//   dL/dpsi   = G^T q
+//   J^T lambda = G^T q,  J = dA/dpsi = (dA/dg) G      (mean-zero subspace: J 1 = 0, 1^T J = 0)
+//   dL/drho~  = e^2 lambda
+//   dL/drho   = (lambda - (lambda . rho) / S) / S,  S = sum(rho)   (ratio clamp inactive)
+// J^T is applied matrix-free: k_adj_vertex forms h_v = sum_c lambda_c dA_c/dg_v over the four
+// cells around each vertex (dA_c/dD1 = (D2y, -D2x)/2, dA_c/dD2 = (-D1y, D1x)/2 with the
+// cell diagonals D1 = g11 - g00 + (e,e), D2 = g01 - g10 + (-e,e)), and k_adj_cells gathers
+// (G^T h)_f over every vertex whose clamped gradient stencil touches cell f. Both are
+// deterministic gathers. lambda solves J^T lambda = b by Richardson iteration
+// preconditioned with -M^+ (M the reference's pseudo-Laplacian, J = -M at psi = 0), using
+// the same cosine-transform Poisson solve as the forward loop; the one-step mode stops at
+// lambda = -M^+ b (one Poisson solve).
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace otm {
+
+__device__ __forceinline__ int clampv(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
+
+// Displacement g of vertex (i, j) from the forward mesh.
+__device__ __forceinline__ double2 disp(const double* fwd, int n, int i, int j) {
+  const size_t v = (size_t)j + (size_t)i * (n + 1);
+  const double dx = 1.0 / (double)n;
+  return make_double2(fwd[2 * v] - (double)i * dx, fwd[2 * v + 1] - (double)j * dx);
+}
+
+// Diagonals of cell (ci, cj).
+__device__ __forceinline__ void cell_diags(const double* fwd, int n, int ci, int cj, double2& D1, double2& D2) {
+  const double e = 1.0 / (double)n;
+  double2 g00 = disp(fwd, n, ci, cj), g10 = disp(fwd, n, ci + 1, cj), g01 = disp(fwd, n, ci, cj + 1),
+          g11 = disp(fwd, n, ci + 1, cj + 1);
+  D1 = make_double2(g11.x - g00.x + e, g11.y - g00.y + e);
+  D2 = make_double2(g01.x - g10.x - e, g01.y - g10.y + e);
+}
+
+// h_v = sum over the cells c around vertex v of lambda_c dA_c / dg_v.
+__global__ void k_adj_vertex(int n, const double* fwd, const double* lambda, double* h) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long V = (long)(n + 1) * (n + 1);
+  if (v >= V) return;
+  const int vi = (int)(v / (n + 1)), vj = (int)(v % (n + 1));
+  double hx = 0.0, hy = 0.0;
+  double2 D1, D2;
+  if (vi < n && vj < n) {  // v00 of cell (vi, vj): -dA/dD1
+    cell_diags(fwd, n, vi, vj, D1, D2);
+    const double l = 0.5 * lambda[(size_t)vi * n + vj];
+    hx += l * -D2.y;
+    hy += l * D2.x;
+  }
+  if (vi > 0 && vj < n) {  // v10 of cell (vi-1, vj): -dA/dD2
+    cell_diags(fwd, n, vi - 1, vj, D1, D2);
+    const double l = 0.5 * lambda[(size_t)(vi - 1) * n + vj];
+    hx += l * D1.y;
+    hy += l * -D1.x;
+  }
+  if (vi < n && vj > 0) {  // v01 of cell (vi, vj-1): dA/dD2
+    cell_diags(fwd, n, vi, vj - 1, D1, D2);
+    const double l = 0.5 * lambda[(size_t)vi * n + vj - 1];
+    hx += l * -D1.y;
+    hy += l * D1.x;
+  }
+  if (vi > 0 && vj > 0) {  // v11 of cell (vi-1, vj-1): dA/dD1
+    cell_diags(fwd, n, vi - 1, vj - 1, D1, D2);
+    const double l = 0.5 * lambda[(size_t)(vi - 1) * n + vj - 1];
+    hx += l * D2.y;
+    hy += l * -D2.x;
+  }
+  h[2 * v] = hx;
+  h[2 * v + 1] = hy;
+}
+
+// (G^T h)_f: vertex (vi, vj) reads cells (clamp(vi-1+a), clamp(vj-1+b)), a, b in {0, 1},
+// with gx coefficient (2a-1) n/2 and gy coefficient (2b-1) n/2
+// (otsolver_2dgrid.cpp:379-422 with clamped indices). Cell (i, j) collects every
+// (vertex, a, b) whose clamped position is (i, j); out = scale * G^T h (+ add).
+__global__ void k_adj_cells(int n, const double* h, double scale, const double* add, double* out) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= (long)n * n) return;
+  const int i = (int)(f / n), j = (int)(f % n);
+  // row choices: (vi, a) with clamp(vi - 1 + a) == i
+  int ri[3], ra[3], nr = 0;
+  ri[nr] = i + 1; ra[nr++] = 0;
+  ri[nr] = i; ra[nr++] = 1;
+  if (i == 0) { ri[nr] = 0; ra[nr++] = 0; }
+  if (i == n - 1) { ri[nr] = n; ra[nr++] = 1; }
+  int cj[3], cb[3], nc = 0;
+  cj[nc] = j + 1; cb[nc++] = 0;
+  cj[nc] = j; cb[nc++] = 1;
+  if (j == 0) { cj[nc] = 0; cb[nc++] = 0; }
+  if (j == n - 1) { cj[nc] = n; cb[nc++] = 1; }
+  const double hw = 0.5 * (double)n;
+  double acc = 0.0;
+  for (int p = 0; p < nr; ++p)
+    for (int q = 0; q < nc; ++q) {
+      const size_t v = (size_t)cj[q] + (size_t)ri[p] * (n + 1);
+      acc += hw * ((2 * ra[p] - 1) * h[2 * v] + (2 * cb[q] - 1) * h[2 * v + 1]);
+    }
+  out[f] = scale * acc + (add ? add[f] : 0.0);
+}
+
+// z = -z (the preconditioner is -M^+) and residual norms: out[0] += b.b, out[1] += r.r
+__global__ void k_adj_dot2(long N, const double* b, const double* r, double* partial) {
+  __shared__ double red[64];
+  double v[2] = {0.0, 0.0};
+  for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x) {
+    v[0] += b[f] * b[f];
+    v[1] += r[f] * r[f];
+  }
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = v[0];
+    partial[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
+// lambda += -z
+__global__ void k_adj_axpy(long N, const double* z, double* lambda) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < N) lambda[f] -= z[f];
+}
+
+// dL/drho = (lambda - (lambda . rho) / S) / S, from partial sums of lambda . rho and rho
+__global__ void k_adj_dot_rho(long N, const double* lambda, const double* rho, double* partial) {
+  __shared__ double red[64];
+  double v[2] = {0.0, 0.0};
+  for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x) {
+    v[0] += lambda[f] * rho[f];
+    v[1] += rho[f];
+  }
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = v[0];
+    partial[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
+__global__ void k_adj_finish(long N, const double* lambda, double lr, double S, double* out) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < N) out[f] = (lambda[f] - lr / S) / S;
+}
+
+}  // namespace otm
+
+using namespace otm;
+
+namespace {
+
+// Poisson solve d = M^+ src (cosine transform) on the context's stream, using a
+// one-instance record whose buffers point at src / dst / two temporaries.
+struct PoissonRunner {
+  otm_context* ctx;
+  int n;
+  DevBuf rec, lists;
+  Inst h;
+  int G = 0, rows = 0, cols = 0, reg = 0;
+  PoissonRunner(otm_context* c, int n_, double* t1, double* t2) : ctx(c), n(n_) {
+    SizeTables* T = ctx->tables.at(n).get();
+    std::memset(&h, 0, sizeof(h));
+    h.n = n;
+    h.active = 1;
+    h.t1 = t1;
+    h.t2 = t2;
+    h.C = T->C.as<double>();
+    h.cosk = T->cosk.as<double>();
+    h.tw = T->tw.as<double2>();
+    h.pt = T->pt.as<double2>();
+    h.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
+    std::vector<int> zeros;
+    if (h.fft) {
+      int lg = 0;
+      while ((1 << lg) < n) ++lg;
+      h.logn = lg;
+      reg = dct_reg_supported(n) ? 1 : 0;
+      const int per = reg ? dct_reg_lines_per_block(n) : fft_lines(n);
+      h.nrow = h.ncol = n / per;
+      rows = cols = h.nrow;
+      zeros.assign(rows, 0);
+    } else {
+      int t = (n + 63) / 64;
+      h.ngemm = G = t * t;
+      zeros.assign(G, 0);
+    }
+    rec.reserve(sizeof(Inst));
+    lists.reserve(sizeof(int) * zeros.size());
+    OTM_CUDA(cudaMemcpyAsync(lists.p, zeros.data(), sizeof(int) * zeros.size(), cudaMemcpyHostToDevice, ctx->stream));
+  }
+  void run(const double* src, double* dst);
+};
+
+}  // namespace
+
+// Poisson launches for the adjoint reuse the forward kernels (declared in solver.cu / poisson.cu).
+namespace otm {
+void dense_poisson(otm_context* ctx, Inst* d_inst, const int* gemm_inst, int G);
+}
+
+void PoissonRunner::run(const double* src, double* dst) {
+  h.r[0] = const_cast<double*>(src);
+  h.dhat = dst;
+  OTM_CUDA(cudaMemcpyAsync(rec.p, &h, sizeof(Inst), cudaMemcpyHostToDevice, ctx->stream));
+  Inst* d = rec.as<Inst>();
+  if (h.fft) {
+    if (reg)
+      dct_reg_run(ctx, n, d, lists.as<int>(), 0, rows, lists.as<int>(), 0, cols);
+    else
+      poisson_fft(ctx, d, lists.as<int>(), 0, rows, lists.as<int>(), 0, cols);
+  } else {
+    dense_poisson(ctx, d, lists.as<int>(), G);
+  }
+}
+
+extern "C" void otm_default_adjoint_options(otm_adjoint_options* o) {
+  if (!o) return;
+  o->mode = OTM_ADJOINT_KRYLOV;
+  o->tol = 1e-10;
+  o->max_iter = 100;
+}
+
+extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fwd_xy,
+                           const double* grad_fwd, const otm_adjoint_options* opt, double* grad_density,
+                           otm_adjoint_stats* stats) {
+  return guarded([&] {
+    if (!ctx || !density || !fwd_xy || !grad_fwd || !grad_density) throw BadArg{"otm_adjoint: null argument"};
+    if (n < 1 || n > 16384) throw BadArg{"otm_adjoint: grid size out of range"};
+    otm_adjoint_options o;
+    otm_default_adjoint_options(&o);
+    if (opt) o = *opt;
+    if (o.mode != OTM_ADJOINT_ONE_STEP && o.mode != OTM_ADJOINT_KRYLOV) throw BadArg{"otm_adjoint: unknown mode"};
+    make_current(ctx);
+    if (otm_init(ctx, n) != OTM_OK) throw BadArg{std::string("otm_adjoint: ") + otm_last_error()};
+    cudaStream_t st = ctx->stream;
+    const size_t N = (size_t)n * n, V = (size_t)(n + 1) * (n + 1);
+    const int RB = 256;
+    const int nred = 256;
+    // device scratch: fwd, q, rho, b, lambda, r, z, h, t1, t2, partials
+    const size_t words = 2 * V + 2 * V + N + N + N + N + N + 2 * V + N + N + 2 * nred + 64;
+    DevBuf buf;
+    buf.reserve(sizeof(double) * words);
+    double* p = buf.as<double>();
+    double* d_fwd = p; p += 2 * V;
+    double* d_q = p; p += 2 * V;
+    double* d_rho = p; p += N;
+    double* d_b = p; p += N;
+    double* d_lam = p; p += N;
+    double* d_r = p; p += N;
+    double* d_z = p; p += N;
+    double* d_h = p; p += 2 * V;
+    double* d_t1 = p; p += N;
+    double* d_t2 = p; p += N;
+    double* d_part = p;
+    copy_in(ctx, d_fwd, fwd_xy, sizeof(double) * 2 * V);
+    copy_in(ctx, d_q, grad_fwd, sizeof(double) * 2 * V);
+    copy_in(ctx, d_rho, density, sizeof(double) * N);
+    const unsigned gN = (unsigned)((N + RB - 1) / RB), gV = (unsigned)((V + RB - 1) / RB);
+    // b = G^T q
+    launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_q, 1.0, (const double*)nullptr, d_b);
+    PoissonRunner P(ctx, n, d_t1, d_t2);
+    auto norms = [&](const double* a, const double* b2, double out[2]) {
+      launch(ctx, "adj_dot", k_adj_dot2, nred, RB, (long)N, a, b2, d_part);
+      std::vector<double> hp(2 * nred);
+      OTM_CUDA(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * 2 * nred, cudaMemcpyDeviceToHost, st));
+      OTM_CUDA(cudaStreamSynchronize(st));
+      out[0] = out[1] = 0.0;
+      for (int k = 0; k < nred; ++k) {
+        out[0] += hp[2 * k];
+        out[1] += hp[2 * k + 1];
+      }
+    };
+    // lambda_0 = -M^+ b
+    OTM_CUDA(cudaMemsetAsync(d_lam, 0, sizeof(double) * N, st));
+    P.run(d_b, d_z);
+    launch(ctx, "adj_axpy", k_adj_axpy, gN, RB, (long)N, (const double*)d_z, d_lam);
+    int iters = 1;
+    double rel = -1.0;
+    if (o.mode == OTM_ADJOINT_KRYLOV) {
+      while (true) {
+        // r = b - J^T lambda
+        launch(ctx, "adj_vertex", k_adj_vertex, gV, RB, n, (const double*)d_fwd, (const double*)d_lam, d_h);
+        launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_h, -1.0, (const double*)d_b, d_r);
+        double nr[2];
+        norms(d_b, d_r, nr);
+        rel = nr[0] > 0 ? std::sqrt(nr[1] / nr[0]) : 0.0;
+        if (!(rel > o.tol) || iters >= o.max_iter) break;
+        P.run(d_r, d_z);
+        launch(ctx, "adj_axpy", k_adj_axpy, gN, RB, (long)N, (const double*)d_z, d_lam);
+        ++iters;
+      }
+    }
+    // chain through the density normalisation
+    launch(ctx, "adj_dot", k_adj_dot_rho, nred, RB, (long)N, (const double*)d_lam, (const double*)d_rho, d_part);
+    std::vector<double> hp(2 * nred);
+    OTM_CUDA(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * 2 * nred, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    double lr = 0.0, S = 0.0;
+    for (int k = 0; k < nred; ++k) {
+      lr += hp[2 * k];
+      S += hp[2 * k + 1];
+    }
+    bool odev = is_device_ptr(grad_density);
+    double* out = odev ? grad_density : d_z;
+    launch(ctx, "adj_finish", k_adj_finish, gN, RB, (long)N, (const double*)d_lam, lr, S, out);
+    OTM_CUDA(cudaGetLastError());
+    if (!odev) copy_out(ctx, grad_density, out, sizeof(double) * N);
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    if (stats) {
+      stats->iterations = iters;
+      stats->relative_residual = rel;
+    }
+    return (int)OTM_OK;
+  });
+}

@@ -661,6 +661,11 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
 
 static SizeTables* init_size(otm_context* ctx, int n);
 
+// The dense-product Poisson solve for one record (used by the adjoint).
+void dense_poisson(otm_context* ctx, Inst* d_inst, const int* gemm_inst, int G) {
+  for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_inst, gemm_inst, s, 1);
+}
+
 // Runs the whole solve for `count` instances whose raw densities have been copied
 // into their rho buffers. Host-side copies of the final records are returned.
 static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, const otm_solver_options& o) {

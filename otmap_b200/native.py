@@ -40,6 +40,17 @@ class SolveStatsC(C.Structure):
                 ("initial_residual", C.c_double)]
 
 
+class AdjointOptionsC(C.Structure):
+    _fields_ = [("mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int)]
+
+
+class AdjointStatsC(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("relative_residual", C.c_double)]
+
+
+ADJOINT_ONE_STEP, ADJOINT_KRYLOV = 0, 1
+
+
 class OtmError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"otmap_b200 error {code}: {msg}")
@@ -69,6 +80,9 @@ SIGNATURES = {
     "otm_solve_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(SolverOptionsC), C.c_void_p, C.c_void_p,
                                     C.POINTER(SolveStatsC), C.c_void_p]),
     "otm_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "otm_default_adjoint_options": (None, [C.POINTER(AdjointOptionsC)]),
+    "otm_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(AdjointOptionsC),
+                              C.c_void_p, C.POINTER(AdjointStatsC)]),
     "otm_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "otm_launch_count": (C.c_long, [C.c_void_p]),
     "otm_profile": (C.c_int, [C.c_void_p, C.c_int]),

@@ -1,0 +1,116 @@
+"""The implicit adjoint (otm_adjoint) against an FP64 reference gradient built from
+explicit sparse Jacobians, and against central finite differences of tightly converged
+GPU solves, including the softmax-logits workload at 512^2 through torch.autograd."""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TIGHT = 1e-24  # forward threshold for gradient checks (the implicit gradient assumes F = 0)
+
+
+def _solve(N, ctx, n, dens, threshold=TIGHT):
+    fwd = np.empty(((n + 1) ** 2, 2))
+    opt = N.default_options()
+    opt.threshold = threshold
+    st = N.SolveStatsC()
+    N.check(N.lib().otm_solve(ctx.handle, n, N.ptr(dens), C.byref(opt), N.ptr(fwd), None, C.byref(st)))
+    return fwd, st
+
+
+def _adjoint(N, ctx, n, dens, fwd, q, mode, tol=1e-12):
+    g = np.empty(n * n)
+    opt = N.AdjointOptionsC()
+    N.lib().otm_default_adjoint_options(C.byref(opt))
+    opt.mode = mode
+    opt.tol = tol
+    st = N.AdjointStatsC()
+    N.check(N.lib().otm_adjoint(ctx.handle, n, N.ptr(dens), N.ptr(fwd), N.ptr(np.ascontiguousarray(q)),
+                                C.byref(opt), N.ptr(g), C.byref(st)))
+    return g, st
+
+
+@pytest.mark.parametrize("n", [16, 33, 64])
+def test_adjoint_matches_fp64_reference(n):
+    from adjoint_ref import reference_gradient
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    ctx = N.Context(0)
+    dens = W.to_cells(W.gaussian_mixture(n, 200 + n))
+    fwd, st = _solve(N, ctx, n, dens)
+    assert st.residual < 1e-20
+    q = np.random.default_rng(n).standard_normal(((n + 1) ** 2, 2))
+    ref, _ = reference_gradient(fwd, dens, q, n)
+    g, ast = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_KRYLOV)
+    rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
+    assert rel <= 1e-8, (rel, ast.iterations, ast.relative_residual)
+    g1, _ = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_ONE_STEP)
+    rel1 = np.linalg.norm(g1 - ref) / np.linalg.norm(ref)
+    assert rel1 < 0.5  # one Poisson solve: an approximation, reported by the bench
+    ctx.close()
+
+
+def test_adjoint_matches_finite_differences():
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    n = 32
+    ctx = N.Context(0)
+    dens = W.to_cells(W.blurred_shapes(n, 4, sigma_px=1.5))
+    fwd, _ = _solve(N, ctx, n, dens)
+    rng = np.random.default_rng(5)
+    q = rng.standard_normal(fwd.shape)
+    g, _ = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_KRYLOV)
+    h = 1e-6
+    for _ in range(4):
+        u = rng.standard_normal(n * n)
+        u /= np.linalg.norm(u)
+        fp, _ = _solve(N, ctx, n, dens + h * u)
+        fm, _ = _solve(N, ctx, n, dens - h * u)
+        fd = np.sum(q * (fp - fm)) / (2 * h)
+        assert abs(fd - g @ u) <= 1e-5 * max(abs(fd), 1e-3 * np.linalg.norm(g)), (fd, g @ u)
+    ctx.close()
+
+
+def test_logit_gradient_512_softmax_blur():
+    """Density = blur(softmax(z)) (sigma 8 px), loss = mean over 4096 random vertices of
+    |T(x_i) - y_i|^2; autograd gradient w.r.t. the logits against central differences
+    along 32 random unit directions (h = 1e-4)."""
+    import torch
+
+    from otmap_b200.autograd import blur_torch, transport_map
+
+    n = 512
+    torch.manual_seed(0)
+    dev = torch.device("cuda", 0)
+    gen = torch.Generator(device="cpu").manual_seed(1)
+    z0 = torch.randn((n, n), generator=gen, dtype=torch.float64).to(dev)
+    V = (n + 1) ** 2
+    idx = torch.randperm(V, generator=gen)[:4096].to(dev)
+    y = torch.rand((4096, 2), generator=gen, dtype=torch.float64).to(dev)
+
+    def density(z):
+        p = torch.softmax(z.reshape(-1), 0).reshape(n, n)
+        return blur_torch(p, 8.0).t().reshape(-1)  # image [y][x] -> cells (f = y + x n)
+
+    def loss(z, adjoint="krylov"):
+        fwd = transport_map(density(z), n, threshold=TIGHT, adjoint=adjoint)
+        return ((fwd[idx] - y) ** 2).sum(1).mean()
+
+    z = z0.clone().requires_grad_(True)
+    L = loss(z)
+    (grad,) = torch.autograd.grad(L, z)
+    h = 1e-4
+    errs = []
+    with torch.no_grad():
+        for k in range(32):
+            u = torch.randn((n, n), generator=gen, dtype=torch.float64).to(dev)
+            u /= u.norm()
+            fd = (loss(z0 + h * u) - loss(z0 - h * u)) / (2 * h)
+            ad = (grad * u).sum()
+            errs.append(abs(float(fd - ad)) / max(abs(float(fd)), 1e-12))
+    assert max(errs) <= 1e-4, errs
