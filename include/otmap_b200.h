@@ -151,20 +151,21 @@ int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* densi
  * otsolver_2dgrid.cpp:53-55 (the max_ratio clamp must be inactive).
  *   OTM_ADJOINT_ONE_STEP  lambda = -M^+ G^T dL/dfwd: one cosine-transform Poisson solve
  *                         (M the reference's pseudo-Laplacian, J = -M at psi = 0)
- *   OTM_ADJOINT_KRYLOV    Richardson iteration on J^T preconditioned by -M^+ until the
- *                         relative residual is <= tol (or max_iter iterations) */
+ *   OTM_ADJOINT_KRYLOV    restarted GMRES on J^T, right-preconditioned by M^+, until the
+ *                         relative residual is <= tol (or max_iter Poisson solves) */
 #define OTM_ADJOINT_ONE_STEP 0
 #define OTM_ADJOINT_KRYLOV 1
 typedef struct {
   int mode;
   double tol;
-  int max_iter;
+  int max_iter;  /* Poisson solves at most */
+  int restart;   /* Krylov basis size before a restart */
 } otm_adjoint_options;
 typedef struct {
   int iterations;            /* Poisson solves used */
   double relative_residual;  /* |G^T q - J^T lambda| / |G^T q| (Krylov mode; -1 in one-step mode) */
 } otm_adjoint_stats;
-void otm_default_adjoint_options(otm_adjoint_options* opt); /* Krylov, tol 1e-10, 100 iterations */
+void otm_default_adjoint_options(otm_adjoint_options* opt); /* Krylov, tol 1e-10, 2000 solves, restart 40 */
 /*   density    cells: the raw density given to otm_solve
  *   fwd_xy     vertices: the forward mesh otm_solve returned
  *   grad_fwd   vertices: dL/dfwd (x, y per vertex)

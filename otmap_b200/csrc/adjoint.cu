@@ -13,11 +13,14 @@
 // cells around each vertex (dA_c/dD1 = (D2y, -D2x)/2, dA_c/dD2 = (-D1y, D1x)/2 with the
 // cell diagonals D1 = g11 - g00 + (e,e), D2 = g01 - g10 + (-e,e)), and k_adj_cells gathers
 // (G^T h)_f over every vertex whose clamped gradient stencil touches cell f. Both are
-// deterministic gathers. lambda solves J^T lambda = b by Richardson iteration
-// preconditioned with -M^+ (M the reference's pseudo-Laplacian, J = -M at psi = 0), using
-// the same cosine-transform Poisson solve as the forward loop; the one-step mode stops at
-// lambda = -M^+ b (one Poisson solve).
+// deterministic gathers. lambda solves J^T lambda = b by restarted GMRES right-
+// preconditioned with the pseudo-inverse of M (the reference's pseudo-Laplacian; J = -M at
+// psi = 0), using the same cosine-transform Poisson solve as the forward loop; the
+// one-step mode stops at lambda = -M^+ b (one Poisson solve). For strongly deformed maps
+// J departs far from -M (a plain preconditioned fixed-point iteration diverges there),
+// hence the Krylov method.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -109,19 +112,54 @@ __global__ void k_adj_cells(int n, const double* h, double scale, const double* 
   out[f] = scale * acc + (add ? add[f] : 0.0);
 }
 
-// z = -z (the preconditioner is -M^+) and residual norms: out[0] += b.b, out[1] += r.r
-__global__ void k_adj_dot2(long N, const double* b, const double* r, double* partial) {
-  __shared__ double red[64];
-  double v[2] = {0.0, 0.0};
-  for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x) {
-    v[0] += b[f] * b[f];
-    v[1] += r[f] * r[f];
+// partial[b * (m+1) + i] = sum over this block's cells of w . V_i, i < m (basis vectors
+// stored contiguously with stride `ld`), and partial[b * (m+1) + m] = w . w.
+__global__ void k_adj_multidot(long N, const double* w, const double* V, long ld, int m, double* partial) {
+  __shared__ double red[32];
+  const int P = m + 1;
+  for (int i = 0; i < P; ++i) {
+    const double* vi = i < m ? V + (size_t)i * ld : w;
+    double s = 0.0;
+    for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x)
+      s = fma(w[f], vi[f], s);
+    double v[1] = {s};
+    block_sum<1>(v, red);
+    if (threadIdx.x == 0) partial[(size_t)blockIdx.x * P + i] = v[0];
   }
-  block_sum<2>(v, red);
-  if (threadIdx.x == 0) {
-    partial[2 * blockIdx.x] = v[0];
-    partial[2 * blockIdx.x + 1] = v[1];
-  }
+}
+
+// w = a * w - sum_i c_i V_i (i < m); c in device memory
+__global__ void k_adj_combine(long N, double* w, double a, const double* V, long ld, int m, const double* c) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= N) return;
+  double x = a * w[f];
+  for (int i = 0; i < m; ++i) x = fma(-c[i], V[(size_t)i * ld + f], x);
+  w[f] = x;
+}
+
+// out = sum_i c_i V_i
+__global__ void k_adj_span(long N, double* out, const double* V, long ld, int m, const double* c) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= N) return;
+  double x = 0.0;
+  for (int i = 0; i < m; ++i) x = fma(c[i], V[(size_t)i * ld + f], x);
+  out[f] = x;
+}
+
+// v = b - v
+__global__ void k_adj_resid(long N, const double* b, double* v) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < N) v[f] = b[f] - v[f];
+}
+
+__global__ void k_adj_scale(long N, double* v, double a) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < N) v[f] *= a;
+}
+
+__global__ void k_adj_add(long N, const double* z, double* lambda) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < N) lambda[f] += z[f];
 }
 
 // lambda += -z
@@ -224,7 +262,8 @@ extern "C" void otm_default_adjoint_options(otm_adjoint_options* o) {
   if (!o) return;
   o->mode = OTM_ADJOINT_KRYLOV;
   o->tol = 1e-10;
-  o->max_iter = 100;
+  o->max_iter = 2000;
+  o->restart = 40;
 }
 
 extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fwd_xy,
@@ -243,8 +282,11 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     const size_t N = (size_t)n * n, V = (size_t)(n + 1) * (n + 1);
     const int RB = 256;
     const int nred = 256;
-    // device scratch: fwd, q, rho, b, lambda, r, z, h, t1, t2, partials
-    const size_t words = 2 * V + 2 * V + N + N + N + N + N + 2 * V + N + N + 2 * nred + 64;
+    const int m = o.mode == OTM_ADJOINT_KRYLOV ? std::max(1, std::min(o.restart, 200)) : 1;
+    const size_t ld = (N + 31) / 32 * 32;
+    // device scratch: fwd, q, rho, b, lambda, z, h, t1, t2, basis (m+1), coefficients, partials
+    const size_t words = 2 * V + 2 * V + N + N + N + N + 2 * V + N + N + (size_t)(m + 1) * ld + (m + 2) +
+                         (size_t)nred * (m + 2) + 64;
     DevBuf buf;
     buf.reserve(sizeof(double) * words);
     double* p = buf.as<double>();
@@ -253,11 +295,12 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     double* d_rho = p; p += N;
     double* d_b = p; p += N;
     double* d_lam = p; p += N;
-    double* d_r = p; p += N;
     double* d_z = p; p += N;
     double* d_h = p; p += 2 * V;
     double* d_t1 = p; p += N;
     double* d_t2 = p; p += N;
+    double* d_V = p; p += (size_t)(m + 1) * ld;
+    double* d_c = p; p += m + 2;
     double* d_part = p;
     copy_in(ctx, d_fwd, fwd_xy, sizeof(double) * 2 * V);
     copy_in(ctx, d_q, grad_fwd, sizeof(double) * 2 * V);
@@ -266,40 +309,109 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     // b = G^T q
     launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_q, 1.0, (const double*)nullptr, d_b);
     PoissonRunner P(ctx, n, d_t1, d_t2);
-    auto norms = [&](const double* a, const double* b2, double out[2]) {
-      launch(ctx, "adj_dot", k_adj_dot2, nred, RB, (long)N, a, b2, d_part);
-      std::vector<double> hp(2 * nred);
-      OTM_CUDA(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * 2 * nred, cudaMemcpyDeviceToHost, st));
+    std::vector<double> hp;
+    // dots of w against the first k basis vectors and w.w, summed on the host in block order
+    auto multidot = [&](const double* w, int k, std::vector<double>& out) {
+      launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, w, (const double*)d_V, (long)ld, k, d_part);
+      hp.resize((size_t)nred * (k + 1));
+      OTM_CUDA(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, st));
       OTM_CUDA(cudaStreamSynchronize(st));
-      out[0] = out[1] = 0.0;
-      for (int k = 0; k < nred; ++k) {
-        out[0] += hp[2 * k];
-        out[1] += hp[2 * k + 1];
-      }
+      out.assign(k + 1, 0.0);
+      for (int blk = 0; blk < nred; ++blk)
+        for (int i = 0; i <= k; ++i) out[i] += hp[(size_t)blk * (k + 1) + i];
     };
-    // lambda_0 = -M^+ b
+    // J^T applied to x (cells), into out
+    auto apply_jt = [&](const double* x, double* out) {
+      launch(ctx, "adj_vertex", k_adj_vertex, gV, RB, n, (const double*)d_fwd, x, d_h);
+      launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_h, 1.0, (const double*)nullptr, out);
+    };
     OTM_CUDA(cudaMemsetAsync(d_lam, 0, sizeof(double) * N, st));
-    P.run(d_b, d_z);
-    launch(ctx, "adj_axpy", k_adj_axpy, gN, RB, (long)N, (const double*)d_z, d_lam);
-    int iters = 1;
+    int solves = 0;
     double rel = -1.0;
-    if (o.mode == OTM_ADJOINT_KRYLOV) {
-      while (true) {
-        // r = b - J^T lambda
-        launch(ctx, "adj_vertex", k_adj_vertex, gV, RB, n, (const double*)d_fwd, (const double*)d_lam, d_h);
-        launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_h, -1.0, (const double*)d_b, d_r);
-        double nr[2];
-        norms(d_b, d_r, nr);
-        rel = nr[0] > 0 ? std::sqrt(nr[1] / nr[0]) : 0.0;
-        if (!(rel > o.tol) || iters >= o.max_iter) break;
-        P.run(d_r, d_z);
-        launch(ctx, "adj_axpy", k_adj_axpy, gN, RB, (long)N, (const double*)d_z, d_lam);
-        ++iters;
+    if (o.mode == OTM_ADJOINT_ONE_STEP) {
+      // lambda = -M^+ b
+      P.run(d_b, d_z);
+      ++solves;
+      launch(ctx, "adj_axpy", k_adj_axpy, gN, RB, (long)N, (const double*)d_z, d_lam);
+    } else {
+      // Restarted GMRES(m) on J^T lambda = b, right-preconditioned: J^T M^+ y = b, lambda = M^+ y.
+      // Classical Gram-Schmidt applied twice; Givens rotations and the small triangular
+      // solve on the host.
+      std::vector<double> dots;
+      multidot(d_b, 0, dots);
+      const double bnorm = std::sqrt(dots[0]);
+      std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m);
+      auto Hs = [&](int i, int j) -> double& { return H[(size_t)i * m + j]; };
+      rel = bnorm > 0 ? 1.0 : 0.0;
+      bool first = true;
+      while (bnorm > 0) {
+        double* v0 = d_V;
+        double rnorm;
+        if (first) {
+          OTM_CUDA(cudaMemcpyAsync(v0, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+          rnorm = bnorm;
+          first = false;
+        } else {
+          apply_jt(d_lam, v0);
+          launch(ctx, "adj_resid", k_adj_resid, gN, RB, (long)N, (const double*)d_b, v0);
+          multidot(v0, 0, dots);
+          rnorm = std::sqrt(dots[0]);
+        }
+        rel = rnorm / bnorm;
+        if (!(rel > o.tol) || solves >= o.max_iter) break;
+        launch(ctx, "adj_scale", k_adj_scale, gN, RB, (long)N, v0, 1.0 / rnorm);
+        std::fill(gv.begin(), gv.end(), 0.0);
+        gv[0] = rnorm;
+        int k = 0;
+        for (int j = 0; j < m && solves < o.max_iter; ++j) {
+          double* vj = d_V + (size_t)j * ld;
+          double* w = d_V + (size_t)(j + 1) * ld;
+          P.run(vj, d_z);
+          ++solves;
+          apply_jt(d_z, w);
+          for (int pass = 0; pass < 2; ++pass) {
+            multidot(w, j + 1, dots);
+            for (int i = 0; i <= j; ++i) Hs(i, j) = (pass ? Hs(i, j) : 0.0) + dots[i];
+            OTM_CUDA(cudaMemcpyAsync(d_c, dots.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, st));
+            launch(ctx, "adj_combine", k_adj_combine, gN, RB, (long)N, w, 1.0, (const double*)d_V, (long)ld, j + 1,
+                   (const double*)d_c);
+          }
+          multidot(w, 0, dots);
+          const double hn = std::sqrt(dots[0]);
+          Hs(j + 1, j) = hn;
+          if (hn > 0) launch(ctx, "adj_scale", k_adj_scale, gN, RB, (long)N, w, 1.0 / hn);
+          for (int i = 0; i < j; ++i) {  // previous rotations
+            const double t = cs[i] * Hs(i, j) + sn[i] * Hs(i + 1, j);
+            Hs(i + 1, j) = -sn[i] * Hs(i, j) + cs[i] * Hs(i + 1, j);
+            Hs(i, j) = t;
+          }
+          const double den = std::hypot(Hs(j, j), Hs(j + 1, j));
+          cs[j] = den > 0 ? Hs(j, j) / den : 1.0;
+          sn[j] = den > 0 ? Hs(j + 1, j) / den : 0.0;
+          Hs(j, j) = den;
+          Hs(j + 1, j) = 0.0;
+          gv[j + 1] = -sn[j] * gv[j];
+          gv[j] = cs[j] * gv[j];
+          k = j + 1;
+          if (!(std::fabs(gv[j + 1]) / bnorm > o.tol) || hn == 0) break;
+        }
+        for (int i = k - 1; i >= 0; --i) {  // H y = g
+          double t = gv[i];
+          for (int l = i + 1; l < k; ++l) t -= Hs(i, l) * y[l];
+          y[i] = t / Hs(i, i);
+        }
+        // lambda += M^+ (V y)
+        OTM_CUDA(cudaMemcpyAsync(d_c, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
+        launch(ctx, "adj_span", k_adj_span, gN, RB, (long)N, d_h, (const double*)d_V, (long)ld, k,
+               (const double*)d_c);
+        P.run(d_h, d_z);
+        ++solves;
+        launch(ctx, "adj_add", k_adj_add, gN, RB, (long)N, (const double*)d_z, d_lam);
       }
     }
     // chain through the density normalisation
     launch(ctx, "adj_dot", k_adj_dot_rho, nred, RB, (long)N, (const double*)d_lam, (const double*)d_rho, d_part);
-    std::vector<double> hp(2 * nred);
+    hp.assign(2 * nred, 0.0);
     OTM_CUDA(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * 2 * nred, cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
     double lr = 0.0, S = 0.0;
@@ -315,7 +427,7 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();
     if (stats) {
-      stats->iterations = iters;
+      stats->iterations = solves;
       stats->relative_residual = rel;
     }
     return (int)OTM_OK;

@@ -41,7 +41,7 @@ class SolveStatsC(C.Structure):
 
 
 class AdjointOptionsC(C.Structure):
-    _fields_ = [("mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int)]
+    _fields_ = [("mode", C.c_int), ("tol", C.c_double), ("max_iter", C.c_int), ("restart", C.c_int)]
 
 
 class AdjointStatsC(C.Structure):

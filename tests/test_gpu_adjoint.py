@@ -9,13 +9,17 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-TIGHT = 1e-24  # forward threshold for gradient checks (the implicit gradient assumes F = 0)
+# The implicit gradient assumes F = 0: gradient checks run the forward solve to the
+# FP64 floor of its residual (about 1e-16 in the reference's measure) by iterating a
+# fixed number of times with threshold 0.
+FLOOR_ITERS = 300
 
 
-def _solve(N, ctx, n, dens, threshold=TIGHT):
+def _solve(N, ctx, n, dens, threshold=0.0, max_iter=FLOOR_ITERS):
     fwd = np.empty(((n + 1) ** 2, 2))
     opt = N.default_options()
     opt.threshold = threshold
+    opt.max_iter = max_iter
     st = N.SolveStatsC()
     N.check(N.lib().otm_solve(ctx.handle, n, N.ptr(dens), C.byref(opt), N.ptr(fwd), None, C.byref(st)))
     return fwd, st
@@ -42,7 +46,7 @@ def test_adjoint_matches_fp64_reference(n):
     ctx = N.Context(0)
     dens = W.to_cells(W.gaussian_mixture(n, 200 + n))
     fwd, st = _solve(N, ctx, n, dens)
-    assert st.residual < 1e-20
+    assert st.residual < 1e-12
     q = np.random.default_rng(n).standard_normal(((n + 1) ** 2, 2))
     ref, _ = reference_gradient(fwd, dens, q, n)
     g, ast = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_KRYLOV)
@@ -98,7 +102,7 @@ def test_logit_gradient_512_softmax_blur():
         return blur_torch(p, 8.0).t().reshape(-1)  # image [y][x] -> cells (f = y + x n)
 
     def loss(z, adjoint="krylov"):
-        fwd = transport_map(density(z), n, threshold=TIGHT, adjoint=adjoint)
+        fwd = transport_map(density(z), n, threshold=0.0, max_iter=FLOOR_ITERS, adjoint=adjoint)
         return ((fwd[idx] - y) ** 2).sum(1).mean()
 
     z = z0.clone().requires_grad_(True)
