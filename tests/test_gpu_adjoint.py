@@ -52,9 +52,26 @@ def test_adjoint_matches_fp64_reference(n):
     g, ast = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_KRYLOV)
     rel = np.linalg.norm(g - ref) / np.linalg.norm(ref)
     assert rel <= 1e-8, (rel, ast.iterations, ast.relative_residual)
-    g1, _ = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_ONE_STEP)
-    rel1 = np.linalg.norm(g1 - ref) / np.linalg.norm(ref)
-    assert rel1 < 0.5  # one Poisson solve: an approximation, reported by the bench
+    ctx.close()
+
+
+@pytest.mark.parametrize("n,sigma,bound", [(128, 2.0, 0.15), (256, 4.0, 0.08)])
+def test_one_step_adjoint_on_smooth_density(n, sigma, bound):
+    """The one-Poisson-solve adjoint approximates J^{-T} by -M^+; on the smooth
+    softmax-blur densities it is meant for, its gradient is within a few percent (it is
+    no approximation at all for sharp densities, where J departs far from -M)."""
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    ctx = N.Context(0)
+    _, img = W.softmax_logits(n, 0, sigma_px=sigma)
+    dens = W.to_cells(img)
+    fwd, _ = _solve(N, ctx, n, dens)
+    q = np.random.default_rng(n).standard_normal(((n + 1) ** 2, 2))
+    g, _ = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_KRYLOV)
+    g1, st1 = _adjoint(N, ctx, n, dens, fwd, q, N.ADJOINT_ONE_STEP)
+    assert st1.iterations == 1
+    assert np.linalg.norm(g1 - g) / np.linalg.norm(g) < bound
     ctx.close()
 
 
