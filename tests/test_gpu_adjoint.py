@@ -130,7 +130,7 @@ def test_logit_gradient_512_softmax_blur():
     L = loss(z)
     (grad,) = torch.autograd.grad(L, z)
     h = 1e-4
-    errs = []
+    errs, abs_errs = [], []
     with torch.no_grad():
         for k in range(32):
             u = torch.randn((n, n), generator=gen, dtype=torch.float64).to(dev)
@@ -138,5 +138,10 @@ def test_logit_gradient_512_softmax_blur():
             fd = (loss(z0 + h * u) - loss(z0 - h * u)) / (2 * h)
             ad = (grad * u).sum()
             errs.append(abs(float(fd - ad)) / max(abs(float(fd)), 1e-12))
+            abs_errs.append(abs(float(fd - ad)) / float(grad.norm()))
+    # relative errors blow up on directions with a near-zero derivative; the error measured
+    # against the gradient norm bounds every direction
     print("logit FD relative errors:", sorted(errs))
-    assert np.median(errs) <= 5e-3 and max(errs) <= 5e-2, errs
+    print("logit FD errors / |grad|:", sorted(abs_errs))
+    assert np.median(errs) <= 5e-3, errs
+    assert max(abs_errs) <= 1e-3, abs_errs
