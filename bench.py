@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations timed per step")
     return p.parse_args()
 
@@ -309,6 +310,8 @@ def run_ours(args):
             tot += a.elapsed_time(b)
         plain = {"value": B / (tot / 1e3), "unit": UNIT, "form": "one otm_solve call per density, same kernels"}
 
+    adjoint = None if args.no_adjoint else bench_adjoint(ctx, stream)
+
     peaks = load_peaks()
     cell_iters = args.steps * sum(st.iterations * nn * nn for st, nn in zip(st_list, ns))
     roof = roofline(prof, cell_iters, args.steps, peaks)
@@ -325,7 +328,7 @@ def run_ours(args):
                 "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
                 "iterations": iters, "final_residual_max": max(resid), "gpu_launches": launches,
-                "e2e": e2e, "plain": plain, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "e2e": e2e, "plain": plain, "adjoint": adjoint, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:
@@ -333,6 +336,65 @@ def run_ours(args):
 
         dist.destroy_process_group()
     ctx.close()
+
+
+def bench_adjoint(ctx, stream, n=512, repeats=3):
+    """Cost of the implicit adjoint on the softmax-logits workload (512^2, density =
+    blur(softmax(z)), sigma 8 px): gradient time over the time of one forward iteration."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    _, img = W.softmax_logits(n, 0, sigma_px=8.0)
+    dens = torch.from_numpy(W.to_cells(img)).cuda()
+    V = (n + 1) ** 2
+    fwd = torch.empty((V, 2), dtype=torch.float64, device="cuda")
+    q = torch.randn((V, 2), dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    out = {}
+    grads = {}
+
+    def timed(fn):
+        best = None
+        for _ in range(repeats):
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            r = fn()
+            b.record(stream)
+            b.synchronize()
+            t = a.elapsed_time(b)
+            best = t if best is None else min(best, t)
+        return best, r
+
+    opt = N.default_options()
+    opt.threshold = THRESHOLD
+    st = N.SolveStatsC()
+    ctx.init(n)
+    t_solve, _ = timed(lambda: N.check(N.lib().otm_solve(ctx.handle, n, C.c_void_p(dens.data_ptr()), C.byref(opt),
+                                                         C.c_void_p(fwd.data_ptr()), None, C.byref(st))))
+    per_iter = t_solve / max(st.iterations, 1)
+    for name, mode in (("one_step", N.ADJOINT_ONE_STEP), ("krylov", N.ADJOINT_KRYLOV)):
+        ao = N.AdjointOptionsC()
+        N.lib().otm_default_adjoint_options(C.byref(ao))
+        ao.mode = mode
+        ast = N.AdjointStatsC()
+        g = torch.empty(n * n, dtype=torch.float64, device="cuda")
+        t, _ = timed(lambda: N.check(N.lib().otm_adjoint(ctx.handle, n, C.c_void_p(dens.data_ptr()),
+                                                        C.c_void_p(fwd.data_ptr()), C.c_void_p(q.data_ptr()),
+                                                        C.byref(ao), C.c_void_p(g.data_ptr()), C.byref(ast))))
+        grads[name] = g.double().cpu().numpy()
+        out[name] = {"ms": t, "per_forward_iteration": t / per_iter, "poisson_solves": ast.iterations,
+                     "relative_residual": ast.relative_residual}
+    ref = grads["krylov"]
+    out["one_step"]["relative_error_vs_krylov"] = float(np.linalg.norm(grads["one_step"] - ref) / np.linalg.norm(ref))
+    out.update({"workload": f"{n}^2 blur(softmax(N(0,1) logits)), sigma 8 px; dL/dfwd random",
+                "forward_solve_ms": t_solve, "forward_iterations": st.iterations, "forward_iteration_ms": per_iter})
+    return out
 
 
 def cpu_baseline(density_cells, n):
