@@ -52,6 +52,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--mixed-count", type=int, default=64)
     p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations timed per step")
     return p.parse_args()
 
@@ -311,6 +313,7 @@ def run_ours(args):
         plain = {"value": B / (tot / 1e3), "unit": UNIT, "form": "one otm_solve call per density, same kernels"}
 
     adjoint = None if args.no_adjoint else bench_adjoint(ctx, stream)
+    mixed = None if args.no_mixed else bench_mixed(stream, args.mixed_count)
 
     peaks = load_peaks()
     cell_iters = args.steps * sum(st.iterations * nn * nn for st, nn in zip(st_list, ns))
@@ -328,7 +331,7 @@ def run_ours(args):
                 "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
                 "iterations": iters, "final_residual_max": max(resid), "gpu_launches": launches,
-                "e2e": e2e, "plain": plain, "adjoint": adjoint, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "e2e": e2e, "plain": plain, "adjoint": adjoint, "batched_mixed": mixed, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:
@@ -336,6 +339,82 @@ def run_ours(args):
 
         dist.destroy_process_group()
     ctx.close()
+
+
+def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
+    """Many uneven instances: `count` Gaussian mixtures (4..16 components, floor 1e-3), n
+    drawn log-uniformly from {128, 256, 512, 1024}, residual <= 1e-6. Batched = one
+    otm_solve_batch call (device-side graph loop); plain = one otm_solve call per instance
+    with the host-driven loop. Throughput in 1024^2-equivalent solves/s (sum n^2 / 1024^2)."""
+    import ctypes as C
+
+    import torch
+
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    imgs = W.batched_mixtures(count, seed=11)
+    ns = [im.shape[0] for im in imgs]
+    eq = sum(n * n for n in ns) / 1024.0 ** 2
+    dev = [torch.from_numpy(W.to_cells(im)).cuda() for im in imgs]
+    outs = [torch.empty(((n + 1) ** 2, 2), dtype=torch.float64, device="cuda") for n in ns]
+    opt = N.default_options()
+    opt.threshold = threshold
+    ctx = N.Context(torch.cuda.current_device())
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    for n in sorted(set(ns)):
+        ctx.init(n)
+    stats = (N.SolveStatsC * count)()
+    ns_c = (C.c_int * count)(*ns)
+    dp = (C.c_void_p * count)(*[d.data_ptr() for d in dev])
+    fp = (C.c_void_p * count)(*[f.data_ptr() for f in outs])
+
+    def timed(fn, reps):
+        best = None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            t = a.elapsed_time(b)
+            best = t if best is None else min(best, t)
+        return best
+
+    batch = lambda: N.check(N.lib().otm_solve_batch(ctx.handle, count, ns_c, dp, C.byref(opt), fp, None, stats))
+    batch()  # warm-up: builds the graph
+    l0 = ctx.launch_count()
+    t_batch = timed(batch, repeats)
+    launches = (ctx.launch_count() - l0) // repeats
+    iters = [stats[k].iterations for k in range(count)]
+    ctx_plain = N.Context(torch.cuda.current_device())
+    ctx_plain.set_loop(N.LOOP_HOST)
+    for n in sorted(set(ns)):
+        ctx_plain.init(n)
+    stream_p = torch.cuda.ExternalStream(ctx_plain.stream())
+
+    def plain():
+        for k in range(count):
+            N.check(N.lib().otm_solve(ctx_plain.handle, ns[k], C.c_void_p(dev[k].data_ptr()), C.byref(opt),
+                                      C.c_void_p(outs[k].data_ptr()), None, None))
+
+    plain()
+    torch.cuda.synchronize()
+    t0 = __import__("time").perf_counter()
+    plain()
+    torch.cuda.synchronize()
+    t_plain = 1e3 * (__import__("time").perf_counter() - t0)
+    ctx.close()
+    ctx_plain.close()
+    return {"workload": f"{count} Gaussian mixtures, n log-uniform in {{128,256,512,1024}}, residual <= {threshold:g}",
+            "sizes": {str(n): ns.count(n) for n in sorted(set(ns))}, "equivalent_1024_solves": eq,
+            "batched_ms": t_batch, "batched_value": eq / (t_batch / 1e3), "batched_gpu_launches": launches,
+            "plain_ms": t_plain, "plain_value": eq / (t_plain / 1e3),
+            "unit": "1024^2-equivalent solves/s", "batched_over_plain": t_plain / t_batch,
+            "plain_timing": "host wall clock around 64 sequential otm_solve calls (each synchronous)",
+            "iterations_min_max": [min(iters), max(iters)]}
 
 
 def bench_adjoint(ctx, stream, n=512, repeats=3):

@@ -183,6 +183,15 @@ int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fw
 #define OTM_POISSON_AUTO 0
 #define OTM_POISSON_DENSE 1
 #define OTM_POISSON_FFT 2
+/*   OTM_OPT_LOOP: how the iteration loop is driven.
+ *     OTM_LOOP_GRAPH (default) one CUDA graph launch per solve: the iteration kernels sit
+ *                    in the body of a device-side WHILE node that stops when no instance
+ *                    is active (no host round trip between iterations)
+ *     OTM_LOOP_HOST  kernels launched from the host, loop test read back every 4
+ *                    iterations (used while per-kernel profiling is on) */
+#define OTM_OPT_LOOP 2
+#define OTM_LOOP_GRAPH 0
+#define OTM_LOOP_HOST 1
 int otm_set_option(otm_context* ctx, int key, int value);
 
 /* ---- allocation-free solve (no counterpart in the reference) ----

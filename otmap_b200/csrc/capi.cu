@@ -179,6 +179,14 @@ extern "C" int otm_set_option(otm_context* ctx, int key, int value) {
     ctx->poisson_mode = value;
     return OTM_OK;
   }
+  if (key == OTM_OPT_LOOP) {
+    if (value != OTM_LOOP_GRAPH && value != OTM_LOOP_HOST) {
+      set_error("otm_set_option: unknown loop mode");
+      return OTM_ERR_BAD_ARG;
+    }
+    ctx->loop_mode = value;
+    return OTM_OK;
+  }
   set_error("otm_set_option: unknown option");
   return OTM_ERR_BAD_ARG;
 }

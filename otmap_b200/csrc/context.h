@@ -68,7 +68,16 @@ struct Workspace {
     int n, reg, roff, rcnt, coff, ccnt;
   };
   std::vector<Segment> segments;
+  // the iteration loop captured as a CUDA graph with a device-side WHILE node
+  cudaGraphExec_t graph_exec = nullptr;
+  long graph_body_kernels = 0;
+  DevBuf loopctl;  // LoopCtl (solver.cu)
+  void drop_graph() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec = nullptr;
+  }
   ~Workspace() {
+    drop_graph();
     if (h_pinned) cudaFreeHost(h_pinned);
   }
 };
@@ -101,6 +110,7 @@ struct otm_context {
   int num_sms = 0;
   long launches = 0;  // kernels launched by this context since creation
   int poisson_mode = 0;  // OTM_POISSON_AUTO / _DENSE / _FFT
+  int loop_mode = 0;     // OTM_LOOP_GRAPH (0) / OTM_LOOP_HOST (1)
   otm::Profiler prof;
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   otm::Workspace ws;

@@ -260,17 +260,20 @@ int dct_reg_lines_per_block(int n) {
   }
 }
 
+void dct_reg_attrs(int device) {
+  static bool done[64] = {};
+  if (device < 64 && done[device]) return;
+  RegDct<8, 8>::attrs();
+  RegDct<8, 16>::attrs();
+  RegDct<16, 16>::attrs();
+  RegDct<16, 32>::attrs();
+  RegDct<32, 32>::attrs();
+  if (device < 64) done[device] = true;
+}
+
 void dct_reg_run(otm_context* ctx, int n, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,
                  int coff, int ccnt) {
-  static bool done[64] = {};
-  if (ctx->device < 64 && !done[ctx->device]) {
-    RegDct<8, 8>::attrs();
-    RegDct<8, 16>::attrs();
-    RegDct<16, 16>::attrs();
-    RegDct<16, 32>::attrs();
-    RegDct<32, 32>::attrs();
-    done[ctx->device] = true;
-  }
+  dct_reg_attrs(ctx->device);
   switch (n) {
     case 64: RegDct<8, 8>::run(ctx, d_insts, row_inst, roff, rcnt, col_inst, coff, ccnt); break;
     case 128: RegDct<8, 16>::run(ctx, d_insts, row_inst, roff, rcnt, col_inst, coff, ccnt); break;

@@ -131,6 +131,12 @@ bool dct_reg_supported(int n);
 int dct_reg_lines_per_block(int n);
 void dct_reg_run(otm_context* ctx, int n, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,
                  int coff, int ccnt);
+// Dynamic shared-memory limits of the kernels of each family (set once per device,
+// before any stream capture).
+void sweep_attrs(int device);
+void dct_reg_attrs(int device);
+void poisson_fft_attrs(int device);
+
 // Two-pass stencil sweep of an iteration (stencil.cu).
 int strip_blocks(int n);
 void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);

@@ -192,17 +192,21 @@ __global__ __launch_bounds__(FT) void k_fft_rows_inv(const Inst* insts, const in
   }
 }
 
+static const int smem_rows = padded(FFT_ELEMS) * sizeof(double2);
+static const int smem_cols = padded(FFT_ELEMS) * sizeof(double2) + FFT_ELEMS * sizeof(double);
+
+void poisson_fft_attrs(int device) {
+  static bool attr[64] = {};  // per device ordinal
+  if (device < 64 && attr[device]) return;
+  OTM_CUDA(cudaFuncSetAttribute(k_fft_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
+  OTM_CUDA(cudaFuncSetAttribute(k_fft_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
+  OTM_CUDA(cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cols));
+  if (device < 64) attr[device] = true;
+}
+
 void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int roff, int nrow_items,
                  const int* col_inst, int coff, int ncol_items) {
-  static bool attr[64] = {};  // per device ordinal
-  const int smem_rows = padded(FFT_ELEMS) * sizeof(double2);
-  const int smem_cols = padded(FFT_ELEMS) * sizeof(double2) + FFT_ELEMS * sizeof(double);
-  if (ctx->device < 64 && !attr[ctx->device]) {
-    OTM_CUDA(cudaFuncSetAttribute(k_fft_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
-    OTM_CUDA(cudaFuncSetAttribute(k_fft_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_rows));
-    OTM_CUDA(cudaFuncSetAttribute(k_fft_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_cols));
-    attr[ctx->device] = true;
-  }
+  poisson_fft_attrs(ctx->device);
   if (nrow_items <= 0) return;
   launch_smem(ctx, "fft_rows_fwd", k_fft_rows_fwd, nrow_items, FT, smem_rows, (const Inst*)d_insts, row_inst, roff);
   launch_smem(ctx, "fft_cols", k_fft_cols, ncol_items, FT, smem_cols, (const Inst*)d_insts, col_inst, coff);

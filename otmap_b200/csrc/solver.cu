@@ -590,6 +590,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
   }
   bool same = ws.sizes == sizes && ws.mode == ctx->poisson_mode;
   if (!same) {
+    ws.drop_graph();
     ws.insts.reserve(sizeof(Inst) * count);
     ws.tile_inst.reserve(sizeof(int) * tiles);
     ws.gemm_inst.reserve(sizeof(int) * (gemm > 0 ? gemm : 1));
@@ -666,6 +667,90 @@ void dense_poisson(otm_context* ctx, Inst* d_inst, const int* gemm_inst, int G) 
   for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_inst, gemm_inst, s, 1);
 }
 
+// Bound on the device-side loop: the WHILE node stops after `cap` bodies whatever the
+// instances report, and flags it.
+struct LoopCtl {
+  unsigned int count, cap;
+  int error, pad;
+};
+
+// Body tail of the graph loop: continue while any instance is active.
+__global__ void k_loop_check(const Inst* insts, int count, LoopCtl* ctl, cudaGraphConditionalHandle h) {
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int q = threadIdx.x; q < count; q += blockDim.x)
+    if (insts[q].active) any = 1;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned int c = ++ctl->count;
+    unsigned int go = any && c < ctl->cap;
+    if (any && !(c < ctl->cap)) ctl->error = 1;
+    cudaGraphSetConditional(h, go);
+  }
+}
+
+// Launches one iteration of every active instance (Poisson solve + the two sweeps).
+static void launch_iteration(otm_context* ctx, Inst* d_insts) {
+  Workspace& ws = ctx->ws;
+  const int G = ws.total_gemm;
+  if (G > 0)
+    for (int s = 0; s < 4; ++s)
+      launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, ws.gemm_inst.as<int>(), s, 1);
+  for (const auto& sg : ws.segments) {
+    if (sg.reg)
+      dct_reg_run(ctx, sg.n, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff,
+                  sg.ccnt);
+    else
+      poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff, sg.ccnt);
+  }
+  sweep_sums(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
+  sweep_update(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
+}
+
+// Captures the iteration loop of the current workspace into a graph with a WHILE node.
+static void build_loop_graph(otm_context* ctx, int count) {
+  Workspace& ws = ctx->ws;
+  cudaStream_t st = ctx->stream;
+  sweep_attrs(ctx->device);
+  dct_reg_attrs(ctx->device);
+  poisson_fft_attrs(ctx->device);
+  ws.loopctl.reserve(sizeof(LoopCtl));
+  cudaGraph_t g = nullptr;
+  OTM_CUDA(cudaGraphCreate(&g, 0));
+  try {
+    cudaGraphConditionalHandle handle;
+    OTM_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    OTM_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &params));
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    const long before = ctx->launches;
+    OTM_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+      launch_iteration(ctx, ws.insts.as<Inst>());
+      launch(ctx, "loop_check", k_loop_check, 1, 256, (const Inst*)ws.insts.as<Inst>(), count,
+             ws.loopctl.as<LoopCtl>(), handle);
+    } catch (...) {
+      cudaGraph_t dummy;
+      cudaStreamEndCapture(st, &dummy);
+      throw;
+    }
+    OTM_CUDA(cudaStreamEndCapture(st, &body));
+    ws.graph_body_kernels = ctx->launches - before;
+    ctx->launches = before;  // captured, not executed
+    OTM_CUDA(cudaGraphInstantiate(&ws.graph_exec, g, 0));
+  } catch (...) {
+    cudaGraphDestroy(g);
+    throw;
+  }
+  cudaGraphDestroy(g);
+}
+
 // Runs the whole solve for `count` instances whose raw densities have been copied
 // into their rho buffers. Host-side copies of the final records are returned.
 static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, const otm_solver_options& o) {
@@ -686,9 +771,8 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
   Inst* d_insts = ws.insts.as<Inst>();
   OTM_CUDA(cudaMemcpyAsync(d_insts, h.data(), sizeof(Inst) * count, cudaMemcpyHostToDevice, st));
   const int* ti = ws.tile_inst.as<int>();
-  const int* gi = ws.gemm_inst.as<int>();
   double* part = ws.partials.as<double>();
-  const int T = ws.total_tiles, G = ws.total_gemm;
+  const int T = ws.total_tiles;
 
   launch(ctx, "density_sum", k_density_sum, T, NT, d_insts, ti, part);
   launch(ctx, "density_scale", k_density_scale, T, NT, d_insts, ti, part);
@@ -697,30 +781,29 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
   OTM_CUDA(cudaGetLastError());
 
   Inst* hp = static_cast<Inst*>(ws.h_pinned);
-  int launched = 0;
-  const int chunk = 4;
-  while (true) {
+  if (ctx->loop_mode == OTM_LOOP_GRAPH && !ctx->prof.on) {
+    if (!ws.graph_exec) build_loop_graph(ctx, count);
+    LoopCtl c = {0u, (unsigned int)o.max_iter + 2u, 0, 0};
+    OTM_CUDA(cudaMemcpyAsync(ws.loopctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaGraphLaunch(ws.graph_exec, st));
     OTM_CUDA(cudaMemcpyAsync(hp, d_insts, sizeof(Inst) * count, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaMemcpyAsync(&c, ws.loopctl.p, sizeof(c), cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
-    ctx->prof.flush();
-    bool any = false;
-    for (int q = 0; q < count; ++q) any |= hp[q].active != 0;
-    if (!any || launched >= o.max_iter) break;
-    for (int c = 0; c < chunk && launched < o.max_iter; ++c, ++launched) {
-      if (G > 0)
-        for (int s = 0; s < 4; ++s) launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, gi, s, 1);
-      for (const auto& sg : ws.segments) {
-        if (sg.reg)
-          dct_reg_run(ctx, sg.n, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff,
-                      sg.ccnt);
-        else
-          poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff,
-                      sg.ccnt);
-      }
-      sweep_sums(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
-      sweep_update(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
+    ctx->launches += ws.graph_body_kernels * (long)c.count;
+    if (c.error) throw CudaError{cudaErrorLaunchTimeout, "device loop exceeded its iteration bound"};
+  } else {
+    int launched = 0;
+    const int chunk = 4;
+    while (true) {
+      OTM_CUDA(cudaMemcpyAsync(hp, d_insts, sizeof(Inst) * count, cudaMemcpyDeviceToHost, st));
+      OTM_CUDA(cudaStreamSynchronize(st));
+      ctx->prof.flush();
+      bool any = false;
+      for (int q = 0; q < count; ++q) any |= hp[q].active != 0;
+      if (!any || launched >= o.max_iter) break;
+      for (int c = 0; c < chunk && launched < o.max_iter; ++c, ++launched) launch_iteration(ctx, d_insts);
+      OTM_CUDA(cudaGetLastError());
     }
-    OTM_CUDA(cudaGetLastError());
   }
   std::vector<Inst> out(hp, hp + count);
   return out;

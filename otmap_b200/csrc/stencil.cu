@@ -388,7 +388,7 @@ int strip_blocks(int n) {
   return (strips + SWARPS - 1) / SWARPS;
 }
 
-static void sweep_attrs(int device) {
+void sweep_attrs(int device) {
   static bool done[64] = {};
   if (device < 64 && done[device]) return;
   OTM_CUDA(cudaFuncSetAttribute(k_sweep_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,

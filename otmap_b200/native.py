@@ -25,6 +25,8 @@ ERR_NOT_INIT = -5
 CONVERGED, MAX_ITER, SMALL_STEP, NONFINITE = 0, 1, 2, 3
 OPT_POISSON = 1
 POISSON_AUTO, POISSON_DENSE, POISSON_FFT = 0, 1, 2
+OPT_LOOP = 2
+LOOP_GRAPH, LOOP_HOST = 0, 1
 OUTCOMES = {CONVERGED: "converged", MAX_ITER: "max_iter", SMALL_STEP: "small_step", NONFINITE: "nonfinite"}
 
 _dp = C.POINTER(C.c_double)
@@ -158,6 +160,9 @@ class Context:
 
     def set_poisson(self, mode: int):
         check(lib().otm_set_option(self._h, OPT_POISSON, int(mode)))
+
+    def set_loop(self, mode: int):
+        check(lib().otm_set_option(self._h, OPT_LOOP, int(mode)))
 
     def stream(self) -> int:
         s = C.c_void_p()

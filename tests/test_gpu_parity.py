@@ -172,3 +172,25 @@ def test_mixed_batch_uses_both_transforms(ot):
         single = s.solve(W.to_cells(img))
         assert m.stats.iterations == single.stats.iterations
         assert np.array_equal(m.fwd_mesh(), single.fwd_mesh())
+
+
+def test_graph_loop_matches_host_loop(ot):
+    """The device-side loop (one CUDA graph launch, WHILE node) and the host-driven loop
+    run the same kernels: identical iterations and forward meshes; the graph is reused
+    for a second batch of the same sizes and rebuilt for new sizes."""
+    from otmap_b200 import native
+    from otmap_b200 import workloads as W
+
+    batches = [[W.gaussian_mixture(n, 300 + k) for k, n in enumerate([64, 128, 40, 256])],
+               [W.gaussian_mixture(n, 400 + k) for k, n in enumerate([64, 128, 40, 256])],
+               [W.gaussian_mixture(n, 500 + k) for k, n in enumerate([32, 512])]]
+    results = {}
+    for mode in (native.LOOP_GRAPH, native.LOOP_HOST):
+        ctx = native.Context(0)
+        ctx.set_loop(mode)
+        results[mode] = [ot.solve_batch(b, context=ctx) for b in batches]
+    for bg, bh in zip(results[native.LOOP_GRAPH], results[native.LOOP_HOST]):
+        for mg, mh in zip(bg, bh):
+            assert mg.stats.iterations == mh.stats.iterations
+            assert mg.stats.outcome == mh.stats.outcome
+            assert np.array_equal(mg.fwd_mesh(), mh.fwd_mesh())
