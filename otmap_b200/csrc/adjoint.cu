@@ -157,6 +157,11 @@ __global__ void k_adj_scale(long N, double* v, double a) {
   if (f < N) v[f] *= a;
 }
 
+__global__ void k_adj_neg(long N, const double* z, double* lambda) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < N) lambda[f] = -z[f];
+}
+
 __global__ void k_adj_add(long N, const double* z, double* lambda) {
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f < N) lambda[f] += z[f];
@@ -168,95 +173,125 @@ __global__ void k_adj_axpy(long N, const double* z, double* lambda) {
   if (f < N) lambda[f] -= z[f];
 }
 
-// dL/drho = (lambda - (lambda . rho) / S) / S, from partial sums of lambda . rho and rho
-__global__ void k_adj_dot_rho(long N, const double* lambda, const double* rho, double* partial) {
+// sums[0] = lambda . rho, sums[1] = sum rho, reduced in a fixed order by one block
+__global__ void k_adj_rho_sums(long N, const double* lambda, const double* rho, double* sums) {
   __shared__ double red[64];
   double v[2] = {0.0, 0.0};
-  for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x) {
-    v[0] += lambda[f] * rho[f];
+  for (long f = threadIdx.x; f < N; f += blockDim.x) {
+    v[0] = fma(lambda[f], rho[f], v[0]);
     v[1] += rho[f];
   }
   block_sum<2>(v, red);
   if (threadIdx.x == 0) {
-    partial[2 * blockIdx.x] = v[0];
-    partial[2 * blockIdx.x + 1] = v[1];
+    sums[0] = v[0];
+    sums[1] = v[1];
   }
 }
 
-__global__ void k_adj_finish(long N, const double* lambda, double lr, double S, double* out) {
+__global__ void k_adj_finish(long N, const double* lambda, const double* sums, double* out) {
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (f < N) out[f] = (lambda[f] - lr / S) / S;
+  if (f < N) out[f] = (lambda[f] - sums[0] / sums[1]) / sums[1];
 }
 
 }  // namespace otm
 
 using namespace otm;
 
-namespace {
-
-// Poisson solve d = M^+ src (cosine transform) on the context's stream, using a
-// one-instance record whose buffers point at src / dst / two temporaries.
-struct PoissonRunner {
-  otm_context* ctx;
-  int n;
-  DevBuf rec, lists;
-  Inst h;
-  int G = 0, rows = 0, cols = 0, reg = 0;
-  PoissonRunner(otm_context* c, int n_, double* t1, double* t2) : ctx(c), n(n_) {
-    SizeTables* T = ctx->tables.at(n).get();
-    std::memset(&h, 0, sizeof(h));
-    h.n = n;
-    h.active = 1;
-    h.t1 = t1;
-    h.t2 = t2;
-    h.C = T->C.as<double>();
-    h.cosk = T->cosk.as<double>();
-    h.tw = T->tw.as<double2>();
-    h.pt = T->pt.as<double2>();
-    h.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
-    std::vector<int> zeros;
-    if (h.fft) {
-      int lg = 0;
-      while ((1 << lg) < n) ++lg;
-      h.logn = lg;
-      reg = dct_reg_supported(n) ? 1 : 0;
-      const int per = reg ? dct_reg_lines_per_block(n) : fft_lines(n);
-      h.nrow = h.ncol = n / per;
-      rows = cols = h.nrow;
-      zeros.assign(rows, 0);
-    } else {
-      int t = (n + 63) / 64;
-      h.ngemm = G = t * t;
-      zeros.assign(G, 0);
-    }
-    rec.reserve(sizeof(Inst));
-    lists.reserve(sizeof(int) * zeros.size());
-    OTM_CUDA(cudaMemcpyAsync(lists.p, zeros.data(), sizeof(int) * zeros.size(), cudaMemcpyHostToDevice, ctx->stream));
-  }
-  void run(const double* src, double* dst);
-};
-
-}  // namespace
-
-// Poisson launches for the adjoint reuse the forward kernels (declared in solver.cu / poisson.cu).
 namespace otm {
 void dense_poisson(otm_context* ctx, Inst* d_inst, const int* gemm_inst, int G);
+
+// Adjoint workspace of one grid size, kept by the context: device vectors, the Krylov
+// basis and one Poisson record per (source, destination) pair the solver uses, so a call
+// allocates nothing and uploads nothing but its inputs' pointers.
+struct AdjointWs : otm_context::Erased {
+  int n = 0, m = 0;
+  size_t N = 0, V = 0, ld = 0;
+  DevBuf buf, recs, lists;
+  double *b, *lam, *z, *h, *t1, *t2, *Vb, *c, *part, *sums;
+  int G = 0, rows = 0, cols = 0, reg = 0, fft = 0;
+  // record k: src = basis vector k (k < m+1); record m+1: src = b; record m+2: src = h; dst = z
+  Inst* rec(int k) { return recs.as<Inst>() + k; }
+};
+
+static AdjointWs* adjoint_ws(otm_context* ctx, int n, int m) {
+  auto& slot = ctx->adjoint[n];
+  if (slot && static_cast<AdjointWs*>(slot.get())->m >= m) return static_cast<AdjointWs*>(slot.get());
+  auto* W = new AdjointWs;
+  W->n = n;
+  W->m = m;
+  W->N = (size_t)n * n;
+  W->V = (size_t)(n + 1) * (n + 1);
+  W->ld = (W->N + 31) / 32 * 32;
+  const int nred = 256;
+  const size_t words = W->ld * 6 + 2 * W->V + (size_t)(m + 1) * W->ld + (m + 2) + (size_t)nred * (m + 2) + 64;
+  W->buf.reserve(sizeof(double) * words);
+  double* p = W->buf.as<double>();
+  W->b = p; p += W->ld;
+  W->lam = p; p += W->ld;
+  W->z = p; p += W->ld;
+  W->t1 = p; p += W->ld;
+  W->t2 = p; p += W->ld;
+  W->h = p; p += 2 * W->V + W->ld;
+  W->Vb = p; p += (size_t)(m + 1) * W->ld;
+  W->c = p; p += m + 2;
+  W->sums = p; p += 2;
+  W->part = p;
+  SizeTables* T = ctx->tables.at(n).get();
+  Inst base;
+  std::memset(&base, 0, sizeof(base));
+  base.n = n;
+  base.active = 1;
+  base.t1 = W->t1;
+  base.t2 = W->t2;
+  base.C = T->C.as<double>();
+  base.cosk = T->cosk.as<double>();
+  base.tw = T->tw.as<double2>();
+  base.pt = T->pt.as<double2>();
+  base.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
+  W->fft = base.fft;
+  int items;
+  if (base.fft) {
+    int lg = 0;
+    while ((1 << lg) < n) ++lg;
+    base.logn = lg;
+    W->reg = dct_reg_supported(n) ? 1 : 0;
+    const int per = W->reg ? dct_reg_lines_per_block(n) : fft_lines(n);
+    base.nrow = base.ncol = n / per;
+    W->rows = W->cols = items = base.nrow;
+  } else {
+    int t = (n + 63) / 64;
+    base.ngemm = W->G = items = t * t;
+  }
+  std::vector<Inst> recs(m + 3, base);
+  for (int k = 0; k <= m; ++k) recs[k].r[0] = W->Vb + (size_t)k * W->ld;
+  recs[m + 1].r[0] = W->b;
+  recs[m + 2].r[0] = W->h;
+  for (auto& r : recs) r.dhat = W->z;
+  W->recs.reserve(sizeof(Inst) * recs.size());
+  W->lists.reserve(sizeof(int) * items);
+  std::vector<int> zeros(items, 0);
+  OTM_CUDA(cudaMemcpyAsync(W->recs.p, recs.data(), sizeof(Inst) * recs.size(), cudaMemcpyHostToDevice, ctx->stream));
+  OTM_CUDA(cudaMemcpyAsync(W->lists.p, zeros.data(), sizeof(int) * items, cudaMemcpyHostToDevice, ctx->stream));
+  OTM_CUDA(cudaStreamSynchronize(ctx->stream));
+  slot.reset(W);
+  return W;
 }
 
-void PoissonRunner::run(const double* src, double* dst) {
-  h.r[0] = const_cast<double*>(src);
-  h.dhat = dst;
-  OTM_CUDA(cudaMemcpyAsync(rec.p, &h, sizeof(Inst), cudaMemcpyHostToDevice, ctx->stream));
-  Inst* d = rec.as<Inst>();
-  if (h.fft) {
-    if (reg)
-      dct_reg_run(ctx, n, d, lists.as<int>(), 0, rows, lists.as<int>(), 0, cols);
+// z = M^+ (source of record k)
+static void poisson_rec(otm_context* ctx, AdjointWs* W, int k) {
+  Inst* d = W->rec(k);
+  const int* L = W->lists.as<int>();
+  if (W->fft) {
+    if (W->reg)
+      dct_reg_run(ctx, W->n, d, L, 0, W->rows, L, 0, W->cols);
     else
-      poisson_fft(ctx, d, lists.as<int>(), 0, rows, lists.as<int>(), 0, cols);
+      poisson_fft(ctx, d, L, 0, W->rows, L, 0, W->cols);
   } else {
-    dense_poisson(ctx, d, lists.as<int>(), G);
+    dense_poisson(ctx, d, L, W->G);
   }
 }
+
+}  // namespace otm
 
 extern "C" void otm_default_adjoint_options(otm_adjoint_options* o) {
   if (!o) return;
@@ -279,38 +314,34 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     make_current(ctx);
     if (otm_init(ctx, n) != OTM_OK) throw BadArg{std::string("otm_adjoint: ") + otm_last_error()};
     cudaStream_t st = ctx->stream;
-    const size_t N = (size_t)n * n, V = (size_t)(n + 1) * (n + 1);
-    const int RB = 256;
-    const int nred = 256;
     const int m = o.mode == OTM_ADJOINT_KRYLOV ? std::max(1, std::min(o.restart, 200)) : 1;
-    const size_t ld = (N + 31) / 32 * 32;
-    // device scratch: fwd, q, rho, b, lambda, z, h, t1, t2, basis (m+1), coefficients, partials
-    const size_t words = 2 * V + 2 * V + N + N + N + N + 2 * V + N + N + (size_t)(m + 1) * ld + (m + 2) +
-                         (size_t)nred * (m + 2) + 64;
-    DevBuf buf;
-    buf.reserve(sizeof(double) * words);
-    double* p = buf.as<double>();
-    double* d_fwd = p; p += 2 * V;
-    double* d_q = p; p += 2 * V;
-    double* d_rho = p; p += N;
-    double* d_b = p; p += N;
-    double* d_lam = p; p += N;
-    double* d_z = p; p += N;
-    double* d_h = p; p += 2 * V;
-    double* d_t1 = p; p += N;
-    double* d_t2 = p; p += N;
-    double* d_V = p; p += (size_t)(m + 1) * ld;
-    double* d_c = p; p += m + 2;
-    double* d_part = p;
-    copy_in(ctx, d_fwd, fwd_xy, sizeof(double) * 2 * V);
-    copy_in(ctx, d_q, grad_fwd, sizeof(double) * 2 * V);
-    copy_in(ctx, d_rho, density, sizeof(double) * N);
+    AdjointWs* W = adjoint_ws(ctx, n, m);
+    const size_t N = W->N, V = W->V, ld = W->ld;
+    const int RB = 256, nred = 256;
+    // inputs: used in place when they are device memory, else staged into the workspace
+    auto stage = [&](const double* src, double* tmp, size_t words) -> const double* {
+      if (is_device_ptr(src)) return src;
+      copy_in(ctx, tmp, src, sizeof(double) * words);
+      return tmp;
+    };
+    if (!is_device_ptr(fwd_xy) || !is_device_ptr(grad_fwd) || !is_device_ptr(density)) {
+      ctx->staging.reserve(sizeof(double) * (4 * V + N));
+    }
+    double* stg = ctx->staging.as<double>();
+    const double* d_fwd = stage(fwd_xy, stg, 2 * V);
+    const double* d_q = stage(grad_fwd, stg + 2 * V, 2 * V);
+    const double* d_rho = stage(density, stg + 4 * V, N);
     const unsigned gN = (unsigned)((N + RB - 1) / RB), gV = (unsigned)((V + RB - 1) / RB);
+    double* d_b = W->b;
+    double* d_lam = W->lam;
+    double* d_z = W->z;
+    double* d_h = W->h;
+    double* d_V = W->Vb;
+    double* d_c = W->c;
+    double* d_part = W->part;
     // b = G^T q
-    launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_q, 1.0, (const double*)nullptr, d_b);
-    PoissonRunner P(ctx, n, d_t1, d_t2);
+    launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, d_q, 1.0, (const double*)nullptr, d_b);
     std::vector<double> hp;
-    // dots of w against the first k basis vectors and w.w, summed on the host in block order
     auto multidot = [&](const double* w, int k, std::vector<double>& out) {
       launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, w, (const double*)d_V, (long)ld, k, d_part);
       hp.resize((size_t)nred * (k + 1));
@@ -320,25 +351,25 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
       for (int blk = 0; blk < nred; ++blk)
         for (int i = 0; i <= k; ++i) out[i] += hp[(size_t)blk * (k + 1) + i];
     };
-    // J^T applied to x (cells), into out
     auto apply_jt = [&](const double* x, double* out) {
-      launch(ctx, "adj_vertex", k_adj_vertex, gV, RB, n, (const double*)d_fwd, x, d_h);
+      launch(ctx, "adj_vertex", k_adj_vertex, gV, RB, n, d_fwd, x, d_h);
       launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_h, 1.0, (const double*)nullptr, out);
     };
-    OTM_CUDA(cudaMemsetAsync(d_lam, 0, sizeof(double) * N, st));
     int solves = 0;
     double rel = -1.0;
     if (o.mode == OTM_ADJOINT_ONE_STEP) {
-      // lambda = -M^+ b
-      P.run(d_b, d_z);
+      // lambda = -M^+ b: the solve writes z, lambda = -z
+      poisson_rec(ctx, W, W->m + 1);
       ++solves;
-      launch(ctx, "adj_axpy", k_adj_axpy, gN, RB, (long)N, (const double*)d_z, d_lam);
+      launch(ctx, "adj_scale", k_adj_neg, gN, RB, (long)N, (const double*)d_z, d_lam);
     } else {
+      OTM_CUDA(cudaMemsetAsync(d_lam, 0, sizeof(double) * N, st));
       // Restarted GMRES(m) on J^T lambda = b, right-preconditioned: J^T M^+ y = b, lambda = M^+ y.
       // Classical Gram-Schmidt applied twice; Givens rotations and the small triangular
       // solve on the host.
       std::vector<double> dots;
-      multidot(d_b, 0, dots);
+      OTM_CUDA(cudaMemcpyAsync(d_V, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+      multidot(d_V, 0, dots);
       const double bnorm = std::sqrt(dots[0]);
       std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m);
       auto Hs = [&](int i, int j) -> double& { return H[(size_t)i * m + j]; };
@@ -348,7 +379,6 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
         double* v0 = d_V;
         double rnorm;
         if (first) {
-          OTM_CUDA(cudaMemcpyAsync(v0, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
           rnorm = bnorm;
           first = false;
         } else {
@@ -364,9 +394,8 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
         gv[0] = rnorm;
         int k = 0;
         for (int j = 0; j < m && solves < o.max_iter; ++j) {
-          double* vj = d_V + (size_t)j * ld;
           double* w = d_V + (size_t)(j + 1) * ld;
-          P.run(vj, d_z);
+          poisson_rec(ctx, W, j);  // z = M^+ v_j
           ++solves;
           apply_jt(d_z, w);
           for (int pass = 0; pass < 2; ++pass) {
@@ -404,24 +433,16 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
         OTM_CUDA(cudaMemcpyAsync(d_c, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
         launch(ctx, "adj_span", k_adj_span, gN, RB, (long)N, d_h, (const double*)d_V, (long)ld, k,
                (const double*)d_c);
-        P.run(d_h, d_z);
+        poisson_rec(ctx, W, W->m + 2);  // z = M^+ h
         ++solves;
         launch(ctx, "adj_add", k_adj_add, gN, RB, (long)N, (const double*)d_z, d_lam);
       }
     }
-    // chain through the density normalisation
-    launch(ctx, "adj_dot", k_adj_dot_rho, nred, RB, (long)N, (const double*)d_lam, (const double*)d_rho, d_part);
-    hp.assign(2 * nred, 0.0);
-    OTM_CUDA(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * 2 * nred, cudaMemcpyDeviceToHost, st));
-    OTM_CUDA(cudaStreamSynchronize(st));
-    double lr = 0.0, S = 0.0;
-    for (int k = 0; k < nred; ++k) {
-      lr += hp[2 * k];
-      S += hp[2 * k + 1];
-    }
+    // chain through the density normalisation, reduced and applied on the device
+    launch(ctx, "adj_rho_sums", k_adj_rho_sums, 1, 1024, (long)N, (const double*)d_lam, d_rho, W->sums);
     bool odev = is_device_ptr(grad_density);
     double* out = odev ? grad_density : d_z;
-    launch(ctx, "adj_finish", k_adj_finish, gN, RB, (long)N, (const double*)d_lam, lr, S, out);
+    launch(ctx, "adj_finish", k_adj_finish, gN, RB, (long)N, (const double*)d_lam, (const double*)W->sums, out);
     OTM_CUDA(cudaGetLastError());
     if (!odev) copy_out(ctx, grad_density, out, sizeof(double) * N);
     OTM_CUDA(cudaStreamSynchronize(st));

@@ -115,6 +115,11 @@ struct otm_context {
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   otm::Workspace ws;
   otm::DevBuf staging;  // device staging for host inputs/outputs
+  // adjoint workspaces per grid size (adjoint.cu); type-erased to keep this header small
+  struct Erased {
+    virtual ~Erased() = default;
+  };
+  std::map<int, std::unique_ptr<Erased>> adjoint;
 };
 
 struct otm_map {
