@@ -256,8 +256,12 @@ static AdjointWs* adjoint_ws(otm_context* ctx, int n, int m) {
     base.logn = lg;
     W->reg = dct_reg_supported(n) ? 1 : 0;
     const int per = W->reg ? dct_reg_lines_per_block(n) : fft_lines(n);
-    base.nrow = base.ncol = n / per;
-    W->rows = W->cols = items = base.nrow;
+    const int cper = W->reg ? dct_reg_cols_per_block(n) : fft_lines(n);
+    base.nrow = n / per;
+    base.ncol = n / cper;
+    W->rows = base.nrow;
+    W->cols = base.ncol;
+    items = std::max(W->rows, W->cols);
   } else {
     int t = (n + 63) / 64;
     base.ngemm = W->G = items = t * t;

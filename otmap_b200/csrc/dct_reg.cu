@@ -174,55 +174,105 @@ __global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_inv(const Inst* insts, 
       [&](int m, double2 v) { x[makhoul_src(m, n)] = v.x; });
 }
 
-// CB columns per block; the tile holds them (n rows x (CB + 1) doubles).
+// Column pass, lanes across columns: a block owns CB consecutive columns. Thread
+// (c = tid % CB, s = tid / CB) holds, for column l0 + c, the samples N2*m1 + s (s < N2) of
+// step 1 -- loaded straight from global memory, CB consecutive doubles per row -- and the
+// outputs k1 = s (s < N1) of step 4. One shared region (n x CB doubles plus a pad per k1
+// row) serves in turn as the step-3 transpose buffer, the exchange tile for the DCT-III
+// pairs (k, n - k) and the staging tile of the coalesced store.
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32, 2) void k_dct_cols(const Inst* insts, const int* col_inst, int seg) {
-  constexpr int n = N1 * N2, LPW = 32 / N2, CB = RW * LPW, TS = CB + 1;
+struct ColGeom {
+  static constexpr int n = N1 * N2;
+  static constexpr int CB = 256 / N2;  // columns per block (256 threads)
+  static constexpr int KS = N2 * CB + 1;  // padded stride of a k1 row of the transpose buffer
+  static constexpr int SMEM = (N1 * KS > n * CB ? N1 * KS : n * CB);  // doubles
+};
+
+template <int N1, int N2>
+__device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)[N2], double* sh, int c, int s,
+                                                  const double2* __restrict__ tw, bool conj) {
+  using GG = ColGeom<N1, N2>;
+  constexpr int n = GG::n, CB = GG::CB, KS = GG::KS;
+  fft_reg<N1>(v, tw, n, conj);
+#pragma unroll
+  for (int r = 0; r < N1; ++r) {
+    const int k1 = rbrev<N1>(r);
+    if (k1 != 0) v[r] = cmul(v[r], twid(tw, s * k1, n, conj));
+  }
+#pragma unroll
+  for (int part = 0; part < 2; ++part) {
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < N1; ++r) sh[rbrev<N1>(r) * KS + s * CB + c] = part ? v[r].y : v[r].x;
+    __syncthreads();
+    if (s < N1) {
+#pragma unroll
+      for (int m2 = 0; m2 < N2; ++m2) {
+        const double x = sh[s * KS + m2 * CB + c];
+        if (part)
+          u[m2].y = x;
+        else
+          u[m2].x = x;
+      }
+    }
+  }
+  if (s < N1) fft_reg<N2>(u, tw, n, conj);
+}
+
+template <int N1, int N2>
+__global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const int* col_inst, int seg) {
+  using GG = ColGeom<N1, N2>;
+  constexpr int n = GG::n, CB = GG::CB;
   extern __shared__ double sbuf[];
-  double* tile = sbuf + CB * N1 * (N2 + 1);
   const int item = seg + blockIdx.x;
   const Inst& I = insts[col_inst[item]];
   if (!I.active) return;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
-  const int c = warp * LPW + sub;  // this line's column within the block
-  const int l0 = (item - I.col0) * CB;
-  double* buf = sbuf + c * N1 * (N2 + 1);
+  const int c = threadIdx.x % CB, s = threadIdx.x / CB;
+  const int l0 = (item - I.col0) * CB, l = l0 + c;
   double* T = I.t1;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
-  for (int e = threadIdx.x; e < n * CB; e += RW * 32) {
-    int i = e / CB, cc = e - i * CB;
-    tile[i * TS + cc] = T[(size_t)i * n + l0 + cc];
+  const double cl = I.cosk[l];
+  double2 v[N1];
+  double2 u[N2];
+  // forward DCT-II along the column
+#pragma unroll
+  for (int m1 = 0; m1 < N1; ++m1) v[m1] = make_double2(T[(size_t)makhoul_src(N2 * m1 + s, n) * n + l], 0.0);
+  col_fft_transpose<N1, N2>(v, u, sbuf, c, s, tw, false);
+  __syncthreads();
+  if (s < N1) {
+    // coefficient k = s + N1 k2: divide by lambda_kl, keep s_k U_k in the exchange tile [k][c]
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int k = s + N1 * rbrev<N2>(r);
+      const double sk = dct_s(k, n);
+      const double X = post2(u[r], __ldg(&pt[k]), sk);
+      const double lam = 2.0 - 2.0 * I.cosk[k] * cl;
+      const double U = (k == 0 && l == 0) ? 0.0 : X / lam;
+      sbuf[k * CB + c] = sk * U;
+    }
   }
   __syncthreads();
-  const int l = l0 + c;
-  const double cl = I.cosk[l];
-  // forward DCT-II along the column, divide by lambda, keep s_k * U_k in the tile
-  fft_line<N1, N2>(
-      t, buf, tw, false, [&](int m1) { return make_double2(tile[makhoul_src(N2 * m1 + t, n) * TS + c], 0.0); },
-      [&](int k, double2 V) {
-        const double sk = dct_s(k, n);
-        const double X = post2(V, __ldg(&pt[k]), sk);
-        const double lam = 2.0 - 2.0 * I.cosk[k] * cl;
-        const double U = (k == 0 && l == 0) ? 0.0 : X / lam;
-        tile[k * TS + c] = sk * U;  // column c only: this line's step-1 reads are done
-      });
+  // inverse DCT-III along the column
+#pragma unroll
+  for (int m1 = 0; m1 < N1; ++m1) {
+    const int k = N2 * m1 + s;
+    const double a = sbuf[k * CB + c], b = k == 0 ? 0.0 : sbuf[(n - k) * CB + c];
+    v[m1] = pre3(k, a, b, __ldg(&pt[k]));
+  }
+  col_fft_transpose<N1, N2>(v, u, sbuf, c, s, tw, true);
   __syncthreads();
-  __syncwarp();
-  // inverse DCT-III along the column: step 1 reads this column's s_k U_k from the tile;
-  // its outputs overwrite the column only after every lane of the line is past step 1
-  fft_line<N1, N2>(
-      t, buf, tw, true,
-      [&](int m1) {
-        const int k = N2 * m1 + t;
-        const double a = tile[k * TS + c], b = k == 0 ? 0.0 : tile[(n - k) * TS + c];
-        return pre3(k, a, b, __ldg(&pt[k]));
-      },
-      [&](int m, double2 v) { tile[makhoul_src(m, n) * TS + c] = v.x; });
+  if (s < N1) {
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int m = s + N1 * rbrev<N2>(r);
+      sbuf[makhoul_src(m, n) * CB + c] = u[r].x;
+    }
+  }
   __syncthreads();
-  for (int e = threadIdx.x; e < n * CB; e += RW * 32) {
-    int i = e / CB, cc = e - i * CB;
-    T[(size_t)i * n + l0 + cc] = tile[i * TS + cc];
+  for (int e = threadIdx.x; e < n * CB; e += 256) {
+    const int i = e / CB, cc = e - i * CB;
+    T[(size_t)i * n + l0 + cc] = sbuf[i * CB + cc];
   }
 }
 
@@ -230,7 +280,8 @@ template <int N1, int N2>
 struct RegDct {
   static constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
   static size_t rows_smem() { return sizeof(double) * LPB * N1 * (N2 + 1); }
-  static size_t cols_smem() { return rows_smem() + sizeof(double) * n * (LPB + 1); }
+  static size_t cols_smem() { return sizeof(double) * ColGeom<N1, N2>::SMEM; }
+  static constexpr int CB = ColGeom<N1, N2>::CB;
   static void attrs() {
     OTM_CUDA(cudaFuncSetAttribute(k_dct_rows_fwd<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)rows_smem()));
@@ -241,7 +292,7 @@ struct RegDct {
   }
   static void run(otm_context* ctx, Inst* d, const int* ri, int roff, int rcnt, const int* ci, int coff, int ccnt) {
     launch_smem(ctx, "dct_rows_fwd", k_dct_rows_fwd<N1, N2>, rcnt, RW * 32, rows_smem(), (const Inst*)d, ri, roff);
-    launch_smem(ctx, "dct_cols", k_dct_cols<N1, N2>, ccnt, RW * 32, cols_smem(), (const Inst*)d, ci, coff);
+    launch_smem(ctx, "dct_cols", k_dct_cols<N1, N2>, ccnt, 256, cols_smem(), (const Inst*)d, ci, coff);
     launch_smem(ctx, "dct_rows_inv", k_dct_rows_inv<N1, N2>, rcnt, RW * 32, rows_smem(), (const Inst*)d, ri, roff);
   }
 };
@@ -257,6 +308,16 @@ int dct_reg_lines_per_block(int n) {
     case 256: return RegDct<16, 16>::LPB;
     case 512: return RegDct<16, 32>::LPB;
     default: return RegDct<32, 32>::LPB;
+  }
+}
+
+int dct_reg_cols_per_block(int n) {
+  switch (n) {
+    case 64: return RegDct<8, 8>::CB;
+    case 128: return RegDct<8, 16>::CB;
+    case 256: return RegDct<16, 16>::CB;
+    case 512: return RegDct<16, 32>::CB;
+    default: return RegDct<32, 32>::CB;
   }
 }
 

@@ -129,6 +129,7 @@ void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int roff,
 // Register-resident variant for n in {64, ..., 1024} (dct_reg.cu).
 bool dct_reg_supported(int n);
 int dct_reg_lines_per_block(int n);
+int dct_reg_cols_per_block(int n);
 void dct_reg_run(otm_context* ctx, int n, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,
                  int coff, int ccnt);
 // Dynamic shared-memory limits of the kernels of each family (set once per device,

@@ -576,12 +576,13 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
       Inst& I = h[order[k]];
       const int reg = dct_reg_supported(I.n) ? 1 : 0;
       const int per = reg ? dct_reg_lines_per_block(I.n) : fft_lines(I.n);
+      const int cper = reg ? dct_reg_cols_per_block(I.n) : fft_lines(I.n);
       if (segs.empty() || segs.back().n != I.n || segs.back().reg != reg)
         segs.push_back({I.n, reg, rows, 0, cols, 0});
       I.row0 = rows;
       I.nrow = I.n / per;
       I.col0 = cols;
-      I.ncol = I.n / per;
+      I.ncol = I.n / cper;
       rows += I.nrow;
       cols += I.ncol;
       segs.back().rcnt += I.nrow;
