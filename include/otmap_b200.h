@@ -15,7 +15,17 @@
  *   otm_map_create        TransportMap::TransportMap               transport_map.h:33-35, transport_map.cpp:30-34
  *   otm_map_init_inverse  TransportMap::init_inverse               transport_map.h:41, transport_map.cpp:36-43
  *   otm_map_inverse       apply_inverse_map / TransportMap::inv    transport_map.h:44,66-68, transport_map.cpp:50-128
+ *   otm_map_inverse_mode  TransportMap::inv / inv_fast             transport_map.h:44-45, transport_map.cpp:50-102
  *   otm_rasterize         rasterize_image (both overloads)         utils/rasterizer.h:21-22, utils/rasterizer.cpp:188-308
+ *   otm_rasterize_mode    rasterize_image with RasterImageOption   utils/rasterizer.h:16-22, utils/rasterizer.cpp:188-302
+ *   otm_rasterize_mesh    rasterize_image on any tri/quad mesh     utils/rasterizer.cpp:36-185, 188-302
+ *   otm_transport_cost    transport_cost                           transport_map.h:70, transport_map.cpp:131-215
+ *   otm_mesh_blend        interpolate (bilinear / linear blend)    apps/barycenters.cpp:127-139, 250-276
+ *   otm_barycenter        interpolate + synthetize_and_save_image  apps/barycenters.cpp:250-290
+ *   otm_grid_faces        generate_quad_mesh's faces               utils/mesh_utils.cpp:90-122
+ *   otm_write_off         Surface_mesh::write (.off)               surface_mesh/IO_off.cpp:312-380
+ *   otm_read_off          Surface_mesh::read (.off)                surface_mesh/IO_off.cpp:45-300
+ *   otm_prune_empty_faces prune_empty_faces                        utils/mesh_utils.cpp:124-141
  *
  * Buffer conventions (identical to the reference's in-memory layouts):
  *   n        grid size, N = n*n cells, V = (n+1)*(n+1) vertices
@@ -133,6 +143,15 @@ int otm_map_init_inverse(otm_map* map);
  *   missing optional: number of points with no face */
 int otm_map_inverse(otm_map* map, double* points, long count, int* face, int* nhits, long* missing);
 
+/* otm_map_inverse with the face choice of TransportMap::inv (OTM_INV_DENSEST, the rule
+ * above) or of TransportMap::inv_fast (OTM_INV_FIRST: the first containing face and its
+ * own weights, transport_map.cpp:94-98). The reference's "first" is the first in its
+ * BVH traversal; here it is the lowest face index. Both agree wherever one face
+ * contains the point. */
+#define OTM_INV_DENSEST 0
+#define OTM_INV_FIRST 1
+int otm_map_inverse_mode(otm_map* map, double* points, long count, int mode, int* face, int* nhits, long* missing);
+
 /* rasterize_image (utils/rasterizer.cpp:188-308), PerFace mode on the quad mesh of
  * an (n+1)^2 grid whose vertex positions are `xy`: each pixel whose centre lies in a
  * face (bilinear coordinates in [0,1]) gets float(1/N) * density[f] / |area f|, the
@@ -140,6 +159,92 @@ int otm_map_inverse(otm_map* map, double* points, long count, int* face, int* nh
  * unit density (rasterizer.cpp:305-308). img receives rows*cols doubles. */
 int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
                   double* img);
+
+/* rasterize_image's RasterImageOption (utils/rasterizer.h:16-19). */
+#define OTM_RIO_PER_VERTEX 0
+#define OTM_RIO_PER_FACE 1
+
+/* rasterize_image (utils/rasterizer.cpp:188-302) of the (n+1)^2 grid mesh `xy` with
+ * either option. OTM_RIO_PER_FACE is otm_rasterize. OTM_RIO_PER_VERTEX gives each
+ * vertex float(1/N) * (float sum of 1/|area| over its faces, in face order) / (its
+ * face count), and each covered pixel of the winning face the float sum over the
+ * face's corners of (vertex 0's value * float(weight)) -- the reference's
+ * interpolation reads vertex 0 for every corner (rasterizer.cpp:177). The density
+ * values are not used by that option; only their count sets the scale. */
+int otm_rasterize_mode(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
+                       int mode, double* img);
+
+/* rasterize_image on an indexed face set of triangles and quads (the reference's
+ * Surface_mesh overload for meshes other than the grid, e.g. after
+ * prune_empty_faces): nv vertices xy[2*nv]; face f has corners
+ * face_vertices[face_start[f] .. face_start[f+1]) (3 or 4, face_start[0] = 0) in
+ * circulation order. density[cells] per face (cells >= nf; its length sets the
+ * scale float(1/cells)), NULL = unit density over the nf faces. Triangles use the
+ * barycentric transform of rasterizer.cpp:36-58, quads the bilinear coordinates. */
+int otm_rasterize_mesh(otm_context* ctx, int nv, const double* xy, int nf, const int* face_start,
+                       const int* face_vertices, const double* density, int cells, int rows, int cols, int mode,
+                       double* img);
+
+/* transport_cost (transport_map.cpp:131-215) between the (n+1)^2 grid meshes src_xy
+ * and dst_xy with per-cell density (a quad mesh with as many faces as cells, so the
+ * reference takes its per-triangle branch on each face's circulation (v3, v0, v1)).
+ *   per_face  optional double[N]: density*area*cost of each face / the integral
+ *   cost      out: sum(per-face costs) / integral(density*area)
+ * Per-face terms are computed as the reference computes them; the two sums are
+ * fixed-order tree reductions (the reference sums sequentially), so cost and the
+ * normalised per-face values agree to a few ulps. */
+int otm_transport_cost(otm_context* ctx, int n, const double* src_xy, const double* dst_xy, const double* density,
+                       double* per_face, double* cost);
+
+/* interpolate (apps/barycenters.cpp:250-276): out = sum_k weights[k] * meshes[k],
+ * accumulated left to right per coordinate, as bilerp/lerp (barycenters.cpp:127-139)
+ * evaluate it. Bilinear barycenters of four maps at (alpha, beta) use weights
+ * ((1-a)(1-b), a(1-b), a b, (1-a) b); linear ones of two maps (1-a, a).
+ * count <= 64 meshes of 2*(n+1)^2 doubles each. */
+int otm_mesh_blend(otm_context* ctx, int n, int count, const double* const* meshes, const double* weights,
+                   double* out);
+
+/* One barycenter image (apps/barycenters.cpp:250-290): blends the inverse meshes as
+ * otm_mesh_blend, rasterizes the blend with unit density (PerFace, rows x cols) and
+ * rescales it by expected_mean / mean(image) (synthetize_and_save_image,
+ * barycenters.cpp:280-290). mesh_out (optional) receives the blended mesh,
+ * raster_mean (optional) the mean of the image before rescaling. */
+int otm_barycenter(otm_context* ctx, int n, int count, const double* const* inv_meshes, const double* weights,
+                   double expected_mean, int rows, int cols, double* mesh_out, double* img, double* raster_mean);
+
+/* ---- meshes as indexed face sets, OFF files (host-side; no device needed) ----
+ *
+ * A mesh other than the grid is nv vertices xy[2*nv] and nf faces; face f's corners
+ * are face_vertices[face_start[f] .. face_start[f+1]) (face_start[0] = 0) in the
+ * order the reference's face circulator visits them. */
+
+/* The faces of the (n+1)^2 grid mesh (utils/mesh_utils.cpp:110-121): face_start[N+1],
+ * face_vertices[4N], face f = j + i*n with corners (i,j), (i+1,j), (i+1,j+1), (i,j+1). */
+int otm_grid_faces(int n, int* face_start, int* face_vertices);
+
+/* Writes an ASCII OFF file byte for byte as Surface_mesh::write does for these meshes
+ * (surface_mesh/IO_off.cpp:312-380): "OFF", "nv nf 0", one "%.10f %.10f %.10f" line
+ * per vertex (z = 0, surface_mesh/types.h:50), one "valence i0 i1 ..." line per face. */
+int otm_write_off(const char* path, int nv, const double* xy, int nf, const int* face_start,
+                  const int* face_vertices);
+
+/* Reads an OFF file as Surface_mesh::read does (surface_mesh/IO_off.cpp:45-300):
+ * [ST][C][N]OFF headers, ASCII or BINARY; z and per-vertex normals, colours and
+ * texture coordinates are dropped. Call with xy == NULL to get *nv, *nf and *nidx (the
+ * total corner count); call again with arrays of at least those sizes (*nv, *nf,
+ * *nidx hold the capacities on input). Faces are taken as listed (the reference's
+ * add_face also rejects non-manifold faces; such files are not supported). */
+int otm_read_off(const char* path, int* nv, int* nf, int* nidx, double* xy, int* face_start, int* face_vertices);
+
+/* prune_empty_faces (utils/mesh_utils.cpp:124-141): removes the faces whose density is
+ * 0 (a mesh with nf = 2*cells is a triangulated grid: face f reads cell f/2), then the
+ * vertices left without a face, and renumbers both in the order
+ * Surface_mesh::garbage_collection leaves them (surface_mesh/Surface_mesh.cpp:1975-2110:
+ * each hole, front to back, takes the last survivor). Outputs are sized like the
+ * inputs (start_out nf+1); *nv_out and *nf_out receive the kept counts. */
+int otm_prune_empty_faces(int nv, const double* xy, int nf, const int* face_start, const int* face_vertices,
+                          const double* density, int cells, int* nv_out, double* xy_out, int* nf_out,
+                          int* start_out, int* idx_out);
 
 /* ---- implicit adjoint (no counterpart in the reference, which has no derivatives) ----
  *

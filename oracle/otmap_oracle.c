@@ -775,6 +775,210 @@ void oro_rasterize(int n, const double* xy, const double* density, int rows, int
 }
 
 /* ------------------------------------------------------------------------- */
+/* rasterize_image on an indexed face set of triangles and quads, both options
+ * (rasterizer.cpp:36-58 BarycentricTransform, 86-185 rasterize_face, 188-302).
+ * mode 0 = RIO_PerVertexDensity, 1 = RIO_PerFaceDensity. Faces in index order, the
+ * last face covering a pixel wins. PerVertex: per-vertex float accumulation of
+ * 1/|area| in face order, value = float(scale) * value / count, and the fragment
+ * value is the float sum of (vertex 0's value * float(weight)) over the corners
+ * (the reference's interpolation loop reads verts[0] each time). */
+static void tri_bary(const double q[2], const double p[8], double w[4]) {
+  double m00 = p[0] - p[4], m10 = p[1] - p[5]; /* column s1 - s3 */
+  double m01 = p[2] - p[4], m11 = p[3] - p[5]; /* column s2 - s3 */
+  double invdet = 1.0 / (m00 * m11 - m10 * m01);
+  double t00 = m11 * invdet, t10 = -m10 * invdet, t01 = -m01 * invdet, t11 = m00 * invdet;
+  double vx = q[0] - p[4], vy = q[1] - p[5];
+  double b0 = t00 * vx + t01 * vy, b1 = t10 * vx + t11 * vy;
+  w[0] = b0;
+  w[1] = b1;
+  w[2] = 1.0 - b0 - b1;
+  w[3] = 0.0;
+}
+
+static int load_mesh_face(const double* xy, const int* start, const int* idx, int f, double p[8], int vid[4]) {
+  int c = start[f + 1] - start[f];
+  for (int k = 0; k < 4; ++k) {
+    int v = idx[start[f] + (k < c ? k : c - 1)];
+    vid[k] = v;
+    p[2 * k] = xy[2 * v];
+    p[2 * k + 1] = xy[2 * v + 1];
+  }
+  return c;
+}
+
+static double mesh_face_area(const double p[8], int c) {
+  if (c == 3) return fabs(signed_area3(p, p + 2, p + 4));
+  return fabs(signed_area3(p, p + 2, p + 4) + signed_area3(p, p + 4, p + 6));
+}
+
+void oro_rasterize_mesh(int nv, const double* xy, int nf, const int* start, const int* idx, const double* density,
+                        int cells, int rows, int cols, int mode, int stale_weights, double* img) {
+  float scale = (float)(1. / (double)(density ? cells : nf));
+  float* value = NULL;
+  double stale[4] = {0, 0, 0, 0};
+  memset(img, 0, sizeof(double) * (size_t)rows * cols);
+  if (mode == 0) {
+    value = (float*)calloc((size_t)(nv > 0 ? nv : 1), sizeof(float));
+    double* div = (double*)calloc((size_t)(nv > 0 ? nv : 1), sizeof(double));
+    for (int f = 0; f < nf; ++f) {
+      double p[8];
+      int vid[4];
+      int c = load_mesh_face(xy, start, idx, f, p, vid);
+      double area = mesh_face_area(p, c);
+      for (int k = start[f]; k < start[f + 1]; ++k) {
+        value[idx[k]] = (float)((double)value[idx[k]] + 1. / area);
+        div[idx[k]] += 1.;
+      }
+    }
+    for (int v = 0; v < nv; ++v) value[v] = (float)((double)(scale * value[v]) / div[v]);
+    free(div);
+  }
+  for (int f = 0; f < nf; ++f) {
+    double p[8];
+    int vid[4];
+    int c = load_mesh_face(xy, start, idx, f, p, vid);
+    double in_mass = scale * (density ? density[f] : 1.0);
+    double fvalue = in_mass / mesh_face_area(p, c);
+    double ulx = dmin(dmin(dmin(p[0], p[2]), p[4]), p[6]);
+    double uly = dmin(dmin(dmin(p[1], p[3]), p[5]), p[7]);
+    double lrx = dmax(dmax(dmax(p[0], p[2]), p[4]), p[6]);
+    double lry = dmax(dmax(dmax(p[1], p[3]), p[5]), p[7]);
+    int x0 = (int)(ulx * (double)cols), y0 = (int)(uly * (double)rows);
+    if (x0 < 0) x0 = 0;
+    if (y0 < 0) y0 = 0;
+    int x1 = (int)(lrx * (double)cols) + 1, y1 = (int)(lry * (double)rows) + 1;
+    if (x1 > cols) x1 = cols;
+    if (y1 > rows) y1 = rows;
+    for (int y = y0; y < y1; ++y)
+      for (int x = x0; x < x1; ++x) {
+        double q[2] = {((double)x + 0.5) / (double)cols, ((double)y + 0.5) / (double)rows};
+        double w[4];
+        if (c == 3) {
+          tri_bary(q, p, w);
+        } else if (oro_bilinear_weights(q, p, w)) {
+          memcpy(stale, w, sizeof w);
+        } else {
+          if (!stale_weights) continue;
+          memcpy(w, stale, sizeof w);
+        }
+        if (!(w[0] <= 1.0f && w[1] <= 1.0f && w[2] <= 1.0f && w[3] <= 1.0f && w[0] >= 0.0f && w[1] >= 0.0f &&
+              w[2] >= 0.0f && w[3] >= 0.0f))
+          continue;
+        if (mode == 0) {
+          float v0 = value[vid[0]], acc = 0.0f;
+          for (int k = 0; k < c; ++k) acc = acc + v0 * (float)w[k];
+          img[(size_t)y * cols + x] = (double)acc;
+        } else {
+          img[(size_t)y * cols + x] = fvalue;
+        }
+      }
+  }
+  free(value);
+}
+
+void oro_grid_faces(int n, int* start, int* idx) {
+  for (int f = 0; f < n * n; ++f) {
+    int i = f / n, j = f % n;
+    start[f] = 4 * f;
+    idx[4 * f] = VID(i, j);
+    idx[4 * f + 1] = VID(i + 1, j);
+    idx[4 * f + 2] = VID(i + 1, j + 1);
+    idx[4 * f + 3] = VID(i, j + 1);
+  }
+  start[n * n] = 4 * n * n;
+}
+
+/* interpolate (apps/barycenters.cpp:250-276): out = sum_k w_k mesh_k, left to right. */
+void oro_mesh_blend(long V2, int count, const double* const* meshes, const double* w, double* out) {
+  for (long t = 0; t < V2; ++t) {
+    double acc = w[0] * meshes[0][t];
+    for (int k = 1; k < count; ++k) acc = acc + w[k] * meshes[k][t];
+    out[t] = acc;
+  }
+}
+
+/* prune_empty_faces (mesh_utils.cpp:124-141) followed by Surface_mesh's
+ * garbage_collection (Surface_mesh.cpp:1975-2110): faces with zero density are
+ * removed, then every vertex left without a face; survivors are compacted by the
+ * two-cursor exchange of garbage_collection (vertices and faces separately). A
+ * triangulated grid (nf = 2 cells) reads cell f/2 for face f. */
+static int compact(int count, const char* dead_in, int* newpos) {
+  char* dead = (char*)malloc((size_t)(count > 0 ? count : 1));
+  int* at = (int*)malloc(sizeof(int) * (size_t)(count > 0 ? count : 1));
+  for (int i = 0; i < count; ++i) {
+    dead[i] = dead_in[i];
+    at[i] = i;
+    newpos[i] = -1;
+  }
+  int kept = 0;
+  if (count > 0) {
+    int i0 = 0, i1 = count - 1;
+    for (;;) {
+      while (!dead[i0] && i0 < i1) ++i0;
+      while (dead[i1] && i0 < i1) --i1;
+      if (i0 >= i1) break;
+      char td = dead[i0];
+      dead[i0] = dead[i1];
+      dead[i1] = td;
+      int ta = at[i0];
+      at[i0] = at[i1];
+      at[i1] = ta;
+    }
+    kept = dead[i0] ? i0 : i0 + 1;
+  }
+  for (int pos = 0; pos < kept; ++pos) newpos[at[pos]] = pos;
+  free(dead);
+  free(at);
+  return kept;
+}
+
+int oro_prune_empty_faces(int nv, const double* xy, int nf, const int* start, const int* idx, const double* density,
+                          int cells, int* nv_out, double* xy_out, int* nf_out, int* start_out, int* idx_out) {
+  char* fdead = (char*)calloc((size_t)(nf > 0 ? nf : 1), 1);
+  char* touched = (char*)calloc((size_t)(nv > 0 ? nv : 1), 1);
+  char* live = (char*)calloc((size_t)(nv > 0 ? nv : 1), 1);
+  char* vdead = (char*)calloc((size_t)(nv > 0 ? nv : 1), 1);
+  int* fpos = (int*)malloc(sizeof(int) * (size_t)(nf > 0 ? nf : 1));
+  int* vpos = (int*)malloc(sizeof(int) * (size_t)(nv > 0 ? nv : 1));
+  int* from = (int*)malloc(sizeof(int) * (size_t)(nf > 0 ? nf : 1));
+  const int pairs = (nf == 2 * cells);
+  for (int f = 0; f < nf; ++f) {
+    fdead[f] = density[pairs ? f / 2 : f] == 0;
+    for (int k = start[f]; k < start[f + 1]; ++k) {
+      if (fdead[f])
+        touched[idx[k]] = 1;
+      else
+        live[idx[k]] = 1;
+    }
+  }
+  for (int v = 0; v < nv; ++v) vdead[v] = touched[v] && !live[v];
+  *nv_out = compact(nv, vdead, vpos);
+  *nf_out = compact(nf, fdead, fpos);
+  for (int v = 0; v < nv; ++v)
+    if (vpos[v] >= 0) {
+      xy_out[2 * vpos[v]] = xy[2 * v];
+      xy_out[2 * vpos[v] + 1] = xy[2 * v + 1];
+    }
+  for (int f = 0; f < nf; ++f)
+    if (fpos[f] >= 0) from[fpos[f]] = f;
+  int k = 0;
+  start_out[0] = 0;
+  for (int q = 0; q < *nf_out; ++q) {
+    int f = from[q];
+    for (int t = start[f]; t < start[f + 1]; ++t) idx_out[k++] = vpos[idx[t]];
+    start_out[q + 1] = k;
+  }
+  free(from);
+  free(fdead);
+  free(touched);
+  free(live);
+  free(vdead);
+  free(fpos);
+  free(vpos);
+  return 0;
+}
+
+/* ------------------------------------------------------------------------- */
 /* transport_map.cpp:131-215 for a quad grid mesh: the face count equals the
  * density size, so the reference takes its per-triangle branch (:184-199) on the
  * first three vertices of each face's circulation, which for a Surface_mesh quad

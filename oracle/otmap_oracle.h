@@ -79,6 +79,20 @@ int oro_inside_quad(const double q[2], const double p[8]);
 void oro_rasterize(int n, const double* xy, const double* density, int rows, int cols, int stale_weights,
                    double* img);
 
+/* ---- rasterize_image on an indexed triangle/quad mesh, both options ----
+ * (utils/rasterizer.cpp:36-58, 86-185, 188-302). mode 0 = RIO_PerVertexDensity,
+ * 1 = RIO_PerFaceDensity. Face f's corners are idx[start[f] .. start[f+1]). density
+ * NULL = unit density over nf faces; otherwise cells = its length (sets the scale). */
+void oro_rasterize_mesh(int nv, const double* xy, int nf, const int* start, const int* idx, const double* density,
+                        int cells, int rows, int cols, int mode, int stale_weights, double* img);
+/* The (n+1)^2 grid's faces as an indexed face set (start[N+1], idx[4N]). */
+void oro_grid_faces(int n, int* start, int* idx);
+/* interpolate (apps/barycenters.cpp:250-276): out[t] = sum_k w[k] meshes[k][t]. */
+void oro_mesh_blend(long V2, int count, const double* const* meshes, const double* w, double* out);
+/* prune_empty_faces (utils/mesh_utils.cpp:124-141) + Surface_mesh::garbage_collection. */
+int oro_prune_empty_faces(int nv, const double* xy, int nf, const int* start, const int* idx, const double* density,
+                          int cells, int* nv_out, double* xy_out, int* nf_out, int* start_out, int* idx_out);
+
 /* ---- transport_cost for an (n+1)^2 quad grid (transport_map.cpp:131-215, quad branch) ---- */
 double oro_transport_cost(int n, const double* src_xy, const double* dst_xy, const double* density,
                           double* per_face);

@@ -63,6 +63,12 @@ def lib():
         L.oro_rasterize.argtypes = [C.c_int, _dp, _dp, C.c_int, C.c_int, C.c_int, _dp]
         L.oro_transport_cost.argtypes = [C.c_int, _dp, _dp, _dp, _dp]
         L.oro_transport_cost.restype = C.c_double
+        L.oro_rasterize_mesh.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, _dp]
+        L.oro_grid_faces.argtypes = [C.c_int, _ip, _ip]
+        L.oro_mesh_blend.argtypes = [C.c_long, C.c_int, C.POINTER(_dp), _dp, _dp]
+        L.oro_prune_empty_faces.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_int, _ip, _dp, _ip, _ip, _ip]
+        L.oro_prune_empty_faces.restype = C.c_int
         _lib = L
     return _lib
 
@@ -211,3 +217,54 @@ def grid_vertices(n):
     X = np.repeat(t, n + 1)
     Y = np.tile(t, n + 1)
     return np.stack([X, Y], axis=1)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _pi(a):
+    return a.ctypes.data_as(_ip)
+
+
+def grid_faces(n):
+    """The (n+1)^2 grid's quads as (start[N+1], idx[4N]) in circulation order."""
+    start = np.zeros(n * n + 1, dtype=np.int32)
+    idx = np.zeros(4 * n * n, dtype=np.int32)
+    lib().oro_grid_faces(n, _pi(start), _pi(idx))
+    return start, idx
+
+
+def rasterize_mesh(xy, start, idx, density, rows, cols, per_vertex=False, stale_weights=True):
+    """rasterize_image on an indexed triangle/quad mesh; image is [y][x]."""
+    xy = _f64(xy).reshape(-1, 2)
+    start, idx = _i32(start), _i32(idx)
+    img = np.zeros((rows, cols))
+    d = None if density is None else _f64(density)
+    lib().oro_rasterize_mesh(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx),
+                             None if d is None else _p(d), 0 if d is None else d.size, rows, cols,
+                             0 if per_vertex else 1, int(bool(stale_weights)), _p(img))
+    return img
+
+
+def mesh_blend(meshes, weights):
+    """out = sum_k weights[k] * meshes[k] (apps/barycenters.cpp:250-276)."""
+    ms = [_f64(m) for m in meshes]
+    w = _f64(weights)
+    out = np.empty_like(ms[0])
+    arr = (_dp * len(ms))(*[_p(m) for m in ms])
+    lib().oro_mesh_blend(ms[0].size, len(ms), arr, _p(w), _p(out))
+    return out
+
+
+def prune_empty_faces(xy, start, idx, density):
+    """prune_empty_faces + garbage collection -> (xy, start, idx)."""
+    xy = _f64(xy).reshape(-1, 2)
+    start, idx, d = _i32(start), _i32(idx), _f64(density)
+    nv, nf = C.c_int(0), C.c_int(0)
+    xo = np.zeros_like(xy)
+    so = np.zeros_like(start)
+    io = np.zeros_like(idx)
+    lib().oro_prune_empty_faces(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx), _p(d), d.size,
+                                C.byref(nv), _p(xo), C.byref(nf), _pi(so), _pi(io))
+    return xo[:nv.value].copy(), so[:nf.value + 1].copy(), io[:so[nf.value]].copy()

@@ -54,6 +54,19 @@ def lib():
         L.otref_1d_params.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
         L.otref_line_search.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp]
         L.otref_line_search.restype = C.c_double
+        L.otref_rasterize_mesh.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_int, C.c_int, C.c_int,
+                                           C.c_int, _dp]
+        L.otref_rasterize_mesh.restype = C.c_double
+        L.otref_barycenter.argtypes = [C.c_int, C.c_int, C.POINTER(_dp), C.c_double, C.c_double, _dp, C.c_int,
+                                       C.c_int, _dp, _dp]
+        L.otref_barycenter.restype = C.c_double
+        L.otref_image_mean.argtypes = [_dp, C.c_int, C.c_int]
+        L.otref_image_mean.restype = C.c_double
+        L.otref_prune.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_int, _ip, _dp, _ip, _ip, _ip]
+        L.otref_write_off.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, C.c_char_p]
+        L.otref_write_off.restype = C.c_int
+        L.otref_read_off.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _ip, _dp, _ip, _ip, _ip]
+        L.otref_read_off.restype = C.c_int
         _lib = L
     return _lib
 
@@ -190,3 +203,77 @@ def transport_cost(src_xy, dst_xy, n, density, per_face=False):
     c = lib().otref_transport_cost(_p(_f64(src_xy)), _p(_f64(dst_xy)), int(n), _p(_f64(density)),
                                    None if pf is None else _p(pf))
     return (c, pf) if per_face else c
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _pi(a):
+    return a.ctypes.data_as(_ip)
+
+
+def rasterize_mesh(xy, start, idx, density, rows, cols, per_vertex=False):
+    """rasterize_image (otlib/utils/rasterizer.cpp:188-302) of an indexed tri/quad mesh."""
+    xy = _f64(xy).reshape(-1, 2)
+    start, idx = _i32(start), _i32(idx)
+    img = np.zeros((rows, cols))
+    d = None if density is None else _f64(density)
+    lib().otref_rasterize_mesh(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx),
+                               None if d is None else _p(d), 0 if d is None else d.size, rows, cols,
+                               int(bool(per_vertex)), _p(img))
+    return img
+
+
+def barycenter(n, inv_meshes, alpha, beta, means, rows, cols):
+    """One image of apps/barycenters.cpp:250-290 (4 maps: bilinear, 2 maps: linear).
+    Returns (blended mesh, image, expected mean)."""
+    ms = [_f64(m) for m in inv_meshes]
+    arr = (_dp * len(ms))(*[_p(m) for m in ms])
+    mv = _f64(means)
+    mesh = np.empty_like(ms[0])
+    img = np.zeros((rows, cols))
+    e = lib().otref_barycenter(int(n), len(ms), arr, float(alpha), float(beta), _p(mv), rows, cols, _p(mesh),
+                               _p(img))
+    return mesh, img, e
+
+
+def image_mean(img):
+    """Eigen MatrixXd::mean() of an image given [y][x]."""
+    img = _f64(img)
+    return lib().otref_image_mean(_p(img), img.shape[0], img.shape[1])
+
+
+def prune_empty_faces(xy, start, idx, density):
+    """prune_empty_faces (otlib/utils/mesh_utils.cpp:124-141) on an indexed mesh."""
+    xy = _f64(xy).reshape(-1, 2)
+    start, idx, d = _i32(start), _i32(idx), _f64(density)
+    nv, nf = C.c_int(0), C.c_int(0)
+    xo = np.zeros_like(xy)
+    so = np.zeros_like(start)
+    io = np.zeros_like(idx)
+    lib().otref_prune(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx), _p(d), d.size, C.byref(nv),
+                      _p(xo), C.byref(nf), _pi(so), _pi(io))
+    return xo[:nv.value].copy(), so[:nf.value + 1].copy(), io[:so[nf.value]].copy()
+
+
+def write_off(path, xy, start, idx):
+    """Surface_mesh::write (otlib/surface_mesh/IO_off.cpp:312-380)."""
+    xy = _f64(xy).reshape(-1, 2)
+    start, idx = _i32(start), _i32(idx)
+    ok = lib().otref_write_off(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx), str(path).encode())
+    if not ok:
+        raise OSError(f"reference could not write {path}")
+
+
+def read_off(path, cap_v, cap_f, cap_i):
+    """Surface_mesh::read (otlib/surface_mesh/IO_off.cpp:255-300) -> (xy, start, idx)."""
+    xy = np.zeros((cap_v, 2))
+    start = np.zeros(cap_f + 1, dtype=np.int32)
+    idx = np.zeros(cap_i, dtype=np.int32)
+    nv, nf = C.c_int(0), C.c_int(0)
+    r = lib().otref_read_off(str(path).encode(), cap_v, cap_f, cap_i, C.byref(nv), _p(xy), C.byref(nf), _pi(start),
+                             _pi(idx))
+    if r != 1:
+        raise OSError(f"reference could not read {path} ({r})")
+    return xy[:nv.value].copy(), start[:nf.value + 1].copy(), idx[:start[nf.value]].copy()

@@ -8,6 +8,8 @@
 //   apply_inverse_map / BVH2D::query_all      otlib/transport_map.cpp:105-128, otlib/utils/bvh2d.cpp:84-92
 //   rasterize_image                           otlib/utils/rasterizer.cpp:188-308
 //   transport_cost                            otlib/transport_map.cpp:131-215
+//   rasterize_image on indexed meshes, prune_empty_faces, Surface_mesh OFF read/write,
+//   and the barycenter image of apps/barycenters.cpp:250-290
 // plus unit probes of the solver's protected steps through a derived class.
 //
 // Buffer conventions (shared with the product C ABI):
@@ -376,6 +378,142 @@ double otref_line_search(void* hp, const double* psi, const double* dir, const d
     r1[i] = rr1[i];
   }
   return res;
+}
+
+// ---- meshes other than the grid, barycenters, mesh IO ----
+
+// Indexed face set -> Surface_mesh (add_face keeps the given circulation order).
+static void load_indexed_mesh(Surface_mesh& mesh, int nv, const double* xy, int nf, const int* start,
+                              const int* idx) {
+  std::vector<Surface_mesh::Vertex> vs(nv);
+  for (int v = 0; v < nv; ++v) vs[v] = mesh.add_vertex(surface_mesh::Point(xy[2 * v], xy[2 * v + 1]));
+  std::vector<Surface_mesh::Vertex> fv;
+  for (int f = 0; f < nf; ++f) {
+    fv.clear();
+    for (int k = start[f]; k < start[f + 1]; ++k) fv.push_back(vs[idx[k]]);
+    mesh.add_face(fv);
+  }
+}
+
+// rasterize_image (rasterizer.cpp:188-302) of an indexed triangle/quad mesh.
+double otref_rasterize_mesh(int nv, const double* xy, int nf, const int* start, const int* idx,
+                            const double* density, int cells, int rows, int cols, int per_vertex, double* img) {
+  CsrGuard g;
+  Surface_mesh mesh;
+  load_indexed_mesh(mesh, nv, xy, nf, start, idx);
+  MatrixXd im(rows, cols);
+  auto opt = per_vertex ? otmap::RIO_PerVertexDensity : otmap::RIO_PerFaceDensity;
+  double t0 = now_s();
+  if (density) {
+    VectorXd d = Map<const VectorXd>(density, (Index)cells);
+    otmap::rasterize_image(mesh, d, im, opt);
+  } else {
+    otmap::rasterize_image(mesh, im, opt);
+  }
+  double t1 = now_s();
+  for (int y = 0; y < rows; ++y)
+    for (int x = 0; x < cols; ++x) img[(size_t)y * cols + x] = im(y, x);
+  return t1 - t0;
+}
+
+// One barycenter image as apps/barycenters.cpp:250-290 forms it: the inverse meshes
+// (count 4: bilinear at (alpha, beta); count 2: linear at alpha) blended vertex by
+// vertex with the bilerp/lerp expressions of barycenters.cpp:127-139 (written out
+// here: the app is not part of otlib), rasterized with unit density, rescaled to the
+// blended density mean. Returns the expected mean.
+double otref_barycenter(int n, int count, const double* const* inv, double alpha, double beta,
+                        const double* means, int rows, int cols, double* mesh_out, double* img) {
+  CsrGuard g;
+  Surface_mesh res;
+  load_grid_mesh(res, n, inv[0]);
+  auto& pts = res.points();
+  const double u = alpha, v = beta;
+  for (size_t k = 0; k < pts.size(); ++k) {
+    Vector2d a0(inv[0][2 * k], inv[0][2 * k + 1]), a1(inv[1][2 * k], inv[1][2 * k + 1]);
+    if (count == 4) {
+      Vector2d a2(inv[2][2 * k], inv[2][2 * k + 1]), a3(inv[3][2 * k], inv[3][2 * k + 1]);
+      pts[k] = (1. - u) * (1. - v) * a0 + (u) * (1. - v) * a1 + (u) * (v)*a2 + (1. - u) * (v)*a3;
+    } else {
+      pts[k] = (1. - u) * a0 + u * a1;
+    }
+  }
+  double expected = count == 4 ? (1. - u) * (1. - v) * means[0] + (u) * (1. - v) * means[1] +
+                                     (u) * (v)*means[2] + (1. - u) * (v)*means[3]
+                               : (1. - u) * means[0] + u * means[1];
+  MatrixXd im(rows, cols);
+  otmap::rasterize_image(res, im);
+  im = im * (expected / im.mean());
+  for (size_t k = 0; k < pts.size(); ++k) {
+    mesh_out[2 * k] = pts[k][0];
+    mesh_out[2 * k + 1] = pts[k][1];
+  }
+  for (int y = 0; y < rows; ++y)
+    for (int x = 0; x < cols; ++x) img[(size_t)y * cols + x] = im(y, x);
+  return expected;
+}
+
+// Mean of a rows x cols image as Eigen's MatrixXd::mean() forms it.
+double otref_image_mean(const double* img, int rows, int cols) {
+  MatrixXd im(rows, cols);
+  for (int y = 0; y < rows; ++y)
+    for (int x = 0; x < cols; ++x) im(y, x) = img[(size_t)y * cols + x];
+  return im.mean();
+}
+
+// prune_empty_faces (mesh_utils.cpp:124-141) of an indexed mesh; the result is read
+// back in the garbage-collected order. Outputs sized by the input (nv, nf, start[nf]).
+void otref_prune(int nv, const double* xy, int nf, const int* start, const int* idx, const double* density,
+                 int cells, int* nv_out, double* xy_out, int* nf_out, int* start_out, int* idx_out) {
+  CsrGuard g;
+  Surface_mesh mesh;
+  load_indexed_mesh(mesh, nv, xy, nf, start, idx);
+  VectorXd d = Map<const VectorXd>(density, (Index)cells);
+  otmap::prune_empty_faces(mesh, d);
+  *nv_out = (int)mesh.n_vertices();
+  *nf_out = (int)mesh.n_faces();
+  for (int v = 0; v < *nv_out; ++v) {
+    auto p = mesh.position(Surface_mesh::Vertex(v));
+    xy_out[2 * v] = p[0];
+    xy_out[2 * v + 1] = p[1];
+  }
+  int k = 0;
+  start_out[0] = 0;
+  for (int f = 0; f < *nf_out; ++f) {
+    for (auto v : mesh.vertices(Surface_mesh::Face(f))) idx_out[k++] = v.idx();
+    start_out[f + 1] = k;
+  }
+}
+
+// Surface_mesh::write (IO_off.cpp:312-380) of an indexed mesh; 1 on success.
+int otref_write_off(int nv, const double* xy, int nf, const int* start, const int* idx, const char* path) {
+  Surface_mesh mesh;
+  load_indexed_mesh(mesh, nv, xy, nf, start, idx);
+  return mesh.write(path) ? 1 : 0;
+}
+
+// Surface_mesh::read (IO_off.cpp:255-300) -> indexed arrays (capacities given).
+int otref_read_off(const char* path, int cap_v, int cap_f, int cap_i, int* nv, double* xy, int* nf, int* start,
+                   int* idx) {
+  Surface_mesh mesh;
+  if (!mesh.read(path)) return 0;
+  *nv = (int)mesh.n_vertices();
+  *nf = (int)mesh.n_faces();
+  if (*nv > cap_v || *nf > cap_f) return -1;
+  for (int v = 0; v < *nv; ++v) {
+    auto p = mesh.position(Surface_mesh::Vertex(v));
+    xy[2 * v] = p[0];
+    xy[2 * v + 1] = p[1];
+  }
+  int k = 0;
+  start[0] = 0;
+  for (int f = 0; f < *nf; ++f) {
+    for (auto v : mesh.vertices(Surface_mesh::Face(f))) {
+      if (k >= cap_i) return -1;
+      idx[k++] = v.idx();
+    }
+    start[f + 1] = k;
+  }
+  return 1;
 }
 
 }  // extern "C"

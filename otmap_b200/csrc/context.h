@@ -144,6 +144,11 @@ void copy_in(otm_context* ctx, void* dst, const void* src, size_t bytes);
 // Copies `bytes` from src (device) into dst (host or device), on the context stream.
 void copy_out(otm_context* ctx, void* dst, const void* src, size_t bytes);
 
+// Rasterizes the (n+1)^2 grid mesh xy (device) into img (device, rows*cols), in
+// OTM_RIO_PER_FACE or OTM_RIO_PER_VERTEX mode; density (device) NULL = unit density.
+void raster_grid(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols, int mode,
+                 double* img);
+
 // Launches `kernel` on the context stream, counting it and (when profiling) bracketing
 // it with CUDA events.
 template <class K, class... Args>

@@ -1,5 +1,5 @@
 // Point location in the forward mesh (TransportMap inversion) and rasterization of
-// a deformed grid mesh, for sm_100a.
+// the deformed grid mesh or of any triangle/quad mesh, for sm_100a.
 //
 // Both run on a uniform bin grid built on the GPU: faces are binned by their
 // bounding boxes (count, exclusive scan, scatter) and each query -- a point to
@@ -220,7 +220,7 @@ constexpr int MAXHITS = 8;
 // order; with several hits the reference keeps the weights of its first hit and the
 // face of the densest later one (transport_map.cpp:70-85), which is reproduced.
 __global__ void k_inverse(const double* xy, const double* density, int n, int B, const int* starts,
-                          const int* faces, const double4* boxes, double* pts, long P, int* face_out,
+                          const int* faces, const double4* boxes, double* pts, long P, int first_hit, int* face_out,
                           int* nhits_out, unsigned long long* missing) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
@@ -272,7 +272,7 @@ __global__ void k_inverse(const double* xy, const double* density, int n, int B,
   }
   int f = hf[0];
   int kmax = nh < MAXHITS ? nh : MAXHITS;
-  if (nh > 1) {
+  if (nh > 1 && !first_hit) {
     double best = density[f];
     for (int k = 1; k < kmax; ++k) {
       double dk = density[hf[k]];
@@ -304,25 +304,76 @@ __global__ void k_inverse(const double* xy, const double* density, int n, int B,
   if (face_out) face_out[i] = f;
 }
 
-// ---- rasterization (utils/rasterizer.cpp:162-236) ----
+// ---- rasterization (utils/rasterizer.cpp:36-58, 86-185, 188-302) ----
 
 constexpr int RT = 16;  // pixel tile edge for face binning
 
-struct FaceRaster {
-  int x0, x1, y0, y1;  // pixel box [x0,x1) x [y0,y1), as rasterize_face computes it
-  double value;        // float(1/N) * density / |area|
+// A mesh to rasterize: the quads of the (n+1)^2 grid (start == nullptr), or an indexed
+// face set of triangles and quads whose face f lists vertices idx[start[f] .. start[f+1])
+// in the order the reference's face circulator visits them.
+struct MeshRef {
+  const double* xy;
+  int n;       // grid size (grid meshes only)
+  int nf;      // faces
+  int nv;      // vertices
+  const int* start;
+  const int* idx;
 };
 
-__device__ __forceinline__ FaceRaster face_raster(const double* xy, const double* density, int n, float scale,
-                                                  int rows, int cols, int f) {
+// Loads face f's corners; returns its valence (3 or 4). Triangles repeat their last
+// corner in slot 3, which leaves their bounding box unchanged.
+__device__ __forceinline__ int load_face(const MeshRef& m, int f, Quad& p, int vid[4]) {
+  if (!m.start) {
+    load_quad(m.xy, m.n, f, p, vid);
+    return 4;
+  }
+  const int s = m.start[f];
+  const int c = m.start[f + 1] - s;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    vid[k] = m.idx[s + (k < c ? k : c - 1)];
+    p.x[k] = m.xy[2 * (size_t)vid[k]];
+    p.y[k] = m.xy[2 * (size_t)vid[k] + 1];
+  }
+  return c;
+}
+
+// |area| of a face as rasterize_image takes it (eigen_addons.h:18-23).
+__device__ __forceinline__ double face_abs_area(const Quad& p, int c) {
+  if (c == 3) return fabs(signed_area3(p.x[0], p.y[0], p.x[1], p.y[1], p.x[2], p.y[2]));
+  return fabs(signed_area3(p.x[0], p.y[0], p.x[1], p.y[1], p.x[2], p.y[2]) +
+              signed_area3(p.x[0], p.y[0], p.x[2], p.y[2], p.x[3], p.y[3]));
+}
+
+// BarycentricTransform (rasterizer.cpp:36-58): T = [s1-s3 | s2-s3], inverted as Eigen
+// inverts a 2x2 matrix (adjugate times 1/det), b = T^-1 (q - s3), bary = (b0, b1, 1-b0-b1).
+__device__ __forceinline__ void tri_weights(double qx, double qy, const Quad& p, double w[4]) {
+  const double m00 = p.x[0] - p.x[2], m10 = p.y[0] - p.y[2];
+  const double m01 = p.x[1] - p.x[2], m11 = p.y[1] - p.y[2];
+  const double invdet = 1.0 / (m00 * m11 - m10 * m01);
+  const double t00 = m11 * invdet, t10 = -m10 * invdet, t01 = -m01 * invdet, t11 = m00 * invdet;
+  const double vx = qx - p.x[2], vy = qy - p.y[2];
+  const double b0 = t00 * vx + t01 * vy;
+  const double b1 = t10 * vx + t11 * vy;
+  w[0] = b0;
+  w[1] = b1;
+  w[2] = 1.0 - b0 - b1;
+  w[3] = 0.0;
+}
+
+struct FaceRaster {
+  int x0, x1, y0, y1;  // pixel box [x0,x1) x [y0,y1), as rasterize_face computes it
+  double value;        // PerFace value: float(1/N) * density / |area|
+};
+
+__device__ __forceinline__ FaceRaster face_raster(const MeshRef& m, const double* density, float scale, int rows,
+                                                  int cols, int f) {
   Quad p;
   int vid[4];
-  load_quad(xy, n, f, p, vid);
+  const int c = load_face(m, f, p, vid);
   FaceRaster r;
   double in_mass = scale * (density ? density[f] : 1.0);
-  double area = fabs(signed_area3(p.x[0], p.y[0], p.x[1], p.y[1], p.x[2], p.y[2]) +
-                     signed_area3(p.x[0], p.y[0], p.x[2], p.y[2], p.x[3], p.y[3]));
-  r.value = in_mass / area;
+  r.value = in_mass / face_abs_area(p, c);
   double ulx = fmin(fmin(fmin(p.x[0], p.x[1]), p.x[2]), p.x[3]);
   double uly = fmin(fmin(fmin(p.y[0], p.y[1]), p.y[2]), p.y[3]);
   double lrx = fmax(fmax(fmax(p.x[0], p.x[1]), p.x[2]), p.x[3]);
@@ -343,20 +394,20 @@ __device__ __forceinline__ FaceRaster face_raster(const double* xy, const double
   return r;
 }
 
-__global__ void k_raster_count(const double* xy, const double* density, int n, float scale, int rows, int cols,
-                               int TX, FaceRaster* fr, int* counts) {
+__global__ void k_raster_count(MeshRef m, const double* density, float scale, int rows, int cols, int TX,
+                               FaceRaster* fr, int* counts) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= n * n) return;
-  FaceRaster r = face_raster(xy, density, n, scale, rows, cols, f);
+  if (f >= m.nf) return;
+  FaceRaster r = face_raster(m, density, scale, rows, cols, f);
   fr[f] = r;
   if (r.x0 >= r.x1 || r.y0 >= r.y1) return;
   for (int ty = r.y0 / RT; ty <= (r.y1 - 1) / RT; ++ty)
     for (int tx = r.x0 / RT; tx <= (r.x1 - 1) / RT; ++tx) atomicAdd(&counts[ty * TX + tx], 1);
 }
 
-__global__ void k_raster_fill(const FaceRaster* fr, int n, int TX, const int* starts, int* cursor, int* faces) {
+__global__ void k_raster_fill(const FaceRaster* fr, int nf, int TX, const int* starts, int* cursor, int* faces) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= n * n) return;
+  if (f >= nf) return;
   FaceRaster r = fr[f];
   if (r.x0 >= r.x1 || r.y0 >= r.y1) return;
   for (int ty = r.y0 / RT; ty <= (r.y1 - 1) / RT; ++ty)
@@ -369,11 +420,12 @@ __global__ void k_raster_fill(const FaceRaster* fr, int n, int TX, const int* st
 // Weights the reference's sequential loop would test at (f, x, y) when its bilinear
 // solve fails there (D < 0): its Vector4d is never written, and the optimised build
 // then reads the weights of the most recent successful solve. Walk back through the
-// loop order -- earlier pixels of face f's box row by row, then earlier faces -- to
+// loop order -- earlier pixels of face f's box row by row, then earlier quads -- to
 // the most recent pixel whose solve succeeds. Bounded; gives zeros (the start state)
-// when it runs out, as the sequential emulation does before any solve.
-__device__ void stale_weights(const double* xy, int n, int rows, int cols, const FaceRaster* fr, int f, int x,
-                              int y, double w[4]) {
+// when it runs out, as the sequential emulation does before any solve. Triangles
+// never touch that Vector4d and are passed over.
+__device__ void stale_weights(const MeshRef& m, int rows, int cols, const FaceRaster* fr, int f, int x, int y,
+                              double w[4]) {
   int steps = 0;
   const int limit = 1 << 22;
   while (steps < limit) {
@@ -385,9 +437,12 @@ __device__ void stale_weights(const double* xy, int n, int rows, int cols, const
       --y;
       x = r.x1 - 1;
     } else {
-      // last pixel of the previous face with a non-empty box
+      // last pixel of the previous quad with a non-empty box
       int g = f - 1;
-      while (g >= 0 && (fr[g].x0 >= fr[g].x1 || fr[g].y0 >= fr[g].y1) && steps < limit) {
+      while (g >= 0 && steps < limit) {
+        const bool empty = fr[g].x0 >= fr[g].x1 || fr[g].y0 >= fr[g].y1;
+        const bool tri = m.start && (m.start[g + 1] - m.start[g] == 3);
+        if (!empty && !tri) break;
         --g;
         ++steps;
       }
@@ -399,21 +454,27 @@ __device__ void stale_weights(const double* xy, int n, int rows, int cols, const
     ++steps;
     Quad p;
     int vid[4];
-    load_quad(xy, n, f, p, vid);
+    load_face(m, f, p, vid);
     double qx = ((double)x + 0.5) / (double)cols, qy = ((double)y + 0.5) / (double)rows;
     if (bilinear_weights(qx, qy, p, w)) return;
   }
   w[0] = w[1] = w[2] = w[3] = 0.0;
 }
 
-__global__ void k_raster(const double* xy, int n, int rows, int cols, int TX, const FaceRaster* fr,
-                         const int* starts, const int* faces, double* img) {
+// One thread per pixel: the highest-index face whose test accepts the pixel centre
+// wins (the reference's sequential loop overwrites in face order). PerFace writes the
+// face value; PerVertex (vval != nullptr) writes the float interpolation of
+// rasterize_face's loop, which scales vertex 0's value by each weight
+// (rasterizer.cpp:123-130, 174-181) and sums in float.
+__global__ void k_raster(MeshRef m, int rows, int cols, int TX, const FaceRaster* fr, const int* starts,
+                         const int* faces, const float* vval, double* img) {
   int x = blockIdx.x * blockDim.x + threadIdx.x;
   int y = blockIdx.y * blockDim.y + threadIdx.y;
   if (x >= cols || y >= rows) return;
   int b = (y / RT) * TX + (x / RT);
   double qx = ((double)x + 0.5) / (double)cols, qy = ((double)y + 0.5) / (double)rows;
-  int best = -1;
+  int best = -1, bc = 0, bv0 = 0;
+  double bw[4] = {0, 0, 0, 0};
   for (int k = starts[b]; k < starts[b + 1]; ++k) {
     int f = faces[k];
     if (f <= best) continue;
@@ -421,12 +482,100 @@ __global__ void k_raster(const double* xy, int n, int rows, int cols, int TX, co
     if (x < r.x0 || x >= r.x1 || y < r.y0 || y >= r.y1) continue;
     Quad p;
     int vid[4];
-    load_quad(xy, n, f, p, vid);
+    const int c = load_face(m, f, p, vid);
     double w[4];
-    if (!bilinear_weights(qx, qy, p, w)) stale_weights(xy, n, rows, cols, fr, f, x, y, w);
-    if (weights_inside(w)) best = f;
+    if (c == 3) {
+      tri_weights(qx, qy, p, w);
+    } else if (!bilinear_weights(qx, qy, p, w)) {
+      stale_weights(m, rows, cols, fr, f, x, y, w);
+    }
+    if (weights_inside(w)) {
+      best = f;
+      bc = c;
+      bv0 = vid[0];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) bw[q] = w[q];
+    }
   }
-  img[(size_t)y * cols + x] = best >= 0 ? fr[best].value : 0.0;
+  double out = 0.0;
+  if (best >= 0) {
+    if (vval) {
+      const float v0 = vval[bv0];
+      float acc = 0.0f;
+      for (int q = 0; q < bc; ++q) acc = acc + v0 * (float)bw[q];
+      out = (double)acc;
+    } else {
+      out = fr[best].value;
+    }
+  }
+  img[(size_t)y * cols + x] = out;
+}
+
+// PerVertex values (rasterizer.cpp:240-271) on the grid mesh: each vertex sums, in
+// float and in face order, 1/|area| over its faces, then takes float(scale) * value /
+// (number of faces) with the reference's float and double steps.
+__global__ void k_vertex_values_grid(const double* xy, int n, float scale, float* value) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long V = (long)(n + 1) * (n + 1);
+  if (v >= V) return;
+  const int vi = (int)(v / (n + 1)), vj = (int)(v % (n + 1));
+  float acc = 0.0f;
+  double div = 0.0;
+  // faces around vertex (vi, vj) in increasing index j + i*n
+  const int ci[4] = {vi - 1, vi - 1, vi, vi}, cj[4] = {vj - 1, vj, vj - 1, vj};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    if (ci[k] < 0 || cj[k] < 0 || ci[k] >= n || cj[k] >= n) continue;
+    Quad p;
+    int vid[4];
+    load_quad(xy, n, cj[k] + ci[k] * n, p, vid);
+    acc = (float)((double)acc + 1. / face_abs_area(p, 4));
+    div += 1.;
+  }
+  value[v] = (float)((double)(scale * acc) / div);
+}
+
+// Indexed meshes: vertex -> face lists (count, scan, scatter, then each list sorted by
+// face index so the float sums run in the reference's face order).
+__global__ void k_vf_count(MeshRef m, int* counts) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  for (int k = m.start[f]; k < m.start[f + 1]; ++k) atomicAdd(&counts[m.idx[k]], 1);
+}
+
+__global__ void k_vf_fill(MeshRef m, const int* vstart, int* cursor, int* vfaces, double* inv_area) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  Quad p;
+  int vid[4];
+  const int c = load_face(m, f, p, vid);
+  inv_area[f] = 1. / face_abs_area(p, c);
+  for (int k = m.start[f]; k < m.start[f + 1]; ++k) {
+    const int v = m.idx[k];
+    vfaces[vstart[v] + atomicAdd(&cursor[v], 1)] = f;
+  }
+}
+
+__global__ void k_vertex_values_mesh(int nv, const int* vstart, int* vfaces, const double* inv_area, float scale,
+                                     float* value) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int s = vstart[v], e = vstart[v + 1];
+  for (int a = s + 1; a < e; ++a) {  // insertion sort: lists are short
+    int f = vfaces[a], b = a;
+    while (b > s && vfaces[b - 1] > f) {
+      vfaces[b] = vfaces[b - 1];
+      --b;
+    }
+    vfaces[b] = f;
+  }
+  float acc = 0.0f;
+  double div = 0.0;
+  for (int a = s; a < e; ++a) {
+    acc = (float)((double)acc + inv_area[vfaces[a]]);
+    div += 1.;
+  }
+  value[v] = (float)((double)(scale * acc) / div);
 }
 
 // ---- host ----
@@ -504,9 +653,11 @@ extern "C" int otm_map_init_inverse(otm_map* m) {
   });
 }
 
-extern "C" int otm_map_inverse(otm_map* m, double* points, long count, int* face, int* nhits, long* missing) {
+extern "C" int otm_map_inverse_mode(otm_map* m, double* points, long count, int mode, int* face, int* nhits,
+                                   long* missing) {
   return guarded([&] {
     if (!m) throw BadArg{"otm_map_inverse: null map"};
+    if (mode != OTM_INV_DENSEST && mode != OTM_INV_FIRST) throw BadArg{"otm_map_inverse: unknown mode"};
     if (count < 0 || (count > 0 && !points)) throw BadArg{"otm_map_inverse: bad points"};
     otm_context* ctx = m->ctx;
     make_current(ctx);
@@ -533,8 +684,8 @@ extern "C" int otm_map_inverse(otm_map* m, double* points, long count, int* face
     unsigned grid = (unsigned)((count + 255) / 256);
     launch(ctx, "inverse", k_inverse, grid, 256, (const double*)m->fwd.as<double>(),
            (const double*)m->density.as<double>(), m->n, m->bins, (const int*)m->bin_start.as<int>(),
-           (const int*)m->bin_faces.as<int>(), (const double4*)m->face_box.as<double4>(), dp, (long)count, df, dh,
-           dm);
+           (const int*)m->bin_faces.as<int>(), (const double4*)m->face_box.as<double4>(), dp, (long)count,
+           mode == OTM_INV_FIRST ? 1 : 0, df, dh, dm);
     OTM_CUDA(cudaGetLastError());
     if (!pdev) OTM_CUDA(cudaMemcpyAsync(points, dp, bp, cudaMemcpyDeviceToHost, st));
     if (face && !fdev) OTM_CUDA(cudaMemcpyAsync(face, df, bf, cudaMemcpyDeviceToHost, st));
@@ -548,19 +699,105 @@ extern "C" int otm_map_inverse(otm_map* m, double* points, long count, int* face
   });
 }
 
-extern "C" int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
-                             double* img) {
+extern "C" int otm_map_inverse(otm_map* m, double* points, long count, int* face, int* nhits, long* missing) {
+  return otm_map_inverse_mode(m, points, count, OTM_INV_DENSEST, face, nhits, missing);
+}
+
+namespace otm {
+
+// Rasterizes mesh m (all pointers on the device) into img (device, rows*cols).
+static void raster_mesh(otm_context* ctx, const MeshRef& m, const double* density, int cells, int rows, int cols,
+                        int mode, double* img) {
+  cudaStream_t st = ctx->stream;
+  const int nf = m.nf;
+  const int TX = (cols + RT - 1) / RT, TY = (rows + RT - 1) / RT, nb = TX * TY;
+  DevBuf fr, counts, starts, sums, faces, vval;
+  fr.reserve(sizeof(FaceRaster) * (size_t)(nf > 0 ? nf : 1));
+  counts.reserve(sizeof(int) * nb);
+  starts.reserve(sizeof(int) * (nb + 1));
+  sums.reserve(sizeof(int) * ((nb + SCAN_B - 1) / SCAN_B + 1));
+  OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
+  // rasterizer.cpp:193 keeps 1/density.size() in a float
+  const float scale = (float)(1. / (double)(density ? cells : nf));
+  const int fblocks = nf > 0 ? (nf + 255) / 256 : 1;
+  launch(ctx, "raster_count", k_raster_count, fblocks, 256, m, density, scale, rows, cols, TX, fr.as<FaceRaster>(),
+         counts.as<int>());
+  exclusive_scan(st, counts.as<int>(), starts.as<int>(), sums.as<int>(), nb);
+  int total = 0;
+  OTM_CUDA(cudaMemcpyAsync(&total, starts.as<int>() + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
+  OTM_CUDA(cudaStreamSynchronize(st));
+  faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1));
+  OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
+  launch(ctx, "raster_fill", k_raster_fill, fblocks, 256, (const FaceRaster*)fr.as<FaceRaster>(), nf, TX,
+         (const int*)starts.as<int>(), counts.as<int>(), faces.as<int>());
+  const float* pv = nullptr;
+  if (mode == OTM_RIO_PER_VERTEX) {
+    vval.reserve(sizeof(float) * (size_t)(m.nv > 0 ? m.nv : 1));
+    const unsigned vb = (unsigned)((m.nv + 255) / 256);
+    if (!m.start) {
+      launch(ctx, "vertex_values", k_vertex_values_grid, vb, 256, m.xy, m.n, scale, vval.as<float>());
+    } else {
+      DevBuf vcount, vstart, vsums, vfaces, inv_area;
+      int nref = 0;
+      OTM_CUDA(cudaMemcpyAsync(&nref, m.start + nf, sizeof(int), cudaMemcpyDeviceToHost, st));
+      vcount.reserve(sizeof(int) * m.nv);
+      vstart.reserve(sizeof(int) * (m.nv + 1));
+      vsums.reserve(sizeof(int) * ((m.nv + SCAN_B - 1) / SCAN_B + 1));
+      inv_area.reserve(sizeof(double) * (size_t)(nf > 0 ? nf : 1));
+      OTM_CUDA(cudaMemsetAsync(vcount.p, 0, sizeof(int) * m.nv, st));
+      launch(ctx, "vf_count", k_vf_count, fblocks, 256, m, vcount.as<int>());
+      exclusive_scan(st, vcount.as<int>(), vstart.as<int>(), vsums.as<int>(), m.nv);
+      OTM_CUDA(cudaStreamSynchronize(st));
+      vfaces.reserve(sizeof(int) * (size_t)(nref > 0 ? nref : 1));
+      OTM_CUDA(cudaMemsetAsync(vcount.p, 0, sizeof(int) * m.nv, st));
+      launch(ctx, "vf_fill", k_vf_fill, fblocks, 256, m, (const int*)vstart.as<int>(), vcount.as<int>(),
+             vfaces.as<int>(), inv_area.as<double>());
+      launch(ctx, "vertex_values", k_vertex_values_mesh, vb, 256, m.nv, (const int*)vstart.as<int>(),
+             vfaces.as<int>(), (const double*)inv_area.as<double>(), scale, vval.as<float>());
+      OTM_CUDA(cudaStreamSynchronize(st));  // the temporaries above are freed on return
+    }
+    pv = vval.as<float>();
+  }
+  dim3 blk(32, 8), grd((cols + 31) / 32, (rows + 7) / 8);
+  launch(ctx, "raster", k_raster, grd, blk, m, rows, cols, TX, (const FaceRaster*)fr.as<FaceRaster>(),
+         (const int*)starts.as<int>(), (const int*)faces.as<int>(), pv, img);
+  OTM_CUDA(cudaGetLastError());
+  OTM_CUDA(cudaStreamSynchronize(st));  // fr, faces, vval are freed on return
+}
+
+void raster_grid(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols, int mode,
+                 double* img) {
+  MeshRef m{xy, n, n * n, (n + 1) * (n + 1), nullptr, nullptr};
+  raster_mesh(ctx, m, density, n * n, rows, cols, mode, img);
+}
+
+// Host-side check of an indexed face set (the kernels index with it unchecked).
+static void check_faces(int nv, int nf, const int* start, const int* idx) {
+  if (start[0] != 0) throw BadArg{"otm_rasterize_mesh: face_start[0] must be 0"};
+  for (int f = 0; f < nf; ++f) {
+    const int c = start[f + 1] - start[f];
+    if (c != 3 && c != 4) throw BadArg{"otm_rasterize_mesh: faces must be triangles or quads"};
+  }
+  const int total = start[nf];
+  for (int k = 0; k < total; ++k)
+    if (idx[k] < 0 || idx[k] >= nv) throw BadArg{"otm_rasterize_mesh: vertex index out of range"};
+}
+
+}  // namespace otm
+
+extern "C" int otm_rasterize_mode(otm_context* ctx, int n, const double* xy, const double* density, int rows,
+                                  int cols, int mode, double* img) {
   return guarded([&] {
     if (!ctx || !xy || !img) throw BadArg{"otm_rasterize: null argument"};
     if (n < 1 || n > 16384 || rows < 1 || cols < 1 || rows > 65536 || cols > 65536)
       throw BadArg{"otm_rasterize: size out of range"};
+    if (mode != OTM_RIO_PER_VERTEX && mode != OTM_RIO_PER_FACE) throw BadArg{"otm_rasterize: unknown mode"};
     make_current(ctx);
     cudaStream_t st = ctx->stream;
     const int N = n * n;
     size_t V = (size_t)(n + 1) * (n + 1);
-    const int TX = (cols + RT - 1) / RT, TY = (rows + RT - 1) / RT, nb = TX * TY;
     size_t pix = (size_t)rows * cols;
-    DevBuf dxy, dden, dimg, fr, counts, starts, sums, faces;
+    DevBuf dxy, dden, dimg;
     const double* pxy = xy;
     if (!is_device_ptr(xy)) {
       dxy.reserve(sizeof(double) * 2 * V);
@@ -579,26 +816,70 @@ extern "C" int otm_rasterize(otm_context* ctx, int n, const double* xy, const do
       dimg.reserve(sizeof(double) * pix);
       pimg = dimg.as<double>();
     }
-    fr.reserve(sizeof(FaceRaster) * N);
-    counts.reserve(sizeof(int) * nb);
-    starts.reserve(sizeof(int) * (nb + 1));
-    sums.reserve(sizeof(int) * ((nb + SCAN_B - 1) / SCAN_B + 1));
-    OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
-    float scale = (float)(1. / (double)N);  // rasterizer.cpp:193 keeps this in a float
-    launch(ctx, "raster_count", k_raster_count, (N + 255) / 256, 256, pxy, pden, n, scale, rows, cols, TX,
-           fr.as<FaceRaster>(), counts.as<int>());
-    exclusive_scan(st, counts.as<int>(), starts.as<int>(), sums.as<int>(), nb);
-    int total = 0;
-    OTM_CUDA(cudaMemcpyAsync(&total, starts.as<int>() + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
+    raster_grid(ctx, n, pxy, pden, rows, cols, mode, pimg);
+    if (!idev) OTM_CUDA(cudaMemcpyAsync(img, pimg, sizeof(double) * pix, cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
-    faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1));
-    OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
-    launch(ctx, "raster_fill", k_raster_fill, (N + 255) / 256, 256, (const FaceRaster*)fr.as<FaceRaster>(), n, TX,
-           (const int*)starts.as<int>(), counts.as<int>(), faces.as<int>());
-    dim3 blk(32, 8), grd((cols + 31) / 32, (rows + 7) / 8);
-    launch(ctx, "raster", k_raster, grd, blk, pxy, n, rows, cols, TX, (const FaceRaster*)fr.as<FaceRaster>(),
-           (const int*)starts.as<int>(), (const int*)faces.as<int>(), pimg);
-    OTM_CUDA(cudaGetLastError());
+    ctx->prof.flush();
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
+                             double* img) {
+  return otm_rasterize_mode(ctx, n, xy, density, rows, cols, OTM_RIO_PER_FACE, img);
+}
+
+extern "C" int otm_rasterize_mesh(otm_context* ctx, int nv, const double* xy, int nf, const int* face_start,
+                                  const int* face_vertices, const double* density, int cells, int rows, int cols,
+                                  int mode, double* img) {
+  return guarded([&] {
+    if (!ctx || !img || nv < 0 || nf < 0 || (nv > 0 && !xy) || (nf > 0 && (!face_start || !face_vertices)))
+      throw BadArg{"otm_rasterize_mesh: null argument"};
+    if (rows < 1 || cols < 1 || rows > 65536 || cols > 65536) throw BadArg{"otm_rasterize_mesh: size out of range"};
+    if (mode != OTM_RIO_PER_VERTEX && mode != OTM_RIO_PER_FACE) throw BadArg{"otm_rasterize_mesh: unknown mode"};
+    if (density && cells < nf) throw BadArg{"otm_rasterize_mesh: density shorter than the face count"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    // host copies of the topology, validated before any kernel indexes with it
+    std::vector<int> hstart((size_t)nf + 1, 0);
+    if (nf > 0) copy_out(ctx, hstart.data(), face_start, sizeof(int) * ((size_t)nf + 1));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    const int total = nf > 0 ? hstart[nf] : 0;
+    if (total < 0 || total > 4 * nf) throw BadArg{"otm_rasterize_mesh: bad face_start"};
+    std::vector<int> hidx((size_t)(total > 0 ? total : 1));
+    if (total > 0) copy_out(ctx, hidx.data(), face_vertices, sizeof(int) * (size_t)total);
+    OTM_CUDA(cudaStreamSynchronize(st));
+    if (nf > 0) check_faces(nv, nf, hstart.data(), hidx.data());
+    const size_t pix = (size_t)rows * cols;
+    DevBuf dxy, dden, dimg, dstart, didx;
+    const double* pxy = xy;
+    if (nv > 0 && !is_device_ptr(xy)) {
+      dxy.reserve(sizeof(double) * 2 * (size_t)nv);
+      OTM_CUDA(cudaMemcpyAsync(dxy.p, xy, sizeof(double) * 2 * (size_t)nv, cudaMemcpyHostToDevice, st));
+      pxy = dxy.as<double>();
+    }
+    const double* pden = density;
+    if (density && !is_device_ptr(density)) {
+      dden.reserve(sizeof(double) * (size_t)cells);
+      OTM_CUDA(cudaMemcpyAsync(dden.p, density, sizeof(double) * (size_t)cells, cudaMemcpyHostToDevice, st));
+      pden = dden.as<double>();
+    }
+    bool idev = is_device_ptr(img);
+    double* pimg = img;
+    if (!idev) {
+      dimg.reserve(sizeof(double) * pix);
+      pimg = dimg.as<double>();
+    }
+    if (nf == 0) {
+      OTM_CUDA(cudaMemsetAsync(pimg, 0, sizeof(double) * pix, st));
+    } else {
+      dstart.reserve(sizeof(int) * ((size_t)nf + 1));
+      didx.reserve(sizeof(int) * (size_t)total);
+      OTM_CUDA(cudaMemcpyAsync(dstart.p, hstart.data(), sizeof(int) * ((size_t)nf + 1), cudaMemcpyHostToDevice, st));
+      OTM_CUDA(cudaMemcpyAsync(didx.p, hidx.data(), sizeof(int) * (size_t)total, cudaMemcpyHostToDevice, st));
+      MeshRef m{pxy, 0, nf, nv, dstart.as<int>(), didx.as<int>()};
+      raster_mesh(ctx, m, pden, cells, rows, cols, mode, pimg);
+    }
     if (!idev) OTM_CUDA(cudaMemcpyAsync(img, pimg, sizeof(double) * pix, cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();

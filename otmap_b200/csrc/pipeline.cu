@@ -1,0 +1,246 @@
+// Operations around the solve that the reference's callers use: blending inverse maps
+// and rendering the blend (bilinear barycenters, apps/barycenters.cpp:127-139, 250-290)
+// and the transport cost of a mesh map (otlib/transport_map.cpp:131-215). Compiled
+// without FMA contraction so the per-element arithmetic rounds as the reference's does.
+
+#include <algorithm>
+#include <vector>
+
+#include "context.h"
+
+namespace otm {
+
+// out = sum_k w_k mesh_k, left to right (bilerp / lerp of apps/barycenters.cpp:127-139).
+__global__ void k_blend(long V2, int count, const double* const* meshes, const double* w, double* out) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= V2) return;
+  double acc = w[0] * meshes[0][t];
+  for (int k = 1; k < count; ++k) acc = acc + w[k] * meshes[k][t];
+  out[t] = acc;
+}
+
+__device__ __forceinline__ double sarea3(double ax, double ay, double bx, double by, double cx, double cy) {
+  return 0.5 * ((bx - ax) * (cy - ay) - (by - ay) * (cx - ax));
+}
+
+// transport_cost, quad grid mesh: per face the triangle (v3, v0, v1) of its circulation
+// (transport_map.cpp:184-199), with partial sums of density*area and of the costs.
+__global__ void k_cost_faces(int n, const double* src, const double* dst, const double* density, double* per_face,
+                             double* partial) {
+  __shared__ double red[64];
+  const long N = (long)n * n;
+  double v[2] = {0.0, 0.0};
+  for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / n), j = (int)(f % n);
+    const long t[3] = {(long)(j + 1) + (long)i * (n + 1), (long)j + (long)i * (n + 1),
+                       (long)j + (long)(i + 1) * (n + 1)};
+    const double area = sarea3(src[2 * t[0]], src[2 * t[0] + 1], src[2 * t[1]], src[2 * t[1] + 1], src[2 * t[2]],
+                               src[2 * t[2] + 1]);
+    double dx[3], dy[3];
+    for (int k = 0; k < 3; ++k) {
+      dx[k] = dst[2 * t[k]] - src[2 * t[k]];
+      dy[k] = dst[2 * t[k] + 1] - src[2 * t[k] + 1];
+    }
+    auto dist2 = [&](double l1, double l2, double l3) {
+      double x = l1 * dx[0] + l2 * dx[1] + l3 * dx[2];
+      double y = l1 * dy[0] + l2 * dy[1] + l3 * dy[2];
+      return x * x + y * y;
+    };
+    double cost = (dist2(0.5, 0.5, 0) + dist2(0, 0.5, 0.5) + dist2(0.5, 0, 0.5)) / 3.0;
+    const double da = density[f] * area;
+    cost = da * cost;
+    if (per_face) per_face[f] = cost;
+    v[0] += da;
+    v[1] += cost;
+  }
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = v[0];
+    partial[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
+// integral and total from the partials (fixed order), per_face /= integral.
+__global__ void k_cost_finish(long N, int nblocks, const double* partial, double* per_face, double* result) {
+  __shared__ double red[64];
+  __shared__ double s_int;
+  double v[2] = {0.0, 0.0};
+  for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    v[0] += partial[2 * b];
+    v[1] += partial[2 * b + 1];
+  }
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    s_int = v[0];
+    result[0] = v[1] / v[0];
+    result[1] = v[0];
+  }
+  __syncthreads();
+  if (per_face)
+    for (long f = threadIdx.x; f < N; f += blockDim.x) per_face[f] /= s_int;
+}
+
+// Sum of img in a fixed order: per-block partials over a grid-stride loop.
+__global__ void k_img_partials(long count, const double* img, double* partial) {
+  __shared__ double red[32];
+  double v[1] = {0.0};
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (long)gridDim.x * blockDim.x)
+    v[0] += img[t];
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
+}
+
+// img *= expected_mean / mean(img) (apps/barycenters.cpp:284); every block forms the
+// same total from the partials in the same order.
+__global__ void k_img_rescale(long count, int nparts, const double* partial, double expected_mean, double* img,
+                              double* mean_out) {
+  __shared__ double red[32];
+  __shared__ double s_factor;
+  double v[1] = {0.0};
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) v[0] += partial[b];
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) {
+    const double mean = v[0] / (double)count;
+    s_factor = expected_mean / mean;
+    if (blockIdx.x == 0 && mean_out) *mean_out = mean;
+  }
+  __syncthreads();
+  const double factor = s_factor;
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (long)gridDim.x * blockDim.x)
+    img[t] = img[t] * factor;
+}
+
+// Device copies of `count` meshes of V2 doubles: device pointers are used in place,
+// host ones are staged into `stage`.
+static std::vector<const double*> stage_meshes(otm_context* ctx, const double* const* meshes, int count, size_t V2,
+                                               double* stage) {
+  std::vector<const double*> ptrs(count);
+  for (int k = 0; k < count; ++k) {
+    if (!meshes[k]) throw BadArg{"null mesh"};
+    if (is_device_ptr(meshes[k])) {
+      ptrs[k] = meshes[k];
+    } else {
+      double* d = stage + V2 * k;
+      OTM_CUDA(cudaMemcpyAsync(d, meshes[k], sizeof(double) * V2, cudaMemcpyHostToDevice, ctx->stream));
+      ptrs[k] = d;
+    }
+  }
+  return ptrs;
+}
+
+}  // namespace otm
+
+using namespace otm;
+
+extern "C" int otm_mesh_blend(otm_context* ctx, int n, int count, const double* const* meshes, const double* weights,
+                              double* out) {
+  return guarded([&] {
+    if (!ctx || !meshes || !weights || !out || count < 1 || count > 64) throw BadArg{"otm_mesh_blend: bad arguments"};
+    if (n < 1 || n > 16384) throw BadArg{"otm_mesh_blend: grid size out of range"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    const size_t V2 = 2 * (size_t)(n + 1) * (n + 1);
+    DevBuf buf;
+    buf.reserve(sizeof(double) * (V2 * (count + 1) + count + 8) + sizeof(double*) * count);
+    double* base = buf.as<double>();
+    std::vector<const double*> ptrs = stage_meshes(ctx, meshes, count, V2, base);
+    double* d_out = base + V2 * count;
+    double* d_w = d_out + V2;
+    const double** d_ptrs = reinterpret_cast<const double**>(d_w + count + (count & 1));
+    OTM_CUDA(cudaMemcpyAsync(d_w, weights, sizeof(double) * count, cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(d_ptrs, ptrs.data(), sizeof(double*) * count, cudaMemcpyHostToDevice, st));
+    const bool odev = is_device_ptr(out);
+    double* dst = odev ? out : d_out;
+    launch(ctx, "blend", k_blend, (unsigned)((V2 + 255) / 256), 256, (long)V2, count, (const double* const*)d_ptrs,
+           (const double*)d_w, dst);
+    OTM_CUDA(cudaGetLastError());
+    if (!odev) OTM_CUDA(cudaMemcpyAsync(out, dst, sizeof(double) * V2, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_transport_cost(otm_context* ctx, int n, const double* src_xy, const double* dst_xy,
+                                  const double* density, double* per_face, double* cost) {
+  return guarded([&] {
+    if (!ctx || !src_xy || !dst_xy || !density || !cost) throw BadArg{"otm_transport_cost: null argument"};
+    if (n < 1 || n > 16384) throw BadArg{"otm_transport_cost: grid size out of range"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    const size_t V2 = 2 * (size_t)(n + 1) * (n + 1), N = (size_t)n * n;
+    const int nb = 512;
+    DevBuf buf;
+    buf.reserve(sizeof(double) * (2 * V2 + 2 * N + 2 * nb + 8));
+    double* p = buf.as<double>();
+    auto in = [&](const double* src, double* tmp, size_t words) -> const double* {
+      if (is_device_ptr(src)) return src;
+      OTM_CUDA(cudaMemcpyAsync(tmp, src, sizeof(double) * words, cudaMemcpyHostToDevice, st));
+      return tmp;
+    };
+    const double* d_src = in(src_xy, p, V2);
+    const double* d_dst = in(dst_xy, p + V2, V2);
+    const double* d_den = in(density, p + 2 * V2, N);
+    double* d_pf = per_face ? (is_device_ptr(per_face) ? per_face : p + 2 * V2 + N) : nullptr;
+    double* d_part = p + 2 * V2 + 2 * N;
+    double* d_res = d_part + 2 * nb;
+    launch(ctx, "cost_faces", k_cost_faces, nb, 256, n, d_src, d_dst, d_den, d_pf, d_part);
+    launch(ctx, "cost_finish", k_cost_finish, 1, 1024, (long)N, nb, (const double*)d_part, d_pf, d_res);
+    OTM_CUDA(cudaGetLastError());
+    double res[2];
+    OTM_CUDA(cudaMemcpyAsync(res, d_res, sizeof(res), cudaMemcpyDeviceToHost, st));
+    if (per_face && !is_device_ptr(per_face))
+      OTM_CUDA(cudaMemcpyAsync(per_face, d_pf, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    *cost = res[0];
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_barycenter(otm_context* ctx, int n, int count, const double* const* inv_meshes,
+                              const double* weights, double expected_mean, int rows, int cols, double* mesh_out,
+                              double* img, double* raster_mean) {
+  return guarded([&] {
+    if (!ctx || !inv_meshes || !weights || !img || count < 1 || count > 64)
+      throw BadArg{"otm_barycenter: bad arguments"};
+    if (n < 1 || n > 16384 || rows < 1 || cols < 1 || rows > 65536 || cols > 65536)
+      throw BadArg{"otm_barycenter: size out of range"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    const size_t V2 = 2 * (size_t)(n + 1) * (n + 1), pix = (size_t)rows * cols;
+    const int nparts = 512;
+    DevBuf buf;
+    buf.reserve(sizeof(double) * (V2 * (count + 1) + count + pix + nparts + 16) + sizeof(double*) * count);
+    double* base = buf.as<double>();
+    std::vector<const double*> ptrs = stage_meshes(ctx, inv_meshes, count, V2, base);
+    double* d_mesh = base + V2 * count;
+    double* d_w = d_mesh + V2;
+    double* d_img = d_w + count + (count & 1);
+    double* d_part = d_img + pix;
+    double* d_mean = d_part + nparts;
+    const double** d_ptrs = reinterpret_cast<const double**>(d_mean + 8);
+    OTM_CUDA(cudaMemcpyAsync(d_w, weights, sizeof(double) * count, cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(d_ptrs, ptrs.data(), sizeof(double*) * count, cudaMemcpyHostToDevice, st));
+    const bool mdev = mesh_out && is_device_ptr(mesh_out);
+    double* pm = mdev ? mesh_out : d_mesh;
+    launch(ctx, "blend", k_blend, (unsigned)((V2 + 255) / 256), 256, (long)V2, count, (const double* const*)d_ptrs,
+           (const double*)d_w, pm);
+    const bool idev = is_device_ptr(img);
+    double* pi = idev ? img : d_img;
+    raster_grid(ctx, n, pm, nullptr, rows, cols, OTM_RIO_PER_FACE, pi);
+    launch(ctx, "img_partials", k_img_partials, nparts, 256, (long)pix, (const double*)pi, d_part);
+    const unsigned sb = (unsigned)std::min<size_t>((pix + 255) / 256, (size_t)4 * ctx->num_sms);
+    launch(ctx, "img_rescale", k_img_rescale, sb, 256, (long)pix, nparts, (const double*)d_part, expected_mean, pi,
+           d_mean);
+    OTM_CUDA(cudaGetLastError());
+    if (mesh_out && !mdev) OTM_CUDA(cudaMemcpyAsync(mesh_out, pm, sizeof(double) * V2, cudaMemcpyDeviceToHost, st));
+    if (!idev) OTM_CUDA(cudaMemcpyAsync(img, pi, sizeof(double) * pix, cudaMemcpyDeviceToHost, st));
+    double mean = 0;
+    OTM_CUDA(cudaMemcpyAsync(&mean, d_mean, sizeof(double), cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    if (raster_mean) *raster_mean = mean;
+    return (int)OTM_OK;
+  });
+}

@@ -27,6 +27,8 @@ OPT_POISSON = 1
 POISSON_AUTO, POISSON_DENSE, POISSON_FFT = 0, 1, 2
 OPT_LOOP = 2
 LOOP_GRAPH, LOOP_HOST = 0, 1
+RIO_PER_VERTEX, RIO_PER_FACE = 0, 1
+INV_DENSEST, INV_FIRST = 0, 1
 OUTCOMES = {CONVERGED: "converged", MAX_ITER: "max_iter", SMALL_STEP: "small_step", NONFINITE: "nonfinite"}
 
 _dp = C.POINTER(C.c_double)
@@ -78,7 +80,25 @@ SIGNATURES = {
     "otm_map_init_inverse": (C.c_int, [C.c_void_p]),
     "otm_map_inverse": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_void_p, C.c_void_p,
                                   C.POINTER(C.c_long)]),
+    "otm_map_inverse_mode": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.POINTER(C.c_long)]),
     "otm_rasterize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "otm_rasterize_mode": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                     C.c_void_p]),
+    "otm_rasterize_mesh": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "otm_transport_cost": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.POINTER(C.c_double)]),
+    "otm_mesh_blend": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp, C.c_void_p]),
+    "otm_barycenter": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp, C.c_double, C.c_int,
+                                 C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
+    "otm_grid_faces": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
+    "otm_write_off": (C.c_int, [C.c_char_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "otm_read_off": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,
+                               C.c_void_p, C.c_void_p]),
+    "otm_prune_empty_faces": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.POINTER(C.c_int), C.c_void_p, C.POINTER(C.c_int), C.c_void_p,
+                                        C.c_void_p]),
     "otm_solve_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.POINTER(SolverOptionsC), C.c_void_p, C.c_void_p,
                                     C.POINTER(SolveStatsC), C.c_void_p]),
     "otm_set_option": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),

@@ -111,15 +111,23 @@ class TransportMap:
         self.apply_inverse(q)
         return q[0]
 
-    def apply_inverse(self, points: np.ndarray, face=None, nhits=None) -> int:
-        """In place on a (P, 2) float64 array; returns the number of points with no face."""
+    def inv_fast(self, p) -> np.ndarray:
+        """transport_map.h:45: the first containing face (lowest index) and its weights."""
+        q = np.array(p, dtype=np.float64).reshape(1, 2)
+        self.apply_inverse(q, fast=True)
+        return q[0]
+
+    def apply_inverse(self, points: np.ndarray, face=None, nhits=None, fast: bool = False) -> int:
+        """In place on a (P, 2) float64 array; returns the number of points with no face.
+        fast=False chooses faces as inv does, fast=True as inv_fast."""
         import ctypes as C
 
         if points.dtype != np.float64 or not points.flags["C_CONTIGUOUS"]:
             raise TypeError("points must be a C-contiguous float64 (P, 2) array")
         missing = C.c_long(0)
-        _n.check(_n.lib().otm_map_inverse(self._device_map(), _n.ptr(points), points.shape[0], _n.ptr(face),
-                                          _n.ptr(nhits), C.byref(missing)))
+        mode = _n.INV_FIRST if fast else _n.INV_DENSEST
+        _n.check(_n.lib().otm_map_inverse_mode(self._device_map(), _n.ptr(points), points.shape[0], mode,
+                                               _n.ptr(face), _n.ptr(nhits), C.byref(missing)))
         return missing.value
 
 
@@ -180,22 +188,216 @@ def apply_inverse_map(tmap: TransportMap, points: np.ndarray, verbose_level: int
         print(f"Error: no face found for {missing} point(s).", file=sys.stderr)
 
 
-def rasterize_image(mesh: np.ndarray, density_per_face, img: np.ndarray, n: int | None = None,
-                    context=None) -> None:
-    """rasterize_image (rasterizer.cpp:188-308), PerFace mode, into the pre-sized
-    float64 array img[rows, cols] (row = y). mesh is the (V, 2) vertex array of an
-    (n+1)^2 grid mesh; density_per_face None = unit density."""
-    ctx = context or _n.default_context()
-    mesh = np.ascontiguousarray(mesh, dtype=np.float64)
+class RasterImageOption(enum.IntEnum):
+    """otmap::RasterImageOption (utils/rasterizer.h:16-19)."""
+
+    RIO_PerVertexDensity = 0
+    RIO_PerFaceDensity = 1
+
+
+RIO_PerVertexDensity = RasterImageOption.RIO_PerVertexDensity
+RIO_PerFaceDensity = RasterImageOption.RIO_PerFaceDensity
+
+
+@dataclass
+class Mesh:
+    """A triangle/quad mesh as an indexed face set: vertex positions (V, 2) and face f's
+    corners face_vertices[face_start[f]:face_start[f+1]] in circulation order. The
+    counterpart of the reference's Surface_mesh for meshes other than the grid."""
+
+    xy: np.ndarray
+    face_start: np.ndarray
+    face_vertices: np.ndarray
+
+    @staticmethod
+    def grid(n: int, xy: np.ndarray | None = None) -> "Mesh":
+        """The (n+1)^2 grid mesh (mesh_utils.cpp:90-122), at `xy` (default: the origin grid)."""
+        start = np.empty(n * n + 1, dtype=np.int32)
+        idx = np.empty(4 * n * n, dtype=np.int32)
+        _n.check(_n.lib().otm_grid_faces(n, _n.ptr(start), _n.ptr(idx)))
+        pts = grid_vertices(n) if xy is None else np.ascontiguousarray(xy, dtype=np.float64).reshape(-1, 2)
+        return Mesh(pts.copy(), start, idx)
+
+    @property
+    def n_vertices(self) -> int:
+        return int(self.xy.shape[0])
+
+    @property
+    def n_faces(self) -> int:
+        return int(self.face_start.size - 1)
+
+    def _arrays(self):
+        return (np.ascontiguousarray(self.xy, dtype=np.float64).reshape(-1, 2),
+                np.ascontiguousarray(self.face_start, np.int32), np.ascontiguousarray(self.face_vertices, np.int32))
+
+    def write(self, path: str) -> None:
+        """Surface_mesh::write for .off (surface_mesh/IO_off.cpp:312-380)."""
+        xy, st, ix = self._arrays()
+        _n.check(_n.lib().otm_write_off(str(path).encode(), xy.shape[0], _n.ptr(xy), st.size - 1, _n.ptr(st),
+                                        _n.ptr(ix)))
+
+    @staticmethod
+    def read(path: str) -> "Mesh":
+        """Surface_mesh::read for .off (surface_mesh/IO_off.cpp:45-300)."""
+        import ctypes as C
+
+        nv, nf, ni = C.c_int(0), C.c_int(0), C.c_int(0)
+        _n.check(_n.lib().otm_read_off(str(path).encode(), C.byref(nv), C.byref(nf), C.byref(ni), None, None, None))
+        xy = np.empty((nv.value, 2))
+        st = np.empty(nf.value + 1, dtype=np.int32)
+        ix = np.empty(max(ni.value, 1), dtype=np.int32)
+        _n.check(_n.lib().otm_read_off(str(path).encode(), C.byref(nv), C.byref(nf), C.byref(ni), _n.ptr(xy),
+                                       _n.ptr(st), _n.ptr(ix)))
+        return Mesh(xy, st, ix[:ni.value].copy())
+
+
+def _grid_n(xy: np.ndarray, n: int | None) -> int:
     if n is None:
-        n = int(round(np.sqrt(mesh.shape[0]))) - 1
-    if (n + 1) ** 2 != mesh.shape[0]:
+        n = int(round(np.sqrt(xy.shape[0]))) - 1
+    if n < 1 or (n + 1) ** 2 != xy.shape[0]:
         raise ValueError("mesh is not an (n+1)^2 grid")
+    return n
+
+
+def write_off(path: str, mesh, n: int | None = None) -> None:
+    """Writes a grid mesh ((V, 2) vertex array) or a Mesh as .off, as Surface_mesh::write."""
+    if not isinstance(mesh, Mesh):
+        xy = np.ascontiguousarray(mesh, dtype=np.float64).reshape(-1, 2)
+        mesh = Mesh.grid(_grid_n(xy, n), xy)
+    mesh.write(path)
+
+
+def rasterize_image(mesh, density_per_face, img: np.ndarray, opt: RasterImageOption = RIO_PerFaceDensity,
+                    n: int | None = None, context=None) -> None:
+    """rasterize_image (rasterizer.cpp:188-308) into the pre-sized float64 array
+    img[rows, cols] (row = y). mesh is the (V, 2) vertex array of an (n+1)^2 grid mesh
+    or a Mesh of triangles and quads; density_per_face None = unit density."""
+    ctx = context or _n.default_context()
     if img.dtype != np.float64 or not img.flags["C_CONTIGUOUS"]:
         raise TypeError("img must be a C-contiguous float64 array")
-    d = None if density_per_face is None else _as_cells(density_per_face)
     rows, cols = img.shape
-    _n.check(_n.lib().otm_rasterize(ctx.handle, n, _n.ptr(mesh), _n.ptr(d), rows, cols, _n.ptr(img)))
+    opt = int(opt)
+    if isinstance(mesh, Mesh):
+        xy, st, ix = mesh._arrays()
+        d = None if density_per_face is None else np.ascontiguousarray(density_per_face, dtype=np.float64).ravel()
+        _n.check(_n.lib().otm_rasterize_mesh(ctx.handle, xy.shape[0], _n.ptr(xy), st.size - 1, _n.ptr(st),
+                                             _n.ptr(ix), _n.ptr(d), 0 if d is None else d.size, rows, cols, opt,
+                                             _n.ptr(img)))
+        return
+    xy = np.ascontiguousarray(mesh, dtype=np.float64).reshape(-1, 2)
+    n = _grid_n(xy, n)
+    d = None if density_per_face is None else _as_cells(density_per_face)
+    _n.check(_n.lib().otm_rasterize_mode(ctx.handle, n, _n.ptr(xy), _n.ptr(d), rows, cols, opt, _n.ptr(img)))
+
+
+def transport_cost(src_mesh, dst_mesh, density_per_face, cost_per_face: bool = False, context=None):
+    """transport_cost (transport_map.h:70, transport_map.cpp:131-215) between two
+    (n+1)^2 grid meshes; with cost_per_face=True returns (cost, per-face costs)."""
+    import ctypes as C
+
+    ctx = context or _n.default_context()
+    src = np.ascontiguousarray(src_mesh, dtype=np.float64).reshape(-1, 2)
+    dst = np.ascontiguousarray(dst_mesh, dtype=np.float64).reshape(-1, 2)
+    n = _grid_n(src, None)
+    if dst.shape != src.shape:
+        raise ValueError("meshes differ in size")
+    d = _as_cells(density_per_face)
+    if d.size != n * n:
+        raise ValueError("density does not match the mesh")
+    pf = np.empty(n * n) if cost_per_face else None
+    c = C.c_double(0)
+    _n.check(_n.lib().otm_transport_cost(ctx.handle, n, _n.ptr(src), _n.ptr(dst), _n.ptr(d), _n.ptr(pf), C.byref(c)))
+    return (c.value, pf) if cost_per_face else c.value
+
+
+def prune_empty_faces(mesh, density) -> Mesh:
+    """prune_empty_faces (mesh_utils.cpp:124-141) on a grid vertex array or a Mesh;
+    returns the pruned Mesh (the reference edits its Surface_mesh in place)."""
+    import ctypes as C
+
+    if not isinstance(mesh, Mesh):
+        xy = np.ascontiguousarray(mesh, dtype=np.float64).reshape(-1, 2)
+        mesh = Mesh.grid(_grid_n(xy, None), xy)
+    xy, st, ix = mesh._arrays()
+    d = np.ascontiguousarray(density, dtype=np.float64).ravel()
+    xo = np.empty_like(xy)
+    so = np.empty_like(st)
+    io = np.empty_like(ix)
+    nv, nf = C.c_int(0), C.c_int(0)
+    _n.check(_n.lib().otm_prune_empty_faces(xy.shape[0], _n.ptr(xy), st.size - 1, _n.ptr(st), _n.ptr(ix), _n.ptr(d),
+                                            d.size, C.byref(nv), _n.ptr(xo), C.byref(nf), _n.ptr(so), _n.ptr(io)))
+    return Mesh(xo[:nv.value].copy(), so[:nf.value + 1].copy(), io[:so[nf.value]].copy())
+
+
+def bilinear_weights(alpha: float, beta: float):
+    """Weights of bilerp(alpha, beta, a0..a3) (apps/barycenters.cpp:127-134)."""
+    a, b = float(alpha), float(beta)
+    return [(1. - a) * (1. - b), a * (1. - b), a * b, (1. - a) * b]
+
+
+def linear_weights(alpha: float):
+    """Weights of lerp(alpha, a0, a1) (apps/barycenters.cpp:136-139)."""
+    a = float(alpha)
+    return [1. - a, a]
+
+
+def _blend_args(inv_maps, alpha, beta):
+    ms = [np.ascontiguousarray(m, dtype=np.float64).reshape(-1, 2) for m in inv_maps]
+    if len(ms) == 4 and beta is not None:
+        w = bilinear_weights(alpha, beta)
+    elif len(ms) == 2:
+        w = linear_weights(alpha)
+    else:
+        raise ValueError("barycenters take 2 maps (alpha) or 4 maps (alpha, beta)")
+    return ms, w
+
+
+def interpolate(inv_maps, alpha: float, beta: float | None = None, context=None) -> np.ndarray:
+    """interpolate (apps/barycenters.cpp:250-276): the bilinear (4 maps, alpha and beta)
+    or linear (2 maps) blend of inverse meshes, vertex by vertex, on the GPU."""
+    import ctypes as C
+
+    ctx = context or _n.default_context()
+    ms, w = _blend_args(inv_maps, alpha, beta)
+    n = _grid_n(ms[0], None)
+    out = np.empty_like(ms[0])
+    arr = (C.c_void_p * len(ms))(*[m.ctypes.data for m in ms])
+    wc = (C.c_double * len(w))(*w)
+    _n.check(_n.lib().otm_mesh_blend(ctx.handle, n, len(ms), arr, wc, _n.ptr(out)))
+    return out
+
+
+def barycenter_image(inv_maps, alpha: float, beta: float | None, density_means, res: int, context=None):
+    """One image of the barycenters demo (apps/barycenters.cpp:250-290): interpolate the
+    inverse meshes, rasterize with unit density at res x res, rescale to the blended
+    mean of the input densities. Returns (image[res, res], blended mesh)."""
+    import ctypes as C
+
+    ctx = context or _n.default_context()
+    ms, w = _blend_args(inv_maps, alpha, beta)
+    m = [float(x) for x in density_means]
+    if len(ms) == 4:
+        a, b = float(alpha), float(beta)
+        expected = (1. - a) * (1. - b) * m[0] + a * (1. - b) * m[1] + a * b * m[2] + (1. - a) * b * m[3]
+    else:
+        a = float(alpha)
+        expected = (1. - a) * m[0] + a * m[1]
+    n = _grid_n(ms[0], None)
+    img = np.empty((res, res))
+    mesh = np.empty_like(ms[0])
+    arr = (C.c_void_p * len(ms))(*[x.ctypes.data for x in ms])
+    wc = (C.c_double * len(w))(*w)
+    _n.check(_n.lib().otm_barycenter(ctx.handle, n, len(ms), arr, wc, expected, res, res, _n.ptr(mesh), _n.ptr(img),
+                                     None))
+    return img, mesh
+
+
+def compose(tmap_u: TransportMap, tmap_v: TransportMap, verbose_level: int = 0) -> np.ndarray:
+    """The map u -> v of apps/otmap.cpp:120-126: map u's forward mesh pulled through the
+    inverse of map v. Returns the composite (n_u+1)^2 vertex array."""
+    pts = np.array(tmap_u.fwd_mesh(), dtype=np.float64, copy=True)
+    apply_inverse_map(tmap_v, pts, verbose_level)
+    return pts
 
 
 def solve_batch(densities, opt: SolverOptions | None = None, context=None):

@@ -1,0 +1,181 @@
+"""Parity of the CUDA rows around the solver (through the C ABI) with the reference's
+golden vectors: the PerVertex raster option, triangle and pruned meshes, barycenter
+blending and images, transport costs and composite maps. Bit-exact except where the
+reference sums sequentially and the GPU in a fixed tree order (costs, image means):
+there the tolerance is a few ulps, stated per test."""
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden
+
+pytestmark = pytest.mark.gpu
+
+SUM_RTOL = 1e-13  # sequential vs tree-ordered sums of ~1e3..1e6 positive terms
+
+
+@pytest.fixture(scope="module")
+def ot():
+    from otmap_b200 import otmap
+
+    return otmap
+
+
+@pytest.mark.parametrize("name", golden_names("rasterpv_"))
+def test_per_vertex_raster_bit_exact(name, ot):
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    n = int(g["n"])
+    for key in g:
+        if not key.startswith("img_"):
+            continue
+        tag, size = key[4:].split("_")
+        rows, cols = map(int, size.split("x"))
+        dens = s["adjusted"] if tag == "dens" else None
+        img = np.empty((rows, cols))
+        ot.rasterize_image(s["fwd"], dens, img, ot.RIO_PerVertexDensity, n=n)
+        assert np.array_equal(img, g[key]), key
+        # the same mesh as an indexed face set takes the general path
+        img2 = np.empty((rows, cols))
+        ot.rasterize_image(ot.Mesh.grid(n, s["fwd"]), dens, img2, ot.RIO_PerVertexDensity)
+        assert np.array_equal(img2, g[key]), key
+
+
+@pytest.mark.parametrize("name", golden_names("raster_"))
+def test_per_face_raster_through_indexed_mesh(name, ot):
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    n = int(g["n"])
+    mesh = ot.Mesh.grid(n, s["fwd"])
+    for key in g:
+        if not key.startswith("img_"):
+            continue
+        tag, size = key[4:].split("_")
+        rows, cols = map(int, size.split("x"))
+        img = np.empty((rows, cols))
+        ot.rasterize_image(mesh, s["adjusted"] if tag == "dens" else None, img)
+        assert np.array_equal(img, g[key]), key
+
+
+@pytest.mark.parametrize("name", golden_names("meshraster_"))
+def test_triangle_and_pruned_mesh_raster_bit_exact(name, ot):
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    rows, cols = g["tri_dens_face"].shape
+    tri = ot.Mesh(s["fwd"], g["tri_start"], g["tri_idx"])
+    pruned = ot.Mesh(g["pruned_xy"], g["pruned_start"], g["pruned_idx"])
+    tpruned = ot.Mesh(g["tpruned_xy"], g["tpruned_start"], g["tpruned_idx"])
+    for mode, opt in [("face", ot.RIO_PerFaceDensity), ("vertex", ot.RIO_PerVertexDensity)]:
+        for mesh, dens, key in [(tri, np.repeat(s["adjusted"], 2), f"tri_dens_{mode}"),
+                                (tri, None, f"tri_unit_{mode}"), (pruned, None, f"pruned_unit_{mode}"),
+                                (tpruned, None, f"tpruned_unit_{mode}")]:
+            img = np.empty((rows, cols))
+            ot.rasterize_image(mesh, dens, img, opt)
+            assert np.array_equal(img, g[key]), key
+
+
+def test_mesh_raster_rejects_bad_topology(ot):
+    from otmap_b200 import native
+
+    img = np.empty((8, 8))
+    bad = ot.Mesh(np.zeros((3, 2)), np.array([0, 3], np.int32), np.array([0, 1, 3], np.int32))
+    with pytest.raises(native.OtmError):
+        ot.rasterize_image(bad, None, img)
+    pent = ot.Mesh(np.zeros((5, 2)), np.array([0, 5], np.int32), np.arange(5, dtype=np.int32))
+    with pytest.raises(native.OtmError):
+        ot.rasterize_image(pent, None, img)
+    empty = ot.Mesh(np.zeros((0, 2)), np.zeros(1, np.int32), np.zeros(0, np.int32))
+    ot.rasterize_image(empty, None, img)
+    assert not img.any()
+
+
+def test_barycenter_blend_and_images(ot):
+    g = load_golden("barycenter_shapes_n32.npz")
+    n = int(g["n"])
+    inv = list(g["inv"])
+    for k, (a, b) in enumerate(g["pairs"]):
+        assert np.array_equal(ot.interpolate(inv, a, b), g[f"mesh_{k}"])
+        img, mesh = ot.barycenter_image(inv, a, b, g["means"], n)
+        assert np.array_equal(mesh, g[f"mesh_{k}"])
+        np.testing.assert_allclose(img, g[f"img_{k}"], rtol=SUM_RTOL, atol=0)
+    for k, a in enumerate(g["lalphas"]):
+        assert np.array_equal(ot.interpolate(inv[:2], a), g[f"lmesh_{k}"])
+        img, _ = ot.barycenter_image(inv[:2], a, None, g["means"][:2], n)
+        np.testing.assert_allclose(img, g[f"limg_{k}"], rtol=SUM_RTOL, atol=0)
+
+
+def test_barycenter_pipeline_from_densities(ot):
+    """The whole demo on the GPU: batched solves of the four densities, inverse of the
+    grid vertices, one barycenter image whose mean is the blended density mean."""
+    g = load_golden("barycenter_shapes_n32.npz")
+    n = int(g["n"])
+    maps = ot.solve_batch(list(g["images"]))
+    inv = []
+    for k, m in enumerate(maps):
+        assert np.abs(m.fwd_mesh() - g["fwd"][k]).max() <= 1e-6
+        pts = ot.grid_vertices(n)
+        nh = np.zeros(pts.shape[0], dtype=np.int32)
+        m.apply_inverse(pts, None, nh)
+        assert (nh >= 1).all()
+        assert np.abs(pts - g["inv"][k]).max() <= 1e-4
+        inv.append(pts)
+    img, _ = ot.barycenter_image(inv, 0.25, 0.5, g["means"], n)
+    assert np.isfinite(img).all()
+    np.testing.assert_allclose(img.mean(), float(g["expected_1"]), rtol=1e-12)
+
+
+def test_inverse_fast_mode_agrees_on_single_hits(ot):
+    s = load_golden("solve_mix_n64_s1.npz")
+    g = load_golden("inverse_mix_n64_s1.npz")
+    tm = ot.TransportMap(64, s["fwd"], s["adjusted"])
+    a = np.ascontiguousarray(g["points"].copy())
+    b = a.copy()
+    nh = np.zeros(a.shape[0], dtype=np.int32)
+    tm.apply_inverse(a, None, nh)
+    tm.apply_inverse(b, fast=True)
+    one = nh == 1
+    assert np.array_equal(a[one], b[one])
+    assert np.array_equal(b[one], g["inverse"][one])
+
+
+@pytest.mark.parametrize("name", golden_names("cost_"))
+def test_transport_cost_matches_reference(name, ot):
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    n = int(g["n"])
+    c, pf = ot.transport_cost(ot.grid_vertices(n), s["fwd"], s["adjusted"], cost_per_face=True)
+    np.testing.assert_allclose(c, float(g["cost"]), rtol=SUM_RTOL, atol=0)
+    np.testing.assert_allclose(pf, g["per_face"], rtol=SUM_RTOL, atol=0)
+    assert ot.transport_cost(ot.grid_vertices(n), s["fwd"], s["adjusted"]) == c
+
+
+def test_composite_maps_and_costs(ot):
+    g = load_golden("compose_mix_n32_n37.npz")
+    u = load_golden(str(g["u"]) + ".npz")
+    v = load_golden(str(g["v"]) + ".npz")
+    tu = ot.TransportMap(int(u["n"]), u["fwd"], u["adjusted"])
+    tv = ot.TransportMap(int(v["n"]), v["fwd"], v["adjusted"])
+    uv, vu = ot.compose(tu, tv), ot.compose(tv, tu)
+    one = g["nhits_uv"] == 1
+    assert np.array_equal(uv[one], g["map_uv"][one])
+    one = g["nhits_vu"] == 1
+    assert np.array_equal(vu[one], g["map_vu"][one])
+    c = ot.transport_cost(ot.grid_vertices(int(u["n"])), uv, u["adjusted"])
+    np.testing.assert_allclose(c, float(g["cost_uv"]), rtol=SUM_RTOL)
+    c = ot.transport_cost(ot.grid_vertices(int(v["n"])), vu, v["adjusted"])
+    np.testing.assert_allclose(c, float(g["cost_vu"]), rtol=SUM_RTOL)
+
+
+def test_large_transport_cost_against_oracle(ot, oracle_port):
+    """1024^2 grid, a smooth displacement and a random density: GPU cost vs the
+    oracle's sequential restatement."""
+    n = 1024
+    rng = np.random.default_rng(11)
+    src = ot.grid_vertices(n)
+    dst = src + 0.01 * np.sin(7 * src[:, ::-1] + rng.random(2))
+    dens = rng.random(n * n) + 0.1
+    c_o = oracle_port.transport_cost(src, dst, dens, n)
+    c, pf = ot.transport_cost(src, dst, dens, cost_per_face=True)
+    np.testing.assert_allclose(c, c_o, rtol=1e-12)
+    assert np.isfinite(pf).all()
+    np.testing.assert_allclose(pf.sum(), c, rtol=1e-12)
