@@ -192,6 +192,7 @@ int guarded(F&& f) {
     return OTM_ERR_BAD_ARG;
   } catch (const CudaError& e) {
     set_error(std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")");
+    cudaGetLastError();  // a non-sticky error must not resurface in the next call's check
     return OTM_ERR_CUDA;
   } catch (const std::exception& e) {
     set_error(e.what());

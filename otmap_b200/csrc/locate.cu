@@ -13,6 +13,7 @@
 
 #include <cfloat>
 #include <cmath>
+#include <cstring>
 #include <vector>
 
 #include "context.h"
@@ -840,15 +841,22 @@ extern "C" int otm_rasterize_mesh(otm_context* ctx, int nv, const double* xy, in
     if (density && cells < nf) throw BadArg{"otm_rasterize_mesh: density shorter than the face count"};
     make_current(ctx);
     cudaStream_t st = ctx->stream;
-    // host copies of the topology, validated before any kernel indexes with it
+    // host copies of the topology (from host or device memory), validated before any
+    // kernel indexes with it
+    auto to_host = [&](int* dst, const int* src, size_t count) {
+      if (is_device_ptr(src)) {
+        OTM_CUDA(cudaMemcpyAsync(dst, src, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+        OTM_CUDA(cudaStreamSynchronize(st));
+      } else {
+        std::memcpy(dst, src, sizeof(int) * count);
+      }
+    };
     std::vector<int> hstart((size_t)nf + 1, 0);
-    if (nf > 0) copy_out(ctx, hstart.data(), face_start, sizeof(int) * ((size_t)nf + 1));
-    OTM_CUDA(cudaStreamSynchronize(st));
+    if (nf > 0) to_host(hstart.data(), face_start, (size_t)nf + 1);
     const int total = nf > 0 ? hstart[nf] : 0;
     if (total < 0 || total > 4 * nf) throw BadArg{"otm_rasterize_mesh: bad face_start"};
     std::vector<int> hidx((size_t)(total > 0 ? total : 1));
-    if (total > 0) copy_out(ctx, hidx.data(), face_vertices, sizeof(int) * (size_t)total);
-    OTM_CUDA(cudaStreamSynchronize(st));
+    if (total > 0) to_host(hidx.data(), face_vertices, (size_t)total);
     if (nf > 0) check_faces(nv, nf, hstart.data(), hidx.data());
     const size_t pix = (size_t)rows * cols;
     DevBuf dxy, dden, dimg, dstart, didx;
