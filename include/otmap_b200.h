@@ -22,6 +22,7 @@
  *   otm_transport_cost    transport_cost                           transport_map.h:70, transport_map.cpp:131-215
  *   otm_mesh_blend        interpolate (bilinear / linear blend)    apps/barycenters.cpp:127-139, 250-276
  *   otm_barycenter        interpolate + synthetize_and_save_image  apps/barycenters.cpp:250-290
+ *   otm_sample_image      sample_transportmap_to_image             utils/stochastic_rasterizer.cpp:19-88
  *   otm_grid_faces        generate_quad_mesh's faces               utils/mesh_utils.cpp:90-122
  *   otm_write_off         Surface_mesh::write (.off)               surface_mesh/IO_off.cpp:312-380
  *   otm_read_off          Surface_mesh::read (.off)                surface_mesh/IO_off.cpp:45-300
@@ -211,6 +212,21 @@ int otm_mesh_blend(otm_context* ctx, int n, int count, const double* const* mesh
  * raster_mean (optional) the mean of the image before rescaling. */
 int otm_barycenter(otm_context* ctx, int n, int count, const double* const* inv_meshes, const double* weights,
                    double expected_mean, int rows, int cols, double* mesh_out, double* img, double* raster_mean);
+
+/* sample_transportmap_to_image (utils/stochastic_rasterizer.cpp:19-88): draws
+ * samples_per_face[f] random points in each face f -- uniform bilinear coordinates
+ * (u, v) in a quad, uniform barycentric coordinates (1-sqrt(r1), sqrt(r1)(1-r2),
+ * sqrt(r1) r2) in a triangle, mapped through the face's corners as the reference maps
+ * them -- and counts them in img[rows*cols] (row-major [y][x]; pixel (int(y/dy),
+ * int(x/dx))); points off the unit square are dropped. The mesh is the (grid_n+1)^2
+ * grid (grid_n > 0: nv, nf must match, the face arrays are ignored) or an indexed
+ * triangle/quad mesh (grid_n = 0). The random numbers come from a counter-based
+ * generator keyed by (seed, face, sample), so an image is reproducible from its seed;
+ * the reference draws from the process-wide std::rand() stream instead, so its images
+ * agree with these in distribution, not sample by sample. */
+int otm_sample_image(otm_context* ctx, int nv, const double* xy, int nf, const int* face_start,
+                     const int* face_vertices, int grid_n, const int* samples_per_face, unsigned long long seed,
+                     int rows, int cols, double* img);
 
 /* ---- meshes as indexed face sets, OFF files (host-side; no device needed) ----
  *

@@ -46,11 +46,13 @@ namespace otmap {
 #ifdef OTMAP_B200_EIGEN
 using Point = Eigen::Vector2d;
 using Vector = Eigen::VectorXd;
+using IndexVector = Eigen::VectorXi;
 using Image = Eigen::MatrixXd;
 inline Vector make_vector(long n, double value = 0.0) { return Vector::Constant(n, value); }
 #else
 using Point = std::array<double, 2>;
 using Vector = std::vector<double>;
+using IndexVector = std::vector<int>;
 // Column-major image with rows = y, like the reference's Eigen::MatrixXd.
 class Image {
  public:
@@ -399,6 +401,31 @@ inline void rasterize_image(const Mesh& mesh, const Vector& density_per_face, Im
 
 inline void rasterize_image(const Mesh& mesh, Image& img, RasterImageOption opt = RIO_PerFaceDensity) {
   rasterize_image(mesh, make_vector(0), img, opt);
+}
+
+// stochastic_rasterizer.h: sample_transportmap_to_image (stochastic_rasterizer.cpp:19-88).
+// img must be sized beforehand; counts of random points per pixel. The points come from
+// a counter-based generator keyed by `seed` (the reference uses std::rand()).
+inline void sample_transportmap_to_image(const Mesh& mesh, const IndexVector& sample_per_face, Image& img,
+                                         unsigned long long seed = 0) {
+  if ((long)sample_per_face.size() != (long)mesh.n_faces())
+    throw std::runtime_error("sample_transportmap_to_image: one sample count per face");
+  const long rows = img.rows(), cols = img.cols();
+  std::vector<double> buf((size_t)(rows * cols));
+  const int g = mesh.grid_size();
+  detail::check(otm_sample_image(detail::default_context()->get(), mesh.n_vertices(), mesh.raw(), mesh.n_faces(),
+                                 g > 0 ? nullptr : mesh.face_start().data(),
+                                 g > 0 ? nullptr : mesh.face_indices().data(), g, sample_per_face.data(), seed,
+                                 (int)rows, (int)cols, buf.data()),
+                "sample_transportmap_to_image");
+  detail::from_row_major(buf, img);
+}
+
+inline void sample_transportmap_to_image(const Mesh& mesh, Image& img, int sample_per_face,
+                                         unsigned long long seed = 0) {
+  IndexVector spf(mesh.n_faces());
+  for (int f = 0; f < mesh.n_faces(); ++f) spf[f] = sample_per_face;
+  sample_transportmap_to_image(mesh, spf, img, seed);
 }
 
 // mesh_utils.h: prune_empty_faces (mesh_utils.cpp:124-141), in place.

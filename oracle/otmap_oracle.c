@@ -979,6 +979,51 @@ int oro_prune_empty_faces(int nv, const double* xy, int nf, const int* start, co
 }
 
 /* ------------------------------------------------------------------------- */
+/* sample_transportmap_to_image (stochastic_rasterizer.cpp:19-88) with the library's
+ * counter-based generator in place of std::rand(): the splitmix64 output function
+ * (Steele, Lea & Flood, OOPSLA 2014) of a (seed, face, sample, draw) key. */
+static unsigned long long mix64(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+static double splat_uniform(unsigned long long key, long sample, int draw) {
+  unsigned long long x = mix64(key + (unsigned long long)(2 * sample + draw + 1) * 0x9e3779b97f4a7c15ULL);
+  return (double)(x >> 11) * 0x1.0p-53;
+}
+
+void oro_sample_image(int nv, const double* xy, int nf, const int* start, const int* idx, const int* spf,
+                      unsigned long long seed, int rows, int cols, double* img) {
+  (void)nv;
+  memset(img, 0, sizeof(double) * (size_t)rows * cols);
+  const double dx = 1. / (double)cols, dy = 1. / (double)rows;
+  for (int f = 0; f < nf; ++f) {
+    double p[8];
+    int vid[4];
+    int c = load_mesh_face(xy, start, idx, f, p, vid);
+    unsigned long long key = mix64(seed ^ mix64((unsigned long long)(f + 1) * 0xd1b54a32d192ed03ULL));
+    for (long s = 0; s < spf[f]; ++s) {
+      double px, py;
+      if (c == 3) {
+        double r1 = sqrt(splat_uniform(key, s, 0)), r2 = splat_uniform(key, s, 1);
+        double b0 = 1. - r1, b1 = r1 * (1. - r2), b2 = r1 * r2;
+        px = b0 * p[0] + b1 * p[2] + b2 * p[4];
+        py = b0 * p[1] + b1 * p[3] + b2 * p[5];
+      } else {
+        double u = splat_uniform(key, s, 0), v = splat_uniform(key, s, 1);
+        double w0 = (1. - u) * (1 - v), w1 = (u) * (1 - v), w2 = (u) * (v), w3 = (1. - u) * (v);
+        px = w0 * p[0] + w1 * p[2] + w2 * p[4] + w3 * p[6];
+        py = w0 * p[1] + w1 * p[3] + w2 * p[5] + w3 * p[7];
+      }
+      if (!(px >= 0 && py >= 0 && px <= 1 && py <= 1)) continue;
+      int pi = (int)(py / dy), pj = (int)(px / dx);
+      if (pi < rows && pj < cols) img[(size_t)pi * cols + pj] += 1.0;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------- */
 /* transport_map.cpp:131-215 for a quad grid mesh: the face count equals the
  * density size, so the reference takes its per-triangle branch (:184-199) on the
  * first three vertices of each face's circulation, which for a Surface_mesh quad

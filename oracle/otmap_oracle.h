@@ -93,6 +93,11 @@ void oro_mesh_blend(long V2, int count, const double* const* meshes, const doubl
 int oro_prune_empty_faces(int nv, const double* xy, int nf, const int* start, const int* idx, const double* density,
                           int cells, int* nv_out, double* xy_out, int* nf_out, int* start_out, int* idx_out);
 
+/* sample_transportmap_to_image (utils/stochastic_rasterizer.cpp:19-88) with the
+ * library's counter-based generator; img row-major [rows][cols]. */
+void oro_sample_image(int nv, const double* xy, int nf, const int* start, const int* idx, const int* spf,
+                      unsigned long long seed, int rows, int cols, double* img);
+
 /* ---- transport_cost for an (n+1)^2 quad grid (transport_map.cpp:131-215, quad branch) ---- */
 double oro_transport_cost(int n, const double* src_xy, const double* dst_xy, const double* density,
                           double* per_face);

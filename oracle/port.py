@@ -69,6 +69,7 @@ def lib():
         L.oro_mesh_blend.argtypes = [C.c_long, C.c_int, C.POINTER(_dp), _dp, _dp]
         L.oro_prune_empty_faces.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_int, _ip, _dp, _ip, _ip, _ip]
         L.oro_prune_empty_faces.restype = C.c_int
+        L.oro_sample_image.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _ip, C.c_ulonglong, C.c_int, C.c_int, _dp]
         _lib = L
     return _lib
 
@@ -268,3 +269,13 @@ def prune_empty_faces(xy, start, idx, density):
     lib().oro_prune_empty_faces(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx), _p(d), d.size,
                                 C.byref(nv), _p(xo), C.byref(nf), _pi(so), _pi(io))
     return xo[:nv.value].copy(), so[:nf.value + 1].copy(), io[:so[nf.value]].copy()
+
+
+def sample_image(xy, start, idx, spf, seed, rows, cols):
+    """Stochastic splat with the library's generator; image is [y][x]."""
+    xy = _f64(xy).reshape(-1, 2)
+    start, idx, spf = _i32(start), _i32(idx), _i32(spf)
+    img = np.zeros((rows, cols))
+    lib().oro_sample_image(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx), _pi(spf), int(seed), rows,
+                           cols, _p(img))
+    return img

@@ -67,6 +67,7 @@ def lib():
         L.otref_write_off.restype = C.c_int
         L.otref_read_off.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _ip, _dp, _ip, _ip, _ip]
         L.otref_read_off.restype = C.c_int
+        L.otref_sample_image.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _ip, C.c_uint, C.c_int, C.c_int, _dp]
         _lib = L
     return _lib
 
@@ -277,3 +278,13 @@ def read_off(path, cap_v, cap_f, cap_i):
     if r != 1:
         raise OSError(f"reference could not read {path} ({r})")
     return xy[:nv.value].copy(), start[:nf.value + 1].copy(), idx[:start[nf.value]].copy()
+
+
+def sample_image(xy, start, idx, spf, seed, rows, cols):
+    """sample_transportmap_to_image (otlib/utils/stochastic_rasterizer.cpp:19-88) after srand(seed)."""
+    xy = _f64(xy).reshape(-1, 2)
+    start, idx, spf = _i32(start), _i32(idx), _i32(spf)
+    img = np.zeros((rows, cols))
+    lib().otref_sample_image(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx), _pi(spf), int(seed), rows,
+                             cols, _p(img))
+    return img

@@ -22,9 +22,11 @@
 #include "utils/bvh2d.h"
 #include "utils/mesh_utils.h"
 #include "utils/rasterizer.h"
+#include "utils/stochastic_rasterizer.h"
 
 #include <xmmintrin.h>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <iostream>
 #include <memory>
@@ -514,6 +516,23 @@ int otref_read_off(const char* path, int cap_v, int cap_f, int cap_i, int* nv, d
     start[f + 1] = k;
   }
   return 1;
+}
+
+// sample_transportmap_to_image (stochastic_rasterizer.cpp:19-88) after srand(seed).
+void otref_sample_image(int nv, const double* xy, int nf, const int* start, const int* idx, const int* spf,
+                        unsigned int seed, int rows, int cols, double* img) {
+  CsrGuard g;
+  Surface_mesh mesh;
+  load_indexed_mesh(mesh, nv, xy, nf, start, idx);
+  VectorXi s = Map<const VectorXi>(spf, nf);
+  MatrixXd im(rows, cols);
+  std::srand(seed);
+  {
+    CoutCapture cap;
+    otmap::sample_transportmap_to_image(mesh, s, im);
+  }
+  for (int y = 0; y < rows; ++y)
+    for (int x = 0; x < cols; ++x) img[(size_t)y * cols + x] = im(y, x);
 }
 
 }  // extern "C"

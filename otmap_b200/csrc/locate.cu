@@ -704,6 +704,57 @@ extern "C" int otm_map_inverse(otm_map* m, double* points, long count, int* face
   return otm_map_inverse_mode(m, points, count, OTM_INV_DENSEST, face, nhits, missing);
 }
 
+// ---- stochastic splatting (utils/stochastic_rasterizer.cpp:19-88) ----
+
+// Counter-based uniform doubles in [0, 1): the splitmix64 output function (Steele, Lea
+// and Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014) applied to
+// a key made of (seed, face, sample, draw), so any sample can be drawn independently.
+__host__ __device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+__device__ __forceinline__ double splat_uniform(unsigned long long face_key, long sample, int draw) {
+  const unsigned long long x = mix64(face_key + (unsigned long long)(2 * sample + draw + 1) * 0x9e3779b97f4a7c15ULL);
+  return (double)(x >> 11) * 0x1.0p-53;
+}
+
+// One warp per face: each of the face's samples is a random point of the face (uniform
+// bilinear coordinates for a quad, uniform barycentric ones for a triangle), counted in
+// the pixel that contains it. Counts are integers, so the atomic additions are exact and
+// the image does not depend on their order.
+__global__ void k_splat(MeshRef m, const int* spf, unsigned long long seed, int rows, int cols, double* img) {
+  const int lane = threadIdx.x & 31;
+  const long f = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (f >= m.nf) return;
+  const int ns = spf[f];
+  if (ns <= 0) return;
+  Quad p;
+  int vid[4];
+  const int c = load_face(m, (int)f, p, vid);
+  const unsigned long long key = mix64(seed ^ mix64((unsigned long long)(f + 1) * 0xd1b54a32d192ed03ULL));
+  const double dx = 1. / double(cols), dy = 1. / double(rows);
+  for (long s = lane; s < ns; s += 32) {
+    double px, py;
+    if (c == 3) {
+      const double r1 = sqrt(splat_uniform(key, s, 0)), r2 = splat_uniform(key, s, 1);
+      const double b0 = 1. - r1, b1 = r1 * (1. - r2), b2 = r1 * r2;
+      px = b0 * p.x[0] + b1 * p.x[1] + b2 * p.x[2];
+      py = b0 * p.y[0] + b1 * p.y[1] + b2 * p.y[2];
+    } else {
+      const double u = splat_uniform(key, s, 0), v = splat_uniform(key, s, 1);
+      const double w0 = (1. - u) * (1 - v), w1 = (u) * (1 - v), w2 = (u) * (v), w3 = (1. - u) * (v);
+      px = w0 * p.x[0] + w1 * p.x[1] + w2 * p.x[2] + w3 * p.x[3];
+      py = w0 * p.y[0] + w1 * p.y[1] + w2 * p.y[2] + w3 * p.y[3];
+    }
+    // stochastic_rasterizer.cpp:71-83: points off the unit square (or not finite) are dropped
+    if (!(px >= 0 && py >= 0 && px <= 1 && py <= 1)) continue;
+    const int pi = (int)(py / dy), pj = (int)(px / dx);
+    if (pi < rows && pj < cols) atomicAdd(&img[(size_t)pi * cols + pj], 1.0);
+  }
+}
+
 namespace otm {
 
 // Rasterizes mesh m (all pointers on the device) into img (device, rows*cols).
@@ -888,6 +939,83 @@ extern "C" int otm_rasterize_mesh(otm_context* ctx, int nv, const double* xy, in
       MeshRef m{pxy, 0, nf, nv, dstart.as<int>(), didx.as<int>()};
       raster_mesh(ctx, m, pden, cells, rows, cols, mode, pimg);
     }
+    if (!idev) OTM_CUDA(cudaMemcpyAsync(img, pimg, sizeof(double) * pix, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    return (int)OTM_OK;
+  });
+}
+
+namespace otm {
+static void splat(otm_context* ctx, const MeshRef& m, const int* spf_dev, unsigned long long seed, int rows, int cols,
+                  double* img_dev) {
+  OTM_CUDA(cudaMemsetAsync(img_dev, 0, sizeof(double) * (size_t)rows * cols, ctx->stream));
+  if (m.nf == 0) return;
+  const unsigned blocks = (unsigned)(((long)m.nf * 32 + 255) / 256);
+  launch(ctx, "splat", k_splat, blocks, 256, m, spf_dev, seed, rows, cols, img_dev);
+  OTM_CUDA(cudaGetLastError());
+}
+}  // namespace otm
+
+extern "C" int otm_sample_image(otm_context* ctx, int nv, const double* xy, int nf, const int* face_start,
+                                const int* face_vertices, int grid_n, const int* samples_per_face,
+                                unsigned long long seed, int rows, int cols, double* img) {
+  return guarded([&] {
+    if (!ctx || !img || !samples_per_face || nf < 0 || nv < 0 || (nv > 0 && !xy))
+      throw BadArg{"otm_sample_image: null argument"};
+    if (rows < 1 || cols < 1 || rows > 65536 || cols > 65536) throw BadArg{"otm_sample_image: size out of range"};
+    const bool grid = grid_n > 0;
+    if (grid && (grid_n > 16384 || nf != grid_n * grid_n || nv != (grid_n + 1) * (grid_n + 1)))
+      throw BadArg{"otm_sample_image: grid_n does not match nv and nf"};
+    if (!grid && nf > 0 && (!face_start || !face_vertices)) throw BadArg{"otm_sample_image: null face arrays"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    std::vector<int> hstart, hidx;
+    if (!grid && nf > 0) {
+      auto to_host = [&](std::vector<int>& dst, const int* src, size_t count) {
+        dst.resize(count);
+        if (is_device_ptr(src)) {
+          OTM_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(int) * count, cudaMemcpyDeviceToHost, st));
+          OTM_CUDA(cudaStreamSynchronize(st));
+        } else {
+          std::memcpy(dst.data(), src, sizeof(int) * count);
+        }
+      };
+      to_host(hstart, face_start, (size_t)nf + 1);
+      if (hstart[nf] < 0 || hstart[nf] > 4 * nf) throw BadArg{"otm_sample_image: bad face_start"};
+      to_host(hidx, face_vertices, (size_t)(hstart[nf] > 0 ? hstart[nf] : 1));
+      check_faces(nv, nf, hstart.data(), hidx.data());
+    }
+    const size_t pix = (size_t)rows * cols;
+    DevBuf dxy, dspf, dimg, dstart, didx;
+    const double* pxy = xy;
+    if (nv > 0 && !is_device_ptr(xy)) {
+      dxy.reserve(sizeof(double) * 2 * (size_t)nv);
+      OTM_CUDA(cudaMemcpyAsync(dxy.p, xy, sizeof(double) * 2 * (size_t)nv, cudaMemcpyHostToDevice, st));
+      pxy = dxy.as<double>();
+    }
+    const int* pspf = samples_per_face;
+    if (nf > 0 && !is_device_ptr(samples_per_face)) {
+      dspf.reserve(sizeof(int) * (size_t)nf);
+      OTM_CUDA(cudaMemcpyAsync(dspf.p, samples_per_face, sizeof(int) * (size_t)nf, cudaMemcpyHostToDevice, st));
+      pspf = dspf.as<int>();
+    }
+    const bool idev = is_device_ptr(img);
+    double* pimg = img;
+    if (!idev) {
+      dimg.reserve(sizeof(double) * pix);
+      pimg = dimg.as<double>();
+    }
+    MeshRef m{pxy, grid ? grid_n : 0, nf, nv, nullptr, nullptr};
+    if (!grid && nf > 0) {
+      dstart.reserve(sizeof(int) * ((size_t)nf + 1));
+      didx.reserve(sizeof(int) * hidx.size());
+      OTM_CUDA(cudaMemcpyAsync(dstart.p, hstart.data(), sizeof(int) * hstart.size(), cudaMemcpyHostToDevice, st));
+      OTM_CUDA(cudaMemcpyAsync(didx.p, hidx.data(), sizeof(int) * hidx.size(), cudaMemcpyHostToDevice, st));
+      m.start = dstart.as<int>();
+      m.idx = didx.as<int>();
+    }
+    splat(ctx, m, pspf, seed, rows, cols, pimg);
     if (!idev) OTM_CUDA(cudaMemcpyAsync(img, pimg, sizeof(double) * pix, cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();

@@ -92,6 +92,8 @@ SIGNATURES = {
     "otm_mesh_blend": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp, C.c_void_p]),
     "otm_barycenter": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp, C.c_double, C.c_int,
                                  C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),
+    "otm_sample_image": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                   C.c_void_p, C.c_ulonglong, C.c_int, C.c_int, C.c_void_p]),
     "otm_grid_faces": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p]),
     "otm_write_off": (C.c_int, [C.c_char_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     "otm_read_off": (C.c_int, [C.c_char_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_void_p,

@@ -329,6 +329,55 @@ def prune_empty_faces(mesh, density) -> Mesh:
     return Mesh(xo[:nv.value].copy(), so[:nf.value + 1].copy(), io[:so[nf.value]].copy())
 
 
+def sample_transportmap_to_image(mesh, samples_per_face, img: np.ndarray, seed: int = 0, context=None) -> None:
+    """sample_transportmap_to_image (stochastic_rasterizer.cpp:19-88) into the pre-sized
+    float64 img[rows, cols]: samples_per_face[f] random points per face (an int, or one
+    per face), counted per pixel. Reproducible from `seed` (a counter-based generator
+    in place of the reference's std::rand())."""
+    ctx = context or _n.default_context()
+    if img.dtype != np.float64 or not img.flags["C_CONTIGUOUS"]:
+        raise TypeError("img must be a C-contiguous float64 array")
+    rows, cols = img.shape
+    if isinstance(mesh, Mesh):
+        xy, st, ix = mesh._arrays()
+        grid_n, nf = 0, st.size - 1
+    else:
+        xy = np.ascontiguousarray(mesh, dtype=np.float64).reshape(-1, 2)
+        grid_n = _grid_n(xy, None)
+        nf, st, ix = grid_n * grid_n, None, None
+    spf = np.broadcast_to(np.asarray(samples_per_face, dtype=np.int32), (nf,))
+    spf = np.ascontiguousarray(spf)
+    _n.check(_n.lib().otm_sample_image(ctx.handle, xy.shape[0], _n.ptr(xy), nf, _n.ptr(st), _n.ptr(ix), grid_n,
+                                       _n.ptr(spf), int(seed) & 0xFFFFFFFFFFFFFFFF, rows, cols, _n.ptr(img)))
+
+
+def synthetize_image(map_mesh, img_res: int, target, input_density=None, samples_per_face: int = 300,
+                     seed: int = 0, context=None):
+    """The two renderings of a map in apps/common/generic_tasks.cpp:71-99: stochastic
+    samples (samples per face proportional to input_density, or constant) scaled to the
+    target's mass, and the unit-density raster scaled to the target's mean. Returns
+    (sampled image, raster image), both img_res x img_res, row = y."""
+    t = np.asarray(target, dtype=np.float64).ravel()
+    if isinstance(map_mesh, Mesh):
+        nf = map_mesh.n_faces
+    else:
+        nf = _grid_n(np.asarray(map_mesh).reshape(-1, 2), None) ** 2
+    if input_density is not None:
+        d = np.asarray(input_density, dtype=np.float64).ravel()
+        spf = (samples_per_face * d.size / d.sum() * d).astype(np.int32)
+        if nf == 2 * spf.size:  # a grid of triangles: two faces per cell
+            spf = np.repeat(spf, 2)
+    else:
+        spf = np.full(nf, samples_per_face, dtype=np.int32)
+    sampled = np.empty((img_res, img_res))
+    sample_transportmap_to_image(map_mesh, spf, sampled, seed, context)
+    sampled *= t.sum() / float(samples_per_face * nf)
+    raster = np.empty((img_res, img_res))
+    rasterize_image(map_mesh, None, raster, context=context)
+    raster = raster * t.sum() / t.size
+    return sampled, raster
+
+
 def bilinear_weights(alpha: float, beta: float):
     """Weights of bilerp(alpha, beta, a0..a3) (apps/barycenters.cpp:127-134)."""
     a, b = float(alpha), float(beta)

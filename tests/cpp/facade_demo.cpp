@@ -114,6 +114,10 @@ static int pipeline_mode(const std::string& dir, const std::string& fu, const st
     interpolate(inv, 0.5, mid);
     dump(dir + "/mid.f64", mid.raw(), 2 * (size_t)mid.n_vertices());
   }
+  // stochastic splat of the composite map, 50 samples per face
+  Image sp(nu, nu);
+  sample_transportmap_to_image(tmaps[0].fwd_mesh(), sp, 50, 7);
+  dump_image(dir + "/u_fwd_samples.f64", sp);
   // many solves in one run
   std::vector<Vector> both = {du, dv};
   std::vector<TransportMap> batch = solver.solve_batch(both);

@@ -88,6 +88,9 @@ def test_facade_pipeline_matches_reference_and_python(exe, tmp_path):
     assert np.array_equal(_f64(tmp_path / "map_uv_pruned_raster.f64", (nu + 3, nu)), img)
     q = mv.inv([0.37, 0.61])
     assert (res["inv_x"], res["inv_y"]) == (q[0], q[1])
+    img = np.empty((nu, nu))
+    ot.sample_transportmap_to_image(mu.fwd_mesh(), 50, img, 7)
+    assert np.array_equal(_f64(tmp_path / "u_fwd_samples.f64", (nu, nu)), img)
     for tag, m in (("u", mu), ("v", mv)):
         assert np.array_equal(_f64(tmp_path / f"batch_{tag}_fwd.f64", (-1, 2)), m.fwd_mesh())
 

@@ -196,3 +196,43 @@ def test_mesh_io_rejects_bad_input(ot, tmp_path):
         bad.write(str(tmp_path / "x.off"))
     with pytest.raises(native.OtmError):
         ot.prune_empty_faces(bad, np.ones(1))
+
+
+# ---- stochastic splat: the oracle's generator vs the reference's std::rand() ----
+
+def _zscores(a, b):
+    return (a - b) / np.sqrt(a + b + 1.0)
+
+
+@pytest.mark.parametrize("tri", [False, True])
+def test_oracle_splat_matches_reference_in_distribution(oracle_port, tri):
+    """Same mesh, same samples per face: the two images differ only by sampling noise
+    (per-pixel z-scores of the difference are O(1)) and count the same points."""
+    ref = _ref()
+    g = load_golden("solve_mix_n32_s0.npz")
+    n = 32
+    st, ix = oracle_port.grid_faces(n)
+    if tri:
+        q = ix.reshape(-1, 4)
+        ix = np.stack([q[:, [0, 1, 2]], q[:, [0, 2, 3]]], 1).reshape(-1).astype(np.int32)
+        st = np.arange(0, ix.size + 1, 3, dtype=np.int32)
+    nf = st.size - 1
+    spf = np.full(nf, 1500, np.int32)
+    spf[::7] = 300
+    a = ref.sample_image(g["fwd"], st, ix, spf, 1, n + 5, n)
+    b = oracle_port.sample_image(g["fwd"], st, ix, spf, 1, n + 5, n)
+    assert a.sum() == b.sum() == spf.sum()
+    z = _zscores(a, b)
+    assert np.abs(z).max() < 5.0 and z.std() < 1.3
+
+
+def test_oracle_splat_on_the_origin_grid_is_exact(oracle_port):
+    """On the undeformed grid each face is one pixel: every pixel counts its face's samples."""
+    n = 16
+    st, ix = oracle_port.grid_faces(n)
+    t = np.arange(n + 1) / n
+    xy = np.stack([np.repeat(t, n + 1), np.tile(t, n + 1)], 1)
+    spf = (np.arange(n * n) % 5 + 1).astype(np.int32) * 10
+    img = oracle_port.sample_image(xy, st, ix, spf, 3, n, n)
+    want = spf.reshape(n, n).T  # face f = j + i*n covers pixel (row j, col i)
+    assert np.array_equal(img, want)
