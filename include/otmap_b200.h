@@ -20,6 +20,7 @@
  *   otm_rasterize_mode    rasterize_image with RasterImageOption   utils/rasterizer.h:16-22, utils/rasterizer.cpp:188-302
  *   otm_rasterize_mesh    rasterize_image on any tri/quad mesh     utils/rasterizer.cpp:36-185, 188-302
  *   otm_transport_cost    transport_cost                           transport_map.h:70, transport_map.cpp:131-215
+ *   otm_grid_transport_cost  GridBasedTransportSolver::compute_transport_cost  otsolver_2dgrid.cpp:608-640
  *   otm_mesh_blend        interpolate (bilinear / linear blend)    apps/barycenters.cpp:127-139, 250-276
  *   otm_barycenter        interpolate + synthetize_and_save_image  apps/barycenters.cpp:250-290
  *   otm_sample_image      sample_transportmap_to_image             utils/stochastic_rasterizer.cpp:19-88
@@ -196,6 +197,16 @@ int otm_rasterize_mesh(otm_context* ctx, int nv, const double* xy, int nf, const
  * normalised per-face values agree to a few ulps. */
 int otm_transport_cost(otm_context* ctx, int n, const double* src_xy, const double* dst_xy, const double* density,
                        double* per_face, double* cost);
+
+/* GridBasedTransportSolver::compute_transport_cost (otsolver_2dgrid.cpp:608-640), the
+ * cost the solver reports at verbose level 3: per face, density * e^2 * the mean over
+ * the 2x2 Gauss points of |bilinear interpolation of the corner displacements|^2.
+ *   grads_xy  vertices: displacement of each grid vertex (the solver's vertex
+ *             gradients; fwd_xy - origin recovers them to one rounding)
+ *   per_face  optional double[N] out; total out: their sum (fixed-order tree sum;
+ *             the reference's Eigen sum orders its additions differently) */
+int otm_grid_transport_cost(otm_context* ctx, int n, const double* grads_xy, const double* density,
+                            double* per_face, double* total);
 
 /* interpolate (apps/barycenters.cpp:250-276): out = sum_k weights[k] * meshes[k],
  * accumulated left to right per coordinate, as bilerp/lerp (barycenters.cpp:127-139)

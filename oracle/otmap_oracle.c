@@ -1024,6 +1024,33 @@ void oro_sample_image(int nv, const double* xy, int nf, const int* start, const 
 }
 
 /* ------------------------------------------------------------------------- */
+/* GridBasedTransportSolver::compute_transport_cost (otsolver_2dgrid.cpp:608-640) on
+ * vertex displacements g (V x 2 AoS); returns the sequential sum of the per-face costs. */
+double oro_grid_transport_cost(int n, const double* g, const double* density, double* per_face) {
+  const double e2 = 1.0 / ((double)n * (double)n);
+  const double z1 = sqrt(1. / 3.) / 2. + 0.5, z2 = -sqrt(1. / 3.) / 2. + 0.5;
+  const double zu[4] = {z1, z1, z2, z2}, zv[4] = {z1, z2, z2, z1};
+  double total = 0;
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      int c[4] = {VID(i, j), VID(i + 1, j), VID(i + 1, j + 1), VID(i, j + 1)};
+      double acc = 0;
+      for (int q = 0; q < 4; ++q) {
+        double u = zu[q], v = zv[q];
+        double a0 = (1 - u) * (1 - v), a1 = u * (1 - v), a2 = u * v, a3 = (1 - u) * v;
+        double x = a0 * g[2 * c[0]] + a1 * g[2 * c[1]] + a2 * g[2 * c[2]] + a3 * g[2 * c[3]];
+        double y = a0 * g[2 * c[0] + 1] + a1 * g[2 * c[1] + 1] + a2 * g[2 * c[2] + 1] + a3 * g[2 * c[3] + 1];
+        acc = q == 0 ? x * x + y * y : acc + (x * x + y * y);
+      }
+      int f = j + i * n;
+      double cost = density[f] * e2 * acc / 4.;
+      if (per_face) per_face[f] = cost;
+      total += cost;
+    }
+  return total;
+}
+
+/* ------------------------------------------------------------------------- */
 /* transport_map.cpp:131-215 for a quad grid mesh: the face count equals the
  * density size, so the reference takes its per-triangle branch (:184-199) on the
  * first three vertices of each face's circulation, which for a Surface_mesh quad

@@ -98,6 +98,10 @@ int oro_prune_empty_faces(int nv, const double* xy, int nf, const int* start, co
 void oro_sample_image(int nv, const double* xy, int nf, const int* start, const int* idx, const int* spf,
                       unsigned long long seed, int rows, int cols, double* img);
 
+/* GridBasedTransportSolver::compute_transport_cost (otsolver_2dgrid.cpp:608-640) of
+ * vertex displacements g (V x 2 AoS); returns the sum of per_face (optional). */
+double oro_grid_transport_cost(int n, const double* g, const double* density, double* per_face);
+
 /* ---- transport_cost for an (n+1)^2 quad grid (transport_map.cpp:131-215, quad branch) ---- */
 double oro_transport_cost(int n, const double* src_xy, const double* dst_xy, const double* density,
                           double* per_face);

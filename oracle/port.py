@@ -69,6 +69,8 @@ def lib():
         L.oro_mesh_blend.argtypes = [C.c_long, C.c_int, C.POINTER(_dp), _dp, _dp]
         L.oro_prune_empty_faces.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _dp, C.c_int, _ip, _dp, _ip, _ip, _ip]
         L.oro_prune_empty_faces.restype = C.c_int
+        L.oro_grid_transport_cost.argtypes = [C.c_int, _dp, _dp, _dp]
+        L.oro_grid_transport_cost.restype = C.c_double
         L.oro_sample_image.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _ip, C.c_ulonglong, C.c_int, C.c_int, _dp]
         _lib = L
     return _lib
@@ -279,3 +281,10 @@ def sample_image(xy, start, idx, spf, seed, rows, cols):
     lib().oro_sample_image(xy.shape[0], _p(xy), start.size - 1, _pi(start), _pi(idx), _pi(spf), int(seed), rows,
                            cols, _p(img))
     return img
+
+
+def grid_transport_cost(grads, density, n):
+    """compute_transport_cost restated -> (sum, per-face costs)."""
+    pf = np.zeros(n * n)
+    c = lib().oro_grid_transport_cost(n, _p(_f64(grads)), _p(_f64(density)), _p(pf))
+    return c, pf

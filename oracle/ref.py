@@ -67,6 +67,8 @@ def lib():
         L.otref_write_off.restype = C.c_int
         L.otref_read_off.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, _ip, _dp, _ip, _ip, _ip]
         L.otref_read_off.restype = C.c_int
+        L.otref_grid_transport_cost.argtypes = [C.c_void_p, _dp, _dp, _dp]
+        L.otref_grid_transport_cost.restype = C.c_double
         L.otref_sample_image.argtypes = [C.c_int, _dp, C.c_int, _ip, _ip, _ip, C.c_uint, C.c_int, C.c_int, _dp]
         _lib = L
     return _lib
@@ -118,6 +120,12 @@ class RefSolver:
         return m
 
     # unit probes of the solver's protected steps
+    def grid_transport_cost(self, grads, density):
+        """compute_transport_cost (otsolver_2dgrid.cpp:608-640) -> (sum, per-face costs)."""
+        pf = np.zeros(self.n * self.n)
+        c = lib().otref_grid_transport_cost(self._h, _p(_f64(grads)), _p(_f64(density)), _p(pf))
+        return c, pf
+
     def vertex_gradients(self, psi):
         g = np.zeros(((self.n + 1) ** 2, 2))
         lib().otref_vertex_gradients(self._h, _p(_f64(psi)), _p(g))

@@ -68,6 +68,7 @@ double now_s() {
 struct Probe : public otmap::GridBasedTransportSolver {
   using GridBasedTransportSolver::compute_1D_problem_parameters;
   using GridBasedTransportSolver::compute_residual;
+  using GridBasedTransportSolver::compute_transport_cost;
   using GridBasedTransportSolver::compute_vertex_gradients;
   using GridBasedTransportSolver::solve_1D_problem;
   void set_density(const VectorXd* d) { m_input_density = d; }
@@ -533,6 +534,27 @@ void otref_sample_image(int nv, const double* xy, int nf, const int* start, cons
   }
   for (int y = 0; y < rows; ++y)
     for (int x = 0; x < cols; ++x) img[(size_t)y * cols + x] = im(y, x);
+}
+
+// compute_transport_cost (otsolver_2dgrid.cpp:608-640) of vertex displacements g
+// (V x 2 AoS) against a density; returns the sum the solver prints at verbose >= 3.
+double otref_grid_transport_cost(void* hp, const double* g, const double* density, double* per_face) {
+  CsrGuard cg;
+  auto* h = static_cast<Solver*>(hp);
+  int n = h->n;
+  Index V = (Index)(n + 1) * (n + 1);
+  MatrixX2d G(V, 2);
+  for (Index v = 0; v < V; ++v) {
+    G(v, 0) = g[2 * v];
+    G(v, 1) = g[2 * v + 1];
+  }
+  VectorXd d = Map<const VectorXd>(density, (Index)n * n);
+  VectorXd cost;
+  h->s->set_density(&d);
+  h->s->compute_transport_cost(G, cost);
+  h->s->set_density(nullptr);
+  for (Index i = 0; i < cost.size(); ++i) per_face[i] = cost[i];
+  return cost.sum();
 }
 
 }  // extern "C"

@@ -80,6 +80,42 @@ __global__ void k_cost_finish(long N, int nblocks, const double* partial, double
     for (long f = threadIdx.x; f < N; f += blockDim.x) per_face[f] /= s_int;
 }
 
+// compute_transport_cost (otsolver_2dgrid.cpp:608-640): per face, density * e^2 times
+// the mean over the 2x2 Gauss points (z1, z2 = 1/2 +- sqrt(1/3)/2) of the squared
+// bilinear interpolation of the corner displacements g; partial sums per block.
+__global__ void k_grid_cost(int n, const double* g, const double* density, double e2, double* per_face,
+                            double* partial) {
+  __shared__ double red[32];
+  const long N = (long)n * n;
+  const double z1 = sqrt(1. / 3.) / 2. + 0.5, z2 = -sqrt(1. / 3.) / 2. + 0.5;
+  double v[1] = {0.0};
+  for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(f / n), j = (int)(f % n);
+    const long c[4] = {(long)j + (long)i * (n + 1), (long)j + (long)(i + 1) * (n + 1),
+                       (long)(j + 1) + (long)(i + 1) * (n + 1), (long)(j + 1) + (long)i * (n + 1)};
+    auto dist2 = [&](double u, double w) {
+      const double a0 = (1 - u) * (1 - w), a1 = u * (1 - w), a2 = u * w, a3 = (1 - u) * w;
+      const double x = a0 * g[2 * c[0]] + a1 * g[2 * c[1]] + a2 * g[2 * c[2]] + a3 * g[2 * c[3]];
+      const double y = a0 * g[2 * c[0] + 1] + a1 * g[2 * c[1] + 1] + a2 * g[2 * c[2] + 1] + a3 * g[2 * c[3] + 1];
+      return x * x + y * y;
+    };
+    const double cost =
+        density[f] * e2 * (dist2(z1, z1) + dist2(z1, z2) + dist2(z2, z2) + dist2(z2, z1)) / 4.;
+    if (per_face) per_face[f] = cost;
+    v[0] += cost;
+  }
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) partial[blockIdx.x] = v[0];
+}
+
+__global__ void k_sum_partials(int nparts, const double* partial, double* out) {
+  __shared__ double red[32];
+  double v[1] = {0.0};
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) v[0] += partial[b];
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) *out = v[0];
+}
+
 // Sum of img in a fixed order: per-block partials over a grid-stride loop.
 __global__ void k_img_partials(long count, const double* img, double* partial) {
   __shared__ double red[32];
@@ -241,6 +277,46 @@ extern "C" int otm_barycenter(otm_context* ctx, int n, int count, const double* 
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();
     if (raster_mean) *raster_mean = mean;
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_grid_transport_cost(otm_context* ctx, int n, const double* grads_xy, const double* density,
+                                       double* per_face, double* total) {
+  return guarded([&] {
+    if (!ctx || !grads_xy || !density || !total) throw BadArg{"otm_grid_transport_cost: null argument"};
+    if (n < 1 || n > 16384) throw BadArg{"otm_grid_transport_cost: grid size out of range"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    const size_t V2 = 2 * (size_t)(n + 1) * (n + 1), N = (size_t)n * n;
+    const int nb = 512;
+    DevBuf buf;
+    buf.reserve(sizeof(double) * (V2 + 2 * N + nb + 8));
+    double* p = buf.as<double>();
+    const double* d_g = grads_xy;
+    if (!is_device_ptr(grads_xy)) {
+      OTM_CUDA(cudaMemcpyAsync(p, grads_xy, sizeof(double) * V2, cudaMemcpyHostToDevice, st));
+      d_g = p;
+    }
+    const double* d_den = density;
+    if (!is_device_ptr(density)) {
+      OTM_CUDA(cudaMemcpyAsync(p + V2, density, sizeof(double) * N, cudaMemcpyHostToDevice, st));
+      d_den = p + V2;
+    }
+    double* d_pf = per_face ? (is_device_ptr(per_face) ? per_face : p + V2 + N) : nullptr;
+    double* d_part = p + V2 + 2 * N;
+    double* d_res = d_part + nb;
+    const double e2 = 1.0 / (double(n) * double(n));  // otsolver_2dgrid.cpp:97
+    launch(ctx, "grid_cost", k_grid_cost, nb, 256, n, d_g, d_den, e2, d_pf, d_part);
+    launch(ctx, "sum_partials", k_sum_partials, 1, 512, nb, (const double*)d_part, d_res);
+    OTM_CUDA(cudaGetLastError());
+    double res = 0;
+    OTM_CUDA(cudaMemcpyAsync(&res, d_res, sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (per_face && !is_device_ptr(per_face))
+      OTM_CUDA(cudaMemcpyAsync(per_face, d_pf, sizeof(double) * N, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    *total = res;
     return (int)OTM_OK;
   });
 }

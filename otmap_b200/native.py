@@ -89,6 +89,8 @@ SIGNATURES = {
                                      C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "otm_transport_cost": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                      C.POINTER(C.c_double)]),
+    "otm_grid_transport_cost": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.POINTER(C.c_double)]),
     "otm_mesh_blend": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp, C.c_void_p]),
     "otm_barycenter": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp, C.c_double, C.c_int,
                                  C.c_int, C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]),

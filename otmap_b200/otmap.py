@@ -310,6 +310,22 @@ def transport_cost(src_mesh, dst_mesh, density_per_face, cost_per_face: bool = F
     return (c.value, pf) if cost_per_face else c.value
 
 
+def grid_transport_cost(vertex_displacements, density, per_face: bool = False, context=None):
+    """GridBasedTransportSolver::compute_transport_cost (otsolver_2dgrid.cpp:608-640):
+    the solver's Gauss-quadrature cost of the (V, 2) vertex displacements (a map's
+    fwd_mesh() - origin_mesh()); returns the sum, or (sum, per-face costs)."""
+    import ctypes as C
+
+    ctx = context or _n.default_context()
+    g = np.ascontiguousarray(vertex_displacements, dtype=np.float64).reshape(-1, 2)
+    n = _grid_n(g, None)
+    d = _as_cells(density)
+    pf = np.empty(n * n) if per_face else None
+    t = C.c_double(0)
+    _n.check(_n.lib().otm_grid_transport_cost(ctx.handle, n, _n.ptr(g), _n.ptr(d), _n.ptr(pf), C.byref(t)))
+    return (t.value, pf) if per_face else t.value
+
+
 def prune_empty_faces(mesh, density) -> Mesh:
     """prune_empty_faces (mesh_utils.cpp:124-141) on a grid vertex array or a Mesh;
     returns the pruned Mesh (the reference edits its Surface_mesh in place)."""

@@ -215,6 +215,14 @@ def extra_fixtures(s, maps):
          nhits_uv=nh_uv, nhits_vu=nh_vu, cost_uv=c_uv, cost_vu=c_vu)
     print("compose: multi-hit", int((nh_uv > 1).sum()), int((nh_vu > 1).sum()))
 
+    # the solver's quadrature transport cost (otsolver_2dgrid.cpp:608-640)
+    for name in ["solve_mix_n32_s0", "solve_shapes_n64_s5"]:
+        n, m = maps[name]
+        s.init(n)
+        grads = m.fwd() - grid_vertices(n)
+        total, pf = s.grid_transport_cost(grads, m.density())
+        save("gridcost_" + name[6:] + ".npz", n=n, solve=name, grads=grads, total=total, per_face=pf)
+
 
 def main(groups):
     s, maps = solve_all()

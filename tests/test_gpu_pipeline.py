@@ -222,3 +222,13 @@ def test_synthetize_image_scales(ot):
     sampled, raster = ot.synthetize_image(s["fwd"], 32, s["density"], s["adjusted"], samples_per_face=100, seed=5)
     np.testing.assert_allclose(sampled.sum(), s["density"].sum(), rtol=1e-2)
     assert np.isfinite(raster).all() and raster.max() > 0
+
+
+@pytest.mark.parametrize("name", golden_names("gridcost_"))
+def test_solver_transport_cost_matches_reference(name, ot):
+    """compute_transport_cost: per-face values bit-exact, the sum to a few ulps."""
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    total, pf = ot.grid_transport_cost(g["grads"], s["adjusted"], per_face=True)
+    assert np.array_equal(pf, g["per_face"])
+    np.testing.assert_allclose(total, float(g["total"]), rtol=SUM_RTOL)

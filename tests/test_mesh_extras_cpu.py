@@ -236,3 +236,12 @@ def test_oracle_splat_on_the_origin_grid_is_exact(oracle_port):
     img = oracle_port.sample_image(xy, st, ix, spf, 3, n, n)
     want = spf.reshape(n, n).T  # face f = j + i*n covers pixel (row j, col i)
     assert np.array_equal(img, want)
+
+
+@pytest.mark.parametrize("name", golden_names("gridcost_"))
+def test_oracle_solver_transport_cost(name, oracle_port):
+    g = load_golden(name)
+    s = load_golden(str(g["solve"]) + ".npz")
+    c, pf = oracle_port.grid_transport_cost(g["grads"], s["adjusted"], int(g["n"]))
+    assert np.array_equal(pf, g["per_face"])
+    np.testing.assert_allclose(c, float(g["total"]), rtol=1e-14)
