@@ -11,8 +11,13 @@
 //   step 4  lane k1 (< N1) runs an N2-point FFT on its N2 values in registers, giving
 //           X[k1 + N1*k2].
 // Shared memory then carries each element twice per transform instead of once per
-// radix stage. The column pass stages a tile of CB full columns in shared memory so
-// its global reads and writes are row-contiguous.
+// radix stage. Every transform here is of real data, so each complex FFT carries two
+// lines at once: two rows (or two columns) as its real and imaginary parts. For the
+// DCT-II the two spectra are separated afterwards, A_k = (Z_k + conj Z_{n-k}) / 2 and
+// B_k = (Z_k - conj Z_{n-k}) / 2i; for the DCT-III both inputs are Hermitian, so the
+// real and imaginary parts of the one inverse FFT are the two output lines. The column
+// pass stages a tile of full column pairs in shared memory so its global reads and
+// writes are row-contiguous.
 
 #include "engine.cuh"
 
@@ -76,13 +81,13 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[N], const double2* __restri
   }
 }
 
-// Steps 1-4 for one line. `in(m1)` gives lane t's input sample m = N2*m1 + t; `out(k, X)`
-// receives X_k on lane k1 = k % N1 (only lanes t < N1 call it). buf is this line's
-// N1 x (N2 + 1) shared buffer of doubles (the transpose moves real and imaginary
-// parts in two rounds).
-template <int N1, int N2, class In, class Out>
+// Steps 1-4 for one line. `in(m1)` gives lane t's input sample m = N2*m1 + t; on return
+// lanes t < N1 hold u[r] = X_k for k = t + N1 * rbrev<N2>(r). buf is this line's
+// N1 x (N2 + 1) shared buffer of doubles (the transpose moves real and imaginary parts
+// in two rounds).
+template <int N1, int N2, class In>
 __device__ __forceinline__ void fft_line(int t, double* buf, const double2* __restrict__ tw, bool conj, In in,
-                                         Out out) {
+                                         double2 (&u)[N2]) {
   constexpr int n = N1 * N2;
   double2 v[N1];
 #pragma unroll
@@ -94,7 +99,6 @@ __device__ __forceinline__ void fft_line(int t, double* buf, const double2* __re
     if (k1 != 0) v[r] = cmul(v[r], twid(tw, t * k1, n, conj));
   }
   // transpose through shared memory, real parts then imaginary parts
-  double2 u[N2];
 #pragma unroll
   for (int part = 0; part < 2; ++part) {
 #pragma unroll
@@ -112,12 +116,17 @@ __device__ __forceinline__ void fft_line(int t, double* buf, const double2* __re
     }
     __syncwarp();
   }
-  if (t < N1) {
-    fft_reg<N2>(u, tw, n, conj);
-#pragma unroll
-    for (int r = 0; r < N2; ++r) out(t + N1 * rbrev<N2>(r), u[r]);
-  }
-  __syncwarp();
+  if (t < N1) fft_reg<N2>(u, tw, n, conj);
+}
+
+// Register index holding X_{n-k} on the partner lane, for the X_k held in u[r]:
+// lane t != 0 pairs with lane N1 - t and k2 -> N2 - 1 - k2; lane 0 with itself and
+// k2 -> (N2 - k2) mod N2.
+template <int N2>
+__host__ __device__ constexpr int partner_reg(int r, bool lane0) {
+  const int k2 = rbrev<N2>(r);
+  const int k2p = lane0 ? (N2 - k2) % N2 : N2 - 1 - k2;
+  return rbrev<N2>(k2p);  // rbrev is its own inverse
 }
 
 __device__ __forceinline__ double dct_s(int k, int n) { return k == 0 ? sqrt(1.0 / n) : sqrt(2.0 / n); }
@@ -130,6 +139,7 @@ __device__ __forceinline__ double2 pre3(int k, double a, double b, double2 pt) {
   return make_double2(0.5 * fma(a, pt.x, b * pt.y), 0.5 * fma(a, pt.y, -b * pt.x));
 }
 
+// Forward DCT-II of rows 2p and 2p+1 of r_k (one complex FFT per row pair) -> T.
 template <int N1, int N2>
 __global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_fwd(const Inst* insts, const int* row_inst, int seg) {
   constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
@@ -138,17 +148,43 @@ __global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_fwd(const Inst* insts, 
   const Inst& I = insts[row_inst[item]];
   if (!I.active) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
-  const int row = (item - I.row0) * LPB + warp * LPW + sub;
+  const int row = 2 * ((item - I.row0) * LPB + warp * LPW + sub);
   double* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
-  const double* x = I.r[I.it % 3] + (size_t)row * n;
-  double* y = I.t1 + (size_t)row * n;
+  const double* xa = I.r[I.it % 3] + (size_t)row * n;
+  const double* xb = xa + n;
+  double* ya = I.t1 + (size_t)row * n;
+  double* yb = ya + n;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
+  double2 u[N2];
   fft_line<N1, N2>(
-      t, buf, tw, false, [&](int m1) { return make_double2(x[makhoul_src(N2 * m1 + t, n)], 0.0); },
-      [&](int k, double2 V) { y[k] = post2(V, __ldg(&pt[k]), dct_s(k, n)); });
+      t, buf, tw, false,
+      [&](int m1) {
+        const int src = makhoul_src(N2 * m1 + t, n);
+        return make_double2(xa[src], xb[src]);
+      },
+      u);
+  const int src_lane = (lane - t) + (t < N1 ? (N1 - t) % N1 : 0);
+#pragma unroll
+  for (int r = 0; r < N2; ++r) {
+    const double2 send = (t == 0) ? u[partner_reg<N2>(r, true)] : u[partner_reg<N2>(r, false)];
+    const double px = __shfl_sync(0xffffffffu, send.x, src_lane);
+    const double py = __shfl_sync(0xffffffffu, send.y, src_lane);
+    if (t < N1) {
+      const int k = t + N1 * rbrev<N2>(r);
+      const double2 Z = u[r];
+      const double2 A = make_double2(0.5 * (Z.x + px), 0.5 * (Z.y - py));
+      const double2 B = make_double2(0.5 * (Z.y + py), 0.5 * (px - Z.x));
+      const double2 w = __ldg(&pt[k]);
+      const double sk = dct_s(k, n);
+      ya[k] = post2(A, w, sk);
+      yb[k] = post2(B, w, sk);
+    }
+  }
 }
 
+// Inverse DCT-III of rows 2p and 2p+1 of T -> d_hat: the inputs W^a + i W^b of the two
+// rows go through one inverse FFT; its real and imaginary parts are the two rows.
 template <int N1, int N2>
 __global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_inv(const Inst* insts, const int* row_inst, int seg) {
   constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
@@ -157,34 +193,49 @@ __global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_inv(const Inst* insts, 
   const Inst& I = insts[row_inst[item]];
   if (!I.active) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
-  const int row = (item - I.row0) * LPB + warp * LPW + sub;
+  const int row = 2 * ((item - I.row0) * LPB + warp * LPW + sub);
   double* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
-  const double* X = I.t1 + (size_t)row * n;
-  double* x = I.dhat + (size_t)row * n;
+  const double* Xa = I.t1 + (size_t)row * n;
+  const double* Xb = Xa + n;
+  double* xa = I.dhat + (size_t)row * n;
+  double* xb = xa + n;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
+  double2 u[N2];
   fft_line<N1, N2>(
       t, buf, tw, true,
       [&](int m1) {
         const int k = N2 * m1 + t;
-        double a = dct_s(k, n) * X[k];
-        double b = k == 0 ? 0.0 : dct_s(n - k, n) * X[n - k];
-        return pre3(k, a, b, __ldg(&pt[k]));
+        const double2 w = __ldg(&pt[k]);
+        const double sk = dct_s(k, n), snk = k == 0 ? 0.0 : dct_s(n - k, n);
+        const double2 Wa = pre3(k, sk * Xa[k], k == 0 ? 0.0 : snk * Xa[n - k], w);
+        const double2 Wb = pre3(k, sk * Xb[k], k == 0 ? 0.0 : snk * Xb[n - k], w);
+        return make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
       },
-      [&](int m, double2 v) { x[makhoul_src(m, n)] = v.x; });
+      u);
+  if (t < N1) {
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const int m = makhoul_src(t + N1 * rbrev<N2>(r), n);
+      xa[m] = u[r].x;
+      xb[m] = u[r].y;
+    }
+  }
 }
 
-// Column pass, lanes across columns: a block owns CB consecutive columns. Thread
-// (c = tid % CB, s = tid / CB) holds, for column l0 + c, the samples N2*m1 + s (s < N2) of
-// step 1 -- loaded straight from global memory, CB consecutive doubles per row -- and the
-// outputs k1 = s (s < N1) of step 4. One shared region (n x CB doubles plus a pad per k1
-// row) serves in turn as the step-3 transpose buffer, the exchange tile for the DCT-III
-// pairs (k, n - k) and the staging tile of the coalesced store.
+// Column pass, lanes across column pairs: a block owns CB = 2 CP consecutive columns.
+// Thread (c = tid % CP, s = tid / CP) holds, for the column pair (l0 + 2c, l0 + 2c + 1)
+// packed as one complex line, the samples N2*m1 + s (s < N2) of step 1 -- loaded
+// straight from global memory, 16 bytes per row -- and the outputs k1 = s (s < N1) of
+// step 4. One shared region serves in turn as the step-3 transpose buffer, the
+// exchange tile of the spectra (k with n - k) and the staging tile of the coalesced
+// store.
 template <int N1, int N2>
 struct ColGeom {
   static constexpr int n = N1 * N2;
-  static constexpr int CB = 256 / N2;  // columns per block (256 threads)
-  static constexpr int KS = N2 * CB + 1;  // padded stride of a k1 row of the transpose buffer
+  static constexpr int CP = 256 / N2;     // column pairs per block (256 threads)
+  static constexpr int CB = 2 * CP;       // columns per block
+  static constexpr int KS = N2 * CP + 1;  // padded stride of a k1 row of the transpose buffer
   static constexpr int SMEM = (N1 * KS > n * CB ? N1 * KS : n * CB);  // doubles
 };
 
@@ -192,7 +243,7 @@ template <int N1, int N2>
 __device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)[N2], double* sh, int c, int s,
                                                   const double2* __restrict__ tw, bool conj) {
   using GG = ColGeom<N1, N2>;
-  constexpr int n = GG::n, CB = GG::CB, KS = GG::KS;
+  constexpr int n = GG::n, CP = GG::CP, KS = GG::KS;
   fft_reg<N1>(v, tw, n, conj);
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
@@ -203,12 +254,12 @@ __device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)
   for (int part = 0; part < 2; ++part) {
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < N1; ++r) sh[rbrev<N1>(r) * KS + s * CB + c] = part ? v[r].y : v[r].x;
+    for (int r = 0; r < N1; ++r) sh[rbrev<N1>(r) * KS + s * CP + c] = part ? v[r].y : v[r].x;
     __syncthreads();
     if (s < N1) {
 #pragma unroll
       for (int m2 = 0; m2 < N2; ++m2) {
-        const double x = sh[s * KS + m2 * CB + c];
+        const double x = sh[s * KS + m2 * CP + c];
         if (part)
           u[m2].y = x;
         else
@@ -222,63 +273,81 @@ __device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)
 template <int N1, int N2>
 __global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const int* col_inst, int seg) {
   using GG = ColGeom<N1, N2>;
-  constexpr int n = GG::n, CB = GG::CB;
+  constexpr int n = GG::n, CP = GG::CP, CB = GG::CB;
   extern __shared__ double sbuf[];
+  double2* tile = reinterpret_cast<double2*>(sbuf);  // [k][c]: one column pair per entry
   const int item = seg + blockIdx.x;
   const Inst& I = insts[col_inst[item]];
   if (!I.active) return;
-  const int c = threadIdx.x % CB, s = threadIdx.x / CB;
-  const int l0 = (item - I.col0) * CB, l = l0 + c;
+  const int c = threadIdx.x % CP, s = threadIdx.x / CP;
+  const int l0 = (item - I.col0) * CB, la = l0 + 2 * c;
   double* T = I.t1;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
-  const double cl = I.cosk[l];
+  const double cla = I.cosk[la], clb = I.cosk[la + 1];
   double2 v[N1];
   double2 u[N2];
-  // forward DCT-II along the column
+  // forward DCT-II along the two columns
 #pragma unroll
-  for (int m1 = 0; m1 < N1; ++m1) v[m1] = make_double2(T[(size_t)makhoul_src(N2 * m1 + s, n) * n + l], 0.0);
+  for (int m1 = 0; m1 < N1; ++m1)
+    v[m1] = *reinterpret_cast<const double2*>(T + (size_t)makhoul_src(N2 * m1 + s, n) * n + la);
   col_fft_transpose<N1, N2>(v, u, sbuf, c, s, tw, false);
   __syncthreads();
   if (s < N1) {
-    // coefficient k = s + N1 k2: divide by lambda_kl, keep s_k U_k in the exchange tile [k][c]
+#pragma unroll
+    for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
+  }
+  __syncthreads();
+  if (s < N1) {
+    // coefficient k = s + N1 k2 of both columns: divide by lambda_kl (the (0,0) mode is
+    // dropped), keep s_k U_k
 #pragma unroll
     for (int r = 0; r < N2; ++r) {
       const int k = s + N1 * rbrev<N2>(r);
+      const double2 Z = u[r], P = tile[((n - k) & (n - 1)) * CP + c];
+      const double2 A = make_double2(0.5 * (Z.x + P.x), 0.5 * (Z.y - P.y));
+      const double2 B = make_double2(0.5 * (Z.y + P.y), 0.5 * (P.x - Z.x));
+      const double2 w = __ldg(&pt[k]);
       const double sk = dct_s(k, n);
-      const double X = post2(u[r], __ldg(&pt[k]), sk);
-      const double lam = 2.0 - 2.0 * I.cosk[k] * cl;
-      const double U = (k == 0 && l == 0) ? 0.0 : X / lam;
-      sbuf[k * CB + c] = sk * U;
+      const double Xa = post2(A, w, sk), Xb = post2(B, w, sk);
+      const double lam_a = 2.0 - 2.0 * I.cosk[k] * cla, lam_b = 2.0 - 2.0 * I.cosk[k] * clb;
+      const double Ua = (k == 0 && la == 0) ? 0.0 : Xa / lam_a;
+      const double Ub = Xb / lam_b;
+      u[r] = make_double2(sk * Ua, sk * Ub);
     }
   }
   __syncthreads();
-  // inverse DCT-III along the column
+  if (s < N1) {
+#pragma unroll
+    for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
+  }
+  __syncthreads();
+  // inverse DCT-III along the two columns: W^a + i W^b through one inverse FFT
 #pragma unroll
   for (int m1 = 0; m1 < N1; ++m1) {
     const int k = N2 * m1 + s;
-    const double a = sbuf[k * CB + c], b = k == 0 ? 0.0 : sbuf[(n - k) * CB + c];
-    v[m1] = pre3(k, a, b, __ldg(&pt[k]));
+    const double2 a = tile[k * CP + c];
+    const double2 b = k == 0 ? make_double2(0.0, 0.0) : tile[(n - k) * CP + c];
+    const double2 w = __ldg(&pt[k]);
+    const double2 Wa = pre3(k, a.x, b.x, w), Wb = pre3(k, a.y, b.y, w);
+    v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
   }
   col_fft_transpose<N1, N2>(v, u, sbuf, c, s, tw, true);
   __syncthreads();
   if (s < N1) {
 #pragma unroll
-    for (int r = 0; r < N2; ++r) {
-      const int m = s + N1 * rbrev<N2>(r);
-      sbuf[makhoul_src(m, n) * CB + c] = u[r].x;
-    }
+    for (int r = 0; r < N2; ++r) tile[makhoul_src(s + N1 * rbrev<N2>(r), n) * CP + c] = u[r];
   }
   __syncthreads();
-  for (int e = threadIdx.x; e < n * CB; e += 256) {
-    const int i = e / CB, cc = e - i * CB;
-    T[(size_t)i * n + l0 + cc] = sbuf[i * CB + cc];
+  for (int e = threadIdx.x; e < n * CP; e += 256) {
+    const int i = e / CP, cc = e - i * CP;
+    *reinterpret_cast<double2*>(T + (size_t)i * n + l0 + 2 * cc) = tile[i * CP + cc];
   }
 }
 
 template <int N1, int N2>
 struct RegDct {
-  static constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
+  static constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;  // LPB row pairs per block
   static size_t rows_smem() { return sizeof(double) * LPB * N1 * (N2 + 1); }
   static size_t cols_smem() { return sizeof(double) * ColGeom<N1, N2>::SMEM; }
   static constexpr int CB = ColGeom<N1, N2>::CB;
@@ -301,13 +370,13 @@ struct RegDct {
 
 bool dct_reg_supported(int n) { return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024; }
 
-int dct_reg_lines_per_block(int n) {
+int dct_reg_lines_per_block(int n) {  // rows per block: two per FFT line
   switch (n) {
-    case 64: return RegDct<8, 8>::LPB;
-    case 128: return RegDct<8, 16>::LPB;
-    case 256: return RegDct<16, 16>::LPB;
-    case 512: return RegDct<16, 32>::LPB;
-    default: return RegDct<32, 32>::LPB;
+    case 64: return 2 * RegDct<8, 8>::LPB;
+    case 128: return 2 * RegDct<8, 16>::LPB;
+    case 256: return 2 * RegDct<16, 16>::LPB;
+    case 512: return 2 * RegDct<16, 32>::LPB;
+    default: return 2 * RegDct<32, 32>::LPB;
   }
 }
 
