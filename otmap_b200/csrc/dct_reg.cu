@@ -19,12 +19,23 @@
 // pass stages a tile of full column pairs in shared memory so its global reads and
 // writes are row-contiguous.
 
+#include <cmath>
+#include <vector>
+
 #include "engine.cuh"
 
 namespace otm {
 namespace {
 
 constexpr int RW = 4;  // warps per block
+
+// exp(-2 pi i k / 1024), k < 512, in constant memory. A radix-2 stage of an N-point
+// sub-FFT needs W_N^e = entry e * (1024 / N), an index known at compile time, so the
+// arithmetic reads the twiddle as a constant operand instead of waiting on a load. The
+// entries equal those of the per-size tables (same host formula; the index scaling by a
+// power of two is exact).
+constexpr int CTW = 1024;
+__constant__ double2 c_tw[CTW / 2];
 
 __device__ __forceinline__ double2 cmul(double2 a, double2 w) {
   return make_double2(fma(a.x, w.x, -a.y * w.y), fma(a.x, w.y, a.y * w.x));
@@ -72,7 +83,7 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[N], const double2* __restri
         if (e == 0) {
           v[start + k + span] = d;
         } else {
-          double2 w = __ldg(&tw[e * (n / N)]);
+          double2 w = c_tw[e * (CTW / N)];
           if (conj) w.y = -w.y;
           v[start + k + span] = cmul(d, w);
         }
@@ -81,17 +92,14 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[N], const double2* __restri
   }
 }
 
-// Steps 1-4 for one line. `in(m1)` gives lane t's input sample m = N2*m1 + t; on return
-// lanes t < N1 hold u[r] = X_k for k = t + N1 * rbrev<N2>(r). buf is this line's
-// N1 x (N2 + 1) shared buffer of doubles (the transpose moves real and imaginary parts
-// in two rounds).
-template <int N1, int N2, class In>
-__device__ __forceinline__ void fft_line(int t, double* buf, const double2* __restrict__ tw, bool conj, In in,
-                                         double2 (&u)[N2]) {
+// Steps 1-4 for one line. On entry lane t holds in v[m1] the input sample
+// m = N2*m1 + t; on return lanes t < N1 hold u[r] = X_k for k = t + N1 * rbrev<N2>(r).
+// buf is this line's N1 x (N2 + 1) shared buffer of doubles (the transpose moves real and
+// imaginary parts in two rounds).
+template <int N1, int N2>
+__device__ __forceinline__ void fft_line(int t, double* buf, const double2* __restrict__ tw, bool conj,
+                                         double2 (&v)[N1], double2 (&u)[N2]) {
   constexpr int n = N1 * N2;
-  double2 v[N1];
-#pragma unroll
-  for (int m1 = 0; m1 < N1; ++m1) v[m1] = in(m1);
   fft_reg<N1>(v, tw, n, conj);
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
@@ -156,14 +164,21 @@ __global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_fwd(const Inst* insts, 
   double* yb = ya + n;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
+  // Makhoul order: sample m < n/2 is x[2m], sample m >= n/2 is x[2(n-1-m)+1]. Lane t
+  // loads the pairs x[2(N2 m1 + t)], x[2(N2 m1 + t) + 1] (m1 < N1/2, 16-byte loads): the
+  // first is its own sample m = N2 m1 + t, the second is sample n-1-m, which belongs to
+  // lane N2-1-t at m1' = N1-1-m1 and is passed there by a shuffle.
+  double2 v[N1];
   double2 u[N2];
-  fft_line<N1, N2>(
-      t, buf, tw, false,
-      [&](int m1) {
-        const int src = makhoul_src(N2 * m1 + t, n);
-        return make_double2(xa[src], xb[src]);
-      },
-      u);
+  const int mirror = (lane - t) + (N2 - 1 - t);
+#pragma unroll
+  for (int m1 = 0; m1 < N1 / 2; ++m1) {
+    const double2 pa = __ldcg(reinterpret_cast<const double2*>(xa + 2 * (N2 * m1 + t)));
+    const double2 pb = __ldcg(reinterpret_cast<const double2*>(xb + 2 * (N2 * m1 + t)));
+    v[m1] = make_double2(pa.x, pb.x);
+    v[N1 - 1 - m1] = make_double2(__shfl_sync(0xffffffffu, pa.y, mirror), __shfl_sync(0xffffffffu, pb.y, mirror));
+  }
+  fft_line<N1, N2>(t, buf, tw, false, v, u);
   const int src_lane = (lane - t) + (t < N1 ? (N1 - t) % N1 : 0);
 #pragma unroll
   for (int r = 0; r < N2; ++r) {
@@ -201,24 +216,32 @@ __global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_inv(const Inst* insts, 
   double* xb = xa + n;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
+  double2 v[N1];
   double2 u[N2];
-  fft_line<N1, N2>(
-      t, buf, tw, true,
-      [&](int m1) {
-        const int k = N2 * m1 + t;
-        const double2 w = __ldg(&pt[k]);
-        const double sk = dct_s(k, n), snk = k == 0 ? 0.0 : dct_s(n - k, n);
-        const double2 Wa = pre3(k, sk * Xa[k], k == 0 ? 0.0 : snk * Xa[n - k], w);
-        const double2 Wb = pre3(k, sk * Xb[k], k == 0 ? 0.0 : snk * Xb[n - k], w);
-        return make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
-      },
-      u);
-  if (t < N1) {
 #pragma unroll
-    for (int r = 0; r < N2; ++r) {
-      const int m = makhoul_src(t + N1 * rbrev<N2>(r), n);
-      xa[m] = u[r].x;
-      xb[m] = u[r].y;
+  for (int m1 = 0; m1 < N1; ++m1) {
+    const int k = N2 * m1 + t;
+    const double2 w = __ldg(&pt[k]);
+    const double sk = dct_s(k, n), snk = k == 0 ? 0.0 : dct_s(n - k, n);
+    const double2 Wa = pre3(k, sk * __ldcg(&Xa[k]), k == 0 ? 0.0 : snk * __ldcg(&Xa[n - k]), w);
+    const double2 Wb = pre3(k, sk * __ldcg(&Xb[k]), k == 0 ? 0.0 : snk * __ldcg(&Xb[n - k]), w);
+    v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
+  }
+  fft_line<N1, N2>(t, buf, tw, true, v, u);
+  // Output m = t + N1 k2 goes to x[2m] for m < n/2; its neighbour x[2m+1] is output
+  // n-1-m, held by lane N1-1-t in the register of k2' = N2-1-k2: one shuffle and a
+  // 16-byte store per pair.
+  const int mirror = (lane - t) + (t < N1 ? N1 - 1 - t : 0);
+#pragma unroll
+  for (int r = 0; r < N2; ++r) {
+    if (rbrev<N2>(r) >= N2 / 2) continue;
+    const double2 other = u[rbrev<N2>(N2 - 1 - rbrev<N2>(r))];
+    const double qa = __shfl_sync(0xffffffffu, other.x, mirror);
+    const double qb = __shfl_sync(0xffffffffu, other.y, mirror);
+    if (t < N1) {
+      const int m = t + N1 * rbrev<N2>(r);
+      *reinterpret_cast<double2*>(xa + 2 * m) = make_double2(u[r].x, qa);
+      *reinterpret_cast<double2*>(xb + 2 * m) = make_double2(u[r].y, qb);
     }
   }
 }
@@ -284,13 +307,12 @@ __global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const in
   double* T = I.t1;
   const double2* tw = I.tw;
   const double2* pt = I.pt;
-  const double cla = I.cosk[la], clb = I.cosk[la + 1];
   double2 v[N1];
   double2 u[N2];
-  // forward DCT-II along the two columns
+  // forward DCT-II along the two columns (samples in Makhoul order)
 #pragma unroll
   for (int m1 = 0; m1 < N1; ++m1)
-    v[m1] = *reinterpret_cast<const double2*>(T + (size_t)makhoul_src(N2 * m1 + s, n) * n + la);
+    v[m1] = __ldcg(reinterpret_cast<const double2*>(T + (size_t)makhoul_src(N2 * m1 + s, n) * n + la));
   col_fft_transpose<N1, N2>(v, u, sbuf, c, s, tw, false);
   __syncthreads();
   if (s < N1) {
@@ -301,6 +323,7 @@ __global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const in
   if (s < N1) {
     // coefficient k = s + N1 k2 of both columns: divide by lambda_kl (the (0,0) mode is
     // dropped), keep s_k U_k
+    const double cla = I.cosk[la], clb = I.cosk[la + 1];
 #pragma unroll
     for (int r = 0; r < N2; ++r) {
       const int k = s + N1 * rbrev<N2>(r);
@@ -393,6 +416,12 @@ int dct_reg_cols_per_block(int n) {
 void dct_reg_attrs(int device) {
   static bool done[64] = {};
   if (device < 64 && done[device]) return;
+  {
+    std::vector<double2> tw(CTW / 2);
+    for (int k = 0; k < CTW / 2; ++k)
+      tw[k] = make_double2(std::cos(2.0 * M_PI * k / CTW), -std::sin(2.0 * M_PI * k / CTW));
+    OTM_CUDA(cudaMemcpyToSymbol(c_tw, tw.data(), sizeof(double2) * (CTW / 2)));
+  }
   RegDct<8, 8>::attrs();
   RegDct<8, 16>::attrs();
   RegDct<16, 16>::attrs();

@@ -98,16 +98,20 @@ struct VG {    // vertex gradients (v, j) and (v, j + 1)
 };
 
 // Vertex gradients of vertex row v from cell rows a = v-1 and b = v
-// (otsolver_2dgrid.cpp:379-391 with clamped cells = boundary rules :405-422).
-__device__ __forceinline__ VG vgrad(const Row& a, const Row& b, double hw, int lane) {
+// (otsolver_2dgrid.cpp:379-391 with clamped cells = boundary rules :405-422), divided by
+// the reference's factor n/2: the sweeps carry that factor into the line coefficients
+// (a, b scale by (n/2)^2) and apply it to the sums and the residual update. For
+// power-of-two n the factor is a power of two and every result is bit-identical to
+// scaling each gradient.
+__device__ __forceinline__ VG vgrad(const Row& a, const Row& b, int lane) {
   VG g;
-  g.gx = hw * ((b.l + b.c) - (a.l + a.c));
-  g.gy = hw * ((a.c + b.c) - (a.l + b.l));
+  g.gx = (b.l + b.c) - (a.l + a.c);
+  g.gy = (a.c + b.c) - (a.l + b.l);
   double gxr = __shfl_down_sync(0xffffffffu, g.gx, 1);
   double gyr = __shfl_down_sync(0xffffffffu, g.gy, 1);
   if (lane == 31) {
-    gxr = hw * ((b.c + b.rh) - (a.c + a.rh));
-    gyr = hw * ((a.rh + b.rh) - (a.c + b.c));
+    gxr = (b.c + b.rh) - (a.c + a.rh);
+    gyr = (a.rh + b.rh) - (a.c + b.c);
   }
   g.gxr = gxr;
   g.gyr = gyr;
@@ -192,7 +196,8 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
   Inst& I = insts[strip_inst[blockIdx.x]];
   if (!I.active) return;
   const int n = I.n, it = I.it;
-  const double e = 1.0 / (double)n, hw = 0.5 * (double)n;
+  // gradients are unscaled (vgrad): the shift e of the diagonals becomes e / (n/2)
+  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw;
   const StripCoord sc = strip_coord(I, blockIdx.x);
   const int j = sc.j0 + sc.lane;
   double acc[S_COUNT];
@@ -214,22 +219,29 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
 #pragma unroll
     for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
     VG gp, gh, gq;
+    Row ap, ah, aq;  // grid row row-1 of each stencil field, carried from the previous step
     for (int row = sc.i0; row <= last; ++row) {
       cp_async_wait<RD - 3>();
       __syncwarp();
+      if (row == sc.i0) {
+        ap = R.row_of(row - 1, 0);
+        ah = R.row_of(row - 1, 1);
+        aq = R.row_of(row - 1, 2);
+      }
+      const Row bp = R.row_of(row, 0), bh = R.row_of(row, 1), bq = R.row_of(row, 2);
       // vertex row `row` from grid rows row-1 and row
-      VG np = vgrad(R.row_of(row - 1, 0), R.row_of(row, 0), hw, sc.lane);
-      VG nh = vgrad(R.row_of(row - 1, 1), R.row_of(row, 1), hw, sc.lane);
-      VG nq = vgrad(R.row_of(row - 1, 2), R.row_of(row, 2), hw, sc.lane);
+      VG np = vgrad(ap, bp, sc.lane);
+      VG nh = vgrad(ah, bh, sc.lane);
+      VG nq = vgrad(aq, bq, sc.lane);
       if (row > sc.i0 && j < n) {
         const int c = row - 1;
         Diag G = diag(gp, np), Hd = diag(gh, nh), Qd = diag(gq, nq);
         double a11, b1, a22, b2;
-        line_ab(G, Hd, e, a11, b1);
-        line_ab(G, Qd, e, a22, b2);
+        line_ab(G, Hd, es, a11, b1);
+        line_ab(G, Qd, es, a22, b2);
         double a12 = 0.5 * (Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx);
         double r = R.point(c, 0), jd = r - R.point(c, 1);
-        double hv = R.row_of(c, 1).c, qv = R.row_of(c, 2).c;
+        double hv = ah.c, qv = aq.c;
         acc[S_HH] = fma(hv, hv, acc[S_HH]);
         acc[S_HQ] = fma(hv, qv, acc[S_HQ]);
         acc[S_QQ] = fma(qv, qv, acc[S_QQ]);
@@ -260,6 +272,9 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
       gp = np;
       gh = nh;
       gq = nq;
+      ap = bp;
+      ah = bh;
+      aq = bq;
       __syncwarp();
       R.issue(row - 2 + RD);  // refill the stage of grid row row-2, no longer needed
     }
@@ -270,6 +285,19 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
     double S[S_COUNT];
     reduce_block_partials<S_COUNT>(partials, I.strip0, I.nstrip, S, red);
     if (threadIdx.x == 0) {
+      // restore the (n/2)^2 factor of each line coefficient in the sums
+      const double h2 = hw * hw, h4 = h2 * h2;
+      S[S_JB] *= h2;
+      S[S_JA] *= h2;
+      S[S_B1R] *= h2;
+      S[S_B2R] *= h2;
+      S[S_A11R] *= h2;
+      S[S_A12R] *= h2;
+      S[S_A22R] *= h2;
+#pragma unroll
+      for (int k = S_B1B1; k <= S_B2B2; ++k) S[k] *= h4;
+#pragma unroll
+      for (int k = S_A11B1; k < S_COUNT; ++k) S[k] *= h4;
       if (sqrt(S[S_HH]) <= 2.0 * DBL_MIN) {  // otsolver_2dgrid.cpp:182
         I.active = 0;
         I.outcome = OTM_SMALL_STEP;
@@ -307,7 +335,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
   Inst& I = insts[strip_inst[blockIdx.x]];
   if (!I.active) return;
   const int n = I.n, it = I.it;
-  const double e = 1.0 / (double)n, hw = 0.5 * (double)n, alpha = I.alpha;
+  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw, h2 = hw * hw, alpha = I.alpha;
   const bool use_beta = I.use_beta;
   const double beta = I.beta;
   const StripCoord sc = strip_coord(I, blockIdx.x);
@@ -343,25 +371,33 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
       return d;
     };
     VG gp, gd;
+    Row pc, dc;  // grid row row-1 of psi and of d, carried from the previous step
     for (int row = sc.i0; row <= last; ++row) {
       cp_async_wait<RD - 3>();
       __syncwarp();
-      Row pc = R.row_of(row - 1, 0), dc = drow(row - 1);
-      VG np = vgrad(pc, R.row_of(row, 0), hw, sc.lane);
-      VG nd = vgrad(dc, drow(row), hw, sc.lane);
+      if (row == sc.i0) {
+        pc = R.row_of(row - 1, 0);
+        dc = drow(row - 1);
+      }
+      const Row pb = R.row_of(row, 0), db = drow(row);
+      VG np = vgrad(pc, pb, sc.lane);
+      VG nd = vgrad(dc, db, sc.lane);
       if (row > sc.i0 && j < n) {
         const int c = row - 1;
         const size_t f = (size_t)c * n + j;
         double a, b;
-        line_ab(diag(gp, np), diag(gd, nd), e, a, b);
+        line_ab(diag(gp, np), diag(gd, nd), es, a, b);
         dnew[f] = dc.c;
         psin[f] = pc.c + alpha * dc.c;
-        double r = a * (alpha * alpha) + b * alpha + R.point(c, 0);
+        // (n/2)^2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
+        double r = h2 * (a * (alpha * alpha) + b * alpha) + R.point(c, 0);
         rn[f] = r;
         mx = fmax(mx, r);
       }
       gp = np;
       gd = nd;
+      pc = pb;
+      dc = db;
       __syncwarp();
       R.issue(row - 2 + RD);
     }
