@@ -449,8 +449,13 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     launch(ctx, "adj_finish", k_adj_finish, gN, RB, (long)N, (const double*)d_lam, (const double*)W->sums, out);
     OTM_CUDA(cudaGetLastError());
     if (!odev) copy_out(ctx, grad_density, out, sizeof(double) * N);
+    // a bounded wait inside a transform that gave up flags its record
+    std::vector<Inst> recs_h((size_t)W->m + 3);
+    OTM_CUDA(cudaMemcpyAsync(recs_h.data(), W->rec(0), sizeof(Inst) * recs_h.size(), cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();
+    for (const Inst& r : recs_h)
+      if (r.fault) throw DeviceTimeout{"otm_adjoint: a bounded device-side wait gave up"};
     if (stats) {
       stats->iterations = solves;
       stats->relative_residual = rel;

@@ -28,6 +28,11 @@ struct BadArg {
   std::string what;
 };
 
+// A bounded device-side wait gave up (reported as OTM_ERR_TIMEOUT).
+struct DeviceTimeout {
+  std::string what;
+};
+
 // True when p points into device (or managed) memory; host pointers, registered
 // or not, report false.
 inline bool is_device_ptr(const void* p) {

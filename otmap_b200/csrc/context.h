@@ -190,6 +190,9 @@ int guarded(F&& f) {
   } catch (const BadArg& e) {
     set_error(e.what);
     return OTM_ERR_BAD_ARG;
+  } catch (const DeviceTimeout& e) {
+    set_error(e.what);
+    return OTM_ERR_TIMEOUT;
   } catch (const CudaError& e) {
     set_error(std::string(cudaGetErrorString(e.code)) + " (" + e.where + ")");
     cudaGetLastError();  // a non-sticky error must not resurface in the next call's check

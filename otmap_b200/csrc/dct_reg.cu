@@ -19,6 +19,7 @@
 // pass stages a tile of full column pairs in shared memory so its global reads and
 // writes are row-contiguous.
 
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -147,102 +148,233 @@ __device__ __forceinline__ double2 pre3(int k, double a, double b, double2 pt) {
   return make_double2(0.5 * fma(a, pt.x, b * pt.y), 0.5 * fma(a, pt.y, -b * pt.x));
 }
 
+// ---- row passes: software-pipelined over the warp's work items ----
+//
+// A work item is LPW consecutive row pairs (one per FFT line of the warp), 2*LPW whole
+// rows that are contiguous in global memory; items are numbered within the segment
+// (seg + item indexes the work list, whose entries Inst::row0 counts from). The grid is persistent (as many blocks as
+// fit on the GPU); each warp takes items item, item + stride, ... and keeps one item in
+// flight: as soon as an item's rows are in registers, one lane starts the bulk copy
+// (cp.async.bulk, completion on the warp's mbarrier) of the next item into the warp's
+// shared buffer, and the copy proceeds while the warp computes the FFTs of the current
+// item. Waits are bounded: if one runs out the instance is flagged (Inst::fault) and
+// stopped, and the warp returns after a second bounded wait for its copy.
+
+template <int N1, int N2>
+struct RowGeom {
+  static constexpr int n = N1 * N2, LPW = 32 / N2;
+  static constexpr int DATA = 2 * LPW * n;           // doubles: the item's rows
+  static constexpr int TRANS = LPW * N1 * (N2 + 1);  // doubles: step-3 transpose buffers
+  static constexpr int WARP = DATA + TRANS;          // doubles per warp (even: 16-byte aligned)
+  static constexpr size_t SMEM = sizeof(double) * RW * WARP + 16 * RW;  // + one mbarrier per warp
+};
+
+constexpr long long kWaitCycles = 2000000000LL;  // ~1 s at the B200's clock
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+
+// One lane: expect `bytes` on the barrier and start the bulk copy global -> shared. The
+// proxy fence orders the warp's earlier generic reads of the buffer before the copy's writes.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// Waits until the barrier's phase of parity `parity` has completed; false when the
+// bound ran out first.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  const unsigned a = smem_u32(bar);
+  const long long t0 = clock64();
+  while (true) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+}
+
+// A wait ran out: flag and stop the instance, give the copy in flight one more bounded
+// wait, and leave.
+__device__ __forceinline__ void wait_fault(Inst& I, unsigned long long* bar, unsigned parity, int lane) {
+  if (lane == 0) {
+    atomicExch(&I.fault, 1);
+    I.active = 0;
+  }
+  mbar_wait(bar, parity);
+}
+
 // Forward DCT-II of rows 2p and 2p+1 of r_k (one complex FFT per row pair) -> T.
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_fwd(const Inst* insts, const int* row_inst, int seg) {
-  constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
-  extern __shared__ double sbuf[];
-  const int item = seg + blockIdx.x;
-  const Inst& I = insts[row_inst[item]];
-  if (!I.active) return;
+__global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const int* row_inst, int seg,
+                                                              int items) {
+  using G = RowGeom<N1, N2>;
+  constexpr int n = G::n, LPW = G::LPW;
+  extern __shared__ __align__(16) double sbuf[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
-  const int row = 2 * ((item - I.row0) * LPB + warp * LPW + sub);
-  double* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
-  const double* xa = I.r[I.it % 3] + (size_t)row * n;
-  const double* xb = xa + n;
-  double* ya = I.t1 + (size_t)row * n;
-  double* yb = ya + n;
-  const double2* tw = I.tw;
-  const double2* pt = I.pt;
-  // Makhoul order: sample m < n/2 is x[2m], sample m >= n/2 is x[2(n-1-m)+1]. Lane t
-  // loads the pairs x[2(N2 m1 + t)], x[2(N2 m1 + t) + 1] (m1 < N1/2, 16-byte loads): the
-  // first is its own sample m = N2 m1 + t, the second is sample n-1-m, which belongs to
-  // lane N2-1-t at m1' = N1-1-m1 and is passed there by a shuffle.
-  double2 v[N1];
-  double2 u[N2];
+  double* data = sbuf + warp * G::WARP;
+  double* buf = data + G::DATA + sub * N1 * (N2 + 1);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sbuf + RW * G::WARP) + 2 * warp;
+  const int stride = gridDim.x * RW;
+  if (lane == 0) mbar_init(bar);
+  __syncwarp();
+  auto issue = [&](int it) -> bool {
+    if (it >= items) return false;
+    const Inst& J = insts[row_inst[seg + it]];
+    if (!J.active) return false;
+    if (lane == 0)
+      bulk_load(data, J.r[J.it % 3] + (size_t)(seg + it - J.row0) * G::DATA, sizeof(double) * G::DATA, bar);
+    return true;
+  };
+  unsigned phase = 0;
+  int item = blockIdx.x * RW + warp;
+  bool pending = issue(item);
   const int mirror = (lane - t) + (N2 - 1 - t);
-#pragma unroll
-  for (int m1 = 0; m1 < N1 / 2; ++m1) {
-    const double2 pa = __ldcg(reinterpret_cast<const double2*>(xa + 2 * (N2 * m1 + t)));
-    const double2 pb = __ldcg(reinterpret_cast<const double2*>(xb + 2 * (N2 * m1 + t)));
-    v[m1] = make_double2(pa.x, pb.x);
-    v[N1 - 1 - m1] = make_double2(__shfl_sync(0xffffffffu, pa.y, mirror), __shfl_sync(0xffffffffu, pb.y, mirror));
-  }
-  fft_line<N1, N2>(t, buf, tw, false, v, u);
   const int src_lane = (lane - t) + (t < N1 ? (N1 - t) % N1 : 0);
-#pragma unroll
-  for (int r = 0; r < N2; ++r) {
-    const double2 send = (t == 0) ? u[partner_reg<N2>(r, true)] : u[partner_reg<N2>(r, false)];
-    const double px = __shfl_sync(0xffffffffu, send.x, src_lane);
-    const double py = __shfl_sync(0xffffffffu, send.y, src_lane);
-    if (t < N1) {
-      const int k = t + N1 * rbrev<N2>(r);
-      const double2 Z = u[r];
-      const double2 A = make_double2(0.5 * (Z.x + px), 0.5 * (Z.y - py));
-      const double2 B = make_double2(0.5 * (Z.y + py), 0.5 * (px - Z.x));
-      const double2 w = __ldg(&pt[k]);
-      const double sk = dct_s(k, n);
-      ya[k] = post2(A, w, sk);
-      yb[k] = post2(B, w, sk);
+  while (item < items) {
+    const int next = item + stride;
+    if (!pending) {
+      pending = issue(next);
+      item = next;
+      continue;
     }
+    Inst& I = insts[row_inst[seg + item]];
+    if (!mbar_wait(bar, phase)) {
+      wait_fault(I, bar, phase, lane);
+      return;
+    }
+    phase ^= 1;
+    // Makhoul order: sample m < n/2 is x[2m], sample m >= n/2 is x[2(n-1-m)+1]. Lane t
+    // reads the pairs x[2(N2 m1 + t)], x[2(N2 m1 + t) + 1] (m1 < N1/2): the first is its
+    // own sample m = N2 m1 + t, the second is sample n-1-m, which belongs to lane
+    // N2-1-t at m1' = N1-1-m1 and is passed there by a shuffle.
+    const double* xa = data + sub * 2 * n;
+    const double* xb = xa + n;
+    double2 v[N1];
+    double2 u[N2];
+#pragma unroll
+    for (int m1 = 0; m1 < N1 / 2; ++m1) {
+      const double2 pa = *reinterpret_cast<const double2*>(xa + 2 * (N2 * m1 + t));
+      const double2 pb = *reinterpret_cast<const double2*>(xb + 2 * (N2 * m1 + t));
+      v[m1] = make_double2(pa.x, pb.x);
+      v[N1 - 1 - m1] =
+          make_double2(__shfl_sync(0xffffffffu, pa.y, mirror), __shfl_sync(0xffffffffu, pb.y, mirror));
+    }
+    __syncwarp();
+    pending = issue(next);  // the next item's rows arrive while this one is transformed
+    const int row = (seg + item - I.row0) * 2 * LPW + 2 * sub;
+    double* ya = I.t1 + (size_t)row * n;
+    double* yb = ya + n;
+    const double2* pt = I.pt;
+    fft_line<N1, N2>(t, buf, I.tw, false, v, u);
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      const double2 send = (t == 0) ? u[partner_reg<N2>(r, true)] : u[partner_reg<N2>(r, false)];
+      const double px = __shfl_sync(0xffffffffu, send.x, src_lane);
+      const double py = __shfl_sync(0xffffffffu, send.y, src_lane);
+      if (t < N1) {
+        const int k = t + N1 * rbrev<N2>(r);
+        const double2 Z = u[r];
+        const double2 A = make_double2(0.5 * (Z.x + px), 0.5 * (Z.y - py));
+        const double2 B = make_double2(0.5 * (Z.y + py), 0.5 * (px - Z.x));
+        const double2 w = __ldg(&pt[k]);
+        const double sk = dct_s(k, n);
+        ya[k] = post2(A, w, sk);
+        yb[k] = post2(B, w, sk);
+      }
+    }
+    item = next;
   }
 }
 
 // Inverse DCT-III of rows 2p and 2p+1 of T -> d_hat: the inputs W^a + i W^b of the two
 // rows go through one inverse FFT; its real and imaginary parts are the two rows.
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32, 3) void k_dct_rows_inv(const Inst* insts, const int* row_inst, int seg) {
-  constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;
-  extern __shared__ double sbuf[];
-  const int item = seg + blockIdx.x;
-  const Inst& I = insts[row_inst[item]];
-  if (!I.active) return;
+__global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const int* row_inst, int seg,
+                                                              int items) {
+  using G = RowGeom<N1, N2>;
+  constexpr int n = G::n, LPW = G::LPW;
+  extern __shared__ __align__(16) double sbuf[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
-  const int row = 2 * ((item - I.row0) * LPB + warp * LPW + sub);
-  double* buf = sbuf + (warp * LPW + sub) * N1 * (N2 + 1);
-  const double* Xa = I.t1 + (size_t)row * n;
-  const double* Xb = Xa + n;
-  double* xa = I.dhat + (size_t)row * n;
-  double* xb = xa + n;
-  const double2* tw = I.tw;
-  const double2* pt = I.pt;
-  double2 v[N1];
-  double2 u[N2];
-#pragma unroll
-  for (int m1 = 0; m1 < N1; ++m1) {
-    const int k = N2 * m1 + t;
-    const double2 w = __ldg(&pt[k]);
-    const double sk = dct_s(k, n), snk = k == 0 ? 0.0 : dct_s(n - k, n);
-    const double2 Wa = pre3(k, sk * __ldcg(&Xa[k]), k == 0 ? 0.0 : snk * __ldcg(&Xa[n - k]), w);
-    const double2 Wb = pre3(k, sk * __ldcg(&Xb[k]), k == 0 ? 0.0 : snk * __ldcg(&Xb[n - k]), w);
-    v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
-  }
-  fft_line<N1, N2>(t, buf, tw, true, v, u);
-  // Output m = t + N1 k2 goes to x[2m] for m < n/2; its neighbour x[2m+1] is output
-  // n-1-m, held by lane N1-1-t in the register of k2' = N2-1-k2: one shuffle and a
-  // 16-byte store per pair.
+  double* data = sbuf + warp * G::WARP;
+  double* buf = data + G::DATA + sub * N1 * (N2 + 1);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sbuf + RW * G::WARP) + 2 * warp;
+  const int stride = gridDim.x * RW;
+  if (lane == 0) mbar_init(bar);
+  __syncwarp();
+  auto issue = [&](int it) -> bool {
+    if (it >= items) return false;
+    const Inst& J = insts[row_inst[seg + it]];
+    if (!J.active) return false;
+    if (lane == 0) bulk_load(data, J.t1 + (size_t)(seg + it - J.row0) * G::DATA, sizeof(double) * G::DATA, bar);
+    return true;
+  };
+  unsigned phase = 0;
+  int item = blockIdx.x * RW + warp;
+  bool pending = issue(item);
   const int mirror = (lane - t) + (t < N1 ? N1 - 1 - t : 0);
-#pragma unroll
-  for (int r = 0; r < N2; ++r) {
-    if (rbrev<N2>(r) >= N2 / 2) continue;
-    const double2 other = u[rbrev<N2>(N2 - 1 - rbrev<N2>(r))];
-    const double qa = __shfl_sync(0xffffffffu, other.x, mirror);
-    const double qb = __shfl_sync(0xffffffffu, other.y, mirror);
-    if (t < N1) {
-      const int m = t + N1 * rbrev<N2>(r);
-      *reinterpret_cast<double2*>(xa + 2 * m) = make_double2(u[r].x, qa);
-      *reinterpret_cast<double2*>(xb + 2 * m) = make_double2(u[r].y, qb);
+  while (item < items) {
+    const int next = item + stride;
+    if (!pending) {
+      pending = issue(next);
+      item = next;
+      continue;
     }
+    Inst& I = insts[row_inst[seg + item]];
+    if (!mbar_wait(bar, phase)) {
+      wait_fault(I, bar, phase, lane);
+      return;
+    }
+    phase ^= 1;
+    const double* Xa = data + sub * 2 * n;
+    const double* Xb = Xa + n;
+    const double2* pt = I.pt;
+    double2 v[N1];
+    double2 u[N2];
+#pragma unroll
+    for (int m1 = 0; m1 < N1; ++m1) {
+      const int k = N2 * m1 + t;
+      const double2 w = __ldg(&pt[k]);
+      const double sk = dct_s(k, n), snk = k == 0 ? 0.0 : dct_s(n - k, n);
+      const double2 Wa = pre3(k, sk * Xa[k], k == 0 ? 0.0 : snk * Xa[n - k], w);
+      const double2 Wb = pre3(k, sk * Xb[k], k == 0 ? 0.0 : snk * Xb[n - k], w);
+      v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
+    }
+    __syncwarp();
+    pending = issue(next);
+    const int row = (seg + item - I.row0) * 2 * LPW + 2 * sub;
+    double* xa = I.dhat + (size_t)row * n;
+    double* xb = xa + n;
+    fft_line<N1, N2>(t, buf, I.tw, true, v, u);
+    // Output m = t + N1 k2 goes to x[2m] for m < n/2; its neighbour x[2m+1] is output
+    // n-1-m, held by lane N1-1-t in the register of k2' = N2-1-k2: one shuffle and a
+    // 16-byte store per pair.
+#pragma unroll
+    for (int r = 0; r < N2; ++r) {
+      if (rbrev<N2>(r) >= N2 / 2) continue;
+      const double2 other = u[rbrev<N2>(N2 - 1 - rbrev<N2>(r))];
+      const double qa = __shfl_sync(0xffffffffu, other.x, mirror);
+      const double qb = __shfl_sync(0xffffffffu, other.y, mirror);
+      if (t < N1) {
+        const int m = t + N1 * rbrev<N2>(r);
+        *reinterpret_cast<double2*>(xa + 2 * m) = make_double2(u[r].x, qa);
+        *reinterpret_cast<double2*>(xb + 2 * m) = make_double2(u[r].y, qb);
+      }
+    }
+    item = next;
   }
 }
 
@@ -370,10 +502,11 @@ __global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const in
 
 template <int N1, int N2>
 struct RegDct {
-  static constexpr int n = N1 * N2, LPW = 32 / N2, LPB = RW * LPW;  // LPB row pairs per block
-  static size_t rows_smem() { return sizeof(double) * LPB * N1 * (N2 + 1); }
+  static constexpr int n = N1 * N2, LPW = 32 / N2;
+  static size_t rows_smem() { return RowGeom<N1, N2>::SMEM; }
   static size_t cols_smem() { return sizeof(double) * ColGeom<N1, N2>::SMEM; }
   static constexpr int CB = ColGeom<N1, N2>::CB;
+  static int rows_blocks_per_sm;  // occupancy of the row kernels (set by attrs)
   static void attrs() {
     OTM_CUDA(cudaFuncSetAttribute(k_dct_rows_fwd<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)rows_smem()));
@@ -381,25 +514,32 @@ struct RegDct {
                                   (int)rows_smem()));
     OTM_CUDA(cudaFuncSetAttribute(k_dct_cols<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)cols_smem()));
+    int a = 0, b = 0;
+    OTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_dct_rows_fwd<N1, N2>, RW * 32, rows_smem()));
+    OTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_dct_rows_inv<N1, N2>, RW * 32, rows_smem()));
+    rows_blocks_per_sm = std::max(1, std::min(a, b));
   }
   static void run(otm_context* ctx, Inst* d, const int* ri, int roff, int rcnt, const int* ci, int coff, int ccnt) {
-    launch_smem(ctx, "dct_rows_fwd", k_dct_rows_fwd<N1, N2>, rcnt, RW * 32, rows_smem(), (const Inst*)d, ri, roff);
+    const int grid = std::max(1, std::min((rcnt + RW - 1) / RW, rows_blocks_per_sm * ctx->num_sms));
+    launch_smem(ctx, "dct_rows_fwd", k_dct_rows_fwd<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt);
     launch_smem(ctx, "dct_cols", k_dct_cols<N1, N2>, ccnt, 256, cols_smem(), (const Inst*)d, ci, coff);
-    launch_smem(ctx, "dct_rows_inv", k_dct_rows_inv<N1, N2>, rcnt, RW * 32, rows_smem(), (const Inst*)d, ri, roff);
+    launch_smem(ctx, "dct_rows_inv", k_dct_rows_inv<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt);
   }
 };
+template <int N1, int N2>
+int RegDct<N1, N2>::rows_blocks_per_sm = 1;
 
 }  // namespace
 
 bool dct_reg_supported(int n) { return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024; }
 
-int dct_reg_lines_per_block(int n) {  // rows per block: two per FFT line
+int dct_reg_lines_per_block(int n) {  // rows per row-pass work item: two per FFT line of a warp
   switch (n) {
-    case 64: return 2 * RegDct<8, 8>::LPB;
-    case 128: return 2 * RegDct<8, 16>::LPB;
-    case 256: return 2 * RegDct<16, 16>::LPB;
-    case 512: return 2 * RegDct<16, 32>::LPB;
-    default: return 2 * RegDct<32, 32>::LPB;
+    case 64: return 2 * RegDct<8, 8>::LPW;
+    case 128: return 2 * RegDct<8, 16>::LPW;
+    case 256: return 2 * RegDct<16, 16>::LPW;
+    case 512: return 2 * RegDct<16, 32>::LPW;
+    default: return 2 * RegDct<32, 32>::LPW;
   }
 }
 

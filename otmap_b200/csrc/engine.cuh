@@ -18,7 +18,8 @@ constexpr int GB = 64, GK = 16;           // DCT GEMM tile (GB x GB outputs, GK 
 // the workspace; everything below `it` is loop state updated by the kernels.
 struct Inst {
   int n, tile0, ntiles, gemm0, ngemm;
-  int max_iter, beta_cj, pad0;
+  int max_iter, beta_cj;
+  int fault;  // set on the device when a bounded wait gave up (the instance is stopped)
   double threshold, max_ratio;
   double* psi[2];
   double* r[3];

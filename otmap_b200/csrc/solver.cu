@@ -806,6 +806,8 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
       OTM_CUDA(cudaGetLastError());
     }
   }
+  for (int q = 0; q < count; ++q)
+    if (hp[q].fault) throw DeviceTimeout{"a bounded device-side wait gave up"};
   std::vector<Inst> out(hp, hp + count);
   return out;
 }

@@ -37,7 +37,7 @@ __device__ __forceinline__ int clampn(int v, int n) { return v < 0 ? 0 : (v >= n
 struct Row {   // one field on one grid row around the lane's column j
   double c;    // column j
   double l;    // column j - 1
-  double rh;   // lane 31: column j0 + 32
+  double r;    // column j + 1
 };
 
 // ---- per-warp asynchronous row prefetch (cp.async, 8-byte copies) ----
@@ -87,7 +87,7 @@ struct Ring {
     Row r;
     r.c = d[1 + lane];
     r.l = d[lane];
-    r.rh = d[33];
+    r.r = d[2 + lane];
     return r;
   }
   __device__ __forceinline__ double point(int row, int k) { return stage(row)[NS * 34 + k * 32 + lane]; }
@@ -97,24 +97,20 @@ struct VG {    // vertex gradients (v, j) and (v, j + 1)
   double gx, gy, gxr, gyr;
 };
 
-// Vertex gradients of vertex row v from cell rows a = v-1 and b = v
-// (otsolver_2dgrid.cpp:379-391 with clamped cells = boundary rules :405-422), divided by
-// the reference's factor n/2: the sweeps carry that factor into the line coefficients
-// (a, b scale by (n/2)^2) and apply it to the sums and the residual update. For
-// power-of-two n the factor is a power of two and every result is bit-identical to
-// scaling each gradient.
-__device__ __forceinline__ VG vgrad(const Row& a, const Row& b, int lane) {
+// Vertex gradients of vertex row v at columns j and j+1 from cell rows a = v-1 and
+// b = v (otsolver_2dgrid.cpp:379-391 with clamped cells = boundary rules :405-422),
+// divided by the reference's factor n/2: the sweeps carry that factor into the line
+// coefficients (a, b scale by (n/2)^2) and apply it to the sums and the residual
+// update. For power-of-two n the factor is a power of two and every result is
+// bit-identical to scaling each gradient. The gradient at j+1 is the expression lane j+1
+// evaluates for its own vertex, formed here from the staged column j+1.
+__device__ __forceinline__ VG vgrad(const Row& a, const Row& b) {
   VG g;
+  const double sc = a.c + b.c;
   g.gx = (b.l + b.c) - (a.l + a.c);
-  g.gy = (a.c + b.c) - (a.l + b.l);
-  double gxr = __shfl_down_sync(0xffffffffu, g.gx, 1);
-  double gyr = __shfl_down_sync(0xffffffffu, g.gy, 1);
-  if (lane == 31) {
-    gxr = (b.c + b.rh) - (a.c + a.rh);
-    gyr = (a.rh + b.rh) - (a.c + b.c);
-  }
-  g.gxr = gxr;
-  g.gyr = gyr;
+  g.gy = sc - (a.l + b.l);
+  g.gxr = (b.c + b.r) - (a.c + a.r);
+  g.gyr = (a.r + b.r) - sc;
   return g;
 }
 
@@ -133,15 +129,16 @@ __device__ __forceinline__ Diag diag(const VG& p, const VG& q) {
   return d;
 }
 
-// a(dir) and b(dir; psi) of otsolver_2dgrid.cpp:523-536 from the direction's diagonal
-// differences h and the potential's g.
+// 2a(dir) and 2b(dir; psi) of otsolver_2dgrid.cpp:523-536 from the direction's diagonal
+// differences h and the potential's g (the reference's factor 1/2 is applied, exactly,
+// with the (n/2)^2 scale).
 __device__ __forceinline__ void line_ab(const Diag& g, const Diag& h, double e, double& a, double& b) {
   double diag0a_x = g.ax + e;
   double diag0a_y = g.ay + e;
   double diag0b_x = g.bx - e;
   double diag0b_y = g.by + e;
-  a = 0.5 * (h.ax * h.by - h.ay * h.bx);
-  b = 0.5 * (h.ax * diag0b_y - h.ay * diag0b_x + diag0a_x * h.by - diag0a_y * h.bx);
+  a = h.ax * h.by - h.ay * h.bx;
+  b = h.ax * diag0b_y - h.ay * diag0b_x + diag0a_x * h.by - diag0a_y * h.bx;
 }
 
 struct StripCoord {
@@ -230,16 +227,16 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
       }
       const Row bp = R.row_of(row, 0), bh = R.row_of(row, 1), bq = R.row_of(row, 2);
       // vertex row `row` from grid rows row-1 and row
-      VG np = vgrad(ap, bp, sc.lane);
-      VG nh = vgrad(ah, bh, sc.lane);
-      VG nq = vgrad(aq, bq, sc.lane);
+      VG np = vgrad(ap, bp);
+      VG nh = vgrad(ah, bh);
+      VG nq = vgrad(aq, bq);
       if (row > sc.i0 && j < n) {
         const int c = row - 1;
         Diag G = diag(gp, np), Hd = diag(gh, nh), Qd = diag(gq, nq);
         double a11, b1, a22, b2;
         line_ab(G, Hd, es, a11, b1);
         line_ab(G, Qd, es, a22, b2);
-        double a12 = 0.5 * (Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx);
+        double a12 = Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx;
         double r = R.point(c, 0), jd = r - R.point(c, 1);
         double hv = ah.c, qv = aq.c;
         acc[S_HH] = fma(hv, hv, acc[S_HH]);
@@ -285,8 +282,8 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
     double S[S_COUNT];
     reduce_block_partials<S_COUNT>(partials, I.strip0, I.nstrip, S, red);
     if (threadIdx.x == 0) {
-      // restore the (n/2)^2 factor of each line coefficient in the sums
-      const double h2 = hw * hw, h4 = h2 * h2;
+      // restore the factor (n/2)^2 / 2 of each line coefficient in the sums
+      const double h2 = 0.5 * hw * hw, h4 = h2 * h2;
       S[S_JB] *= h2;
       S[S_JA] *= h2;
       S[S_B1R] *= h2;
@@ -335,7 +332,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
   Inst& I = insts[strip_inst[blockIdx.x]];
   if (!I.active) return;
   const int n = I.n, it = I.it;
-  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw, h2 = hw * hw, alpha = I.alpha;
+  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw, h2 = 0.5 * hw * hw, alpha = I.alpha;
   const bool use_beta = I.use_beta;
   const double beta = I.beta;
   const StripCoord sc = strip_coord(I, blockIdx.x);
@@ -367,7 +364,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
       Row d;
       d.c = h.c + beta * q.c;
       d.l = h.l + beta * q.l;
-      d.rh = h.rh + beta * q.rh;
+      d.r = h.r + beta * q.r;
       return d;
     };
     VG gp, gd;
@@ -380,8 +377,8 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
         dc = drow(row - 1);
       }
       const Row pb = R.row_of(row, 0), db = drow(row);
-      VG np = vgrad(pc, pb, sc.lane);
-      VG nd = vgrad(dc, db, sc.lane);
+      VG np = vgrad(pc, pb);
+      VG nd = vgrad(dc, db);
       if (row > sc.i0 && j < n) {
         const int c = row - 1;
         const size_t f = (size_t)c * n + j;
@@ -389,7 +386,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
         line_ab(diag(gp, np), diag(gd, nd), es, a, b);
         dnew[f] = dc.c;
         psin[f] = pc.c + alpha * dc.c;
-        // (n/2)^2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
+        // (n/2)^2 / 2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
         double r = h2 * (a * (alpha * alpha) + b * alpha) + R.point(c, 0);
         rn[f] = r;
         mx = fmax(mx, r);
