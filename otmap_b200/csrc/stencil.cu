@@ -31,6 +31,7 @@ constexpr int SWARPS = 4;     // strips per block
 constexpr int ST = SW * SWARPS;
 constexpr int KA = SWEEP_SLOTS;  // partial-sum slots per block
 constexpr int RD = 8;         // rows in the per-warp prefetch ring (RD - 3 in flight beyond the two in use)
+static_assert((RD & (RD - 1)) == 0, "the ring depth is a power of two");
 
 __device__ __forceinline__ int clampn(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
 
@@ -62,7 +63,8 @@ struct Ring {
   const double* pf[NP > 0 ? NP : 1];
   int n, j0, lane, rows_end;  // rows beyond rows_end are not fetched
 
-  __device__ __forceinline__ double* stage(int row) { return buf + ((row + 2 * RD) % RD) * STAGE; }
+  // RD is a power of two and row >= -1, so the stage index is a mask of row + RD
+  __device__ __forceinline__ double* stage(int row) { return buf + ((unsigned)(row + RD) & (RD - 1u)) * STAGE; }
 
   // Queues the copies of grid row `row` (clamped) and commits them as one group.
   __device__ __forceinline__ void issue(int row) {
