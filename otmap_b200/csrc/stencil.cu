@@ -219,6 +219,7 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
     for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
     VG gp, gh, gq;
     Row ap, ah, aq;  // grid row row-1 of each stencil field, carried from the previous step
+#pragma unroll 2
     for (int row = sc.i0; row <= last; ++row) {
       cp_async_wait<RD - 3>();
       __syncwarp();
@@ -371,6 +372,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
     };
     VG gp, gd;
     Row pc, dc;  // grid row row-1 of psi and of d, carried from the previous step
+#pragma unroll 2
     for (int row = sc.i0; row <= last; ++row) {
       cp_async_wait<RD - 3>();
       __syncwarp();
