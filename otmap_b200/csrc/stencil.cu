@@ -41,13 +41,21 @@ struct Row {   // one field on one grid row around the lane's column j
   double r;    // column j + 1
 };
 
-// ---- per-warp asynchronous row prefetch (cp.async, 8-byte copies) ----
-// A stage holds one grid row of the strip for every field: stencil fields take 34
-// slots (columns j0-1 .. j0+32, clamped), pointwise fields 32 (columns j0 .. j0+31).
+// ---- per-warp asynchronous row prefetch (cp.async) ----
+// A stage holds one grid row of the strip for every field: stencil fields take 36
+// slots (columns j0-2 .. j0+33; slot 1 + lane is column j - 1), pointwise fields 32
+// (columns j0 .. j0+31). Interior strips (j0 >= 2, j0 + 34 <= n, n even) copy a stencil
+// row with one 16-byte cp.async on 18 lanes (16 column pairs and the two halo pairs) and
+// a pointwise row on 16 lanes; edge strips and odd n use 8-byte copies with clamped
+// columns (the reference's boundary cells).
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   unsigned s = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(double* dst, const double* src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
@@ -57,11 +65,20 @@ __device__ __forceinline__ void cp_async_wait() {
 
 template <int NS, int NP>
 struct Ring {
-  static constexpr int STAGE = NS * 34 + NP * 32;
+  static constexpr int SS = 36;  // slots of a stencil field row
+  static constexpr int STAGE = NS * SS + NP * 32;
   double* buf;  // RD * STAGE doubles (this warp's)
   const double* sf[NS > 0 ? NS : 1];
   const double* pf[NP > 0 ? NP : 1];
   int n, j0, lane, rows_end;  // rows beyond rows_end are not fetched
+  bool interior;              // 16-byte copies (warp-uniform)
+  int soff, gcol;             // this lane's stencil slot and global column (interior copies)
+
+  __device__ __forceinline__ void setup() {
+    interior = (j0 >= 2) && (j0 + 34 <= n) && ((n & 1) == 0);
+    soff = lane < 16 ? 2 + 2 * lane : (lane == 16 ? 0 : 34);
+    gcol = lane < 16 ? j0 + 2 * lane : (lane == 16 ? j0 - 2 : j0 + 32);
+  }
 
   // RD is a power of two and row >= -1, so the stage index is a mask of row + RD
   __device__ __forceinline__ double* stage(int row) { return buf + ((unsigned)(row + RD) & (RD - 1u)) * STAGE; }
@@ -71,28 +88,39 @@ struct Ring {
     if (row <= rows_end) {
       double* st = stage(row);
       const size_t base = (size_t)clampn(row, n) * n;
-      const size_t cj = base + clampn(j0 + lane, n);
+      if (interior) {
+        if (lane < 18) {
 #pragma unroll
-      for (int k = 0; k < NS; ++k) {
-        double* d = st + k * 34;
-        cp_async8(d + 1 + lane, sf[k] + cj);
-        if (lane == 0) cp_async8(d, sf[k] + base + clampn(j0 - 1, n));
-        if (lane == 31) cp_async8(d + 33, sf[k] + base + clampn(j0 + 32, n));
+          for (int k = 0; k < NS; ++k) cp_async16(st + k * SS + soff, sf[k] + base + gcol);
+        }
+        if (lane < 16) {
+#pragma unroll
+          for (int k = 0; k < NP; ++k) cp_async16(st + NS * SS + k * 32 + 2 * lane, pf[k] + base + j0 + 2 * lane);
+        }
+      } else {
+        const size_t cj = base + clampn(j0 + lane, n);
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          double* d = st + k * SS;
+          cp_async8(d + 2 + lane, sf[k] + cj);
+          if (lane == 0) cp_async8(d + 1, sf[k] + base + clampn(j0 - 1, n));
+          if (lane == 31) cp_async8(d + 34, sf[k] + base + clampn(j0 + 32, n));
+        }
+#pragma unroll
+        for (int k = 0; k < NP; ++k) cp_async8(st + NS * SS + k * 32 + lane, pf[k] + cj);
       }
-#pragma unroll
-      for (int k = 0; k < NP; ++k) cp_async8(st + NS * 34 + k * 32 + lane, pf[k] + cj);
     }
     cp_async_commit();
   }
   __device__ __forceinline__ Row row_of(int row, int k) {
-    const double* d = stage(row) + k * 34;
+    const double* d = stage(row) + k * SS;
     Row r;
-    r.c = d[1 + lane];
-    r.l = d[lane];
-    r.r = d[2 + lane];
+    r.c = d[2 + lane];
+    r.l = d[1 + lane];
+    r.r = d[3 + lane];
     return r;
   }
-  __device__ __forceinline__ double point(int row, int k) { return stage(row)[NS * 34 + k * 32 + lane]; }
+  __device__ __forceinline__ double point(int row, int k) { return stage(row)[NS * SS + k * 32 + lane]; }
 };
 
 struct VG {    // vertex gradients (v, j) and (v, j + 1)
@@ -190,7 +218,7 @@ enum {
 };
 
 __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip_inst, double* partials) {
-  extern __shared__ double ring_smem[];
+  extern __shared__ __align__(16) double ring_smem[];
   __shared__ double red[32 * S_COUNT];
   Inst& I = insts[strip_inst[blockIdx.x]];
   if (!I.active) return;
@@ -215,6 +243,7 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
     R.lane = sc.lane;
     const int last = min(sc.i0 + SR, n);  // cell rows i0 .. last-1; grid rows i0-1 .. last
     R.rows_end = last;
+    R.setup();
 #pragma unroll
     for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
     VG gp, gh, gq;
@@ -330,7 +359,7 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
 }
 
 __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* strip_inst, double* partials) {
-  extern __shared__ double ring_smem[];
+  extern __shared__ __align__(16) double ring_smem[];
   __shared__ double red[32];
   Inst& I = insts[strip_inst[blockIdx.x]];
   if (!I.active) return;
@@ -356,6 +385,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
     R.lane = sc.lane;
     const int last = min(sc.i0 + SR, n);
     R.rows_end = last;
+    R.setup();
 #pragma unroll
     for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
     // d = d_hat + beta d_prev, formed from the staged rows exactly as the reference
