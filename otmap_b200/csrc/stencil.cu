@@ -3,7 +3,7 @@
 //
 //   k_sweep_sums   reads psi, d_hat, d_prev, r_k, r_{k-1}; per cell the line
 //                  coefficients of d_hat (b1, a11) and of d_prev (b2, a22) and their
-//                  cross term a12, and 26 partial sums. The last block of an instance
+//                  cross term a12, and 23 partial sums. The last block of an instance
 //                  turns them into |d_hat| (early exit, :182), beta (:248-261, with
 //                  r(psi - eps d_hat) - r_k = -eps b1 + eps^2 a11, exact for the
 //                  quadratic area) and the quartic of the line search for
@@ -212,8 +212,8 @@ enum {
   S_JB, S_JA, S_JJ,            // Jd.b1, Jd.a11, |Jd|^2 with Jd = r_k - r_{k-1}
   S_B1R, S_B2R, S_B1B1, S_B1B2, S_B2B2,
   S_A11R, S_A12R, S_A22R,
-  S_A11B1, S_A11B2, S_A12B1, S_A12B2, S_A22B1, S_A22B2,
-  S_A11A11, S_A11A12, S_A12A12, S_A11A22, S_A12A22, S_A22A22,
+  S_AB0, S_AB1, S_AB2, S_AB3,  // sum a(beta) b(beta) by powers of beta: a11b1, a11b2+a12b1, a12b2+a22b1, a22b2
+  S_AA0, S_AA1, S_AA2, S_AA3, S_AA4,  // a11^2, a11a12, a12^2+2a11a22, a12a22, a22^2
   S_COUNT
 };
 
@@ -285,18 +285,15 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
         acc[S_A11R] = fma(a11, r, acc[S_A11R]);
         acc[S_A12R] = fma(a12, r, acc[S_A12R]);
         acc[S_A22R] = fma(a22, r, acc[S_A22R]);
-        acc[S_A11B1] = fma(a11, b1, acc[S_A11B1]);
-        acc[S_A11B2] = fma(a11, b2, acc[S_A11B2]);
-        acc[S_A12B1] = fma(a12, b1, acc[S_A12B1]);
-        acc[S_A12B2] = fma(a12, b2, acc[S_A12B2]);
-        acc[S_A22B1] = fma(a22, b1, acc[S_A22B1]);
-        acc[S_A22B2] = fma(a22, b2, acc[S_A22B2]);
-        acc[S_A11A11] = fma(a11, a11, acc[S_A11A11]);
-        acc[S_A11A12] = fma(a11, a12, acc[S_A11A12]);
-        acc[S_A12A12] = fma(a12, a12, acc[S_A12A12]);
-        acc[S_A11A22] = fma(a11, a22, acc[S_A11A22]);
-        acc[S_A12A22] = fma(a12, a22, acc[S_A12A22]);
-        acc[S_A22A22] = fma(a22, a22, acc[S_A22A22]);
+        acc[S_AB0] = fma(a11, b1, acc[S_AB0]);
+        acc[S_AB1] = fma(a11, b2, fma(a12, b1, acc[S_AB1]));
+        acc[S_AB2] = fma(a12, b2, fma(a22, b1, acc[S_AB2]));
+        acc[S_AB3] = fma(a22, b2, acc[S_AB3]);
+        acc[S_AA0] = fma(a11, a11, acc[S_AA0]);
+        acc[S_AA1] = fma(a11, a12, acc[S_AA1]);
+        acc[S_AA2] = fma(a12, a12, fma(a11 + a11, a22, acc[S_AA2]));
+        acc[S_AA3] = fma(a12, a22, acc[S_AA3]);
+        acc[S_AA4] = fma(a22, a22, acc[S_AA4]);
       }
       gp = np;
       gh = nh;
@@ -326,7 +323,7 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
 #pragma unroll
       for (int k = S_B1B1; k <= S_B2B2; ++k) S[k] *= h4;
 #pragma unroll
-      for (int k = S_A11B1; k < S_COUNT; ++k) S[k] *= h4;
+      for (int k = S_AB0; k < S_COUNT; ++k) S[k] *= h4;
       if (sqrt(S[S_HH]) <= 2.0 * DBL_MIN) {  // otsolver_2dgrid.cpp:182
         I.active = 0;
         I.outcome = OTM_SMALL_STEP;
@@ -342,10 +339,8 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
         const double sbr = S[S_B1R] + B * S[S_B2R];
         const double sbb = S[S_B1B1] + 2.0 * B * S[S_B1B2] + B2 * S[S_B2B2];
         const double sar = S[S_A11R] + B * S[S_A12R] + B2 * S[S_A22R];
-        const double sab = S[S_A11B1] + B * (S[S_A11B2] + S[S_A12B1]) + B2 * (S[S_A12B2] + S[S_A22B1]) +
-                           B3 * S[S_A22B2];
-        const double saa = S[S_A11A11] + 2.0 * B * S[S_A11A12] + B2 * (S[S_A12A12] + 2.0 * S[S_A11A22]) +
-                           2.0 * B3 * S[S_A12A22] + B4 * S[S_A22A22];
+        const double sab = S[S_AB0] + B * S[S_AB1] + B2 * S[S_AB2] + B3 * S[S_AB3];
+        const double saa = S[S_AA0] + 2.0 * B * S[S_AA1] + B2 * S[S_AA2] + 2.0 * B3 * S[S_AA3] + B4 * S[S_AA4];
         const double ea = 1.0 / ((double)n * (double)n);
         double z[5] = {I.residual * ea, 2.0 * sbr, sbb + 2 * sar, 2.0 * sab, saa};
         double alpha, rmin;
