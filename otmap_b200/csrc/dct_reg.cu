@@ -83,6 +83,9 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[N], const double2* __restri
         const int e = k * (N / (2 * span));
         if (e == 0) {
           v[start + k + span] = d;
+        } else if (4 * e == N) {
+          // W_N^(N/4) = -i (forward) or +i (inverse): a swap instead of a product
+          v[start + k + span] = conj ? make_double2(-d.y, d.x) : make_double2(d.y, -d.x);
         } else {
           double2 w = c_tw[e * (CTW / N)];
           if (conj) w.y = -w.y;
