@@ -53,6 +53,7 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--no-locate", action="store_true")
     p.add_argument("--mixed-count", type=int, default=64)
     p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations timed per step")
     return p.parse_args()
@@ -316,6 +317,7 @@ def run_ours(args):
         plain = {"value": B / (tot / 1e3), "unit": UNIT, "form": "one otm_solve call per density, same kernels"}
 
     adjoint = None if args.no_adjoint else bench_adjoint(ctx, stream)
+    locate = None if args.no_locate else bench_locate(ctx, stream, n, dev_in[0])
     mixed = None if args.no_mixed else bench_mixed(stream, args.mixed_count)
 
     peaks = load_peaks()
@@ -325,7 +327,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(host[0], n)
+        cpu = cpu_baseline(host[0], n, locate_points=None if args.no_locate else LOCATE_POINTS)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -334,7 +336,7 @@ def run_ours(args):
                 "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
                 "iterations": iters, "final_residual_max": max(resid), "gpu_launches": launches,
-                "e2e": e2e, "plain": plain, "adjoint": adjoint, "batched_mixed": mixed, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "e2e": e2e, "plain": plain, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:
@@ -479,8 +481,10 @@ def bench_adjoint(ctx, stream, n=512, repeats=3):
     return out
 
 
-def cpu_baseline(density_cells, n):
-    """The reference (oracle/_ref, compiled from the reference sources) on one host core."""
+def cpu_baseline(density_cells, n, locate_points=None):
+    """The reference (oracle/_ref, compiled from the reference sources) on one host core;
+    with locate_points, also its inversion (BVH build + queries, apply_inverse_map) of that
+    many points and its rasterization of the forward mesh at n x n."""
     from oracle import ref
 
     if not ref.available():
@@ -488,11 +492,89 @@ def cpu_baseline(density_cells, n):
     s = ref.RefSolver()
     t_init = s.init(n)
     m = s.solve(density_cells, threshold=THRESHOLD)
-    return {"value": 1.0 / m.seconds, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"one full {n}^2 solve of the rank-0 instance 0 density ({m.iterations} iterations, "
-                      f"residual {m.residual:.3g}); solve {m.seconds:.2f} s, init (LDLT factorisation, "
-                      f"cached per size by the reference) {t_init:.2f} s excluded",
-            "init_seconds": t_init, "solve_seconds": m.seconds}
+    out = {"value": 1.0 / m.seconds, "unit": UNIT, "cores": 1, "kind": "reference",
+           "sample": f"one full {n}^2 solve of the rank-0 instance 0 density ({m.iterations} iterations, "
+                     f"residual {m.residual:.3g}); solve {m.seconds:.2f} s, init (LDLT factorisation, "
+                     f"cached per size by the reference) {t_init:.2f} s excluded",
+           "init_seconds": t_init, "solve_seconds": m.seconds}
+    if locate_points:
+        from otmap_b200 import workloads as W
+
+        pts = W.random_points(locate_points, LOCATE_SEED)
+        _, t_inv = m.apply_inverse(pts)
+        _, t_ras = ref.rasterize(m.fwd(), n, m.density(), n, n)
+        out["locate"] = {"inverse_queries_per_s": locate_points / t_inv, "inverse_seconds": t_inv,
+                         "raster_pixels_per_s": n * n / t_ras, "raster_seconds": t_ras,
+                         "sample": f"{locate_points} FP32-drawn points through apply_inverse_map (BVH build "
+                                   f"included); rasterize_image of the forward mesh at {n}x{n}; one core"}
+    return out
+
+
+LOCATE_POINTS = 1 << 20
+LOCATE_SEED = 7
+
+
+def bench_locate(ctx, stream, n, dens_dev, repeats=5):
+    """Inversion and rasterization of one n^2 map on the GPU (device-resident buffers):
+    the point locator build, 2^20 FP32-drawn query points through otm_map_inverse, and
+    rasterize_image of the forward mesh at n x n, each timed with CUDA events."""
+    import ctypes as C
+
+    import torch
+
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    V = (n + 1) ** 2
+    fwd = torch.empty((V, 2), dtype=torch.float64, device="cuda")
+    adj = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    opt = N.default_options()
+    opt.threshold = THRESHOLD
+    N.check(N.lib().otm_solve(ctx.handle, n, C.c_void_p(dens_dev.data_ptr()), C.byref(opt),
+                              C.c_void_p(fwd.data_ptr()), C.c_void_p(adj.data_ptr()), None))
+    pts0 = torch.from_numpy(W.random_points(LOCATE_POINTS, LOCATE_SEED)).cuda()
+    pts = pts0.clone()
+    img = torch.empty((n, n), dtype=torch.float64, device="cuda")
+    missing = C.c_long(0)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    build, inv, ras = [], [], []
+    for _ in range(repeats):
+        h = C.c_void_p()
+        N.check(N.lib().otm_map_create(ctx.handle, n, C.c_void_p(fwd.data_ptr()), C.c_void_p(adj.data_ptr()),
+                                       C.byref(h)))
+        torch.cuda.synchronize()
+        a, b = ev(), ev()
+        a.record(stream)
+        N.check(N.lib().otm_map_init_inverse(h))
+        b.record(stream)
+        b.synchronize()
+        build.append(a.elapsed_time(b))
+        pts.copy_(pts0)
+        torch.cuda.synchronize()
+        a, b = ev(), ev()
+        a.record(stream)
+        N.check(N.lib().otm_map_inverse(h, C.c_void_p(pts.data_ptr()), LOCATE_POINTS, None, None, C.byref(missing)))
+        b.record(stream)
+        b.synchronize()
+        inv.append(a.elapsed_time(b))
+        a, b = ev(), ev()
+        a.record(stream)
+        N.check(N.lib().otm_rasterize(ctx.handle, n, C.c_void_p(fwd.data_ptr()), C.c_void_p(adj.data_ptr()), n, n,
+                                      C.c_void_p(img.data_ptr())))
+        b.record(stream)
+        b.synchronize()
+        ras.append(a.elapsed_time(b))
+        N.lib().otm_map_destroy(h)
+    med = lambda v: sorted(v)[len(v) // 2]
+    return {"workload": f"one {n}^2 forward map; {LOCATE_POINTS} query points drawn in FP32 (seed {LOCATE_SEED}); "
+                        f"raster {n}x{n} with the map's density",
+            "locator_build_ms": med(build), "inverse_ms": med(inv), "inverse_queries_per_s": LOCATE_POINTS / (med(inv) / 1e3),
+            "inverse_missing": missing.value, "raster_ms": med(ras), "raster_pixels_per_s": n * n / (med(ras) / 1e3),
+            "timing": "CUDA events around each call, device-resident buffers, median of %d" % repeats}
+
 
 
 # ---------------------------------------------------------------------------

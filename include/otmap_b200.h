@@ -324,6 +324,13 @@ int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fw
 #define OTM_OPT_LOOP 2
 #define OTM_LOOP_GRAPH 0
 #define OTM_LOOP_HOST 1
+/*   OTM_OPT_WAIT_TEST: exercises the bounded device-side waits (for tests). Every wait
+ *     of the row transforms (a bulk copy completing on an mbarrier) is bounded; when one
+ *     runs out, the instance is flagged and stopped and the call returns OTM_ERR_TIMEOUT,
+ *     leaving the context usable. With value 1 those waits expect 16 bytes more than
+ *     their copy brings and give up after about 1 ms, so the path runs on demand;
+ *     0 (default) restores normal operation. */
+#define OTM_OPT_WAIT_TEST 3
 int otm_set_option(otm_context* ctx, int key, int value);
 
 /* ---- allocation-free solve (no counterpart in the reference) ----

@@ -187,6 +187,19 @@ extern "C" int otm_set_option(otm_context* ctx, int key, int value) {
     ctx->loop_mode = value;
     return OTM_OK;
   }
+  if (key == OTM_OPT_WAIT_TEST) {
+    if (value != 0 && value != 1) {
+      set_error("otm_set_option: OTM_OPT_WAIT_TEST takes 0 or 1");
+      return OTM_ERR_BAD_ARG;
+    }
+    if (ctx->wait_test != value) {
+      cudaSetDevice(ctx->device);
+      cudaStreamSynchronize(ctx->stream);
+      ctx->ws.drop_graph();  // the captured launches carry the wait parameters
+    }
+    ctx->wait_test = value;
+    return OTM_OK;
+  }
   set_error("otm_set_option: unknown option");
   return OTM_ERR_BAD_ARG;
 }

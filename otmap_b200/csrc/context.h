@@ -111,6 +111,7 @@ struct otm_context {
   long launches = 0;  // kernels launched by this context since creation
   int poisson_mode = 0;  // OTM_POISSON_AUTO / _DENSE / _FFT
   int loop_mode = 0;     // OTM_LOOP_GRAPH (0) / OTM_LOOP_HOST (1)
+  int wait_test = 0;     // OTM_OPT_WAIT_TEST: bounded waits made to run out
   otm::Profiler prof;
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   otm::Workspace ws;

@@ -172,7 +172,8 @@ struct RowGeom {
   static constexpr size_t SMEM = sizeof(double) * RW * WARP + 16 * RW;  // + one mbarrier per warp
 };
 
-constexpr long long kWaitCycles = 2000000000LL;  // ~1 s at the B200's clock
+constexpr long long kWaitCycles = 2000000000LL;   // ~1 s at the B200's clock
+constexpr long long kTestWaitCycles = 2000000LL;  // ~1 ms (OTM_OPT_WAIT_TEST)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -181,11 +182,13 @@ __device__ __forceinline__ void mbar_init(unsigned long long* bar) {
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
 }
 
-// One lane: expect `bytes` on the barrier and start the bulk copy global -> shared. The
-// proxy fence orders the warp's earlier generic reads of the buffer before the copy's writes.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+// One lane: expect `bytes` (+ `extra`, which never arrive: OTM_OPT_WAIT_TEST) on the
+// barrier and start the bulk copy global -> shared. The proxy fence orders the warp's
+// earlier generic reads of the buffer before the copy's writes.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, unsigned extra,
+                                          unsigned long long* bar) {
   asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes + extra)
                : "memory");
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                    smem_u32(dst)),
@@ -195,7 +198,7 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
 
 // Waits until the barrier's phase of parity `parity` has completed; false when the
 // bound ran out first.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity, long long limit) {
   const unsigned a = smem_u32(bar);
   const long long t0 = clock64();
   while (true) {
@@ -206,24 +209,25 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned pari
         : "r"(a), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   }
 }
 
 // A wait ran out: flag and stop the instance, give the copy in flight one more bounded
 // wait, and leave.
-__device__ __forceinline__ void wait_fault(Inst& I, unsigned long long* bar, unsigned parity, int lane) {
+__device__ __forceinline__ void wait_fault(Inst& I, unsigned long long* bar, unsigned parity, int lane,
+                                           long long limit) {
   if (lane == 0) {
     atomicExch(&I.fault, 1);
     I.active = 0;
   }
-  mbar_wait(bar, parity);
+  mbar_wait(bar, parity, limit);
 }
 
 // Forward DCT-II of rows 2p and 2p+1 of r_k (one complex FFT per row pair) -> T.
 template <int N1, int N2>
 __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const int* row_inst, int seg,
-                                                              int items) {
+                                                              int items, unsigned extra, long long limit) {
   using G = RowGeom<N1, N2>;
   constexpr int n = G::n, LPW = G::LPW;
   extern __shared__ __align__(16) double sbuf[];
@@ -239,7 +243,8 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
     const Inst& J = insts[row_inst[seg + it]];
     if (!J.active) return false;
     if (lane == 0)
-      bulk_load(data, J.r[J.it % 3] + (size_t)(seg + it - J.row0) * G::DATA, sizeof(double) * G::DATA, bar);
+      bulk_load(data, J.r[J.it % 3] + (size_t)(seg + it - J.row0) * G::DATA, sizeof(double) * G::DATA, extra,
+                bar);
     return true;
   };
   unsigned phase = 0;
@@ -255,8 +260,8 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
       continue;
     }
     Inst& I = insts[row_inst[seg + item]];
-    if (!mbar_wait(bar, phase)) {
-      wait_fault(I, bar, phase, lane);
+    if (!mbar_wait(bar, phase, limit)) {
+      wait_fault(I, bar, phase, lane, limit);
       return;
     }
     phase ^= 1;
@@ -307,7 +312,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
 // rows go through one inverse FFT; its real and imaginary parts are the two rows.
 template <int N1, int N2>
 __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const int* row_inst, int seg,
-                                                              int items) {
+                                                              int items, unsigned extra, long long limit) {
   using G = RowGeom<N1, N2>;
   constexpr int n = G::n, LPW = G::LPW;
   extern __shared__ __align__(16) double sbuf[];
@@ -322,7 +327,8 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const 
     if (it >= items) return false;
     const Inst& J = insts[row_inst[seg + it]];
     if (!J.active) return false;
-    if (lane == 0) bulk_load(data, J.t1 + (size_t)(seg + it - J.row0) * G::DATA, sizeof(double) * G::DATA, bar);
+    if (lane == 0)
+      bulk_load(data, J.t1 + (size_t)(seg + it - J.row0) * G::DATA, sizeof(double) * G::DATA, extra, bar);
     return true;
   };
   unsigned phase = 0;
@@ -337,8 +343,8 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const 
       continue;
     }
     Inst& I = insts[row_inst[seg + item]];
-    if (!mbar_wait(bar, phase)) {
-      wait_fault(I, bar, phase, lane);
+    if (!mbar_wait(bar, phase, limit)) {
+      wait_fault(I, bar, phase, lane, limit);
       return;
     }
     phase ^= 1;
@@ -524,9 +530,13 @@ struct RegDct {
   }
   static void run(otm_context* ctx, Inst* d, const int* ri, int roff, int rcnt, const int* ci, int coff, int ccnt) {
     const int grid = std::max(1, std::min((rcnt + RW - 1) / RW, rows_blocks_per_sm * ctx->num_sms));
-    launch_smem(ctx, "dct_rows_fwd", k_dct_rows_fwd<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt);
+    const unsigned extra = ctx->wait_test ? 16u : 0u;
+    const long long limit = ctx->wait_test ? kTestWaitCycles : kWaitCycles;
+    launch_smem(ctx, "dct_rows_fwd", k_dct_rows_fwd<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt, extra,
+                limit);
     launch_smem(ctx, "dct_cols", k_dct_cols<N1, N2>, ccnt, 256, cols_smem(), (const Inst*)d, ci, coff);
-    launch_smem(ctx, "dct_rows_inv", k_dct_rows_inv<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt);
+    launch_smem(ctx, "dct_rows_inv", k_dct_rows_inv<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt, extra,
+                limit);
   }
 };
 template <int N1, int N2>

@@ -27,6 +27,7 @@ OPT_POISSON = 1
 POISSON_AUTO, POISSON_DENSE, POISSON_FFT = 0, 1, 2
 OPT_LOOP = 2
 LOOP_GRAPH, LOOP_HOST = 0, 1
+OPT_WAIT_TEST = 3
 RIO_PER_VERTEX, RIO_PER_FACE = 0, 1
 INV_DENSEST, INV_FIRST = 0, 1
 OUTCOMES = {CONVERGED: "converged", MAX_ITER: "max_iter", SMALL_STEP: "small_step", NONFINITE: "nonfinite"}

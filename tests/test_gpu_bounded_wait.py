@@ -1,0 +1,44 @@
+"""The bounded device-side waits of the row transforms (a bulk copy completing on an
+mbarrier). With OTM_OPT_WAIT_TEST the waits expect bytes that never arrive and give up
+after about 1 ms: the instance is flagged, the call returns OTM_ERR_TIMEOUT, and the
+context stays usable -- the next solve is identical to one that never saw the fault.
+No GPU fault, trap or hang is involved: the wait simply runs out."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def test_wait_runs_out_and_the_context_recovers():
+    from otmap_b200 import native as N
+    from otmap_b200 import otmap as ot
+    from otmap_b200 import workloads as W
+
+    ctx = N.Context(0)
+    n = 64
+    d = W.to_cells(W.gaussian_mixture(n, 5))
+    s = ot.GridBasedTransportSolver(ctx)
+    s.set_verbose_level(0)
+    s.init(n)
+    good = s.solve(d)
+
+    N.check(N.lib().otm_set_option(ctx.handle, N.OPT_WAIT_TEST, 1))
+    for loop in (N.LOOP_GRAPH, N.LOOP_HOST):
+        ctx.set_loop(loop)
+        with pytest.raises(N.OtmError) as e:
+            s.solve(d)
+        assert e.value.code == N.ERR_TIMEOUT
+    batch = [W.gaussian_mixture(k, 9) for k in (64, 128)]
+    with pytest.raises(N.OtmError) as e:
+        ot.solve_batch(batch, context=ctx)
+    assert e.value.code == N.ERR_TIMEOUT
+
+    ctx.set_loop(N.LOOP_GRAPH)
+    N.check(N.lib().otm_set_option(ctx.handle, N.OPT_WAIT_TEST, 0))
+    again = s.solve(d)
+    assert again.stats.iterations == good.stats.iterations
+    assert np.array_equal(again.fwd_mesh(), good.fwd_mesh())
+    maps = ot.solve_batch(batch, context=ctx)
+    assert all(m.stats.outcome == N.CONVERGED for m in maps)
+    ctx.close()
