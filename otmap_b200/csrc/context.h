@@ -116,6 +116,7 @@ struct otm_context {
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   otm::Workspace ws;
   otm::DevBuf staging;  // device staging for host inputs/outputs
+  otm::DevBuf raster_scratch;  // rasterizer face boxes, pixel owners, vertex values (grow-only)
   // adjoint workspaces per grid size (adjoint.cu); type-erased to keep this header small
   struct Erased {
     virtual ~Erased() = default;

@@ -1,11 +1,11 @@
 // Point location in the forward mesh (TransportMap inversion) and rasterization of
 // the deformed grid mesh or of any triangle/quad mesh, for sm_100a.
 //
-// Both run on a uniform bin grid built on the GPU: faces are binned by their
-// bounding boxes (count, exclusive scan, scatter) and each query -- a point to
-// invert, or a pixel centre to shade -- tests only the faces of its bin. The query
-// kernels are atomics-free gathers; the only atomics are the integer bin counters
-// of the build. This file is compiled without FMA contraction: the geometric
+// Inversion runs on a uniform bin grid built on the GPU: faces are binned by their
+// bounding boxes (count, exclusive scan, scatter) and each query point tests only the
+// faces of its bin. Rasterization is face-parallel: each face tests the pixel centres
+// of its box and keeps the highest accepting face index per pixel with an integer
+// atomicMax; a per-pixel pass then writes the values. This file is compiled without FMA contraction: the geometric
 // predicates (utils/mesh_utils.cpp:18-88) then round exactly as the reference's
 // scalar x86-64 build does, which makes the located faces, weights, inverse
 // positions and pixel values bit-identical to the reference wherever the
@@ -307,8 +307,6 @@ __global__ void k_inverse(const double* xy, const double* density, int n, int B,
 
 // ---- rasterization (utils/rasterizer.cpp:36-58, 86-185, 188-302) ----
 
-constexpr int RT = 16;  // pixel tile edge for face binning
-
 // A mesh to rasterize: the quads of the (n+1)^2 grid (start == nullptr), or an indexed
 // face set of triangles and quads whose face f lists vertices idx[start[f] .. start[f+1])
 // in the order the reference's face circulator visits them.
@@ -395,27 +393,10 @@ __device__ __forceinline__ FaceRaster face_raster(const MeshRef& m, const double
   return r;
 }
 
-__global__ void k_raster_count(MeshRef m, const double* density, float scale, int rows, int cols, int TX,
-                               FaceRaster* fr, int* counts) {
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void k_face_boxes(MeshRef m, const double* density, float scale, int rows, int cols, FaceRaster* fr) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= m.nf) return;
-  FaceRaster r = face_raster(m, density, scale, rows, cols, f);
-  fr[f] = r;
-  if (r.x0 >= r.x1 || r.y0 >= r.y1) return;
-  for (int ty = r.y0 / RT; ty <= (r.y1 - 1) / RT; ++ty)
-    for (int tx = r.x0 / RT; tx <= (r.x1 - 1) / RT; ++tx) atomicAdd(&counts[ty * TX + tx], 1);
-}
-
-__global__ void k_raster_fill(const FaceRaster* fr, int nf, int TX, const int* starts, int* cursor, int* faces) {
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nf) return;
-  FaceRaster r = fr[f];
-  if (r.x0 >= r.x1 || r.y0 >= r.y1) return;
-  for (int ty = r.y0 / RT; ty <= (r.y1 - 1) / RT; ++ty)
-    for (int tx = r.x0 / RT; tx <= (r.x1 - 1) / RT; ++tx) {
-      int b = ty * TX + tx;
-      faces[starts[b] + atomicAdd(&cursor[b], 1)] = f;
-    }
+  fr[f] = face_raster(m, density, scale, rows, cols, f);
 }
 
 // Weights the reference's sequential loop would test at (f, x, y) when its bilinear
@@ -462,51 +443,69 @@ __device__ void stale_weights(const MeshRef& m, int rows, int cols, const FaceRa
   w[0] = w[1] = w[2] = w[3] = 0.0;
 }
 
-// One thread per pixel: the highest-index face whose test accepts the pixel centre
-// wins (the reference's sequential loop overwrites in face order). PerFace writes the
-// face value; PerVertex (vval != nullptr) writes the float interpolation of
-// rasterize_face's loop, which scales vertex 0's value by each weight
-// (rasterizer.cpp:123-130, 174-181) and sums in float.
-__global__ void k_raster(MeshRef m, int rows, int cols, int TX, const FaceRaster* fr, const int* starts,
-                         const int* faces, const float* vval, double* img) {
-  int x = blockIdx.x * blockDim.x + threadIdx.x;
-  int y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= cols || y >= rows) return;
-  int b = (y / RT) * TX + (x / RT);
-  double qx = ((double)x + 0.5) / (double)cols, qy = ((double)y + 0.5) / (double)rows;
-  int best = -1, bc = 0, bv0 = 0;
-  double bw[4] = {0, 0, 0, 0};
-  for (int k = starts[b]; k < starts[b + 1]; ++k) {
-    int f = faces[k];
-    if (f <= best) continue;
-    FaceRaster r = fr[f];
-    if (x < r.x0 || x >= r.x1 || y < r.y0 || y >= r.y1) continue;
-    Quad p;
-    int vid[4];
-    const int c = load_face(m, f, p, vid);
-    double w[4];
-    if (c == 3) {
-      tri_weights(qx, qy, p, w);
-    } else if (!bilinear_weights(qx, qy, p, w)) {
-      stale_weights(m, rows, cols, fr, f, x, y, w);
-    }
-    if (weights_inside(w)) {
-      best = f;
-      bc = c;
-      bv0 = vid[0];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) bw[q] = w[q];
+// Weights of face f at the centre of pixel (x, y) as the reference's loop forms them
+// (triangles: the barycentric transform; quads: bilinear coordinates, or the stale
+// weights where that solve fails). Returns the face's valence; vid gets its corners.
+__device__ __forceinline__ int pixel_weights(const MeshRef& m, int rows, int cols, const FaceRaster* fr, int f,
+                                             int x, int y, double w[4], int vid[4]) {
+  Quad p;
+  const int c = load_face(m, f, p, vid);
+  const double qx = ((double)x + 0.5) / (double)cols, qy = ((double)y + 0.5) / (double)rows;
+  if (c == 3) {
+    tri_weights(qx, qy, p, w);
+  } else if (!bilinear_weights(qx, qy, p, w)) {
+    stale_weights(m, rows, cols, fr, f, x, y, w);
+  }
+  return c;
+}
+
+// One thread per face: every pixel centre of its box that the face accepts records the
+// face index with atomicMax, so each pixel ends with the highest accepting index -- the
+// face the reference's sequential loop writes last (rasterizer.cpp:162-236).
+__global__ void k_raster_owner(MeshRef m, int rows, int cols, const FaceRaster* fr, int* owner) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  const FaceRaster r = fr[f];
+  if (r.x0 >= r.x1 || r.y0 >= r.y1) return;
+  Quad p;
+  int vid[4];
+  const int c = load_face(m, f, p, vid);
+  for (int y = r.y0; y < r.y1; ++y) {
+    const double qy = ((double)y + 0.5) / (double)rows;
+    for (int x = r.x0; x < r.x1; ++x) {
+      const double qx = ((double)x + 0.5) / (double)cols;
+      double w[4];
+      if (c == 3) {
+        tri_weights(qx, qy, p, w);
+      } else if (!bilinear_weights(qx, qy, p, w)) {
+        stale_weights(m, rows, cols, fr, f, x, y, w);
+      }
+      if (weights_inside(w)) atomicMax(&owner[(size_t)y * cols + x], f);
     }
   }
+}
+
+// One thread per pixel: the owner's PerFace value, or for PerVertex (vval != nullptr)
+// the float interpolation of rasterize_face's loop, which scales vertex 0's value by
+// each weight (rasterizer.cpp:123-130, 174-181) and sums in float.
+__global__ void k_raster_resolve(MeshRef m, int rows, int cols, const FaceRaster* fr, const int* owner,
+                                 const float* vval, double* img) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= cols || y >= rows) return;
+  const int f = owner[(size_t)y * cols + x];
   double out = 0.0;
-  if (best >= 0) {
+  if (f >= 0) {
     if (vval) {
-      const float v0 = vval[bv0];
+      double w[4];
+      int vid[4];
+      const int c = pixel_weights(m, rows, cols, fr, f, x, y, w, vid);
+      const float v0 = vval[vid[0]];
       float acc = 0.0f;
-      for (int q = 0; q < bc; ++q) acc = acc + v0 * (float)bw[q];
+      for (int q = 0; q < c; ++q) acc = acc + v0 * (float)w[q];
       out = (double)acc;
     } else {
-      out = fr[best].value;
+      out = fr[f].value;
     }
   }
   img[(size_t)y * cols + x] = out;
@@ -762,34 +761,28 @@ static void raster_mesh(otm_context* ctx, const MeshRef& m, const double* densit
                         int mode, double* img) {
   cudaStream_t st = ctx->stream;
   const int nf = m.nf;
-  const int TX = (cols + RT - 1) / RT, TY = (rows + RT - 1) / RT, nb = TX * TY;
-  DevBuf fr, counts, starts, sums, faces, vval;
-  fr.reserve(sizeof(FaceRaster) * (size_t)(nf > 0 ? nf : 1));
-  counts.reserve(sizeof(int) * nb);
-  starts.reserve(sizeof(int) * (nb + 1));
-  sums.reserve(sizeof(int) * ((nb + SCAN_B - 1) / SCAN_B + 1));
-  OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
+  const size_t pix = (size_t)rows * cols;
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_fr = al(sizeof(FaceRaster) * (size_t)(nf > 0 ? nf : 1)), b_own = al(sizeof(int) * pix);
+  const size_t b_vv = al(sizeof(float) * (size_t)(m.nv > 0 ? m.nv : 1));
+  ctx->raster_scratch.reserve(b_fr + b_own + b_vv);  // grows, kept for the next call
+  char* base = ctx->raster_scratch.as<char>();
+  FaceRaster* fr = reinterpret_cast<FaceRaster*>(base);
+  int* owner = reinterpret_cast<int*>(base + b_fr);
+  float* vval = reinterpret_cast<float*>(base + b_fr + b_own);
+  OTM_CUDA(cudaMemsetAsync(owner, 0xff, sizeof(int) * pix, st));  // -1: no face
   // rasterizer.cpp:193 keeps 1/density.size() in a float
   const float scale = (float)(1. / (double)(density ? cells : nf));
   const int fblocks = nf > 0 ? (nf + 255) / 256 : 1;
-  launch(ctx, "raster_count", k_raster_count, fblocks, 256, m, density, scale, rows, cols, TX, fr.as<FaceRaster>(),
-         counts.as<int>());
-  exclusive_scan(st, counts.as<int>(), starts.as<int>(), sums.as<int>(), nb);
-  int total = 0;
-  OTM_CUDA(cudaMemcpyAsync(&total, starts.as<int>() + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
-  OTM_CUDA(cudaStreamSynchronize(st));
-  faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1));
-  OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
-  launch(ctx, "raster_fill", k_raster_fill, fblocks, 256, (const FaceRaster*)fr.as<FaceRaster>(), nf, TX,
-         (const int*)starts.as<int>(), counts.as<int>(), faces.as<int>());
+  launch(ctx, "face_boxes", k_face_boxes, fblocks, 256, m, density, scale, rows, cols, fr);
+  launch(ctx, "raster_owner", k_raster_owner, fblocks, 256, m, rows, cols, (const FaceRaster*)fr, owner);
   const float* pv = nullptr;
+  DevBuf vcount, vstart, vsums, vfaces, inv_area;  // indexed PerVertex temporaries
   if (mode == OTM_RIO_PER_VERTEX) {
-    vval.reserve(sizeof(float) * (size_t)(m.nv > 0 ? m.nv : 1));
     const unsigned vb = (unsigned)((m.nv + 255) / 256);
     if (!m.start) {
-      launch(ctx, "vertex_values", k_vertex_values_grid, vb, 256, m.xy, m.n, scale, vval.as<float>());
+      launch(ctx, "vertex_values", k_vertex_values_grid, vb, 256, m.xy, m.n, scale, vval);
     } else {
-      DevBuf vcount, vstart, vsums, vfaces, inv_area;
       int nref = 0;
       OTM_CUDA(cudaMemcpyAsync(&nref, m.start + nf, sizeof(int), cudaMemcpyDeviceToHost, st));
       vcount.reserve(sizeof(int) * m.nv);
@@ -805,16 +798,15 @@ static void raster_mesh(otm_context* ctx, const MeshRef& m, const double* densit
       launch(ctx, "vf_fill", k_vf_fill, fblocks, 256, m, (const int*)vstart.as<int>(), vcount.as<int>(),
              vfaces.as<int>(), inv_area.as<double>());
       launch(ctx, "vertex_values", k_vertex_values_mesh, vb, 256, m.nv, (const int*)vstart.as<int>(),
-             vfaces.as<int>(), (const double*)inv_area.as<double>(), scale, vval.as<float>());
-      OTM_CUDA(cudaStreamSynchronize(st));  // the temporaries above are freed on return
+             vfaces.as<int>(), (const double*)inv_area.as<double>(), scale, vval);
     }
-    pv = vval.as<float>();
+    pv = vval;
   }
   dim3 blk(32, 8), grd((cols + 31) / 32, (rows + 7) / 8);
-  launch(ctx, "raster", k_raster, grd, blk, m, rows, cols, TX, (const FaceRaster*)fr.as<FaceRaster>(),
-         (const int*)starts.as<int>(), (const int*)faces.as<int>(), pv, img);
+  launch(ctx, "raster_resolve", k_raster_resolve, grd, blk, m, rows, cols, (const FaceRaster*)fr,
+         (const int*)owner, pv, img);
   OTM_CUDA(cudaGetLastError());
-  OTM_CUDA(cudaStreamSynchronize(st));  // fr, faces, vval are freed on return
+  if (m.start && mode == OTM_RIO_PER_VERTEX) OTM_CUDA(cudaStreamSynchronize(st));  // temporaries freed on return
 }
 
 void raster_grid(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols, int mode,
