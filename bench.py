@@ -66,6 +66,30 @@ def dist_env():
     return rank, world, local
 
 
+def rank_first_seed(rank):
+    """Each rank solves its own densities (seeds 1000*rank + k): the batch shards across
+    ranks with no collective on the data path."""
+    return 1000 * rank
+
+
+def max_over_ranks(value, world, device="cuda"):
+    """The slowest rank's time: every rank calls it with its own value (a collective with
+    the same steps on every rank); the identity for one rank."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(instances_per_rank, world, ms_per_step):
+    """Whole-job throughput: the instances of all ranks over the slowest rank's step time."""
+    return instances_per_rank * world / (ms_per_step / 1e3)
+
+
 def densities(n, count, first_seed):
     from otmap_b200 import workloads as W
 
@@ -214,7 +238,7 @@ def run_ours(args):
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
     n, B = args.n, args.batch
     ns = [n] * B
-    host = densities(n, B, 1000 * rank)
+    host = densities(n, B, rank_first_seed(rank))
     dev_in = [torch.from_numpy(d).cuda() for d in host]
     V = (n + 1) ** 2
     dev_out = [torch.empty((V, 2), dtype=torch.float64, device="cuda") for _ in range(B)]
@@ -274,14 +298,9 @@ def run_ours(args):
     # a second pass over the same steps, used only for the kernel breakdown and roofline
     _, _, prof = timed(dev_in, dev_out, args.steps, profile=True)
 
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([t_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
+    t_ms = max_over_ranks(t_ms, world)
     ms_step = t_ms / args.steps
-    value = B * world / (ms_step / 1e3)
+    value = job_value(B, world, ms_step)
     st_list = [stats[k] for k in range(B)]
     iters = [s.iterations for s in st_list]
     resid = [s.residual for s in st_list]
@@ -291,13 +310,8 @@ def run_ours(args):
         h_in = [torch.from_numpy(d).pin_memory() for d in host]
         h_out = [torch.empty((V, 2), dtype=torch.float64).pin_memory() for _ in range(B)]
         e_ms, _, _ = timed(h_in, h_out, args.steps)
-        if world > 1:
-            import torch.distributed as dist
-
-            t = torch.tensor([e_ms], dtype=torch.float64, device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-        e2e = {"value": B * world / (e_ms / args.steps / 1e3), "unit": UNIT,
+        e_ms = max_over_ranks(e_ms, world)
+        e2e = {"value": job_value(B, world, e_ms / args.steps), "unit": UNIT,
                "h2d_bytes_per_step": B * n * n * 8, "d2h_bytes_per_step": B * V * 2 * 8}
 
     plain = None
