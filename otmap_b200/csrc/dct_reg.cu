@@ -141,7 +141,12 @@ __host__ __device__ constexpr int partner_reg(int r, bool lane0) {
   return rbrev<N2>(k2p);  // rbrev is its own inverse
 }
 
-__device__ __forceinline__ double dct_s(int k, int n) { return k == 0 ? sqrt(1.0 / n) : sqrt(2.0 / n); }
+// Orthonormal DCT scale s_k = sqrt(1/n) (k = 0) or sqrt(2/n), the two roots formed once per thread.
+struct DctScale {
+  double s0, s1;
+  __device__ __forceinline__ explicit DctScale(int n) : s0(sqrt(1.0 / n)), s1(sqrt(2.0 / n)) {}
+  __device__ __forceinline__ double operator()(int k) const { return k == 0 ? s0 : s1; }
+};
 __device__ __forceinline__ int makhoul_src(int m, int n) { return m < (n >> 1) ? 2 * m : 2 * (n - 1 - m) + 1; }
 // DCT-II coefficient from V_k: s_k Re(e^{-i pi k / 2n} V_k)
 __device__ __forceinline__ double post2(double2 V, double2 pt, double sk) { return sk * fma(V.x, pt.x, V.y * pt.y); }
@@ -230,6 +235,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
                                                               int items, unsigned extra, long long limit) {
   using G = RowGeom<N1, N2>;
   constexpr int n = G::n, LPW = G::LPW;
+  const DctScale ds(n);
   extern __shared__ __align__(16) double sbuf[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
   double* data = sbuf + warp * G::WARP;
@@ -299,7 +305,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
         const double2 A = make_double2(0.5 * (Z.x + px), 0.5 * (Z.y - py));
         const double2 B = make_double2(0.5 * (Z.y + py), 0.5 * (px - Z.x));
         const double2 w = __ldg(&pt[k]);
-        const double sk = dct_s(k, n);
+        const double sk = ds(k);
         ya[k] = post2(A, w, sk);
         yb[k] = post2(B, w, sk);
       }
@@ -315,6 +321,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const 
                                                               int items, unsigned extra, long long limit) {
   using G = RowGeom<N1, N2>;
   constexpr int n = G::n, LPW = G::LPW;
+  const DctScale ds(n);
   extern __shared__ __align__(16) double sbuf[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
   double* data = sbuf + warp * G::WARP;
@@ -357,7 +364,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const 
     for (int m1 = 0; m1 < N1; ++m1) {
       const int k = N2 * m1 + t;
       const double2 w = __ldg(&pt[k]);
-      const double sk = dct_s(k, n), snk = k == 0 ? 0.0 : dct_s(n - k, n);
+      const double sk = ds(k), snk = k == 0 ? 0.0 : ds(n - k);
       const double2 Wa = pre3(k, sk * Xa[k], k == 0 ? 0.0 : snk * Xa[n - k], w);
       const double2 Wb = pre3(k, sk * Xb[k], k == 0 ? 0.0 : snk * Xb[n - k], w);
       v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
@@ -438,6 +445,7 @@ template <int N1, int N2>
 __global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const int* col_inst, int seg) {
   using GG = ColGeom<N1, N2>;
   constexpr int n = GG::n, CP = GG::CP, CB = GG::CB;
+  const DctScale ds(n);
   extern __shared__ double sbuf[];
   double2* tile = reinterpret_cast<double2*>(sbuf);  // [k][c]: one column pair per entry
   const int item = seg + blockIdx.x;
@@ -472,7 +480,7 @@ __global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const in
       const double2 A = make_double2(0.5 * (Z.x + P.x), 0.5 * (Z.y - P.y));
       const double2 B = make_double2(0.5 * (Z.y + P.y), 0.5 * (P.x - Z.x));
       const double2 w = __ldg(&pt[k]);
-      const double sk = dct_s(k, n);
+      const double sk = ds(k);
       const double Xa = post2(A, w, sk), Xb = post2(B, w, sk);
       const double lam_a = 2.0 - 2.0 * I.cosk[k] * cla, lam_b = 2.0 - 2.0 * I.cosk[k] * clb;
       const double Ua = (k == 0 && la == 0) ? 0.0 : Xa / lam_a;
