@@ -37,7 +37,8 @@ struct Inst {
   int strip0, nstrip;          // first block and block count in the strip work list
   // loop state
   int it, active, outcome, use_beta;
-  unsigned int counter, pad1;
+  unsigned int counter;
+  int srows;  // strip height of the sweeps for this batch (32 or 64 rows)
   double residual, residual0, alpha, beta, linf, dnorm;
   double dens_scale, dens_beta;
 };
@@ -140,7 +141,7 @@ void dct_reg_attrs(int device);
 void poisson_fft_attrs(int device);
 
 // Two-pass stencil sweep of an iteration (stencil.cu).
-int strip_blocks(int n);
+int strip_blocks(int n, int srows);
 void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);
 void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);
 constexpr int SWEEP_SLOTS = 32;  // partial-sum slots per sweep block

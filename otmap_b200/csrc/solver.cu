@@ -540,6 +540,15 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
   std::vector<Inst> h(count);
   size_t cells = 0;
   int tiles = 0, gemm = 0, rows = 0, cols = 0, strips = 0;
+  // Taller sweep strips halve the per-strip overhead (ring prologue, block reduction) when
+  // the batch has blocks to spare; a batch that does not fill the GPU twice over keeps
+  // 32-row strips for parallelism.
+  int srows = 32;
+  {
+    long blocks32 = 0;
+    for (int q = 0; q < count; ++q) blocks32 += strip_blocks(sizes[q], 32);
+    if (blocks32 >= 6L * ctx->num_sms) srows = 64;
+  }
   for (int q = 0; q < count; ++q) {
     int n = sizes[q];
     Inst& I = h[q];
@@ -549,7 +558,8 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.ntiles = tiles_of(n);
     tiles += I.ntiles;
     I.strip0 = strips;
-    I.nstrip = strip_blocks(n);
+    I.srows = srows;
+    I.nstrip = strip_blocks(n, srows);
     strips += I.nstrip;
     I.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
     if (I.fft) {

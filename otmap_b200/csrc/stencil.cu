@@ -14,7 +14,7 @@
 //                  block advances the iteration and tests the loop condition (:160).
 //
 // Geometry: one warp owns a strip of 32 consecutive columns (j, contiguous in memory)
-// and SR rows and walks down it. Grid rows are prefetched asynchronously (cp.async)
+// and Inst::srows rows (32, or 64 when the batch has strips to spare) and walks down it. Grid rows are prefetched asynchronously (cp.async)
 // into a per-warp ring of RD rows in shared memory, so RD-2 rows per warp are in
 // flight while it computes; the previous vertex-gradient row is kept in registers. The
 // strip's two halo columns are staged with the row; neighbours come from the ring. A
@@ -26,7 +26,7 @@
 namespace otm {
 
 constexpr int SW = 32;        // strip width (one warp)
-constexpr int SR = 32;        // strip height (rows per warp)
+// strip height (rows per warp): Inst::srows, 32 or 64 per batch (layout_workspace)
 constexpr int SWARPS = 4;     // strips per block
 constexpr int ST = SW * SWARPS;
 constexpr int KA = SWEEP_SLOTS;  // partial-sum slots per block
@@ -182,7 +182,7 @@ __device__ __forceinline__ StripCoord strip_coord(const Inst& I, int block) {
   const int n = I.n;
   const int cols = (n + SW - 1) / SW;
   const int strip = (block - I.strip0) * SWARPS + s.warp;
-  s.i0 = (strip / cols) * SR;
+  s.i0 = (strip / cols) * I.srows;
   s.j0 = (strip % cols) * SW;
   return s;
 }
@@ -241,7 +241,7 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
     R.n = n;
     R.j0 = sc.j0;
     R.lane = sc.lane;
-    const int last = min(sc.i0 + SR, n);  // cell rows i0 .. last-1; grid rows i0-1 .. last
+    const int last = min(sc.i0 + I.srows, n);  // cell rows i0 .. last-1; grid rows i0-1 .. last
     R.rows_end = last;
     R.setup();
 #pragma unroll
@@ -378,7 +378,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
     R.n = n;
     R.j0 = sc.j0;
     R.lane = sc.lane;
-    const int last = min(sc.i0 + SR, n);
+    const int last = min(sc.i0 + I.srows, n);
     R.rows_end = last;
     R.setup();
 #pragma unroll
@@ -445,8 +445,8 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
   }
 }
 
-int strip_blocks(int n) {
-  const int strips = ((n + SR - 1) / SR) * ((n + SW - 1) / SW);
+int strip_blocks(int n, int srows) {
+  const int strips = ((n + srows - 1) / srows) * ((n + SW - 1) / SW);
   return (strips + SWARPS - 1) / SWARPS;
 }
 
