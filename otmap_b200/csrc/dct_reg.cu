@@ -52,17 +52,11 @@ __host__ __device__ constexpr int rbrev(int r) {
   return out;
 }
 
-// W_n^e with tw[k] = exp(-2 pi i k / n), k < n/2; conj for the inverse kernel.
-__device__ __forceinline__ double2 twid(const double2* __restrict__ tw, int e, int n, bool conj) {
-  e &= n - 1;
-  double2 w;
-  if (e < (n >> 1)) {
-    w = __ldg(&tw[e]);
-  } else {
-    w = __ldg(&tw[e - (n >> 1)]);
-    w.x = -w.x;
-    w.y = -w.y;
-  }
+// Step-2 twiddle of register r on lane t, W_n^(t * rbrev<N1>(r)), from the per-size table
+// tw2[r * N2 + t] (laid out so that a warp's 32 lanes read consecutive entries: one
+// coalesced request per register instead of a gather); conj for the inverse kernel.
+__device__ __forceinline__ double2 twid2(const double2* __restrict__ tw2, int idx, bool conj) {
+  double2 w = __ldg(&tw2[idx]);
   if (conj) w.y = -w.y;
   return w;
 }
@@ -108,7 +102,7 @@ __device__ __forceinline__ void fft_line(int t, double* buf, const double2* __re
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
     const int k1 = rbrev<N1>(r);
-    if (k1 != 0) v[r] = cmul(v[r], twid(tw, t * k1, n, conj));
+    if (k1 != 0) v[r] = cmul(v[r], twid2(tw + (n >> 1), r * N2 + t, conj));
   }
   // transpose through shared memory, real parts then imaginary parts
 #pragma unroll
@@ -419,7 +413,7 @@ __device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
     const int k1 = rbrev<N1>(r);
-    if (k1 != 0) v[r] = cmul(v[r], twid(tw, s * k1, n, conj));
+    if (k1 != 0) v[r] = cmul(v[r], twid2(tw + (n >> 1), r * N2 + s, conj));
   }
 #pragma unroll
   for (int part = 0; part < 2; ++part) {
@@ -553,6 +547,33 @@ int RegDct<N1, N2>::rows_blocks_per_sm = 1;
 }  // namespace
 
 bool dct_reg_supported(int n) { return n == 64 || n == 128 || n == 256 || n == 512 || n == 1024; }
+
+namespace {
+template <int N1, int N2>
+void step2_table(const std::vector<double2>& tw, std::vector<double2>& out) {
+  constexpr int n = N1 * N2;
+  out.resize(n);
+  for (int r = 0; r < N1; ++r)
+    for (int t = 0; t < N2; ++t) {
+      // the entry of the half table tw (k < n/2), negated in the upper half: the same
+      // value the transform would form from tw itself
+      const int e = (t * rbrev<N1>(r)) & (n - 1);
+      double2 w = e < n / 2 ? tw[e] : make_double2(-tw[e - n / 2].x, -tw[e - n / 2].y);
+      out[(size_t)r * N2 + t] = w;
+    }
+}
+}  // namespace
+
+void dct_reg_step2_table(int n, const std::vector<double2>& tw, std::vector<double2>& out) {
+  switch (n) {
+    case 64: step2_table<8, 8>(tw, out); break;
+    case 128: step2_table<8, 16>(tw, out); break;
+    case 256: step2_table<16, 16>(tw, out); break;
+    case 512: step2_table<16, 32>(tw, out); break;
+    case 1024: step2_table<32, 32>(tw, out); break;
+    default: out.clear();
+  }
+}
 
 int dct_reg_lines_per_block(int n) {  // rows per row-pass work item: two per FFT line of a warp
   switch (n) {

@@ -30,7 +30,7 @@ struct Inst {
   double* t2;
   const double* C;
   const double* cosk;
-  const double2* tw;  // exp(-2 pi i k / n), k < n/2 (fast transform)
+  const double2* tw;  // exp(-2 pi i k / n), k < n/2 (fast transform); then the step-2 table
   const double2* pt;  // (cos, sin)(pi k / (2n)), k < n (fast transform)
   int fft, logn;      // fast transform used (n a power of two) / log2 n
   int row0, nrow, col0, ncol;  // first item and item count in the row / column work lists
@@ -130,6 +130,9 @@ void poisson_fft(otm_context* ctx, Inst* d_insts, const int* row_inst, int roff,
                  const int* col_inst, int coff, int ncol_items);
 // Register-resident variant for n in {64, ..., 1024} (dct_reg.cu).
 bool dct_reg_supported(int n);
+// The register transforms' step-2 twiddles W_n^(t k1) in [register][lane] order (n entries),
+// appended to the half table tw of the size.
+void dct_reg_step2_table(int n, const std::vector<double2>& tw, std::vector<double2>& out);
 int dct_reg_lines_per_block(int n);
 int dct_reg_cols_per_block(int n);
 void dct_reg_run(otm_context* ctx, int n, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,

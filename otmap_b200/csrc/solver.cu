@@ -850,9 +850,12 @@ static SizeTables* init_size(otm_context* ctx, int n) {
     std::vector<double2> tw(n / 2), pt(n);
     for (int k = 0; k < n / 2; ++k) tw[k] = make_double2(std::cos(2.0 * M_PI * k / n), -std::sin(2.0 * M_PI * k / n));
     for (int k = 0; k < n; ++k) pt[k] = make_double2(std::cos(M_PI * k / (2.0 * n)), std::sin(M_PI * k / (2.0 * n)));
-    T->tw.reserve(sizeof(double2) * (n / 2));
+    std::vector<double2> tw2;
+    dct_reg_step2_table(n, tw, tw2);
+    tw.insert(tw.end(), tw2.begin(), tw2.end());
+    T->tw.reserve(sizeof(double2) * tw.size());
     T->pt.reserve(sizeof(double2) * n);
-    OTM_CUDA(cudaMemcpyAsync(T->tw.p, tw.data(), sizeof(double2) * (n / 2), cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(T->tw.p, tw.data(), sizeof(double2) * tw.size(), cudaMemcpyHostToDevice, st));
     OTM_CUDA(cudaMemcpyAsync(T->pt.p, pt.data(), sizeof(double2) * n, cudaMemcpyHostToDevice, st));
     OTM_CUDA(cudaStreamSynchronize(st));
   }
