@@ -28,7 +28,7 @@
 namespace otm {
 namespace {
 
-constexpr int RW = 4;  // warps per block
+constexpr int RW = 8;  // warps per block of the row passes (one block per SM at n = 1024)
 
 // exp(-2 pi i k / 1024), k < 512, in constant memory. A radix-2 stage of an N-point
 // sub-FFT needs W_N^e = entry e * (1024 / N), an index known at compile time, so the
@@ -54,8 +54,14 @@ __host__ __device__ constexpr int rbrev(int r) {
 
 // Step-2 twiddle of register r on lane t, W_n^(t * rbrev<N1>(r)), from the per-size table
 // tw2[r * N2 + t] (laid out so that a warp's 32 lanes read consecutive entries: one
-// coalesced request per register instead of a gather); conj for the inverse kernel.
-__device__ __forceinline__ double2 twid2(const double2* __restrict__ tw2, int idx, bool conj) {
+// conflict-free shared-memory or coalesced global request per register instead of a
+// gather); conj for the inverse kernel.
+__device__ __forceinline__ double2 twid2(const double2* tw2, int idx, bool conj) {
+  double2 w = tw2[idx];
+  if (conj) w.y = -w.y;
+  return w;
+}
+__device__ __forceinline__ double2 twid2_global(const double2* __restrict__ tw2, int idx, bool conj) {
   double2 w = __ldg(&tw2[idx]);
   if (conj) w.y = -w.y;
   return w;
@@ -95,14 +101,14 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[N], const double2* __restri
 // buf is this line's N1 x (N2 + 1) shared buffer of doubles (the transpose moves real and
 // imaginary parts in two rounds).
 template <int N1, int N2>
-__device__ __forceinline__ void fft_line(int t, double* buf, const double2* __restrict__ tw, bool conj,
-                                         double2 (&v)[N1], double2 (&u)[N2]) {
+__device__ __forceinline__ void fft_line(int t, double* buf, const double2* tw2, bool conj, double2 (&v)[N1],
+                                         double2 (&u)[N2]) {
   constexpr int n = N1 * N2;
-  fft_reg<N1>(v, tw, n, conj);
+  fft_reg<N1>(v, nullptr, n, conj);
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
     const int k1 = rbrev<N1>(r);
-    if (k1 != 0) v[r] = cmul(v[r], twid2(tw + (n >> 1), r * N2 + t, conj));
+    if (k1 != 0) v[r] = cmul(v[r], twid2(tw2, r * N2 + t, conj));
   }
   // transpose through shared memory, real parts then imaginary parts
 #pragma unroll
@@ -122,7 +128,7 @@ __device__ __forceinline__ void fft_line(int t, double* buf, const double2* __re
     }
     __syncwarp();
   }
-  if (t < N1) fft_reg<N2>(u, tw, n, conj);
+  if (t < N1) fft_reg<N2>(u, nullptr, n, conj);
 }
 
 // Register index holding X_{n-k} on the partner lane, for the X_k held in u[r]:
@@ -168,8 +174,25 @@ struct RowGeom {
   static constexpr int DATA = 2 * LPW * n;           // doubles: the item's rows
   static constexpr int TRANS = LPW * N1 * (N2 + 1);  // doubles: step-3 transpose buffers
   static constexpr int WARP = DATA + TRANS;          // doubles per warp (even: 16-byte aligned)
-  static constexpr size_t SMEM = sizeof(double) * RW * WARP + 16 * RW;  // + one mbarrier per warp
+  static constexpr int TABLES = 2 * n;               // double2: the step-2 twiddles, then pt
+  static constexpr size_t SMEM = sizeof(double) * RW * WARP + sizeof(double2) * TABLES + 16 * RW;  // + mbarriers
 };
+
+// The block's copy of the size's step-2 twiddles (n entries) and post-twiddles pt (n entries),
+// read by every item of the persistent kernel: shared-memory latency instead of L1's.
+template <int N1, int N2>
+__device__ __forceinline__ double2* load_row_tables(double* sbuf, const Inst& I) {
+  using G = RowGeom<N1, N2>;
+  constexpr int n = G::n;
+  double2* tab = reinterpret_cast<double2*>(sbuf + RW * G::WARP);
+  const double2* tw2 = I.tw + (n >> 1);
+  for (int e = threadIdx.x; e < n; e += blockDim.x) {
+    tab[e] = __ldg(&tw2[e]);
+    tab[n + e] = __ldg(&I.pt[e]);
+  }
+  __syncthreads();
+  return tab;
+}
 
 constexpr long long kWaitCycles = 2000000000LL;   // ~1 s at the B200's clock
 constexpr long long kTestWaitCycles = 2000000LL;  // ~1 ms (OTM_OPT_WAIT_TEST)
@@ -225,7 +248,7 @@ __device__ __forceinline__ void wait_fault(Inst& I, unsigned long long* bar, uns
 
 // Forward DCT-II of rows 2p and 2p+1 of r_k (one complex FFT per row pair) -> T.
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const int* row_inst, int seg,
+__global__ __launch_bounds__(RW * 32, 1) void k_dct_rows_fwd(Inst* insts, const int* row_inst, int seg,
                                                               int items, unsigned extra, long long limit) {
   using G = RowGeom<N1, N2>;
   constexpr int n = G::n, LPW = G::LPW;
@@ -234,7 +257,10 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
   double* data = sbuf + warp * G::WARP;
   double* buf = data + G::DATA + sub * N1 * (N2 + 1);
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sbuf + RW * G::WARP) + 2 * warp;
+  if (items <= 0) return;
+  const double2* tab = load_row_tables<N1, N2>(sbuf, insts[row_inst[seg]]);
+  const double2* spt = tab + n;
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sbuf + RW * G::WARP + 2 * G::TABLES) + warp;
   const int stride = gridDim.x * RW;
   if (lane == 0) mbar_init(bar);
   __syncwarp();
@@ -286,8 +312,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
     const int row = (seg + item - I.row0) * 2 * LPW + 2 * sub;
     double* ya = I.t1 + (size_t)row * n;
     double* yb = ya + n;
-    const double2* pt = I.pt;
-    fft_line<N1, N2>(t, buf, I.tw, false, v, u);
+    fft_line<N1, N2>(t, buf, tab, false, v, u);
 #pragma unroll
     for (int r = 0; r < N2; ++r) {
       const double2 send = (t == 0) ? u[partner_reg<N2>(r, true)] : u[partner_reg<N2>(r, false)];
@@ -298,7 +323,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
         const double2 Z = u[r];
         const double2 A = make_double2(0.5 * (Z.x + px), 0.5 * (Z.y - py));
         const double2 B = make_double2(0.5 * (Z.y + py), 0.5 * (px - Z.x));
-        const double2 w = __ldg(&pt[k]);
+        const double2 w = spt[k];
         const double sk = ds(k);
         ya[k] = post2(A, w, sk);
         yb[k] = post2(B, w, sk);
@@ -311,7 +336,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_fwd(Inst* insts, const 
 // Inverse DCT-III of rows 2p and 2p+1 of T -> d_hat: the inputs W^a + i W^b of the two
 // rows go through one inverse FFT; its real and imaginary parts are the two rows.
 template <int N1, int N2>
-__global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const int* row_inst, int seg,
+__global__ __launch_bounds__(RW * 32, 1) void k_dct_rows_inv(Inst* insts, const int* row_inst, int seg,
                                                               int items, unsigned extra, long long limit) {
   using G = RowGeom<N1, N2>;
   constexpr int n = G::n, LPW = G::LPW;
@@ -320,7 +345,10 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
   double* data = sbuf + warp * G::WARP;
   double* buf = data + G::DATA + sub * N1 * (N2 + 1);
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sbuf + RW * G::WARP) + 2 * warp;
+  if (items <= 0) return;
+  const double2* tab = load_row_tables<N1, N2>(sbuf, insts[row_inst[seg]]);
+  const double2* spt = tab + n;
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sbuf + RW * G::WARP + 2 * G::TABLES) + warp;
   const int stride = gridDim.x * RW;
   if (lane == 0) mbar_init(bar);
   __syncwarp();
@@ -351,13 +379,12 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const 
     phase ^= 1;
     const double* Xa = data + sub * 2 * n;
     const double* Xb = Xa + n;
-    const double2* pt = I.pt;
     double2 v[N1];
     double2 u[N2];
 #pragma unroll
     for (int m1 = 0; m1 < N1; ++m1) {
       const int k = N2 * m1 + t;
-      const double2 w = __ldg(&pt[k]);
+      const double2 w = spt[k];
       const double sk = ds(k), snk = k == 0 ? 0.0 : ds(n - k);
       const double2 Wa = pre3(k, sk * Xa[k], k == 0 ? 0.0 : snk * Xa[n - k], w);
       const double2 Wb = pre3(k, sk * Xb[k], k == 0 ? 0.0 : snk * Xb[n - k], w);
@@ -368,7 +395,7 @@ __global__ __launch_bounds__(RW * 32, 2) void k_dct_rows_inv(Inst* insts, const 
     const int row = (seg + item - I.row0) * 2 * LPW + 2 * sub;
     double* xa = I.dhat + (size_t)row * n;
     double* xb = xa + n;
-    fft_line<N1, N2>(t, buf, I.tw, true, v, u);
+    fft_line<N1, N2>(t, buf, tab, true, v, u);
     // Output m = t + N1 k2 goes to x[2m] for m < n/2; its neighbour x[2m+1] is output
     // n-1-m, held by lane N1-1-t in the register of k2' = N2-1-k2: one shuffle and a
     // 16-byte store per pair.
@@ -401,19 +428,20 @@ struct ColGeom {
   static constexpr int CP = 256 / N2;     // column pairs per block (256 threads)
   static constexpr int CB = 2 * CP;       // columns per block
   static constexpr int KS = N2 * CP + 1;  // padded stride of a k1 row of the transpose buffer
-  static constexpr int SMEM = (N1 * KS > n * CB ? N1 * KS : n * CB);  // doubles
+  static constexpr int WORK = (N1 * KS > n * CB ? N1 * KS : n * CB);  // doubles: transpose / tile
+  static constexpr int SMEM = WORK + 5 * n;  // + the tables: step-2 twiddles, pt (double2), cos(pi k / n)
 };
 
 template <int N1, int N2>
 __device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)[N2], double* sh, int c, int s,
-                                                  const double2* __restrict__ tw, bool conj) {
+                                                  const double2* tw2, bool conj) {
   using GG = ColGeom<N1, N2>;
   constexpr int n = GG::n, CP = GG::CP, KS = GG::KS;
-  fft_reg<N1>(v, tw, n, conj);
+  fft_reg<N1>(v, nullptr, n, conj);
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
     const int k1 = rbrev<N1>(r);
-    if (k1 != 0) v[r] = cmul(v[r], twid2(tw + (n >> 1), r * N2 + s, conj));
+    if (k1 != 0) v[r] = cmul(v[r], twid2(tw2, r * N2 + s, conj));
   }
 #pragma unroll
   for (int part = 0; part < 2; ++part) {
@@ -432,82 +460,99 @@ __device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)
       }
     }
   }
-  if (s < N1) fft_reg<N2>(u, tw, n, conj);
+  if (s < N1) fft_reg<N2>(u, nullptr, n, conj);
 }
 
+// Persistent: each block copies the size's tables into shared memory once and then takes
+// the column tiles blockIdx.x, blockIdx.x + gridDim.x, ... of the segment.
 template <int N1, int N2>
-__global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const int* col_inst, int seg) {
+__global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const int* col_inst, int seg, int items) {
   using GG = ColGeom<N1, N2>;
   constexpr int n = GG::n, CP = GG::CP, CB = GG::CB;
   const DctScale ds(n);
-  extern __shared__ double sbuf[];
+  extern __shared__ __align__(16) double sbuf[];
   double2* tile = reinterpret_cast<double2*>(sbuf);  // [k][c]: one column pair per entry
-  const int item = seg + blockIdx.x;
-  const Inst& I = insts[col_inst[item]];
-  if (!I.active) return;
-  const int c = threadIdx.x % CP, s = threadIdx.x / CP;
-  const int l0 = (item - I.col0) * CB, la = l0 + 2 * c;
-  double* T = I.t1;
-  const double2* tw = I.tw;
-  const double2* pt = I.pt;
-  double2 v[N1];
-  double2 u[N2];
-  // forward DCT-II along the two columns (samples in Makhoul order)
-#pragma unroll
-  for (int m1 = 0; m1 < N1; ++m1)
-    v[m1] = __ldcg(reinterpret_cast<const double2*>(T + (size_t)makhoul_src(N2 * m1 + s, n) * n + la));
-  col_fft_transpose<N1, N2>(v, u, sbuf, c, s, tw, false);
-  __syncthreads();
-  if (s < N1) {
-#pragma unroll
-    for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
-  }
-  __syncthreads();
-  if (s < N1) {
-    // coefficient k = s + N1 k2 of both columns: divide by lambda_kl (the (0,0) mode is
-    // dropped), keep s_k U_k
-    const double cla = I.cosk[la], clb = I.cosk[la + 1];
-#pragma unroll
-    for (int r = 0; r < N2; ++r) {
-      const int k = s + N1 * rbrev<N2>(r);
-      const double2 Z = u[r], P = tile[((n - k) & (n - 1)) * CP + c];
-      const double2 A = make_double2(0.5 * (Z.x + P.x), 0.5 * (Z.y - P.y));
-      const double2 B = make_double2(0.5 * (Z.y + P.y), 0.5 * (P.x - Z.x));
-      const double2 w = __ldg(&pt[k]);
-      const double sk = ds(k);
-      const double Xa = post2(A, w, sk), Xb = post2(B, w, sk);
-      const double lam_a = 2.0 - 2.0 * I.cosk[k] * cla, lam_b = 2.0 - 2.0 * I.cosk[k] * clb;
-      const double Ua = (k == 0 && la == 0) ? 0.0 : Xa / lam_a;
-      const double Ub = Xb / lam_b;
-      u[r] = make_double2(sk * Ua, sk * Ub);
+  if (items <= 0) return;
+  double2* stw = reinterpret_cast<double2*>(sbuf + GG::WORK);  // step-2 twiddles, [register][lane]
+  double2* spt = stw + n;                                      // (cos, sin)(pi k / 2n)
+  double* scos = reinterpret_cast<double*>(spt + n);           // cos(pi k / n)
+  {
+    const Inst& I0 = insts[col_inst[seg]];
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+      stw[e] = __ldg(&I0.tw[(n >> 1) + e]);
+      spt[e] = __ldg(&I0.pt[e]);
+      scos[e] = __ldg(&I0.cosk[e]);
     }
   }
-  __syncthreads();
-  if (s < N1) {
+  const int c = threadIdx.x % CP, s = threadIdx.x / CP;
+  for (int b = blockIdx.x; b < items; b += gridDim.x) {
+    const int item = seg + b;
+    const Inst& I = insts[col_inst[item]];
+    if (!I.active) continue;  // uniform over the block
+    const int l0 = (item - I.col0) * CB, la = l0 + 2 * c;
+    double* T = I.t1;
+    double2 v[N1];
+    double2 u[N2];
+    // forward DCT-II along the two columns (samples in Makhoul order)
 #pragma unroll
-    for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
-  }
-  __syncthreads();
-  // inverse DCT-III along the two columns: W^a + i W^b through one inverse FFT
+    for (int m1 = 0; m1 < N1; ++m1)
+      v[m1] = __ldcg(reinterpret_cast<const double2*>(T + (size_t)makhoul_src(N2 * m1 + s, n) * n + la));
+    // the previous tile's last reads of the shared buffers (and the table copy) are done
+    __syncthreads();
+    col_fft_transpose<N1, N2>(v, u, sbuf, c, s, stw, false);
+    __syncthreads();
+    if (s < N1) {
 #pragma unroll
-  for (int m1 = 0; m1 < N1; ++m1) {
-    const int k = N2 * m1 + s;
-    const double2 a = tile[k * CP + c];
-    const double2 b = k == 0 ? make_double2(0.0, 0.0) : tile[(n - k) * CP + c];
-    const double2 w = __ldg(&pt[k]);
-    const double2 Wa = pre3(k, a.x, b.x, w), Wb = pre3(k, a.y, b.y, w);
-    v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
-  }
-  col_fft_transpose<N1, N2>(v, u, sbuf, c, s, tw, true);
-  __syncthreads();
-  if (s < N1) {
+      for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
+    }
+    __syncthreads();
+    if (s < N1) {
+      // coefficient k = s + N1 k2 of both columns: divide by lambda_kl (the (0,0) mode is
+      // dropped), keep s_k U_k
+      const double cla = scos[la], clb = scos[la + 1];
 #pragma unroll
-    for (int r = 0; r < N2; ++r) tile[makhoul_src(s + N1 * rbrev<N2>(r), n) * CP + c] = u[r];
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < n * CP; e += 256) {
-    const int i = e / CP, cc = e - i * CP;
-    *reinterpret_cast<double2*>(T + (size_t)i * n + l0 + 2 * cc) = tile[i * CP + cc];
+      for (int r = 0; r < N2; ++r) {
+        const int k = s + N1 * rbrev<N2>(r);
+        const double2 Z = u[r], P = tile[((n - k) & (n - 1)) * CP + c];
+        const double2 A = make_double2(0.5 * (Z.x + P.x), 0.5 * (Z.y - P.y));
+        const double2 B = make_double2(0.5 * (Z.y + P.y), 0.5 * (P.x - Z.x));
+        const double2 w = spt[k];
+        const double sk = ds(k);
+        const double Xa = post2(A, w, sk), Xb = post2(B, w, sk);
+        const double ck = scos[k];
+        const double lam_a = 2.0 - 2.0 * ck * cla, lam_b = 2.0 - 2.0 * ck * clb;
+        const double Ua = (k == 0 && la == 0) ? 0.0 : Xa / lam_a;
+        const double Ub = Xb / lam_b;
+        u[r] = make_double2(sk * Ua, sk * Ub);
+      }
+    }
+    __syncthreads();
+    if (s < N1) {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
+    }
+    __syncthreads();
+    // inverse DCT-III along the two columns: W^a + i W^b through one inverse FFT
+#pragma unroll
+    for (int m1 = 0; m1 < N1; ++m1) {
+      const int k = N2 * m1 + s;
+      const double2 a = tile[k * CP + c];
+      const double2 b = k == 0 ? make_double2(0.0, 0.0) : tile[(n - k) * CP + c];
+      const double2 w = spt[k];
+      const double2 Wa = pre3(k, a.x, b.x, w), Wb = pre3(k, a.y, b.y, w);
+      v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
+    }
+    col_fft_transpose<N1, N2>(v, u, sbuf, c, s, stw, true);
+    __syncthreads();
+    if (s < N1) {
+#pragma unroll
+      for (int r = 0; r < N2; ++r) tile[makhoul_src(s + N1 * rbrev<N2>(r), n) * CP + c] = u[r];
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * CP; e += 256) {
+      const int i = e / CP, cc = e - i * CP;
+      *reinterpret_cast<double2*>(T + (size_t)i * n + l0 + 2 * cc) = tile[i * CP + cc];
+    }
   }
 }
 
@@ -518,6 +563,7 @@ struct RegDct {
   static size_t cols_smem() { return sizeof(double) * ColGeom<N1, N2>::SMEM; }
   static constexpr int CB = ColGeom<N1, N2>::CB;
   static int rows_blocks_per_sm;  // occupancy of the row kernels (set by attrs)
+  static int cols_blocks_per_sm;  // occupancy of the column kernel
   static void attrs() {
     OTM_CUDA(cudaFuncSetAttribute(k_dct_rows_fwd<N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)rows_smem()));
@@ -529,6 +575,8 @@ struct RegDct {
     OTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_dct_rows_fwd<N1, N2>, RW * 32, rows_smem()));
     OTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_dct_rows_inv<N1, N2>, RW * 32, rows_smem()));
     rows_blocks_per_sm = std::max(1, std::min(a, b));
+    OTM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, k_dct_cols<N1, N2>, 256, cols_smem()));
+    cols_blocks_per_sm = std::max(1, a);
   }
   static void run(otm_context* ctx, Inst* d, const int* ri, int roff, int rcnt, const int* ci, int coff, int ccnt) {
     const int grid = std::max(1, std::min((rcnt + RW - 1) / RW, rows_blocks_per_sm * ctx->num_sms));
@@ -536,13 +584,16 @@ struct RegDct {
     const long long limit = ctx->wait_test ? kTestWaitCycles : kWaitCycles;
     launch_smem(ctx, "dct_rows_fwd", k_dct_rows_fwd<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt, extra,
                 limit);
-    launch_smem(ctx, "dct_cols", k_dct_cols<N1, N2>, ccnt, 256, cols_smem(), (const Inst*)d, ci, coff);
+    const int cgrid = std::max(1, std::min(ccnt, cols_blocks_per_sm * ctx->num_sms));
+    launch_smem(ctx, "dct_cols", k_dct_cols<N1, N2>, cgrid, 256, cols_smem(), (const Inst*)d, ci, coff, ccnt);
     launch_smem(ctx, "dct_rows_inv", k_dct_rows_inv<N1, N2>, grid, RW * 32, rows_smem(), d, ri, roff, rcnt, extra,
                 limit);
   }
 };
 template <int N1, int N2>
 int RegDct<N1, N2>::rows_blocks_per_sm = 1;
+template <int N1, int N2>
+int RegDct<N1, N2>::cols_blocks_per_sm = 1;
 
 }  // namespace
 
