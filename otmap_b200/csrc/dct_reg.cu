@@ -61,11 +61,6 @@ __device__ __forceinline__ double2 twid2(const double2* tw2, int idx, bool conj)
   if (conj) w.y = -w.y;
   return w;
 }
-__device__ __forceinline__ double2 twid2_global(const double2* __restrict__ tw2, int idx, bool conj) {
-  double2 w = __ldg(&tw2[idx]);
-  if (conj) w.y = -w.y;
-  return w;
-}
 
 // In-register radix-2 decimation-in-frequency FFT of N values, natural order in,
 // bit-reversed order out (v[r] = X[rbrev<N>(r)]). Twiddles W_N^k = tw[k * (n / N)].
@@ -96,25 +91,28 @@ __device__ __forceinline__ void fft_reg(double2 (&v)[N], const double2* __restri
   }
 }
 
-// Steps 1-4 for one line. On entry lane t holds in v[m1] the input sample
+// Steps 1-4 for one line. On entry lane t (< N2) holds in v[m1] the input sample
 // m = N2*m1 + t; on return lanes t < N1 hold u[r] = X_k for k = t + N1 * rbrev<N2>(r).
-// buf is this line's N1 x (N2 + 1) shared buffer of doubles (the transpose moves real and
-// imaginary parts in two rounds).
+// Lanes t >= N2 of a wider lane group take no part. buf is this line's N1 x (N2 + 1)
+// shared buffer of doubles (the transpose moves real and imaginary parts in two rounds).
 template <int N1, int N2>
 __device__ __forceinline__ void fft_line(int t, double* buf, const double2* tw2, bool conj, double2 (&v)[N1],
                                          double2 (&u)[N2]) {
   constexpr int n = N1 * N2;
+  const int tt = t < N2 ? t : 0;
   fft_reg<N1>(v, nullptr, n, conj);
 #pragma unroll
   for (int r = 0; r < N1; ++r) {
     const int k1 = rbrev<N1>(r);
-    if (k1 != 0) v[r] = cmul(v[r], twid2(tw2, r * N2 + t, conj));
+    if (k1 != 0) v[r] = cmul(v[r], twid2(tw2, r * N2 + tt, conj));
   }
   // transpose through shared memory, real parts then imaginary parts
 #pragma unroll
   for (int part = 0; part < 2; ++part) {
+    if (t < N2) {
 #pragma unroll
-    for (int r = 0; r < N1; ++r) buf[rbrev<N1>(r) * (N2 + 1) + t] = part ? v[r].y : v[r].x;
+      for (int r = 0; r < N1; ++r) buf[rbrev<N1>(r) * (N2 + 1) + t] = part ? v[r].y : v[r].x;
+    }
     __syncwarp();
     if (t < N1) {
 #pragma unroll
@@ -415,105 +413,101 @@ __global__ __launch_bounds__(RW * 32, 1) void k_dct_rows_inv(Inst* insts, const 
   }
 }
 
-// Column pass, lanes across column pairs: a block owns CB = 2 CP consecutive columns.
-// Thread (c = tid % CP, s = tid / CP) holds, for the column pair (l0 + 2c, l0 + 2c + 1)
-// packed as one complex line, the samples N2*m1 + s (s < N2) of step 1 -- loaded
-// straight from global memory, 16 bytes per row -- and the outputs k1 = s (s < N1) of
-// step 4. One shared region serves in turn as the step-3 transpose buffer, the
-// exchange tile of the spectra (k with n - k) and the staging tile of the coalesced
-// store.
+// Column pass, one warp per column pair (LPW pairs per warp when a line takes fewer than 32
+// lanes), so that the two FFTs and the exchanges between them stay inside the warp. A block
+// of 8 warps owns CPB = 8 LPW consecutive column pairs: it copies their tile of n rows into
+// shared memory with coalesced 16-byte cp.async (rows stored in Makhoul order, row m holding
+// global row makhoul_src(m), so that the lanes of a line read consecutive rows), each warp
+// transforms its pairs -- DCT-II (split N1 x N2), division by lambda, DCT-III (split
+// N2 x N1, which takes the forward output in the lanes where it already lies) -- and the
+// block writes the tile back in global row order. While the warps transform, the tile's
+// space holds, per line, a 2n-double region: the step-3 transpose buffer, and the line's
+// spectrum for the exchanges of X_k with X_{n-k}.
 template <int N1, int N2>
 struct ColGeom {
-  static constexpr int n = N1 * N2;
-  static constexpr int CP = 256 / N2;     // column pairs per block (256 threads)
-  static constexpr int CB = 2 * CP;       // columns per block
-  static constexpr int KS = N2 * CP + 1;  // padded stride of a k1 row of the transpose buffer
-  static constexpr int WORK = (N1 * KS > n * CB ? N1 * KS : n * CB);  // doubles: transpose / tile
-  static constexpr int SMEM = WORK + 5 * n;  // + the tables: step-2 twiddles, pt (double2), cos(pi k / n)
+  static constexpr int n = N1 * N2, LPW = 32 / N2;
+  static constexpr int CT = 256;                // threads per block
+  static constexpr int CPB = (CT / 32) * LPW;   // column pairs per block
+  static constexpr int CB = 2 * CPB;            // columns per block
+  static constexpr int RS = CPB + 1;            // double2 per tile row (odd: conflict-free line reads)
+  static constexpr int TILE = 2 * n * RS;       // doubles
+  static constexpr int LINE = 2 * n;            // doubles: a line's region (spectrum, transpose)
+  static_assert(LINE >= N1 * (N2 + 1) && LINE >= N2 * (N1 + 1), "the transposes fit in a line's region");
+  static_assert((CT / 32) * LPW * LINE <= TILE, "the lines' regions fit in the tile");
+  static constexpr int TABLES = 7 * n;          // doubles: step-2 twiddles (N1 x N2, N2 x N1), pt, cos
+  static constexpr int SMEM = TILE + TABLES;    // doubles
 };
 
-template <int N1, int N2>
-__device__ __forceinline__ void col_fft_transpose(double2 (&v)[N1], double2 (&u)[N2], double* sh, int c, int s,
-                                                  const double2* tw2, bool conj) {
-  using GG = ColGeom<N1, N2>;
-  constexpr int n = GG::n, CP = GG::CP, KS = GG::KS;
-  fft_reg<N1>(v, nullptr, n, conj);
-#pragma unroll
-  for (int r = 0; r < N1; ++r) {
-    const int k1 = rbrev<N1>(r);
-    if (k1 != 0) v[r] = cmul(v[r], twid2(tw2, r * N2 + s, conj));
-  }
-#pragma unroll
-  for (int part = 0; part < 2; ++part) {
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < N1; ++r) sh[rbrev<N1>(r) * KS + s * CP + c] = part ? v[r].y : v[r].x;
-    __syncthreads();
-    if (s < N1) {
-#pragma unroll
-      for (int m2 = 0; m2 < N2; ++m2) {
-        const double x = sh[s * KS + m2 * CP + c];
-        if (part)
-          u[m2].y = x;
-        else
-          u[m2].x = x;
-      }
-    }
-  }
-  if (s < N1) fft_reg<N2>(u, nullptr, n, conj);
-}
+__device__ __forceinline__ int makhoul_inv(int i, int n) { return (i & 1) ? n - 1 - (i >> 1) : (i >> 1); }
 
 // Persistent: each block copies the size's tables into shared memory once and then takes
 // the column tiles blockIdx.x, blockIdx.x + gridDim.x, ... of the segment.
 template <int N1, int N2>
-__global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const int* col_inst, int seg, int items) {
+__global__ __launch_bounds__(ColGeom<N1, N2>::CT, 1) void k_dct_cols(const Inst* insts, const int* col_inst, int seg,
+                                                                     int items) {
   using GG = ColGeom<N1, N2>;
-  constexpr int n = GG::n, CP = GG::CP, CB = GG::CB;
+  constexpr int n = GG::n, CPB = GG::CPB, CB = GG::CB, RS = GG::RS, LPW = GG::LPW;
   const DctScale ds(n);
   extern __shared__ __align__(16) double sbuf[];
-  double2* tile = reinterpret_cast<double2*>(sbuf);  // [k][c]: one column pair per entry
+  double2* tile = reinterpret_cast<double2*>(sbuf);  // [m][pair], rows in Makhoul order
   if (items <= 0) return;
-  double2* stw = reinterpret_cast<double2*>(sbuf + GG::WORK);  // step-2 twiddles, [register][lane]
-  double2* spt = stw + n;                                      // (cos, sin)(pi k / 2n)
+  double2* stw = reinterpret_cast<double2*>(sbuf + GG::TILE);  // step-2 twiddles, N1 x N2 split
+  double2* stw_sw = stw + n;                                   // the same for the N2 x N1 split
+  double2* spt = stw_sw + n;                                   // (cos, sin)(pi k / 2n)
   double* scos = reinterpret_cast<double*>(spt + n);           // cos(pi k / n)
   {
     const Inst& I0 = insts[col_inst[seg]];
+    const double2* tw2 = I0.tw + (n >> 1);
     for (int e = threadIdx.x; e < n; e += blockDim.x) {
-      stw[e] = __ldg(&I0.tw[(n >> 1) + e]);
+      stw[e] = __ldg(&tw2[e]);
+      stw_sw[e] = __ldg(&tw2[n + e]);
       spt[e] = __ldg(&I0.pt[e]);
       scos[e] = __ldg(&I0.cosk[e]);
     }
   }
-  const int c = threadIdx.x % CP, s = threadIdx.x / CP;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, sub = lane / N2, t = lane % N2;
+  const int cp = warp * LPW + sub;  // this lane group's column pair within the block
+  double* buf = sbuf + (warp * LPW + sub) * GG::LINE;  // this line's region of the tile space
+  double2* zl = reinterpret_cast<double2*>(buf);
   for (int b = blockIdx.x; b < items; b += gridDim.x) {
     const int item = seg + b;
     const Inst& I = insts[col_inst[item]];
     if (!I.active) continue;  // uniform over the block
-    const int l0 = (item - I.col0) * CB, la = l0 + 2 * c;
+    const int l0 = (item - I.col0) * CB, la = l0 + 2 * cp;
     double* T = I.t1;
+    // the previous tile's store has read the tile (and the tables are in place)
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * CPB; e += GG::CT) {
+      const int i = e / CPB, cc = e - i * CPB;
+      const unsigned dst = smem_u32(&tile[makhoul_inv(i, n) * RS + cc]);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(T + (size_t)i * n + l0 + 2 * cc)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
     double2 v[N1];
     double2 u[N2];
-    // forward DCT-II along the two columns (samples in Makhoul order)
+    // forward DCT-II of the two columns (one complex line; samples in Makhoul order)
 #pragma unroll
-    for (int m1 = 0; m1 < N1; ++m1)
-      v[m1] = __ldcg(reinterpret_cast<const double2*>(T + (size_t)makhoul_src(N2 * m1 + s, n) * n + la));
-    // the previous tile's last reads of the shared buffers (and the table copy) are done
-    __syncthreads();
-    col_fft_transpose<N1, N2>(v, u, sbuf, c, s, stw, false);
-    __syncthreads();
-    if (s < N1) {
+    for (int m1 = 0; m1 < N1; ++m1) v[m1] = tile[(N2 * m1 + t) * RS + cp];
+    __syncthreads();  // the tile's space now holds the lines' regions
+    fft_line<N1, N2>(t, buf, stw, false, v, u);
+    // Z_k (k = t + N1 rbrev(r)) into the line's region, then each lane separates the two
+    // spectra with Z_{n-k}, divides by lambda_kl (the (0,0) mode is dropped) and keeps
+    // s_k U_k, which goes back to the region for the partner's DCT-III input
+    __syncwarp();
+    if (t < N1) {
 #pragma unroll
-      for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
+      for (int r = 0; r < N2; ++r) zl[t + N1 * rbrev<N2>(r)] = u[r];
     }
-    __syncthreads();
-    if (s < N1) {
-      // coefficient k = s + N1 k2 of both columns: divide by lambda_kl (the (0,0) mode is
-      // dropped), keep s_k U_k
+    __syncwarp();
+    if (t < N1) {
       const double cla = scos[la], clb = scos[la + 1];
 #pragma unroll
       for (int r = 0; r < N2; ++r) {
-        const int k = s + N1 * rbrev<N2>(r);
-        const double2 Z = u[r], P = tile[((n - k) & (n - 1)) * CP + c];
+        const int k = t + N1 * rbrev<N2>(r);
+        const double2 Z = u[r], P = zl[(n - k) & (n - 1)];
         const double2 A = make_double2(0.5 * (Z.x + P.x), 0.5 * (Z.y - P.y));
         const double2 B = make_double2(0.5 * (Z.y + P.y), 0.5 * (P.x - Z.x));
         const double2 w = spt[k];
@@ -526,32 +520,35 @@ __global__ __launch_bounds__(256, 1) void k_dct_cols(const Inst* insts, const in
         u[r] = make_double2(sk * Ua, sk * Ub);
       }
     }
-    __syncthreads();
-    if (s < N1) {
+    __syncwarp();
+    if (t < N1) {
 #pragma unroll
-      for (int r = 0; r < N2; ++r) tile[(s + N1 * rbrev<N2>(r)) * CP + c] = u[r];
+      for (int r = 0; r < N2; ++r) zl[t + N1 * rbrev<N2>(r)] = u[r];
     }
-    __syncthreads();
-    // inverse DCT-III along the two columns: W^a + i W^b through one inverse FFT
+    __syncwarp();
+    // inverse DCT-III of the two columns, split N2 x N1: lane t (< N1) takes the samples
+    // k = t + N1 m1 it holds; U_{n-k} comes from the region
+    double2 w2[N2];
+    double2 x2[N1];
 #pragma unroll
-    for (int m1 = 0; m1 < N1; ++m1) {
-      const int k = N2 * m1 + s;
-      const double2 a = tile[k * CP + c];
-      const double2 b = k == 0 ? make_double2(0.0, 0.0) : tile[(n - k) * CP + c];
+    for (int m1 = 0; m1 < N2; ++m1) {
+      const int k = t < N1 ? t + N1 * m1 : 0;
+      const double2 a = u[rbrev<N2>(m1)];
+      const double2 bb = zl[(n - k) & (n - 1)];
       const double2 w = spt[k];
-      const double2 Wa = pre3(k, a.x, b.x, w), Wb = pre3(k, a.y, b.y, w);
-      v[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
+      const double2 Wa = pre3(k, a.x, bb.x, w), Wb = pre3(k, a.y, bb.y, w);
+      w2[m1] = make_double2(Wa.x - Wb.y, Wa.y + Wb.x);
     }
-    col_fft_transpose<N1, N2>(v, u, sbuf, c, s, stw, true);
-    __syncthreads();
-    if (s < N1) {
+    __syncwarp();  // the region's spectrum is read: it becomes the transpose buffer
+    fft_line<N2, N1>(t, buf, stw_sw, true, w2, x2);
+    __syncthreads();  // every warp is done with its transpose buffer: the space is the tile again
+    // output sample m = t + N2 rbrev<N1>(r) (Makhoul order) of both columns
 #pragma unroll
-      for (int r = 0; r < N2; ++r) tile[makhoul_src(s + N1 * rbrev<N2>(r), n) * CP + c] = u[r];
-    }
+    for (int r = 0; r < N1; ++r) tile[(t + N2 * rbrev<N1>(r)) * RS + cp] = x2[r];
     __syncthreads();
-    for (int e = threadIdx.x; e < n * CP; e += 256) {
-      const int i = e / CP, cc = e - i * CP;
-      *reinterpret_cast<double2*>(T + (size_t)i * n + l0 + 2 * cc) = tile[i * CP + cc];
+    for (int e = threadIdx.x; e < n * CPB; e += GG::CT) {
+      const int i = e / CPB, cc = e - i * CPB;
+      *reinterpret_cast<double2*>(T + (size_t)i * n + l0 + 2 * cc) = tile[makhoul_inv(i, n) * RS + cc];
     }
   }
 }
@@ -616,14 +613,16 @@ void step2_table(const std::vector<double2>& tw, std::vector<double2>& out) {
 }  // namespace
 
 void dct_reg_step2_table(int n, const std::vector<double2>& tw, std::vector<double2>& out) {
+  std::vector<double2> sw;
   switch (n) {
-    case 64: step2_table<8, 8>(tw, out); break;
-    case 128: step2_table<8, 16>(tw, out); break;
-    case 256: step2_table<16, 16>(tw, out); break;
-    case 512: step2_table<16, 32>(tw, out); break;
-    case 1024: step2_table<32, 32>(tw, out); break;
+    case 64: step2_table<8, 8>(tw, out); step2_table<8, 8>(tw, sw); break;
+    case 128: step2_table<8, 16>(tw, out); step2_table<16, 8>(tw, sw); break;
+    case 256: step2_table<16, 16>(tw, out); step2_table<16, 16>(tw, sw); break;
+    case 512: step2_table<16, 32>(tw, out); step2_table<32, 16>(tw, sw); break;
+    case 1024: step2_table<32, 32>(tw, out); step2_table<32, 32>(tw, sw); break;
     default: out.clear();
   }
+  out.insert(out.end(), sw.begin(), sw.end());
 }
 
 int dct_reg_lines_per_block(int n) {  // rows per row-pass work item: two per FFT line of a warp
