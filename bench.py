@@ -43,7 +43,7 @@ SIGMA_PX = 5.0
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--steps", type=int, default=20)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--batch", type=int, default=8)
@@ -123,10 +123,18 @@ class Clocks:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                          "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
                                          stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # the timed region starts once the sampler is running (its first line is written)
+        t0 = time.time()
+        while time.time() - t0 < 3.0 and self.proc.poll() is None:
+            self.f.flush()
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
 
     def stop(self):
         if not self.proc:
@@ -204,7 +212,7 @@ def roofline(prof, cell_iters, steps, peaks):
             "frac": achieved / peaks["hbm_gbs"],
             "traffic": traffic * cells_per_launch if traffic is not None else None,
             "alg_bytes_per_launch": per_launch_bytes, "avg_launch_us": avg_s * 1e6, "launches": cnt,
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs (%s)" % peaks.get("source", "measured"),
+            "peak_source": peaks["source"],
             "traffic_source": "profiles/traffic_per_cell.json (ncu dram__bytes_read+write per cell, scaled)"}
 
 
@@ -212,9 +220,10 @@ def load_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        d["source"] = "measured"
+        d["source"] = "of measured: MEASURED_PEAKS.json hbm_gbs"
         return d
-    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "source": "fallback"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0,
+            "source": "of fallback: 6.65 TB/s, a measured B200 copy bandwidth (MEASURED_PEAKS.json absent)"}
 
 
 def run_ours(args):
