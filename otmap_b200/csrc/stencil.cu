@@ -247,16 +247,12 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
 #pragma unroll
     for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
     VG gp, gh, gq;
-    Row ap, ah, aq;  // grid row row-1 of each stencil field, carried from the previous step
 #pragma unroll 2
     for (int row = sc.i0; row <= last; ++row) {
       cp_async_wait<RD - 3>();
       __syncwarp();
-      if (row == sc.i0) {
-        ap = R.row_of(row - 1, 0);
-        ah = R.row_of(row - 1, 1);
-        aq = R.row_of(row - 1, 2);
-      }
+      // grid row row-1 is still in the ring: read again rather than carried in registers
+      const Row ap = R.row_of(row - 1, 0), ah = R.row_of(row - 1, 1), aq = R.row_of(row - 1, 2);
       const Row bp = R.row_of(row, 0), bh = R.row_of(row, 1), bq = R.row_of(row, 2);
       // vertex row `row` from grid rows row-1 and row
       VG np = vgrad(ap, bp);
@@ -298,9 +294,6 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
       gp = np;
       gh = nh;
       gq = nq;
-      ap = bp;
-      ah = bh;
-      aq = bq;
       __syncwarp();
       R.issue(row - 2 + RD);  // refill the stage of grid row row-2, no longer needed
     }
