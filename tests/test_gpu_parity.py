@@ -136,7 +136,7 @@ def test_bad_arguments_raise(ot):
         ot.GridBasedTransportSolver().solve(np.ones(16))
 
 
-@pytest.mark.parametrize("n", [8, 16, 64, 128, 512])
+@pytest.mark.parametrize("n", [8, 16, 64, 128, 256, 512, 1024])
 def test_fast_and_dense_transforms_agree(n, ot):
     """The fast cosine transform (power-of-two n) and the dense products give the same
     solve: same iterations, positions within 1e-9."""
