@@ -146,7 +146,6 @@ struct DctScale {
   __device__ __forceinline__ explicit DctScale(int n) : s0(sqrt(1.0 / n)), s1(sqrt(2.0 / n)) {}
   __device__ __forceinline__ double operator()(int k) const { return k == 0 ? s0 : s1; }
 };
-__device__ __forceinline__ int makhoul_src(int m, int n) { return m < (n >> 1) ? 2 * m : 2 * (n - 1 - m) + 1; }
 // DCT-II coefficient from V_k: s_k Re(e^{-i pi k / 2n} V_k)
 __device__ __forceinline__ double post2(double2 V, double2 pt, double sk) { return sk * fma(V.x, pt.x, V.y * pt.y); }
 // DCT-III input W_k from Y_k (a) and Y_{n-k} (b)
@@ -418,10 +417,10 @@ __global__ __launch_bounds__(RW * 32, 1) void k_dct_rows_inv(Inst* insts, const 
 // lanes), so that the two FFTs and the exchanges between them stay inside the warp. A block
 // of 8 warps owns CPB = 8 LPW consecutive column pairs: it copies their tile of n rows into
 // shared memory with coalesced 16-byte cp.async (rows stored in Makhoul order, row m holding
-// global row makhoul_src(m), so that the lanes of a line read consecutive rows), each warp
-// transforms its pairs -- DCT-II (split N1 x N2), division by lambda, DCT-III (split
-// N2 x N1, which takes the forward output in the lanes where it already lies) -- and the
-// block writes the tile back in global row order. While the warps transform, the tile's
+// global row 2m for m < n/2 and 2(n-1-m)+1 above, so that the lanes of a line read
+// consecutive rows), each warp transforms its pairs -- DCT-II (split N1 x N2), division by
+// lambda, DCT-III (split N2 x N1, which takes the forward output in the lanes where it
+// already lies) -- and the block writes the tile back in global row order. While the warps transform, the tile's
 // space holds, per line, a 2n-double region: the step-3 transpose buffer, and the line's
 // spectrum for the exchanges of X_k with X_{n-k}.
 template <int N1, int N2>
@@ -584,7 +583,7 @@ __global__ __launch_bounds__(ColGeom<N1, N2>::CT, 1) void k_dct_cols(const Inst*
 
 template <int N1, int N2>
 struct RegDct {
-  static constexpr int n = N1 * N2, LPW = 32 / N2;
+  static constexpr int LPW = 32 / N2;
   static size_t rows_smem() { return RowGeom<N1, N2>::SMEM; }
   static size_t cols_smem() { return sizeof(double) * ColGeom<N1, N2>::SMEM; }
   static constexpr int CB = ColGeom<N1, N2>::CB;
