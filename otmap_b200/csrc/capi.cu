@@ -121,9 +121,13 @@ extern "C" int otm_destroy(otm_context* ctx) {
   if (!ctx) return OTM_OK;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  cudaStream_t st = ctx->stream;
+  if (ctx->side) cudaStreamSynchronize(ctx->side);
+  cudaStream_t st = ctx->stream, side = ctx->side;
+  void* poll = ctx->h_poll;
   delete ctx;
   if (st) cudaStreamDestroy(st);
+  if (side) cudaStreamDestroy(side);
+  if (poll) cudaFreeHost(poll);
   return OTM_OK;
 }
 

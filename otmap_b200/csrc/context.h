@@ -116,6 +116,12 @@ struct otm_context {
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   otm::Workspace ws;
   otm::DevBuf staging;  // device staging for host inputs/outputs
+  // second stream of a batched solve: outputs of instances that stopped while the rest of
+  // the batch iterates (created on first use), its staging and a pinned copy of the records
+  cudaStream_t side = nullptr;
+  otm::DevBuf staging_side;
+  void* h_poll = nullptr;
+  size_t h_poll_bytes = 0;
   otm::DevBuf raster_scratch;  // rasterizer face boxes, pixel owners, vertex values (grow-only)
   // adjoint workspaces per grid size (adjoint.cu); type-erased to keep this header small
   struct Erased {

@@ -26,8 +26,11 @@
 #include <cfloat>
 #include <cmath>
 #include <algorithm>
+#include <chrono>
 #include <cstring>
+#include <functional>
 #include <mutex>
+#include <thread>
 #include <random>
 #include <vector>
 
@@ -763,8 +766,14 @@ static void build_loop_graph(otm_context* ctx, int count) {
 }
 
 // Runs the whole solve for `count` instances whose raw densities have been copied
-// into their rho buffers. Host-side copies of the final records are returned.
-static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, const otm_solver_options& o) {
+// into their rho buffers. Host-side copies of the final records are returned. With
+// `stopped` (device loop only), the host watches the records while the loop runs and
+// calls stopped(q) once for each instance that is no longer active -- its potential and
+// density are final from then on -- so that its outputs can be produced on the side
+// stream while the rest of the batch iterates; `done` marks those instances.
+static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, const otm_solver_options& o,
+                                    const std::function<void(int)>* stopped = nullptr,
+                                    std::vector<char>* done = nullptr) {
   Workspace& ws = ctx->ws;
   cudaStream_t st = ctx->stream;
   const int count = (int)h.size();
@@ -797,6 +806,25 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
     LoopCtl c = {0u, (unsigned int)o.max_iter + 2u, 0, 0};
     OTM_CUDA(cudaMemcpyAsync(ws.loopctl.p, &c, sizeof(c), cudaMemcpyHostToDevice, st));
     OTM_CUDA(cudaGraphLaunch(ws.graph_exec, st));
+    if (stopped && done) {
+      Inst* poll = static_cast<Inst*>(ctx->h_poll);
+      while (true) {
+        const cudaError_t q = cudaStreamQuery(st);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) OTM_CUDA(q);
+        // a racy but harmless read: `active` only ever goes from 1 to 0, and the last
+        // block that clears it has made the instance's arrays final before doing so
+        OTM_CUDA(cudaMemcpyAsync(poll, d_insts, sizeof(Inst) * count, cudaMemcpyDeviceToHost, ctx->side));
+        OTM_CUDA(cudaStreamSynchronize(ctx->side));
+        for (int k = 0; k < count; ++k)
+          if (!(*done)[k] && !poll[k].active && !poll[k].fault) {
+            (*stopped)(k);
+            (*done)[k] = 1;
+          }
+        std::this_thread::sleep_for(std::chrono::microseconds(200));
+      }
+      OTM_CUDA(cudaStreamSynchronize(ctx->side));
+    }
     OTM_CUDA(cudaMemcpyAsync(hp, d_insts, sizeof(Inst) * count, cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaMemcpyAsync(&c, ws.loopctl.p, sizeof(c), cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
@@ -958,9 +986,48 @@ extern "C" int otm_solve_batch(otm_context* ctx, int count, const int* ns, const
     std::vector<Inst> h = layout_workspace(ctx, sizes);
     for (int q = 0; q < count; ++q)
       copy_in(ctx, h[q].rho, density[q], sizeof(double) * (size_t)sizes[q] * sizes[q]);
-    std::vector<Inst> fin = run_solver(ctx, h, o);
     Inst* d_insts = ctx->ws.insts.as<Inst>();
+    // Host outputs of a batch on the device loop: the mesh of an instance that has stopped
+    // is formed and copied out on a second stream while the others still iterate.
+    bool early = count > 1 && ctx->loop_mode == OTM_LOOP_GRAPH && !ctx->prof.on;
+    bool any_host = false;
+    size_t vmax = 0;
     for (int q = 0; q < count; ++q) {
+      any_host |= !is_device_ptr(fwd_xy[q]);
+      vmax = std::max(vmax, (size_t)(sizes[q] + 1) * (sizes[q] + 1));
+    }
+    early = early && any_host;
+    std::vector<char> done(count, 0);
+    std::function<void(int)> stopped = [&](int q) {
+      const int n = sizes[q];
+      const size_t V = (size_t)(n + 1) * (n + 1);
+      const bool dev = is_device_ptr(fwd_xy[q]);
+      double* dst = dev ? fwd_xy[q] : ctx->staging_side.as<double>();
+      ctx->launches++;
+      k_forward_mesh<<<(unsigned)((V + 255) / 256), 256, 0, ctx->side>>>((const Inst*)d_insts, q, dst);
+      OTM_CUDA(cudaGetLastError());
+      if (!dev) OTM_CUDA(cudaMemcpyAsync(fwd_xy[q], dst, sizeof(double) * 2 * V, cudaMemcpyDefault, ctx->side));
+      if (adjusted && adjusted[q])
+        OTM_CUDA(cudaMemcpyAsync(adjusted[q], h[q].rho, sizeof(double) * (size_t)n * n, cudaMemcpyDefault,
+                                 ctx->side));
+    };
+    if (early) {
+      if (!ctx->side) OTM_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+      ctx->staging_side.reserve(sizeof(double) * 2 * vmax);  // before the loop: no allocation inside it
+      const size_t pb = sizeof(Inst) * (size_t)count;
+      if (ctx->h_poll_bytes < pb) {
+        if (ctx->h_poll) cudaFreeHost(ctx->h_poll);
+        ctx->h_poll = nullptr;
+        OTM_CUDA(cudaMallocHost(&ctx->h_poll, pb));
+        ctx->h_poll_bytes = pb;
+      }
+    }
+    std::vector<Inst> fin = early ? run_solver(ctx, h, o, &stopped, &done) : run_solver(ctx, h, o);
+    for (int q = 0; q < count; ++q) {
+      if (done[q]) {
+        if (stats) fill_stats(fin[q], &stats[q]);
+        continue;
+      }
       int n = sizes[q];
       size_t V = (size_t)(n + 1) * (n + 1);
       bool dev = is_device_ptr(fwd_xy[q]);
