@@ -122,7 +122,9 @@ int otm_solve(otm_context* ctx, int n, const double* density, const otm_solver_o
 
 /* `count` independent solves of possibly different sizes, run together on the GPU
  * (each with its own convergence test). Arrays of `count` entries; entries of
- * `adjusted` and `stats` may be NULL as a whole. */
+ * `adjusted` and `stats` may be NULL as a whole. With host output buffers, the
+ * outputs of an instance that has stopped are written (on a second stream of the
+ * context) while the others still iterate; the call returns once all are written. */
 int otm_solve_batch(otm_context* ctx, int count, const int* n, const double* const* density,
                     const otm_solver_options* opt, double* const* fwd_xy, double* const* adjusted,
                     otm_solve_stats* stats);
