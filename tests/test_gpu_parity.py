@@ -194,3 +194,20 @@ def test_graph_loop_matches_host_loop(ot):
             assert mg.stats.iterations == mh.stats.iterations
             assert mg.stats.outcome == mh.stats.outcome
             assert np.array_equal(mg.fwd_mesh(), mh.fwd_mesh())
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 4, 5, 7])
+def test_tiny_grids_match_oracle(n, ot, oracle_port):
+    """Degenerate sizes: a single cell (already converged), and grids smaller than one
+    sweep strip or one transform tile -- same iterations as the oracle, positions within
+    1e-6."""
+    from otmap_b200 import workloads as W
+
+    d = W.to_cells(W.gaussian_mixture(n, 3)) if n >= 2 else np.ones(1)
+    o = oracle_port.solve(d, n)
+    s = ot.GridBasedTransportSolver()
+    s.set_verbose_level(0)
+    s.init(n)
+    m = s.solve(d)
+    assert m.stats.iterations == o.iterations
+    assert np.abs(m.fwd_mesh() - o.fwd).max() <= POS_TOL
