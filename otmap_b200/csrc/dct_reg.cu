@@ -17,7 +17,9 @@
 // B_k = (Z_k - conj Z_{n-k}) / 2i; for the DCT-III both inputs are Hermitian, so the
 // real and imaginary parts of the one inverse FFT are the two output lines. The column
 // pass stages a tile of full column pairs in shared memory so its global reads and
-// writes are row-contiguous.
+// writes are row-contiguous. All three kernels are persistent; each block copies the
+// size's tables (step-2 twiddles in [register][lane] order, post-twiddles, cosines) into
+// shared memory once, so no table read waits on L1 or L2 inside a transform.
 
 #include <algorithm>
 #include <cmath>
