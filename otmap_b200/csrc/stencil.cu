@@ -390,7 +390,7 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
     };
     VG gp, gd;
     Row pc, dc;  // grid row row-1 of psi and of d, carried from the previous step
-#pragma unroll 2
+#pragma unroll 4
     for (int row = sc.i0; row <= last; ++row) {
       cp_async_wait<RD - 3>();
       __syncwarp();
