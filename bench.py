@@ -643,7 +643,7 @@ def run_reference(args):
     # One single-threaded reference process per host core, each on one density of the batch
     # (densities repeated when there are more cores than densities): the throughput of all
     # cores on a steady stream of such densities.
-    P = max(1, min(cores, 64))
+    P = max(1, min(cores, 32))  # each process holds a factorisation of the n^2 Laplacian
     groups = [[seeds[p % total]] for p in range(P)]
     ctxm = mp.get_context("spawn")
     with ctxm.Pool(P) as pool:
