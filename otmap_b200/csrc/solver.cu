@@ -190,23 +190,18 @@ __global__ __launch_bounds__(NT) void k_density_apply(Inst* insts, const int* ti
 // ---------------------------------------------------------------------------
 // Initial residual at psi = 0 (otsolver_2dgrid.cpp:146).
 
+// At psi = 0 every vertex gradient is zero and the quad-area formula (cell_area) reduces
+// exactly to 0.5 * (e*e - e*(-e)) = e*e, so the kernel streams rho without the stencil.
 __global__ __launch_bounds__(NT) void k_residual_init(Inst* insts, const int* tile_inst, double* partials) {
-  __shared__ double s[HI * HJ];
-  __shared__ double gx[VI * VJ], gy[VI * VJ];
   __shared__ double red[32 * 2];
   Inst& I = insts[tile_inst[blockIdx.x]];
   const int n = I.n;
   const double e = 1.0 / (double)n, ea = elem_area(n);
   TileCoord t = tile_coord(I, blockIdx.x);
-  const double* psi = I.psi[0];
-  load_halo(s, n, t.i0, t.j0, [&](size_t g) { return psi[g]; });
-  __syncthreads();
-  vertex_grads(s, gx, gy, 0.5 * (double)n);
-  __syncthreads();
   double v[1] = {0.0};
   double mx = -INFINITY;
   if (t.inside) {
-    double r = cell_area(gx, gy, t.ci, t.cj, e) - ea * I.rho[t.f];
+    double r = e * e - ea * I.rho[t.f];
     I.r[0][t.f] = r;
     v[0] = r * r;
     mx = r;
