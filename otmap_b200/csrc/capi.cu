@@ -123,10 +123,12 @@ extern "C" int otm_destroy(otm_context* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->side) cudaStreamSynchronize(ctx->side);
   cudaStream_t st = ctx->stream, side = ctx->side;
+  cudaEvent_t ready = ctx->side_ready;
   void* poll = ctx->h_poll;
   delete ctx;
   if (st) cudaStreamDestroy(st);
   if (side) cudaStreamDestroy(side);
+  if (ready) cudaEventDestroy(ready);
   if (poll) cudaFreeHost(poll);
   return OTM_OK;
 }

@@ -119,6 +119,7 @@ struct otm_context {
   // second stream of a batched solve: outputs of instances that stopped while the rest of
   // the batch iterates (created on first use), its staging and a pinned copy of the records
   cudaStream_t side = nullptr;
+  cudaEvent_t side_ready = nullptr;  // the batch's records are initialised (set-up kernels done)
   otm::DevBuf staging_side;
   void* h_poll = nullptr;
   size_t h_poll_bytes = 0;

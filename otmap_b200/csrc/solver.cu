@@ -794,6 +794,7 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
   launch(ctx, "density_apply", k_density_apply, T, NT, d_insts, ti);
   launch(ctx, "residual_init", k_residual_init, T, NT, d_insts, ti, part);
   OTM_CUDA(cudaGetLastError());
+  if (stopped) OTM_CUDA(cudaEventRecord(ctx->side_ready, st));
 
   Inst* hp = static_cast<Inst*>(ws.h_pinned);
   if (ctx->loop_mode == OTM_LOOP_GRAPH && !ctx->prof.on) {
@@ -803,6 +804,9 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
     OTM_CUDA(cudaGraphLaunch(ws.graph_exec, st));
     if (stopped && done) {
       Inst* poll = static_cast<Inst*>(ctx->h_poll);
+      // the records start inactive on the host side: watch them only once the set-up
+      // kernels (queued before the graph) have initialised them
+      OTM_CUDA(cudaStreamWaitEvent(ctx->side, ctx->side_ready, 0));
       while (true) {
         const cudaError_t q = cudaStreamQuery(st);
         if (q == cudaSuccess) break;
@@ -1008,6 +1012,7 @@ extern "C" int otm_solve_batch(otm_context* ctx, int count, const int* ns, const
     };
     if (early) {
       if (!ctx->side) OTM_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+      if (!ctx->side_ready) OTM_CUDA(cudaEventCreateWithFlags(&ctx->side_ready, cudaEventDisableTiming));
       ctx->staging_side.reserve(sizeof(double) * 2 * vmax);  // before the loop: no allocation inside it
       const size_t pb = sizeof(Inst) * (size_t)count;
       if (ctx->h_poll_bytes < pb) {
