@@ -211,3 +211,41 @@ def test_tiny_grids_match_oracle(n, ot, oracle_port):
     m = s.solve(d)
     assert m.stats.iterations == o.iterations
     assert np.abs(m.fwd_mesh() - o.fwd).max() <= POS_TOL
+
+
+def test_batch_outputs_host_and_device_mixed(ot):
+    """A batch whose output buffers mix host and device memory: instances that stop early
+    have their mesh and density written while the rest still iterate; every output equals
+    the one of a single solve."""
+    import ctypes as C
+
+    import torch
+
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    sizes = [64, 128, 48, 96]
+    dens = [W.to_cells(W.gaussian_mixture(n, 700 + k)) for k, n in enumerate(sizes)]
+    ctx = N.Context(0)
+    fwd_host = [np.empty(((n + 1) ** 2, 2)) for n in sizes]
+    fwd_dev = [torch.empty(((n + 1) ** 2, 2), dtype=torch.float64, device="cuda") for n in sizes]
+    adj_host = [np.empty(n * n) for n in sizes]
+    fwd_ptrs = [fwd_dev[k].data_ptr() if k % 2 else N.ptr(fwd_host[k]) for k in range(len(sizes))]
+    B = len(sizes)
+    ns = (C.c_int * B)(*sizes)
+    dp = (C.c_void_p * B)(*[N.ptr(d) for d in dens])
+    fp = (C.c_void_p * B)(*fwd_ptrs)
+    ap = (C.c_void_p * B)(*[N.ptr(a) for a in adj_host])
+    stats = (N.SolveStatsC * B)()
+    N.check(N.lib().otm_solve_batch(ctx.handle, B, ns, dp, None, fp, ap, stats))
+    torch.cuda.synchronize()
+    for k, n in enumerate(sizes):
+        s = ot.GridBasedTransportSolver()
+        s.set_verbose_level(0)
+        s.init(n)
+        m = s.solve(dens[k])
+        got = fwd_dev[k].cpu().numpy() if k % 2 else fwd_host[k]
+        assert stats[k].iterations == m.stats.iterations
+        assert np.array_equal(got, m.fwd_mesh())
+        assert np.array_equal(adj_host[k], m.density())
+    ctx.close()
