@@ -274,7 +274,9 @@ __global__ __launch_bounds__(RW * 32, 1) void k_dct_rows_fwd(Inst* insts, const 
     return true;
   };
   unsigned phase = 0;
-  int item = blockIdx.x * RW + warp;
+  // consecutive items go to consecutive blocks, so that a short list (a batch's last few
+  // active instances) still spreads over every SM
+  int item = warp * gridDim.x + blockIdx.x;
   bool pending = issue(item);
   const int mirror = (lane - t) + (N2 - 1 - t);
   const int src_lane = (lane - t) + (t < N1 ? (N1 - t) % N1 : 0);
@@ -361,7 +363,9 @@ __global__ __launch_bounds__(RW * 32, 1) void k_dct_rows_inv(Inst* insts, const 
     return true;
   };
   unsigned phase = 0;
-  int item = blockIdx.x * RW + warp;
+  // consecutive items go to consecutive blocks, so that a short list (a batch's last few
+  // active instances) still spreads over every SM
+  int item = warp * gridDim.x + blockIdx.x;
   bool pending = issue(item);
   const int mirror = (lane - t) + (t < N1 ? N1 - 1 - t : 0);
   while (item < items) {
