@@ -38,7 +38,7 @@ struct Inst {
   // loop state
   int it, active, outcome, use_beta;
   unsigned int counter;
-  int srows;  // strip height of the sweeps for this batch (32 or 64 rows)
+  int srows;  // strip height of the sweeps for this batch (16, 32 or 64 rows)
   double residual, residual0, alpha, beta, linf, dnorm;
   double dens_scale, dens_beta;
 };

@@ -13,12 +13,13 @@
 //                  psi + alpha d and r_k + alpha b + alpha^2 a (:599-604); the last
 //                  block advances the iteration and tests the loop condition (:160).
 //
-// Geometry: one warp owns a strip of 32 consecutive columns (j, contiguous in memory)
-// and Inst::srows rows (32, or 64 when the batch has strips to spare) and walks down it. Grid rows are prefetched asynchronously (cp.async)
-// into a per-warp ring of RD rows in shared memory, so RD-2 rows per warp are in
-// flight while it computes; the previous vertex-gradient row is kept in registers. The
-// strip's two halo columns are staged with the row; neighbours come from the ring. A
-// block is SWARPS strips side by side.
+// Geometry: one warp owns a strip of 32 consecutive columns (j, contiguous in memory) and
+// Inst::srows rows (32; 64 when the batch has strips to spare, 16 when it has too few to
+// fill the SMs) and walks down it. Grid rows are prefetched asynchronously (cp.async) into
+// a per-warp ring of RD rows in shared memory, so RD-2 rows per warp are in flight while
+// it computes; the previous vertex-gradient row is kept in registers. The strip's two halo
+// columns are staged with the row; neighbours come from the ring. A block is SWARPS strips
+// side by side.
 // Per cell the arithmetic is the reference's, in FP64, without FMA contraction.
 
 #include "engine.cuh"
@@ -26,7 +27,7 @@
 namespace otm {
 
 constexpr int SW = 32;        // strip width (one warp)
-// strip height (rows per warp): Inst::srows, 32 or 64 per batch (layout_workspace)
+// strip height (rows per warp): Inst::srows, 16, 32 or 64 per batch (layout_workspace)
 constexpr int SWARPS = 4;     // strips per block
 constexpr int ST = SW * SWARPS;
 constexpr int KA = SWEEP_SLOTS;  // partial-sum slots per block
