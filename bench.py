@@ -56,7 +56,7 @@ def parse():
     p.add_argument("--no-mixed", action="store_true")
     p.add_argument("--no-locate", action="store_true")
     p.add_argument("--mixed-count", type=int, default=64)
-    p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations timed per step")
+    p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations per warm-up step")
     return p.parse_args()
 
 
@@ -326,19 +326,7 @@ def run_ours(args):
 
     plain = None
     if not args.no_plain:
-        # the plain single-instance form: one otm_solve call per density
-        tot = 0.0
-        torch.cuda.synchronize()
-        for k in range(B):
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            N.check(N.lib().otm_solve(ctx.handle, n, C.c_void_p(dev_in[k].data_ptr()), C.byref(opt),
-                                      C.c_void_p(dev_out[k].data_ptr()), None, None))
-            b.record(stream)
-            b.synchronize()
-            tot += a.elapsed_time(b)
-        plain = {"value": B / (tot / 1e3), "unit": UNIT, "form": "one otm_solve call per density, same kernels"}
+        plain = bench_plain(local, n, dev_in, dev_out, opt, steps=min(args.steps, 5))
 
     adjoint = None if args.no_adjoint else bench_adjoint(ctx, stream)
     locate = None if args.no_locate else bench_locate(ctx, stream, n, dev_in[0])
@@ -350,8 +338,12 @@ def run_ours(args):
     kernels = kernel_rates(prof, cell_iters, peaks)
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(host[0], n, locate_points=None if args.no_locate else LOCATE_POINTS)
+        cpu, ref_map = cpu_baseline(host[0], n, locate_points=None if args.no_locate else LOCATE_POINTS)
+        if ref_map is not None:
+            parity = parity_vs_reference(ctx, n, ref_map, dev_out[0], st_list[0],
+                                         None if args.no_locate else LOCATE_POINTS)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -360,7 +352,7 @@ def run_ours(args):
                 "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
                 "iterations": iters, "final_residual_max": max(resid), "gpu_launches": launches,
-                "e2e": e2e, "plain": plain, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "e2e": e2e, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:
@@ -373,8 +365,9 @@ def run_ours(args):
 def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
     """Many uneven instances: `count` Gaussian mixtures (4..16 components, floor 1e-3), n
     drawn log-uniformly from {128, 256, 512, 1024}, residual <= 1e-6. Batched = one
-    otm_solve_batch call (device-side graph loop); plain = one otm_solve call per instance
-    with the host-driven loop. Throughput in 1024^2-equivalent solves/s (sum n^2 / 1024^2)."""
+    otm_solve_batch call; plain = one otm_solve call per instance on its own context; both
+    on the device-side graph loop, timed with CUDA events, best of `repeats`. Throughput in
+    1024^2-equivalent solves/s (sum n^2 / 1024^2)."""
     import ctypes as C
 
     import torch
@@ -418,8 +411,9 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
     t_batch = timed(batch, repeats)
     launches = (ctx.launch_count() - l0) // repeats
     iters = [stats[k].iterations for k in range(count)]
+    # plain: one otm_solve call per instance on a separate context (graph loop; its
+    # workspace cache keeps one workspace and captured graph per size), warmed up first
     ctx_plain = N.Context(torch.cuda.current_device())
-    ctx_plain.set_loop(N.LOOP_HOST)
     for n in sorted(set(ns)):
         ctx_plain.init(n)
     stream_p = torch.cuda.ExternalStream(ctx_plain.stream())
@@ -430,11 +424,18 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
                                       C.c_void_p(outs[k].data_ptr()), None, None))
 
     plain()
-    torch.cuda.synchronize()
-    t0 = __import__("time").perf_counter()
-    plain()
-    torch.cuda.synchronize()
-    t_plain = 1e3 * (__import__("time").perf_counter() - t0)
+    best = None
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream_p)
+        plain()
+        b.record(stream_p)
+        b.synchronize()
+        t = a.elapsed_time(b)
+        best = t if best is None else min(best, t)
+    t_plain = best
     ctx.close()
     ctx_plain.close()
     return {"workload": f"{count} Gaussian mixtures, n log-uniform in {{128,256,512,1024}}, residual <= {threshold:g}",
@@ -442,7 +443,8 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
             "batched_ms": t_batch, "batched_value": eq / (t_batch / 1e3), "batched_gpu_launches": launches,
             "plain_ms": t_plain, "plain_value": eq / (t_plain / 1e3),
             "unit": "1024^2-equivalent solves/s", "batched_over_plain": t_plain / t_batch,
-            "plain_timing": "host wall clock around 64 sequential otm_solve calls (each synchronous)",
+            "plain_timing": f"CUDA events around {count} sequential otm_solve calls on a separate warmed-up context "
+                            "(device-side graph loop, one cached workspace per size), best of %d" % repeats,
             "iterations_min_max": [min(iters), max(iters)]}
 
 
@@ -508,11 +510,13 @@ def bench_adjoint(ctx, stream, n=512, repeats=3):
 def cpu_baseline(density_cells, n, locate_points=None):
     """The reference (oracle/_ref, compiled from the reference sources) on one host core;
     with locate_points, also its inversion (BVH build + queries, apply_inverse_map) of that
-    many points and its rasterization of the forward mesh at n x n."""
+    many points and its rasterization of the forward mesh at n x n. Returns the record and
+    the reference's map (for the parity check)."""
     from oracle import ref
 
     if not ref.available():
-        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference", "sample": "unavailable: oracle/_ref not built"}
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}, None
     s = ref.RefSolver()
     t_init = s.init(n)
     m = s.solve(density_cells, threshold=THRESHOLD)
@@ -531,7 +535,85 @@ def cpu_baseline(density_cells, n, locate_points=None):
                          "raster_pixels_per_s": n * n / t_ras, "raster_seconds": t_ras,
                          "sample": f"{locate_points} FP32-drawn points through apply_inverse_map (BVH build "
                                    f"included); rasterize_image of the forward mesh at {n}x{n}; one core"}
+    return out, m
+
+
+def parity_vs_reference(ctx, n, ref_map, gpu_fwd, gpu_stats, locate_points=None):
+    """Outside the timed region: the benchmarked GPU solve of instance 0 against the
+    reference's own FP64 solve of the same density (max vertex error, iteration counts,
+    final residuals); the GPU's inversion of `locate_points` FP32-drawn points and its
+    raster, both on the reference's forward mesh, against the reference's."""
+    import numpy as np
+
+    from oracle import ref
+    from otmap_b200 import otmap as ot
+    from otmap_b200 import workloads as W
+
+    fwd_ref = ref_map.fwd()
+    dens_ref = ref_map.density()
+    g = gpu_fwd.double().cpu().numpy() if hasattr(gpu_fwd, "cpu") else np.asarray(gpu_fwd)
+    out = {"oracle": "the reference library (oracle/_ref, FP64, Eigen SimplicialLDLT) on the same density",
+           "max_vertex_err": float(np.abs(g - fwd_ref).max()),
+           "iterations_gpu": int(gpu_stats.iterations), "iterations_ref": int(ref_map.iterations),
+           "residual_gpu": float(gpu_stats.residual), "residual_ref": float(ref_map.residual)}
+    if locate_points:
+        pts = W.random_points(locate_points, LOCATE_SEED)
+        pos_ref, _ = ref_map.apply_inverse(pts)
+        nh_ref, _, _ = ref.query_all(fwd_ref, n, pts)
+        tm = ot.TransportMap(n, fwd_ref, dens_ref, context=ctx)
+        p = np.ascontiguousarray(pts.copy())
+        nh = np.zeros(p.shape[0], dtype=np.int32)
+        tm.apply_inverse(p, None, nh)
+        ties = nh_ref > 1
+        diff = (p != pos_ref).any(axis=1)
+        img_ref, _ = ref.rasterize(fwd_ref, n, dens_ref, n, n)
+        img = np.empty((n, n))
+        ot.rasterize_image(fwd_ref, dens_ref, img, n=n, context=ctx)
+        out.update({"inverse_points": int(locate_points), "inverse_nhits_mismatch": int((nh != nh_ref).sum()),
+                    "inverse_position_mismatch": int(diff.sum()), "inverse_ties": int(ties.sum()),
+                    "inverse_tie_position_mismatch": int(diff[ties].sum()),
+                    "raster_pixels": n * n, "raster_pixel_mismatch": int((img != img_ref).sum())})
     return out
+
+
+def bench_plain(device, n, dev_in, dev_out, opt, steps=5):
+    """The plain single-instance form: one otm_solve call per density, on its own context
+    (graph loop, workspace and graph warmed up by an untimed pass), CUDA events around
+    each step of len(dev_in) calls; best step."""
+    import ctypes as C
+
+    import torch
+
+    from otmap_b200 import native as N
+
+    ctx = N.Context(device)
+    ctx.init(n)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", device))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def step():
+        for x, y in zip(dev_in, dev_out):
+            N.check(N.lib().otm_solve(ctx.handle, n, C.c_void_p(x.data_ptr()), C.byref(opt), C.c_void_p(y.data_ptr()),
+                                      None, None))
+
+    step()
+    times = []
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        step()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    ctx.close()
+    B = len(dev_in)
+    return {"value": B / (min(times) / 1e3), "unit": UNIT, "ms_per_step_best": min(times),
+            "ms_per_step_median": sorted(times)[len(times) // 2],
+            "form": f"{B} sequential otm_solve calls per step (one density each) on a separate warmed-up context, "
+                    "device-side graph loop, CUDA events; best of %d steps, L2 flushed between steps" % steps}
 
 
 LOCATE_POINTS = 1 << 20
@@ -606,28 +688,28 @@ def bench_locate(ctx, stream, n, dens_dev, repeats=5):
 
 
 def _ref_worker(args_tuple):
-    n, seeds, sample_iters, steps, warmup = args_tuple
+    n, seed, steps, warmup, sample_iters, barrier = args_tuple
     sys.path.insert(0, ROOT)
     from oracle import ref
 
     from otmap_b200 import workloads as W
 
-    dens = [W.to_cells(W.blurred_shapes(n, s, sigma_px=SIGMA_PX)) for s in seeds]
+    d = W.to_cells(W.blurred_shapes(n, seed, sigma_px=SIGMA_PX))
     s = ref.RefSolver()
     s.init(n)
-    full = []
-    for d in dens:  # one full solve per density: iteration count and full-solve time
+    for _ in range(warmup):  # untimed warm-up: a bounded number of iterations each
+        s.solve(d, threshold=THRESHOLD, max_iter=sample_iters)
+    barrier.wait()
+    t0 = time.time()
+    per_step, its, res = [], [], []
+    for _ in range(steps):  # one step = one whole solve of this process's density
+        a = time.perf_counter()
         m = s.solve(d, threshold=THRESHOLD)
-        full.append((m.iterations, m.seconds))
-    per_step = []
-    for k in range(warmup + steps):
-        t0 = time.perf_counter()
-        for d in dens:
-            s.solve(d, threshold=THRESHOLD, max_iter=sample_iters)
-        dt = time.perf_counter() - t0
-        if k >= warmup:
-            per_step.append(dt)
-    return full, per_step
+        per_step.append(time.perf_counter() - a)
+        its.append(m.iterations)
+        res.append(m.residual)
+    t1 = time.time()
+    return t0, t1, per_step, its, res
 
 
 def run_reference(args):
@@ -640,41 +722,39 @@ def run_reference(args):
     total = B * world
     seeds = [1000 * r + k for r in range(world) for k in range(B)]
     cores = len(os.sched_getaffinity(0))
-    # One single-threaded reference process per host core, each on one density of the batch
-    # (densities repeated when there are more cores than densities): the throughput of all
-    # cores on a steady stream of such densities.
+    # One single-threaded reference process per host core (the reference has no threads),
+    # each solving one density of the batch (densities repeat when there are more cores
+    # than densities): the throughput of all cores on a steady stream of such solves.
     P = max(1, min(cores, 32))  # each process holds a factorisation of the n^2 Laplacian
-    groups = [[seeds[p % total]] for p in range(P)]
     ctxm = mp.get_context("spawn")
-    with ctxm.Pool(P) as pool:
-        res = pool.map(_ref_worker, [(n, g, args.sample_iters, args.steps, 1) for g in groups])
-    # per process: estimated full-solve time of its density = sample time scaled by
-    # (full iterations / sampled iterations); solves/s of the step = sum over processes of
-    # 1 / that time
-    rates = []
-    for k in range(args.steps):
-        rate = 0.0
-        for full, per_step in res:
-            scale = sum(min(it, 10 ** 9) for it, _ in full) / (args.sample_iters * len(full))
-            rate += len(full) / (per_step[k] * scale)
-        rates.append(rate)
-    value = statistics.mean(rates)
-    ms_step = 1e3 * total / value
-    full_times = [t for full, _ in res for _, t in full]
-    its = [it for full, _ in res for it, _ in full]
+    with ctxm.Manager() as mgr:
+        barrier = mgr.Barrier(P)
+        with ctxm.Pool(P) as pool:
+            res = pool.map(_ref_worker, [(n, seeds[p % total], args.steps, args.warmup, args.sample_iters, barrier)
+                                         for p in range(P)])
+    t_start = min(r[0] for r in res)
+    t_end = max(r[1] for r in res)
+    wall = t_end - t_start
+    solves = P * args.steps
+    value = solves / wall
+    ms_step = 1e3 * wall / args.steps
+    its = [it for r in res for it in r[3]]
+    per = [t for r in res for t in r[2]]
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
             "config": config(args, world),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": P, "kind": "reference",
-                             "sample": f"the {total} densities spread over {P} processes of the reference "
-                                       f"library (oracle/_ref, Eigen SimplicialLDLT), one per host core; "
-                                       f"each step times {args.sample_iters} iterations per process and scales "
-                                       f"to the full iteration counts {its} measured by one full solve each "
-                                       f"(mean full solve {statistics.mean(full_times):.2f} s); value = sum "
-                                       f"of the processes' solve rates; ms_per_step = {total} solves at that "
-                                       f"rate; init excluded"},
+                             "sample": f"{P} processes of the reference library (oracle/_ref, Eigen "
+                                       f"SimplicialLDLT, single-threaded), one per host core, each solving one "
+                                       f"of the {total} densities; one step = one whole solve per process "
+                                       f"({P} solves), timed from a common barrier to the last process's end; "
+                                       f"value = {solves} solves / {wall:.1f} s wall; iterations {min(its)}-"
+                                       f"{max(its)}, solve time {min(per):.2f}-{max(per):.2f} s; init "
+                                       f"(factorisation) and {args.warmup} warm-up steps of "
+                                       f"{args.sample_iters} iterations excluded"},
+            "timed_wall_s": wall,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 

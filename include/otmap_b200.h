@@ -337,20 +337,26 @@ int otm_set_option(otm_context* ctx, int key, int value);
 
 /* ---- allocation-free solve (no counterpart in the reference) ----
  *
- * For callers that cannot let a library call cudaMalloc: code that runs while a
- * stream is being captured into a CUDA graph, hosts whose own allocator owns all
- * device memory, and latency-critical loops that must stay off the driver's
- * allocator. otm_solve_noalloc does what otm_solve does for one density but
- * allocates nothing: its working memory is a fixed 8 MiB array in the library's
- * device data, which every GPU that loads the library holds until the process
- * exits. Hence the size limit: n <= OTM_NOALLOC_MAX_N (larger n is rejected with
- * OTM_ERR_BAD_ARG).
+ * For callers that cannot let a library call cudaMalloc: hosts whose own allocator has
+ * reserved all device memory up front (a framework's caching pool, an inference server
+ * that partitions HBM at start-up) and processes under a hard device-memory budget, where
+ * a cudaMalloc in the middle of a run can fail or evict something the host owns.
+ * otm_solve_noalloc does what otm_solve does for one density but allocates nothing: its
+ * working memory is a fixed 8 MiB array in the library's device data, which every GPU
+ * that loads the library holds until the process exits. Hence the size limit:
+ * n <= OTM_NOALLOC_MAX_N (larger n is rejected with OTM_ERR_BAD_ARG).
+ *   - It runs the dense-product Poisson solve (C.X.C^T with the cosine basis, O(n^3) work
+ *     per iteration) and the one-tile-per-block stencil kernels, not the fast transforms
+ *     and fused sweeps of otm_solve; results agree with otm_solve to the solver's
+ *     tolerance (same iteration count, positions within 1e-6), not bit for bit.
  *   - Runs on the calling thread's current device, on `stream` (a cudaStream_t;
  *     NULL = the legacy default stream), and returns when the result is written.
  *   - Buffers may be host or device memory, as for otm_solve; no context needed.
+ *   - It is not for use while `stream` is being captured into a CUDA graph: it copies
+ *     from host memory, synchronises the stream and reads the loop state back to the
+ *     host every 4 iterations, none of which a capture allows.
  *   - The first call on each device looks up the array's device address and checks
- *     the cosine basis against the assembled matrix for that n; make that first call
- *     before any stream capture.
+ *     the cosine basis against the assembled matrix for that n.
  *   - All calls on a device share the one array (it keeps the last call's contents;
  *     each call re-initialises what must start at zero): calls that overlap on the
  *     GPU -- from two threads, or on two streams -- race and give wrong results.

@@ -635,6 +635,26 @@ oro_bvh* oro_bvh_build(int n, const double* fwd_xy) {
   return b;
 }
 
+/* The face order the build leaves in its face array (bvh2d.cpp:167-242) and, per face,
+ * the enlarged box of its leaf: faces_out[pos] = face, leaf_box[4 f .. 4 f + 3]. */
+void oro_bvh_order(int n, const double* fwd_xy, int* faces_out, double* leaf_box) {
+  oro_bvh* b = oro_bvh_build(n, fwd_xy);
+  int N = n * n;
+  for (int p = 0; p < N; ++p) faces_out[p] = b->faces[p];
+  for (int k = 0; k < b->nnodes; ++k) {
+    const oro_node* nd = &b->nodes[k];
+    if (!nd->leaf) continue;
+    for (int p = nd->first; p < nd->first + nd->nb; ++p) {
+      int f = b->faces[p];
+      leaf_box[4 * f] = nd->mn[0];
+      leaf_box[4 * f + 1] = nd->mn[1];
+      leaf_box[4 * f + 2] = nd->mx[0];
+      leaf_box[4 * f + 3] = nd->mx[1];
+    }
+  }
+  oro_bvh_free(b);
+}
+
 void oro_bvh_free(oro_bvh* b) {
   if (!b) return;
   free(b->cen);

@@ -56,6 +56,8 @@ int oro_solve(int n, const double* density_in, const oro_options* opt, double* p
 typedef struct oro_bvh oro_bvh;
 oro_bvh* oro_bvh_build(int n, const double* fwd_xy); /* bvh2d.cpp:29-64 with (4, 24) */
 void oro_bvh_free(oro_bvh* b);
+/* the build's final face array and, per face, the enlarged box of its leaf */
+void oro_bvh_order(int n, const double* fwd_xy, int* faces_out, double* leaf_box);
 /* all hits for one point (already clamped by the caller as inv_impl does); returns count,
  * writes up to cap faces / 4 weights in traversal order */
 int oro_bvh_query_all(const oro_bvh* b, const double q[2], int cap, int* faces, double* bary);

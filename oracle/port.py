@@ -54,6 +54,7 @@ def lib():
         L.oro_bvh_build.argtypes = [C.c_int, _dp]
         L.oro_bvh_build.restype = C.c_void_p
         L.oro_bvh_free.argtypes = [C.c_void_p]
+        L.oro_bvh_order.argtypes = [C.c_int, _dp, _ip, _dp]
         L.oro_bvh_query_all.argtypes = [C.c_void_p, _dp, C.c_int, _ip, _dp]
         L.oro_bvh_query_all.restype = C.c_int
         L.oro_bilinear_weights.argtypes = [_dp, _dp, _dp]
@@ -288,3 +289,13 @@ def grid_transport_cost(grads, density, n):
     pf = np.zeros(n * n)
     c = lib().oro_grid_transport_cost(n, _p(_f64(grads)), _p(_f64(density)), _p(pf))
     return c, pf
+
+
+def bvh_order(fwd_xy, n):
+    """The reference BVH's final face array and each face's leaf box (bvh2d.cpp:29-64,
+    167-242, with the (4, 24) of transport_map.cpp:40) -> (faces[pos], leaf_box[f, 4])."""
+    N = n * n
+    faces = np.zeros(N, dtype=np.int32)
+    boxes = np.zeros((N, 4))
+    lib().oro_bvh_order(int(n), _p(_f64(fwd_xy)), faces.ctypes.data_as(_ip), _p(boxes))
+    return faces, boxes

@@ -1,7 +1,6 @@
 """Builds the CUDA library in-tree: otmap_b200/lib/libotmap_b200.so (sm_100a).
 
     python -m otmap_b200.build            # library only
-    python -m otmap_b200.build --all      # library, C++ facade test driver, oracle
 
 nvcc cross-compiles for sm_100a without a GPU. The host compiler is pinned to the
 system g++ so the library links the system libstdc++ dynamically (a statically
@@ -61,17 +60,6 @@ def build_library(verbose: bool = False) -> str:
     return LIB
 
 
-def build_oracle(reference: bool = True) -> None:
-    """The oracle's C restatement and, when the reference sources are present, the
-    reference library (test infrastructure, see oracle/Makefile)."""
-    _run(["make", "-C", os.path.join(ROOT, "oracle"), "oracle"])
-    ref_root = os.environ.get("OTMAP_REFERENCE", "/root/reference")
-    if reference and os.path.isdir(os.path.join(ref_root, "otlib")):
-        _run(["make", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={ref_root}", "-j8"])
-
-
 if __name__ == "__main__":
     build_library(verbose="-v" in sys.argv)
-    if "--all" in sys.argv:
-        build_oracle()
     print(LIB)

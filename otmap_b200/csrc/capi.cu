@@ -201,7 +201,7 @@ extern "C" int otm_set_option(otm_context* ctx, int key, int value) {
     if (ctx->wait_test != value) {
       cudaSetDevice(ctx->device);
       cudaStreamSynchronize(ctx->stream);
-      ctx->ws.drop_graph();  // the captured launches carry the wait parameters
+      for (auto& w : ctx->workspaces) w->drop_graph();  // the captured launches carry the wait parameters
     }
     ctx->wait_test = value;
     return OTM_OK;

@@ -58,7 +58,6 @@ struct Workspace {
   DevBuf col_inst;   // int per column block of the fast transform
   DevBuf partials;   // double[total_tiles * 8]
   DevBuf arena;      // per-instance cell arrays
-  DevBuf host_rec;   // unused placeholder to keep layout stable
   std::vector<unsigned char> h_insts;  // host mirror of Inst[count]
   void* h_pinned = nullptr;            // pinned staging for Inst readback
   size_t h_pinned_bytes = 0;
@@ -114,7 +113,13 @@ struct otm_context {
   int wait_test = 0;     // OTM_OPT_WAIT_TEST: bounded waits made to run out
   otm::Profiler prof;
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
-  otm::Workspace ws;
+  // Workspaces of the most recent batch configurations (size list + Poisson mode), most
+  // recently used first; a call with a configuration seen before reuses its buffers and
+  // its captured loop graph. At most kWorkspaces are kept.
+  static constexpr int kWorkspaces = 6;
+  std::vector<std::unique_ptr<otm::Workspace>> workspaces;
+  otm::Workspace* wsp = nullptr;  // the workspace of the current call
+  otm::Workspace& ws() { return *wsp; }
   otm::DevBuf staging;  // device staging for host inputs/outputs
   // second stream of a batched solve: outputs of instances that stopped while the rest of
   // the batch iterates (created on first use), its staging and a pinned copy of the records
@@ -142,6 +147,8 @@ struct otm_map {
   otm::DevBuf bin_start;  // int[bins*bins + 1]
   otm::DevBuf bin_faces;  // int[entries]
   otm::DevBuf face_box;   // double4 per face (min x, min y, max x, max y)
+  otm::DevBuf bvh_rank;   // int per face: its position in the reference's BVH face array
+  otm::DevBuf leaf_box;   // double4 per face: the enlarged box of its BVH leaf
   otm::DevBuf scratch;
 };
 

@@ -7,10 +7,11 @@
 // of its box and keeps the highest accepting face index per pixel with an integer
 // atomicMax; a per-pixel pass then writes the values. This file is compiled without FMA contraction: the geometric
 // predicates (utils/mesh_utils.cpp:18-88) then round exactly as the reference's
-// scalar x86-64 build does, which makes the located faces, weights, inverse
-// positions and pixel values bit-identical to the reference wherever the
-// reference's own result does not depend on the order of its BVH traversal.
+// scalar x86-64 build does, and the reference's BVH face order and leaf boxes are
+// rebuilt on the GPU (build_bvh_order), which makes the located faces, hit counts,
+// weights, inverse positions and pixel values bit-identical to the reference.
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
@@ -138,17 +139,29 @@ __global__ void k_scan_local(const int* in, int* out, int* block_sums, int count
   if (threadIdx.x == SCAN_B - 1) block_sums[blockIdx.x] = s[threadIdx.x];
 }
 
-// Scans the block sums in place (sequential over at most a few thousand values) and
-// writes the grand total to out[count].
+// Scans the block sums in place (one block of SCAN_B threads, chunks of SCAN_B values
+// with a running carry) and writes the grand total to out[count].
 __global__ void k_scan_sums(int* block_sums, int nblocks, int* out, int count) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  int acc = 0;
-  for (int b = 0; b < nblocks; ++b) {
-    int v = block_sums[b];
-    block_sums[b] = acc;
-    acc += v;
+  __shared__ int s[SCAN_B];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  for (int c0 = 0; c0 < nblocks; c0 += SCAN_B) {
+    const int g = c0 + threadIdx.x;
+    const int v = g < nblocks ? block_sums[g] : 0;
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < SCAN_B; off <<= 1) {
+      int t = threadIdx.x >= off ? s[threadIdx.x - off] : 0;
+      __syncthreads();
+      s[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (g < nblocks) block_sums[g] = carry + s[threadIdx.x] - v;
+    __syncthreads();
+    if (threadIdx.x == SCAN_B - 1) carry += s[threadIdx.x];
+    __syncthreads();
   }
-  out[count] = acc;
+  if (threadIdx.x == 0) out[count] = carry;
 }
 
 __global__ void k_scan_add(int* out, const int* block_sums, int count) {
@@ -159,8 +172,298 @@ __global__ void k_scan_add(int* out, const int* block_sums, int count) {
 static void exclusive_scan(cudaStream_t st, const int* counts, int* starts, int* block_sums, int count) {
   int nb = (count + SCAN_B - 1) / SCAN_B;
   k_scan_local<<<nb, SCAN_B, 0, st>>>(counts, starts, block_sums, count);
-  k_scan_sums<<<1, 32, 0, st>>>(block_sums, nb, starts, count);
+  k_scan_sums<<<1, SCAN_B, 0, st>>>(block_sums, nb, starts, count);
   k_scan_add<<<nb, SCAN_B, 0, st>>>(starts, block_sums, count);
+}
+
+// ---- the reference's BVH face order (utils/bvh2d.cpp:29-64, 165-242) ----
+//
+// The reference's locator is a BVH over face centroids (leaves of <= 4 faces, depth <= 24,
+// TransportMap::init_inverse, transport_map.cpp:36-43). Two of its properties are visible in
+// results: the order of the hits of a point (increasing position in its permuted face
+// array, the order of the depth-first traversal, bvh2d.cpp:94-162), and that a face is
+// only tested where the point lies in the (slightly enlarged) box of the face's leaf.
+// Both follow from the permutation the build leaves in its face array, which is
+// computed here level by level, all nodes of a level at once:
+//   * node box: min / max over its faces' vertices (order-free, exact), enlarged by
+//     2 eps diag + eps; split dimension = the first largest extent, split value =
+//     float(0.5 (max + min)) of the enlarged box (bvh2d.cpp:178-212);
+//   * split() (bvh2d.cpp:167-176) is a two-ended partition. With S the number of
+//     "small" centroids (c < split value) in [start, end), the k-th "big" element from
+//     the left among the first S positions trades places with the k-th small element
+//     from the right among the others -- exactly the pairs its loop swaps -- so prefix
+//     counts give every element's final position. Its return value is start + S, plus
+//     one when the element then at start + S equals the split value, except in the one
+//     loop exit that skips the final scan (last swap at start + S - 2 and start + S);
+//   * leaves: <= 4 faces, level >= 24, or a split that leaves one side empty.
+// Result per face: rank (position in the final face array) and the box of its leaf.
+
+constexpr int BVH_LEAF = 4, BVH_DEPTH = 24;
+
+struct BvhNode {
+  int start, end;
+  int leaf, dim;
+  float sv;
+  int mid, lo, hi;
+  unsigned long long kmin[2], kmax[2];  // order-preserving keys of the box (atomics)
+  double box[4];                        // enlarged box: min x, min y, max x, max y
+};
+
+__device__ __forceinline__ unsigned long long dkey(double x) {
+  unsigned long long u = (unsigned long long)__double_as_longlong(x);
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+__device__ __forceinline__ double dkey_inv(unsigned long long k) {
+  unsigned long long u = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+  return __longlong_as_double((long long)u);
+}
+
+__device__ __forceinline__ void bvh_node_init(BvhNode& b, int start, int end) {
+  b.start = start;
+  b.end = end;
+  b.leaf = 0;
+  b.lo = b.hi = -1;
+  b.kmin[0] = b.kmin[1] = ~0ull;
+  b.kmax[0] = b.kmax[1] = 0ull;
+}
+
+// Face centroids (bvh2d.cpp:44-58: zero + the corners in circulator order, / 4), face
+// boxes, identity permutation, every position in the root node.
+__global__ void k_bvh_init(const double* xy, int n, int* fac, double2* cen, double4* fbox, int* node_of,
+                           BvhNode* root) {
+  const int N = n * n;
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f == 0) bvh_node_init(*root, 0, N);
+  if (f >= N) return;
+  Quad p;
+  int vid[4];
+  load_quad(xy, n, f, p, vid);
+  double cx = 0.0, cy = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    cx += p.x[k];
+    cy += p.y[k];
+  }
+  cen[f] = make_double2(cx / 4, cy / 4);
+  fbox[f] = make_double4(fmin(fmin(p.x[0], p.x[1]), fmin(p.x[2], p.x[3])),
+                         fmin(fmin(p.y[0], p.y[1]), fmin(p.y[2], p.y[3])),
+                         fmax(fmax(p.x[0], p.x[1]), fmax(p.x[2], p.x[3])),
+                         fmax(fmax(p.y[0], p.y[1]), fmax(p.y[2], p.y[3])));
+  fac[f] = f;
+  node_of[f] = 0;
+}
+
+// Node boxes: per position its face box folded into its node's with 64-bit atomics on
+// order-preserving keys; a warp whose positions share one node reduces first.
+__global__ void k_bvh_bbox(int N, const int* node_of, const double4* fbox, BvhNode* nodes) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = p < N ? node_of[p] : -1;
+  double4 b = k >= 0 ? fbox[p] : make_double4(0, 0, 0, 0);
+  const int k0 = __shfl_sync(0xffffffffu, k, 0);
+  if (__all_sync(0xffffffffu, k == k0) && k0 >= 0) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      b.x = fmin(b.x, __shfl_xor_sync(0xffffffffu, b.x, o));
+      b.y = fmin(b.y, __shfl_xor_sync(0xffffffffu, b.y, o));
+      b.z = fmax(b.z, __shfl_xor_sync(0xffffffffu, b.z, o));
+      b.w = fmax(b.w, __shfl_xor_sync(0xffffffffu, b.w, o));
+    }
+    if ((threadIdx.x & 31) != 0) return;
+  } else if (k < 0) {
+    return;
+  }
+  BvhNode& nd = nodes[k];
+  atomicMin(&nd.kmin[0], dkey(b.x));
+  atomicMin(&nd.kmin[1], dkey(b.y));
+  atomicMax(&nd.kmax[0], dkey(b.z));
+  atomicMax(&nd.kmax[1], dkey(b.w));
+}
+
+// Enlarged box, leaf test by size and depth, split dimension and value (bvh2d.cpp:178-212).
+__global__ void k_bvh_decide(BvhNode* nodes, const int* count, int level) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= *count) return;
+  BvhNode& nd = nodes[k];
+  const double mn[2] = {dkey_inv(nd.kmin[0]), dkey_inv(nd.kmin[1])};
+  const double mx[2] = {dkey_inv(nd.kmax[0]), dkey_inv(nd.kmax[1])};
+  double diag[2];
+#pragma unroll
+  for (int c = 0; c < 2; ++c) {
+    diag[c] = mx[c] - mn[c];
+    const double en = diag[c] * (2. * DBL_EPSILON) + DBL_EPSILON;
+    nd.box[c] = mn[c] - en;
+    nd.box[2 + c] = mx[c] + en;
+  }
+  if (nd.end - nd.start <= BVH_LEAF || level >= BVH_DEPTH) {
+    nd.leaf = 1;
+    return;
+  }
+  nd.dim = diag[1] > diag[0] ? 1 : 0;  // Eigen's maxCoeff: the first of equal maxima
+  nd.sv = (float)(0.5 * (nd.box[2 + nd.dim] + nd.box[nd.dim]));
+}
+
+// small[p] = 1 when position p's centroid lies below its (splitting) node's value.
+__global__ void k_bvh_classify(int N, const int* node_of, const double2* cen, const BvhNode* nodes, int* small) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int k = node_of[p];
+  int s = 0;
+  if (k >= 0 && !nodes[k].leaf) {
+    const double2 c = cen[p];
+    s = (nodes[k].dim ? c.y : c.x) < (double)nodes[k].sv ? 1 : 0;
+  }
+  small[p] = s;
+}
+
+// The partition's pairs: big elements among the first S positions (rank from the left)
+// and small elements after them (rank from the right) record their positions by rank.
+__global__ void k_bvh_slots(int N, const int* node_of, const BvhNode* nodes, const int* small, const int* spre,
+                            int* slot_big, int* slot_small) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int k = node_of[p];
+  if (k < 0 || nodes[k].leaf) return;
+  const int start = nodes[k].start, end = nodes[k].end;
+  const int S = spre[end] - spre[start], q = start + S;
+  if (!small[p] && p < q) {
+    slot_big[start + (p - start) - (spre[p] - spre[start])] = p;
+  } else if (small[p] && p >= q) {
+    slot_small[start + spre[end] - spre[p + 1]] = p;
+  }
+}
+
+// Each big element among the first S positions swaps with its partner (one thread per
+// pair, so the swap is race-free).
+__global__ void k_bvh_swap(int N, const int* node_of, const BvhNode* nodes, const int* small, const int* spre,
+                           const int* slot_small, int* fac, double2* cen, double4* fbox) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int k = node_of[p];
+  if (k < 0 || nodes[k].leaf || small[p]) return;
+  const int start = nodes[k].start, end = nodes[k].end;
+  const int S = spre[end] - spre[start];
+  if (p >= start + S) return;
+  const int r = slot_small[start + (p - start) - (spre[p] - spre[start])];
+  const int tf = fac[p];
+  fac[p] = fac[r];
+  fac[r] = tf;
+  const double2 tc = cen[p];
+  cen[p] = cen[r];
+  cen[r] = tc;
+  const double4 tb = fbox[p];
+  fbox[p] = fbox[r];
+  fbox[r] = tb;
+}
+
+// split()'s return value (bvh2d.cpp:175), the no-improvement leaf test (:214-221) and
+// the children, appended to the next level's list.
+__global__ void k_bvh_children(BvhNode* nodes, const int* count, const int* spre, const int* slot_big,
+                               const int* slot_small, const double2* cen, BvhNode* next, int* next_count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= *count) return;
+  BvhNode& nd = nodes[k];
+  if (nd.leaf) return;
+  const int start = nd.start, end = nd.end, len = end - start;
+  const int S = spre[end] - spre[start];
+  int mid;
+  if (S == len) {
+    mid = end;  // no big element: the loop runs to `end` and both branches give end
+  } else {
+    const int q = start + S;
+    const int m = S - (spre[q] - spre[start]);  // swapped pairs
+    const double2 c = cen[q];
+    int eq = (nd.dim ? c.y : c.x) == (double)nd.sv ? 1 : 0;
+    // the loop exits right after its last swap (at q - 2 and q) without the final scan:
+    // it then tests the small element at q - 1 and returns q
+    if (eq && m >= 1 && slot_big[start + m - 1] == q - 2 && slot_small[start + m - 1] == q) eq = 0;
+    mid = q + eq;
+  }
+  nd.mid = mid;
+  if (mid == start || mid == end) {
+    nd.leaf = 1;
+    return;
+  }
+  const int c0 = atomicAdd(next_count, 2);
+  bvh_node_init(next[c0], start, mid);
+  bvh_node_init(next[c0 + 1], mid, end);
+  nd.lo = c0;
+  nd.hi = c0 + 1;
+}
+
+// Positions of leaves are final: record rank and leaf box per face; the others move to
+// their child node.
+__global__ void k_bvh_assign(int N, int* node_of, const BvhNode* nodes, const int* fac, int* rank, double4* lbox) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= N) return;
+  const int k = node_of[p];
+  if (k < 0) return;
+  const BvhNode& nd = nodes[k];
+  if (nd.leaf) {
+    const int f = fac[p];
+    rank[f] = p;
+    lbox[f] = make_double4(nd.box[0], nd.box[1], nd.box[2], nd.box[3]);
+    node_of[p] = -1;
+  } else {
+    node_of[p] = p < nd.mid ? nd.lo : nd.hi;
+  }
+}
+
+// rank[f] and the leaf box of f for the n^2 quads of the forward mesh xy (device).
+static void build_bvh_order(otm_context* ctx, const double* xy, int n, int* rank, double4* lbox) {
+  cudaStream_t st = ctx->stream;
+  const int N = n * n;
+  const int cap = std::min(1 << BVH_DEPTH, 2 * (N / (BVH_LEAF + 1)) + 2);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const int nsums = (N + 1 + SCAN_B - 1) / SCAN_B + 1;
+  const size_t b_fac = al(sizeof(int) * N), b_cen = al(sizeof(double2) * N), b_box = al(sizeof(double4) * N);
+  const size_t b_int = al(sizeof(int) * (N + 1)), b_nodes = al(sizeof(BvhNode) * cap), b_sums = al(sizeof(int) * nsums);
+  DevBuf buf;
+  buf.reserve(b_fac + b_cen + b_box + 5 * b_int + 2 * b_nodes + b_sums + 256);
+  char* q = buf.as<char>();
+  auto take = [&](size_t b) {
+    char* r = q;
+    q += b;
+    return r;
+  };
+  int* fac = reinterpret_cast<int*>(take(b_fac));
+  double2* cen = reinterpret_cast<double2*>(take(b_cen));
+  double4* fbox = reinterpret_cast<double4*>(take(b_box));
+  int* node_of = reinterpret_cast<int*>(take(b_int));
+  int* small = reinterpret_cast<int*>(take(b_int));
+  int* spre = reinterpret_cast<int*>(take(b_int));
+  int* slot_big = reinterpret_cast<int*>(take(b_int));
+  int* slot_small = reinterpret_cast<int*>(take(b_int));
+  BvhNode* lists[2] = {reinterpret_cast<BvhNode*>(take(b_nodes)), reinterpret_cast<BvhNode*>(take(b_nodes))};
+  int* sums = reinterpret_cast<int*>(take(b_sums));
+  int* counts = reinterpret_cast<int*>(take(256));  // node count of the current and next list
+  const int one = 1;
+  OTM_CUDA(cudaMemcpyAsync(counts, &one, sizeof(int), cudaMemcpyHostToDevice, st));
+  const unsigned ge = (unsigned)((N + 255) / 256);
+  launch(ctx, "bvh_init", k_bvh_init, ge, 256, xy, n, fac, cen, fbox, node_of, lists[0]);
+  for (int level = 0; level <= BVH_DEPTH; ++level) {
+    BvhNode* cur = lists[level & 1];
+    BvhNode* nxt = lists[(level + 1) & 1];
+    int* ccount = counts + (level & 1);
+    int* ncount = counts + ((level + 1) & 1);
+    const int ncap = std::min(level < 30 ? (1 << level) : cap, cap);
+    const unsigned gn = (unsigned)((ncap + 255) / 256);
+    OTM_CUDA(cudaMemsetAsync(ncount, 0, sizeof(int), st));
+    launch(ctx, "bvh_bbox", k_bvh_bbox, ge, 256, N, (const int*)node_of, (const double4*)fbox, cur);
+    launch(ctx, "bvh_decide", k_bvh_decide, gn, 256, cur, (const int*)ccount, level);
+    launch(ctx, "bvh_classify", k_bvh_classify, ge, 256, N, (const int*)node_of, (const double2*)cen,
+           (const BvhNode*)cur, small);
+    exclusive_scan(st, small, spre, sums, N);
+    ctx->launches += 3;
+    launch(ctx, "bvh_slots", k_bvh_slots, ge, 256, N, (const int*)node_of, (const BvhNode*)cur, (const int*)small,
+           (const int*)spre, slot_big, slot_small);
+    launch(ctx, "bvh_swap", k_bvh_swap, ge, 256, N, (const int*)node_of, (const BvhNode*)cur, (const int*)small,
+           (const int*)spre, (const int*)slot_small, fac, cen, fbox);
+    launch(ctx, "bvh_children", k_bvh_children, gn, 256, cur, (const int*)ccount, (const int*)spre,
+           (const int*)slot_big, (const int*)slot_small, (const double2*)cen, nxt, ncount);
+    launch(ctx, "bvh_assign", k_bvh_assign, ge, 256, N, node_of, (const BvhNode*)cur, (const int*)fac, rank, lbox);
+  }
+  OTM_CUDA(cudaGetLastError());
+  OTM_CUDA(cudaStreamSynchronize(st));  // the scratch is released on return
 }
 
 // ---- point location (TransportMap::init_inverse / inv_impl) ----
@@ -217,12 +520,16 @@ __global__ void k_bin_fill(const double* xy, int n, int B, const int* starts, in
 
 constexpr int MAXHITS = 8;
 
-// inv_impl (transport_map.cpp:50-102) per point. Hits are taken in increasing face
-// order; with several hits the reference keeps the weights of its first hit and the
-// face of the densest later one (transport_map.cpp:70-85), which is reproduced.
+// inv_impl (transport_map.cpp:50-102) per point. A face of the point's bin is a hit
+// when the point lies in the box of the face's BVH leaf (the reference only reaches
+// faces through their leaf, bvh2d.cpp:148-161) and passes the face tests of
+// bvh2d.cpp:117-142; hits are ordered by the face's position in the reference's BVH face
+// array, its traversal order. With several hits the reference keeps the weights of its
+// first hit and the face of the densest later one (transport_map.cpp:70-85); the
+// first-hit mode (inv_fast, bvh2d.cpp:66-81) keeps the first.
 __global__ void k_inverse(const double* xy, const double* density, int n, int B, const int* starts,
-                          const int* faces, const double4* boxes, double* pts, long P, int first_hit, int* face_out,
-                          int* nhits_out, unsigned long long* missing) {
+                          const int* faces, const double4* boxes, const int* rank, const double4* lbox, double* pts,
+                          long P, int first_hit, int* face_out, int* nhits_out, unsigned long long* missing) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   double qx = fmin(fmax(pts[2 * i], 0.), 1.);
@@ -232,13 +539,15 @@ __global__ void k_inverse(const double* xy, const double* density, int n, int B,
   int bx = (int)fmin(floor(qx * (double)B), (double)(B - 1));
   int by = (int)fmin(floor(qy * (double)B), (double)(B - 1));
   int b = by * B + bx;
-  int hf[MAXHITS];
+  int hf[MAXHITS], hr[MAXHITS];
   double hw[MAXHITS][4];
   int nh = 0;
   for (int k = starts[b]; k < starts[b + 1]; ++k) {
     int f = faces[k];
     double4 bb = boxes[f];
     if (qx < bb.x || qx > bb.z || qy < bb.y || qy > bb.w) continue;
+    const double4 lb = lbox[f];
+    if (!(lb.x <= qx && lb.y <= qy && qx <= lb.z && qy <= lb.w)) continue;  // AlignedBox::contains
     Quad p;
     int vid[4];
     load_quad(xy, n, f, p, vid);
@@ -246,19 +555,22 @@ __global__ void k_inverse(const double* xy, const double* density, int n, int B,
     if (!inside_quad(qx, qy, p)) continue;
     if (!bilinear_weights(qx, qy, p, w)) continue;
     if (!weights_inside(w)) continue;
-    // insertion in increasing face order
+    // insertion in increasing BVH position
+    const int rk = rank[f];
     int pos = nh < MAXHITS ? nh : MAXHITS - 1;
-    if (nh >= MAXHITS && f > hf[MAXHITS - 1]) {
+    if (nh >= MAXHITS && rk > hr[MAXHITS - 1]) {
       ++nh;
       continue;
     }
-    while (pos > 0 && hf[pos - 1] > f) {
+    while (pos > 0 && hr[pos - 1] > rk) {
       hf[pos] = hf[pos - 1];
+      hr[pos] = hr[pos - 1];
 #pragma unroll
       for (int c = 0; c < 4; ++c) hw[pos][c] = hw[pos - 1][c];
       --pos;
     }
     hf[pos] = f;
+    hr[pos] = rk;
 #pragma unroll
     for (int c = 0; c < 4; ++c) hw[pos][c] = w[c];
     ++nh;
@@ -604,7 +916,9 @@ static void build_locator(otm_map* m) {
   launch(ctx, "bin_fill", k_bin_fill, (N + 255) / 256, 256, xy, n, B, (const int*)m->bin_start.as<int>(),
          counts.as<int>(), m->bin_faces.as<int>());
   OTM_CUDA(cudaGetLastError());
-  OTM_CUDA(cudaStreamSynchronize(st));
+  m->bvh_rank.reserve(sizeof(int) * N);
+  m->leaf_box.reserve(sizeof(double4) * N);
+  build_bvh_order(ctx, xy, n, m->bvh_rank.as<int>(), m->leaf_box.as<double4>());
   m->located = true;
 }
 
@@ -684,7 +998,8 @@ extern "C" int otm_map_inverse_mode(otm_map* m, double* points, long count, int 
     unsigned grid = (unsigned)((count + 255) / 256);
     launch(ctx, "inverse", k_inverse, grid, 256, (const double*)m->fwd.as<double>(),
            (const double*)m->density.as<double>(), m->n, m->bins, (const int*)m->bin_start.as<int>(),
-           (const int*)m->bin_faces.as<int>(), (const double4*)m->face_box.as<double4>(), dp, (long)count,
+           (const int*)m->bin_faces.as<int>(), (const double4*)m->face_box.as<double4>(),
+           (const int*)m->bvh_rank.as<int>(), (const double4*)m->leaf_box.as<double4>(), dp, (long)count,
            mode == OTM_INV_FIRST ? 1 : 0, df, dh, dm);
     OTM_CUDA(cudaGetLastError());
     if (!pdev) OTM_CUDA(cudaMemcpyAsync(points, dp, bp, cudaMemcpyDeviceToHost, st));

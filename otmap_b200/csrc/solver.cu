@@ -6,22 +6,24 @@
 // (Inst) and returns at once when that instance has stopped, so instances of
 // different sizes converge independently inside the same launches.
 //
-// Per iteration (otsolver_2dgrid.cpp:160-220):
-//   k_dct_gemm x4   d_hat = M^+ r_k: orthonormal 2-D DCT-II, divide by the
-//                   eigenvalues of the reference's pseudo-Laplacian, inverse DCT
-//                   (:175-179; the (0,0) mode is dropped = mean-zero projection)
-//   k_beta          |d_hat| (early exit, :182) and the conjugate-Jacobian beta:
-//                   residual at psi - (alpha/2) d_hat (:248-261)
-//   k_coeffs        d = d_hat + beta d_prev, line coefficients a, b per cell and the
-//                   five quartic sums; the last block solves the cubic (:541-595)
-//   k_update        psi += alpha d, r += alpha b + alpha^2 a (:599-605); the last
-//                   block advances the iteration and tests convergence (:160)
-// Stencil kernels stage a (TI+2) x (TJ+2) halo tile of the potential in shared
-// memory, derive the (TI+1) x (TJ+1) vertex gradients there (never stored) and
-// finish with a fixed-order block reduction; the last block of an instance (atomic
-// ticket) reduces the per-tile partials in tile order, so every reduction is
-// run-to-run deterministic. All arithmetic is FP64, compiled without FMA
-// contraction so each cell's operations round as the reference's scalar code does.
+// Per iteration (otsolver_2dgrid.cpp:160-220), for every active instance:
+//   d_hat = M^+ r_k    the cosine-transform Poisson solve (:175-179): register FFT
+//                      transforms (dct_reg.cu) for power-of-two n in 64..1024, shared-
+//                      memory FFTs (poisson.cu) for other powers of two, dense products
+//                      with the cosine basis (k_dct_gemm here) for any other n
+//   k_sweep_sums       |d_hat| (early exit, :182), beta (:248-261) and the quartic of the
+//                      line search; its last block solves the cubic (:541-595)
+//   k_sweep_update     d = d_hat + beta d_prev, psi += alpha d, r += alpha b + alpha^2 a
+//                      (:599-605); its last block advances the iteration and tests the
+//                      loop condition (:160)
+// (stencil.cu). By default the iteration is the body of a device-side WHILE loop in one
+// CUDA graph launch. Set-up (density normalisation, initial residual) and the forward
+// mesh are tile kernels below. k_beta / k_coeffs / k_update are the earlier one-tile-per-
+// block form of the two sweeps, kept for the allocation-free solve at the end of this
+// file. Every reduction is fixed-order (per-block partials, reduced in block order by the
+// last block of the instance), so results are run-to-run identical. All arithmetic is
+// FP64, compiled without FMA contraction so each cell's operations round as the
+// reference's scalar code does.
 
 #include <cfloat>
 #include <cmath>
@@ -533,7 +535,6 @@ static int gemm_tiles_of(int n) {
 // Lays out (or reuses) the workspace for a list of sizes and returns host copies of
 // the instance records with buffer pointers filled in.
 static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<int>& sizes) {
-  Workspace& ws = ctx->ws;
   const int count = (int)sizes.size();
   std::vector<Inst> h(count);
   size_t cells = 0;
@@ -601,7 +602,24 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
       segs.back().ccnt += I.ncol;
     }
   }
-  bool same = ws.sizes == sizes && ws.mode == ctx->poisson_mode;
+  // the workspace of this configuration: a cached one, else a new one (evicting the least
+  // recently used)
+  bool same = false;
+  {
+    auto& W = ctx->workspaces;
+    size_t hit = W.size();
+    for (size_t k = 0; k < W.size(); ++k)
+      if (W[k]->sizes == sizes && W[k]->mode == ctx->poisson_mode) hit = k;
+    if (hit < W.size()) {
+      std::rotate(W.begin(), W.begin() + hit, W.begin() + hit + 1);
+      same = true;
+    } else {
+      if ((int)W.size() >= otm_context::kWorkspaces) W.pop_back();
+      W.insert(W.begin(), std::make_unique<Workspace>());
+    }
+    ctx->wsp = W.front().get();
+  }
+  Workspace& ws = ctx->ws();
   if (!same) {
     ws.drop_graph();
     ws.insts.reserve(sizeof(Inst) * count);
@@ -705,7 +723,7 @@ __global__ void k_loop_check(const Inst* insts, int count, LoopCtl* ctl, cudaGra
 
 // Launches one iteration of every active instance (Poisson solve + the two sweeps).
 static void launch_iteration(otm_context* ctx, Inst* d_insts) {
-  Workspace& ws = ctx->ws;
+  Workspace& ws = ctx->ws();
   const int G = ws.total_gemm;
   if (G > 0)
     for (int s = 0; s < 4; ++s)
@@ -723,7 +741,7 @@ static void launch_iteration(otm_context* ctx, Inst* d_insts) {
 
 // Captures the iteration loop of the current workspace into a graph with a WHILE node.
 static void build_loop_graph(otm_context* ctx, int count) {
-  Workspace& ws = ctx->ws;
+  Workspace& ws = ctx->ws();
   cudaStream_t st = ctx->stream;
   sweep_attrs(ctx->device);
   dct_reg_attrs(ctx->device);
@@ -773,7 +791,7 @@ static void build_loop_graph(otm_context* ctx, int count) {
 static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, const otm_solver_options& o,
                                     const std::function<void(int)>* stopped = nullptr,
                                     std::vector<char>* done = nullptr) {
-  Workspace& ws = ctx->ws;
+  Workspace& ws = ctx->ws();
   cudaStream_t st = ctx->stream;
   const int count = (int)h.size();
   for (auto& I : h) {
@@ -989,7 +1007,7 @@ extern "C" int otm_solve_batch(otm_context* ctx, int count, const int* ns, const
     std::vector<Inst> h = layout_workspace(ctx, sizes);
     for (int q = 0; q < count; ++q)
       copy_in(ctx, h[q].rho, density[q], sizeof(double) * (size_t)sizes[q] * sizes[q]);
-    Inst* d_insts = ctx->ws.insts.as<Inst>();
+    Inst* d_insts = ctx->ws().insts.as<Inst>();
     // Host outputs of a batch on the device loop: the mesh of an instance that has stopped
     // is formed and copied out on a second stream while the others still iterate.
     bool early = count > 1 && ctx->loop_mode == OTM_LOOP_GRAPH && !ctx->prof.on;
@@ -1063,16 +1081,18 @@ extern "C" int otm_solve(otm_context* ctx, int n, const double* density, const o
 // ---------------------------------------------------------------------------
 // Allocation-free solve.
 //
-// Some callers cannot let a library call cudaMalloc: code that runs while a stream
-// is being captured into a CUDA graph (an allocation there breaks or is refused by
-// the capture), hosts that hand every byte of device memory to their own allocator
-// and forbid other allocations, and latency-critical loops that must not hit the
-// driver's allocator. otm_solve_noalloc serves them: it runs the same kernels as
-// otm_solve, but its working memory -- instance record, work lists, partial sums,
-// cosine tables and the per-cell arrays -- lives in one file-scope device array of
-// fixed size, so the call allocates nothing. That array is held by every GPU that
-// loads the library until the process exits, which is why it is kept modest: it
-// bounds the grid size to OTM_NOALLOC_MAX_N.
+// Some callers cannot let a library call cudaMalloc: hosts whose own allocator has
+// reserved all device memory at start-up, and processes under a hard device-memory
+// budget where an allocation in mid-run can fail. otm_solve_noalloc serves them: its
+// working memory -- instance record, work lists, partial sums, cosine tables and the
+// per-cell arrays -- lives in one file-scope device array of fixed size, so the call
+// allocates nothing. That array is held by every GPU that loads the library until the
+// process exits, which is why it is kept modest: it bounds the grid size to
+// OTM_NOALLOC_MAX_N. The solve runs the dense-product Poisson solve (k_dct_gemm, O(n^3)
+// per iteration) and the one-tile-per-block stencil kernels k_beta / k_coeffs /
+// k_update, whose work lists fit the array for any n up to that bound; it matches
+// otm_solve to the solver's tolerance, not bit for bit. It synchronises the stream and
+// reads the loop state back every 4 iterations, so it cannot run inside a stream capture.
 
 namespace otm {
 

@@ -1,6 +1,6 @@
 """A short, fixed solve for kernel profiling (ncu) and quick timing.
 
-    python -m otmap_b200.profile_case [--n 1024] [--batch 2] [--iters 3] [--poisson fft|dense]
+    python tests/profile_case.py [--n 1024] [--batch 2] [--iters 3] [--poisson fft|dense]
 
 Solves `batch` blurred-shape densities of size n for a fixed number of iterations
 (max_iter = iters, so every instance runs exactly that many) through the C ABI, with
@@ -13,8 +13,12 @@ from __future__ import annotations
 import argparse
 import ctypes as C
 import json
+import os
+import sys
 
 import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 
 
 def main():
@@ -28,8 +32,8 @@ def main():
 
     import torch
 
-    from . import native as N
-    from . import workloads as W
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
 
     ctx = N.Context(0)
     ctx.set_poisson(N.POISSON_FFT if a.poisson == "fft" else N.POISSON_DENSE)

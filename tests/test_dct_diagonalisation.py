@@ -5,7 +5,7 @@ DCT pseudo-inverse. The GPU Poisson solve relies on both facts."""
 import numpy as np
 import pytest
 
-from otmap_b200 import dct
+import dct_tables as dct
 
 
 @pytest.mark.parametrize("n", [1, 2, 3, 8, 17, 32, 64])

@@ -39,8 +39,11 @@ def test_facade_builds_without_eigen_and_runs_host_calls(tmp_path):
 
 
 def test_facade_builds_with_eigen(tmp_path):
-    eigen = os.environ.get("OTMAP_REFERENCE", "/root/reference") + "/extern"
-    if not os.path.exists(os.path.join(eigen, "Eigen", "Core")):
+    from oracle.build import reference_root
+
+    root = reference_root()
+    eigen = os.path.join(root, "extern") if root else ""
+    if not root or not os.path.exists(os.path.join(eigen, "Eigen", "Core")):
         pytest.skip("no Eigen headers here")
     exe = facade_build.build(str(tmp_path), eigen_include=eigen)
     r = subprocess.run([exe, "mesh", str(tmp_path)], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)

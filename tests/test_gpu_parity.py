@@ -13,6 +13,24 @@ pytestmark = pytest.mark.gpu
 POS_TOL = 1e-6
 
 
+def chosen_faces(hits, nhits, density):
+    """The face inv_impl keeps (transport_map.cpp:70-85): the first hit, replaced by a
+    later hit whose density exceeds `best_area`, which holds the first hit's density and,
+    after a replacement, the comparison's bool. Hits are in the reference's BVH order."""
+    out = np.full(len(nhits), -1, dtype=np.int64)
+    for i, nh in enumerate(nhits):
+        if nh == 0:
+            continue
+        f = hits[i, 0]
+        best = density[f]
+        for k in range(1, min(nh, hits.shape[1])):
+            if density[hits[i, k]] > best:
+                f = hits[i, k]
+                best = float(density[hits[i, k]] > best)
+        out[i] = f
+    return out
+
+
 @pytest.fixture(scope="module")
 def ot():
     from otmap_b200 import otmap
@@ -85,14 +103,16 @@ def test_inverse_bit_exact(name, ot):
     missing = tm.apply_inverse(pts, face, nh)
     assert np.array_equal(nh, g["nhits"])
     assert missing == int((g["nhits"] == 0).sum())
-    one = g["nhits"] == 1
-    assert np.array_equal(face[one], g["faces"][one, 0])
-    assert np.array_equal(pts[one], g["inverse"][one])
+    hit = g["nhits"] > 0
+    chosen = chosen_faces(g["faces"], g["nhits"], s["adjusted"])
+    assert np.array_equal(face[hit], chosen[hit])
+    assert np.array_equal(pts[hit], g["inverse"][hit])
 
 
 def test_inverse_random_points_1024_shapes(ot, oracle_port):
-    """Forward mesh of an oracle solve at 128^2; 2^16 random FP32 points; bit-exact
-    against the oracle's restatement of the reference BVH query."""
+    """Forward mesh of an oracle solve at 128^2; 2^16 random FP32 points; hit counts,
+    located faces and positions bit-exact against the oracle's restatement of the
+    reference BVH query, points inside several faces included."""
     from otmap_b200 import workloads as W
 
     n = 128
@@ -106,9 +126,48 @@ def test_inverse_random_points_1024_shapes(ot, oracle_port):
     nh = np.zeros(p.shape[0], dtype=np.int32)
     tm.apply_inverse(p, face, nh)
     assert np.array_equal(nh, nh_o)
-    one = nh_o == 1
-    assert np.array_equal(face[one], face_o[one])
-    assert np.array_equal(p[one], pos_o[one])
+    assert np.array_equal(face, face_o)
+    assert np.array_equal(p, pos_o)
+
+
+def test_inverse_ties_at_mesh_vertices_and_edges(ot, oracle_port):
+    """Points inside several faces: the forward mesh's own vertices (shared by up to four
+    faces) and the midpoints of its edges. Hit counts, chosen faces (first hit's weights,
+    densest later face, in the reference's BVH order) and positions bit-exact against the
+    oracle, and against the reference itself when it is built."""
+    from oracle import ref
+    from otmap_b200 import workloads as W
+
+    n = 64
+    d = W.to_cells(W.gaussian_mixture(n, 12))
+    o = oracle_port.solve(d, n)
+    V = o.fwd.reshape(n + 1, n + 1, 2)
+    mids = np.concatenate([(0.5 * (V[1:, :] + V[:-1, :])).reshape(-1, 2), (0.5 * (V[:, 1:] + V[:, :-1])).reshape(-1, 2)])
+    pts = np.ascontiguousarray(np.concatenate([o.fwd, mids]))
+    pos_o, face_o, nh_o, _ = oracle_port.apply_inverse(o.fwd, o.density, n, pts)
+    assert (nh_o > 1).sum() > 1000  # the case under test
+    tm = ot.TransportMap(n, o.fwd, o.density)
+    p = pts.copy()
+    face = np.zeros(p.shape[0], dtype=np.int32)
+    nh = np.zeros(p.shape[0], dtype=np.int32)
+    tm.apply_inverse(p, face, nh)
+    assert np.array_equal(nh, nh_o)
+    assert np.array_equal(face, face_o)
+    assert np.array_equal(p, pos_o)
+    if ref.available():
+        rs = ref.RefSolver()
+        rs.init(n)
+        rm = rs.solve(d)
+        tm2 = ot.TransportMap(n, rm.fwd(), rm.density())
+        V2 = rm.fwd().reshape(n + 1, n + 1, 2)
+        pts2 = np.ascontiguousarray(np.concatenate([rm.fwd(), (0.5 * (V2[1:, :] + V2[:-1, :])).reshape(-1, 2)]))
+        pos_r, _ = rm.apply_inverse(pts2)
+        nh_r, _, _ = ref.query_all(rm.fwd(), n, pts2)
+        q = pts2.copy()
+        nh2 = np.zeros(q.shape[0], dtype=np.int32)
+        tm2.apply_inverse(q, None, nh2)
+        assert np.array_equal(nh2, nh_r)
+        assert np.array_equal(q, pos_r)
 
 
 @pytest.mark.parametrize("name", golden_names("raster_"))
