@@ -54,6 +54,10 @@ def parse():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
     p.add_argument("--no-mixed", action="store_true")
+    p.add_argument("--precision", default="split", choices=["split", "fp64"],
+                   help="headline arithmetic: split (FP32 integration and transforms with FP64 sums, "
+                        "line search and potential; the single-solve workload's stated precision) or fp64")
+    p.add_argument("--no-other-precision", action="store_true")
     p.add_argument("--no-locate", action="store_true")
     p.add_argument("--mixed-count", type=int, default=64)
     p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations per warm-up step")
@@ -173,8 +177,14 @@ class Clocks:
 #   dct_* / fft_* one pass of the cosine transform: reads + writes a line    2 x 8 B
 # Every active instance runs each kernel once per iteration, so the cells a kernel
 # touched over the timed steps are sum over instances of iterations x n^2 (x steps).
+# Split precision (FP32 r, d_hat, d and transform temporaries; FP64 psi):
+#   sweep32_sums    psi 8 + d_hat, d_prev, r_k, r_{k-1} 4 each                    24 B
+#   sweep32_update  reads psi 8, d_hat, d_prev, r_k 4 each; writes psi' 8, d 4, r' 4  36 B
+#   dct32_*         one pass of the FP32 cosine transform                          8 B
 ALG_BYTES_PER_CELL = {"sweep_sums": 40, "sweep_update": 56, "dct_rows_fwd": 16, "dct_cols": 16, "dct_rows_inv": 16,
-                      "fft_rows_fwd": 16, "fft_cols": 16, "fft_rows_inv": 16}
+                      "fft_rows_fwd": 16, "fft_cols": 16, "fft_rows_inv": 16,
+                      "sweep32_sums": 24, "sweep32_update": 36, "dct32_rows_fwd": 8, "dct32_cols": 8,
+                      "dct32_rows_inv": 8}
 
 
 def load_traffic():
@@ -244,25 +254,16 @@ def run_ours(args):
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
-    ctx = N.Context(local)
-    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
     n, B = args.n, args.batch
     ns = [n] * B
     host = densities(n, B, rank_first_seed(rank))
     dev_in = [torch.from_numpy(d).cuda() for d in host]
     V = (n + 1) ** 2
-    dev_out = [torch.empty((V, 2), dtype=torch.float64, device="cuda") for _ in range(B)]
     opt = N.default_options()
     opt.threshold = THRESHOLD
-    stats = (N.SolveStatsC * B)()
     ns_c = (C.c_int * B)(*ns)
-
-    def solve_batch(inp, out):
-        dp = (C.c_void_p * B)(*[x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data for x in inp])
-        fp = (C.c_void_p * B)(*[x.data_ptr() if hasattr(x, "data_ptr") else x.ctypes.data for x in out])
-        N.check(N.lib().otm_solve_batch(ctx.handle, B, ns_c, dp, C.byref(opt), fp, None, stats))
-
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    prec_of = {"split": N.PRECISION_SPLIT, "fp64": N.PRECISION_FP64}
 
     def barrier():
         if world > 1:
@@ -270,67 +271,95 @@ def run_ours(args):
 
             dist.barrier()
 
-    def timed(inp, out, steps, profile=False):
-        ctx.profile(-1)
-        ctx.profile(1 if profile else 0)
-        total = 0.0
-        launches0 = ctx.launch_count()
-        barrier()
-        torch.cuda.synchronize()
-        for _ in range(steps):
-            flush.fill_(1.0)  # L2 flush between steps (outside the events)
+    def measure(precision, with_e2e, with_profile, with_clocks):
+        """One precision: warm-up, the timed steps (device-resident), optionally a profiled
+        pass (host loop, per-kernel events) and the end-to-end pass (pinned host buffers)."""
+        ctx = N.Context(local)
+        ctx.set_precision(prec_of[precision])
+        stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
+        dev_out = [torch.empty((V, 2), dtype=torch.float64, device="cuda") for _ in range(B)]
+        stats = (N.SolveStatsC * B)()
+
+        def solve_batch(inp, out):
+            dp = (C.c_void_p * B)(*[x.data_ptr() for x in inp])
+            fp = (C.c_void_p * B)(*[x.data_ptr() for x in out])
+            N.check(N.lib().otm_solve_batch(ctx.handle, B, ns_c, dp, C.byref(opt), fp, None, stats))
+
+        def timed(inp, out, steps, profile=False):
+            ctx.profile(-1)
+            ctx.profile(1 if profile else 0)
+            total = 0.0
+            launches0 = ctx.launch_count()
+            barrier()
             torch.cuda.synchronize()
-            a = torch.cuda.Event(enable_timing=True)
-            b = torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            solve_batch(inp, out)
-            b.record(stream)
-            b.synchronize()
-            total += a.elapsed_time(b)
-        torch.cuda.synchronize()
-        barrier()
-        launches = ctx.launch_count() - launches0
-        prof = ctx.profile_totals() if profile else None
-        ctx.profile(0)
-        return total, launches, prof
+            for _ in range(steps):
+                flush.fill_(1.0)  # L2 flush between steps (outside the events)
+                torch.cuda.synchronize()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                solve_batch(inp, out)
+                b.record(stream)
+                b.synchronize()
+                total += a.elapsed_time(b)
+            torch.cuda.synchronize()
+            barrier()
+            launches = ctx.launch_count() - launches0
+            prof = ctx.profile_totals() if profile else None
+            ctx.profile(0)
+            return total, launches, prof
 
-    for k in range(B):
         ctx.init(n)
-    for _ in range(args.warmup):
-        solve_batch(dev_in, dev_out)
-    torch.cuda.synchronize()
+        for _ in range(args.warmup):
+            solve_batch(dev_in, dev_out)
+        torch.cuda.synchronize()
+        clocks = Clocks(local) if with_clocks else None
+        if clocks:
+            clocks.start()
+        t_ms, launches, _ = timed(dev_in, dev_out, args.steps)
+        clk = clocks.stop() if clocks else None
+        st_list = [stats[k] for k in range(B)]
+        prof = None
+        if with_profile:
+            # per-kernel CUDA-event timing needs the host-driven loop (events around each
+            # launch): a second pass over the same steps, for the kernel breakdown only
+            _, _, prof = timed(dev_in, dev_out, args.steps, profile=True)
+        t_ms = max_over_ranks(t_ms, world)
+        ms_step = t_ms / args.steps
+        rec = {"precision": precision, "value": job_value(B, world, ms_step), "ms_per_step": ms_step,
+               "iterations": [s.iterations for s in st_list],
+               "final_residual_max": max(s.residual for s in st_list), "gpu_launches": launches}
+        if with_e2e:
+            h_in = [torch.from_numpy(d).pin_memory() for d in host]
+            h_out = [torch.empty((V, 2), dtype=torch.float64).pin_memory() for _ in range(B)]
+            e_ms, _, _ = timed(h_in, h_out, args.steps)
+            e_ms = max_over_ranks(e_ms, world)
+            rec["e2e"] = {"value": job_value(B, world, e_ms / args.steps), "unit": UNIT,
+                          "h2d_bytes_per_step": B * n * n * 8, "d2h_bytes_per_step": B * V * 2 * 8}
+        ctx.close()
+        return rec, dev_out, st_list, prof, clk
 
-    clocks = Clocks(local)
-    clocks.start()
-    t_ms, launches, _ = timed(dev_in, dev_out, args.steps, profile=False)
-    clk = clocks.stop()
-    # per-kernel CUDA-event timing needs the host-driven loop (events around each launch):
-    # a second pass over the same steps, used only for the kernel breakdown and roofline
-    _, _, prof = timed(dev_in, dev_out, args.steps, profile=True)
-
-    t_ms = max_over_ranks(t_ms, world)
-    ms_step = t_ms / args.steps
-    value = job_value(B, world, ms_step)
-    st_list = [stats[k] for k in range(B)]
-    iters = [s.iterations for s in st_list]
-    resid = [s.residual for s in st_list]
-
-    e2e = None
-    if not args.no_e2e:
-        h_in = [torch.from_numpy(d).pin_memory() for d in host]
-        h_out = [torch.empty((V, 2), dtype=torch.float64).pin_memory() for _ in range(B)]
-        e_ms, _, _ = timed(h_in, h_out, args.steps)
-        e_ms = max_over_ranks(e_ms, world)
-        e2e = {"value": job_value(B, world, e_ms / args.steps), "unit": UNIT,
-               "h2d_bytes_per_step": B * n * n * 8, "d2h_bytes_per_step": B * V * 2 * 8}
+    head, dev_out, st_list, prof, clk = measure(args.precision, not args.no_e2e, True, True)
+    other = None
+    other_out = None
+    if not args.no_other_precision:
+        oprec = "fp64" if args.precision == "split" else "split"
+        other, other_out, other_st, _, _ = measure(oprec, not args.no_e2e, False, False)
+    value, ms_step, launches = head["value"], head["ms_per_step"], head["gpu_launches"]
+    e2e = head.get("e2e")
+    ctx = N.Context(local)
+    ctx.set_precision(prec_of[args.precision])
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
 
     plain = None
     if not args.no_plain:
-        plain = bench_plain(local, n, dev_in, dev_out, opt, steps=min(args.steps, 5))
+        plain = bench_plain(local, n, dev_in, [torch.empty((V, 2), dtype=torch.float64, device="cuda")
+                                               for _ in range(B)], opt, prec_of[args.precision],
+                            steps=min(args.steps, 5))
 
     adjoint = None if args.no_adjoint else bench_adjoint(ctx, stream)
     locate = None if args.no_locate else bench_locate(ctx, stream, n, dev_in[0])
-    mixed = None if args.no_mixed else bench_mixed(stream, args.mixed_count)
+    mixed = None if args.no_mixed else bench_mixed(stream, args.mixed_count, precision=prec_of[args.precision])
 
     peaks = load_peaks()
     cell_iters = args.steps * sum(st.iterations * nn * nn for st, nn in zip(st_list, ns))
@@ -344,15 +373,26 @@ def run_ours(args):
         if ref_map is not None:
             parity = parity_vs_reference(ctx, n, ref_map, dev_out[0], st_list[0],
                                          None if args.no_locate else LOCATE_POINTS)
+            parity["precision"] = args.precision
+            if other_out is not None:
+                import numpy as np
+
+                g = other_out[0].double().cpu().numpy()
+                parity["other_precision"] = {
+                    "precision": other["precision"],
+                    "max_vertex_err": float(np.abs(g - ref_map.fwd()).max()),
+                    "iterations_gpu": int(other_st[0].iterations), "residual_gpu": float(other_st[0].residual)}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64",
+                "vs_baseline": None,
+                "dtype": "f32 cells / f64 sums" if args.precision == "split" else "f64",
                 "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
-                "iterations": iters, "final_residual_max": max(resid), "gpu_launches": launches,
-                "e2e": e2e, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "precision": args.precision, "iterations": head["iterations"],
+                "final_residual_max": head["final_residual_max"], "gpu_launches": launches,
+                "e2e": e2e, "other_precision": other, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:
@@ -362,7 +402,7 @@ def run_ours(args):
     ctx.close()
 
 
-def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
+def bench_mixed(stream, count=64, repeats=2, threshold=1e-6, precision=0):
     """Many uneven instances: `count` Gaussian mixtures (4..16 components, floor 1e-3), n
     drawn log-uniformly from {128, 256, 512, 1024}, residual <= 1e-6. Batched = one
     otm_solve_batch call; plain = one otm_solve call per instance on its own context; both
@@ -383,6 +423,7 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
     opt = N.default_options()
     opt.threshold = threshold
     ctx = N.Context(torch.cuda.current_device())
+    ctx.set_precision(precision)
     stream = torch.cuda.ExternalStream(ctx.stream())
     for n in sorted(set(ns)):
         ctx.init(n)
@@ -414,6 +455,7 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6):
     # plain: one otm_solve call per instance on a separate context (graph loop; its
     # workspace cache keeps one workspace and captured graph per size), warmed up first
     ctx_plain = N.Context(torch.cuda.current_device())
+    ctx_plain.set_precision(precision)
     for n in sorted(set(ns)):
         ctx_plain.init(n)
     stream_p = torch.cuda.ExternalStream(ctx_plain.stream())
@@ -576,7 +618,7 @@ def parity_vs_reference(ctx, n, ref_map, gpu_fwd, gpu_stats, locate_points=None)
     return out
 
 
-def bench_plain(device, n, dev_in, dev_out, opt, steps=5):
+def bench_plain(device, n, dev_in, dev_out, opt, precision, steps=5):
     """The plain single-instance form: one otm_solve call per density, on its own context
     (graph loop, workspace and graph warmed up by an untimed pass), CUDA events around
     each step of len(dev_in) calls; best step."""
@@ -587,6 +629,7 @@ def bench_plain(device, n, dev_in, dev_out, opt, steps=5):
     from otmap_b200 import native as N
 
     ctx = N.Context(device)
+    ctx.set_precision(precision)
     ctx.init(n)
     stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", device))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")

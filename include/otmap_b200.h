@@ -333,6 +333,19 @@ int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fw
  *     their copy brings and give up after about 1 ms, so the path runs on demand;
  *     0 (default) restores normal operation. */
 #define OTM_OPT_WAIT_TEST 3
+/*   OTM_OPT_PRECISION: the arithmetic of the iteration.
+ *     OTM_PRECISION_FP64  (default) every per-cell array and operation in FP64: the
+ *                         reference's arithmetic (same iteration counts, positions within
+ *                         1e-6 of the reference's)
+ *     OTM_PRECISION_SPLIT for n a power of two in [64, 1024] (other sizes stay FP64):
+ *                         r, d_hat, d and the cosine transforms in FP32; the potential,
+ *                         every product entering the line-search sums, the sums, beta,
+ *                         the quartic and its root, the residual and the mean-zero
+ *                         projection in FP64. Positions within 1e-5 of the reference's,
+ *                         same stopping threshold on the same tracked residual. */
+#define OTM_OPT_PRECISION 4
+#define OTM_PRECISION_FP64 0
+#define OTM_PRECISION_SPLIT 1
 int otm_set_option(otm_context* ctx, int key, int value);
 
 /* ---- allocation-free solve (no counterpart in the reference) ----

@@ -287,7 +287,7 @@ static void poisson_rec(otm_context* ctx, AdjointWs* W, int k) {
   const int* L = W->lists.as<int>();
   if (W->fft) {
     if (W->reg)
-      dct_reg_run(ctx, W->n, d, L, 0, W->rows, L, 0, W->cols);
+      dct_reg_run(ctx, W->n, false, d, L, 0, W->rows, L, 0, W->cols);
     else
       poisson_fft(ctx, d, L, 0, W->rows, L, 0, W->cols);
   } else {

@@ -206,6 +206,14 @@ extern "C" int otm_set_option(otm_context* ctx, int key, int value) {
     ctx->wait_test = value;
     return OTM_OK;
   }
+  if (key == OTM_OPT_PRECISION) {
+    if (value != OTM_PRECISION_FP64 && value != OTM_PRECISION_SPLIT) {
+      set_error("otm_set_option: unknown precision");
+      return OTM_ERR_BAD_ARG;
+    }
+    ctx->precision = value;
+    return OTM_OK;
+  }
   set_error("otm_set_option: unknown option");
   return OTM_ERR_BAD_ARG;
 }

@@ -62,9 +62,11 @@ struct Workspace {
   void* h_pinned = nullptr;            // pinned staging for Inst readback
   size_t h_pinned_bytes = 0;
   int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0, total_strips = 0;
-  int mode = -1;  // poisson mode the layout was built for
+  int mode = -1;       // poisson mode the layout was built for
+  int precision = -1;  // precision the layout was built for
+  int split_strip0 = 0;  // strips of split-precision instances start here (FP64 ones before)
   struct Segment {  // instances of one size on one transform kernel family
-    int n, reg, roff, rcnt, coff, ccnt;
+    int n, reg, split, roff, rcnt, coff, ccnt;
   };
   std::vector<Segment> segments;
   // the iteration loop captured as a CUDA graph with a device-side WHILE node
@@ -111,6 +113,7 @@ struct otm_context {
   int poisson_mode = 0;  // OTM_POISSON_AUTO / _DENSE / _FFT
   int loop_mode = 0;     // OTM_LOOP_GRAPH (0) / OTM_LOOP_HOST (1)
   int wait_test = 0;     // OTM_OPT_WAIT_TEST: bounded waits made to run out
+  int precision = 0;     // OTM_PRECISION_FP64 / _SPLIT
   otm::Profiler prof;
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   // Workspaces of the most recent batch configurations (size list + Poisson mode), most

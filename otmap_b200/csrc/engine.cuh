@@ -33,6 +33,7 @@ struct Inst {
   const double2* tw;  // exp(-2 pi i k / n), k < n/2 (fast transform); then the step-2 table
   const double2* pt;  // (cos, sin)(pi k / (2n)), k < n (fast transform)
   int fft, logn;      // fast transform used (n a power of two) / log2 n
+  int split;          // split precision: r, d_hat, d, t1 hold FP32 values (psi, rho FP64)
   int row0, nrow, col0, ncol;  // first item and item count in the row / column work lists
   int strip0, nstrip;          // first block and block count in the strip work list
   // loop state
@@ -135,7 +136,8 @@ bool dct_reg_supported(int n);
 void dct_reg_step2_table(int n, const std::vector<double2>& tw, std::vector<double2>& out);
 int dct_reg_lines_per_block(int n);
 int dct_reg_cols_per_block(int n);
-void dct_reg_run(otm_context* ctx, int n, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,
+// fp32: the FP32 kernels (r_k, the transform temporary t1 and d_hat are FP32 arrays).
+void dct_reg_run(otm_context* ctx, int n, bool fp32, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,
                  int coff, int ccnt);
 // Dynamic shared-memory limits of the kernels of each family (set once per device,
 // before any stream capture).
@@ -145,8 +147,12 @@ void poisson_fft_attrs(int device);
 
 // Two-pass stencil sweep of an iteration (stencil.cu).
 int strip_blocks(int n, int srows);
-void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);
-void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials);
+// Blocks base .. base + nblocks - 1 of the strip work list; split = the split-precision
+// kernels (FP32 r, d_hat, d arrays).
+void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int base, int nblocks, bool split,
+                double* partials);
+void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int base, int nblocks, bool split,
+                  double* partials);
 constexpr int SWEEP_SLOTS = 32;  // partial-sum slots per sweep block
 
 // Elements staged in shared memory per block of the transform kernels.

@@ -204,7 +204,14 @@ __global__ __launch_bounds__(NT) void k_residual_init(Inst* insts, const int* ti
   double mx = -INFINITY;
   if (t.inside) {
     double r = e * e - ea * I.rho[t.f];
-    I.r[0][t.f] = r;
+    if (I.split) {
+      // FP32 residual: the sums below start from the stored (rounded) values
+      const float rf = (float)r;
+      reinterpret_cast<float*>(I.r[0])[t.f] = rf;
+      r = rf;
+    } else {
+      I.r[0][t.f] = r;
+    }
     v[0] = r * r;
     mx = r;
   }
@@ -538,7 +545,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
   const int count = (int)sizes.size();
   std::vector<Inst> h(count);
   size_t cells = 0;
-  int tiles = 0, gemm = 0, rows = 0, cols = 0, strips = 0;
+  int tiles = 0, gemm = 0, rows = 0, cols = 0, strips = 0, split_strip0 = 0;
   // Taller sweep strips halve the per-strip overhead (ring prologue, block reduction) when
   // the batch has blocks to spare; a batch that does not fill the GPU twice over keeps
   // 32-row strips for parallelism, and one with fewer 32-row blocks than SMs takes 16-row
@@ -560,11 +567,10 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.tile0 = tiles;
     I.ntiles = tiles_of(n);
     tiles += I.ntiles;
-    I.strip0 = strips;
     I.srows = srows;
     I.nstrip = strip_blocks(n, srows);
-    strips += I.nstrip;
     I.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
+    I.split = (ctx->precision == OTM_PRECISION_SPLIT && I.fft && dct_reg_supported(n)) ? 1 : 0;
     if (I.fft) {
       int lg = 0;
       while ((1 << lg) < n) ++lg;
@@ -576,6 +582,16 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     }
     // 11 cell arrays per instance, each padded to 32 doubles (256 bytes)
     cells += 11 * (((size_t)n * n + 31) / 32 * 32);
+  }
+  // sweep work list: the FP64 instances' strips, then the split-precision ones' (two
+  // launches of each sweep when a batch has both)
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) split_strip0 = strips;
+    for (int q = 0; q < count; ++q)
+      if (h[q].split == pass) {
+        h[q].strip0 = strips;
+        strips += h[q].nstrip;
+      }
   }
   // fast-transform work lists, grouped into one segment per (kernel family, size)
   std::vector<Workspace::Segment> segs;
@@ -591,7 +607,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
       const int per = reg ? dct_reg_lines_per_block(I.n) : fft_lines(I.n);
       const int cper = reg ? dct_reg_cols_per_block(I.n) : fft_lines(I.n);
       if (segs.empty() || segs.back().n != I.n || segs.back().reg != reg)
-        segs.push_back({I.n, reg, rows, 0, cols, 0});
+        segs.push_back({I.n, reg, I.split, rows, 0, cols, 0});
       I.row0 = rows;
       I.nrow = I.n / per;
       I.col0 = cols;
@@ -609,7 +625,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     auto& W = ctx->workspaces;
     size_t hit = W.size();
     for (size_t k = 0; k < W.size(); ++k)
-      if (W[k]->sizes == sizes && W[k]->mode == ctx->poisson_mode) hit = k;
+      if (W[k]->sizes == sizes && W[k]->mode == ctx->poisson_mode && W[k]->precision == ctx->precision) hit = k;
     if (hit < W.size()) {
       std::rotate(W.begin(), W.begin() + hit, W.begin() + hit + 1);
       same = true;
@@ -648,6 +664,8 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     OTM_CUDA(cudaStreamSynchronize(st));
     ws.sizes = sizes;
     ws.mode = ctx->poisson_mode;
+    ws.precision = ctx->precision;
+    ws.split_strip0 = split_strip0;
     ws.total_tiles = tiles;
     ws.total_gemm = gemm;
     ws.total_rows = rows;
@@ -730,13 +748,18 @@ static void launch_iteration(otm_context* ctx, Inst* d_insts) {
       launch(ctx, "dct_gemm", k_dct_gemm, G, 256, (const Inst*)d_insts, ws.gemm_inst.as<int>(), s, 1);
   for (const auto& sg : ws.segments) {
     if (sg.reg)
-      dct_reg_run(ctx, sg.n, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff,
+      dct_reg_run(ctx, sg.n, sg.split != 0, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff,
                   sg.ccnt);
     else
       poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff, sg.ccnt);
   }
-  sweep_sums(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
-  sweep_update(ctx, d_insts, ws.strip_inst.as<int>(), ws.total_strips, ws.sweep_partials.as<double>());
+  const int* si = ws.strip_inst.as<int>();
+  double* sp = ws.sweep_partials.as<double>();
+  const int s64 = ws.split_strip0, s32 = ws.total_strips - ws.split_strip0;
+  sweep_sums(ctx, d_insts, si, 0, s64, false, sp);
+  sweep_sums(ctx, d_insts, si, s64, s32, true, sp);
+  sweep_update(ctx, d_insts, si, 0, s64, false, sp);
+  sweep_update(ctx, d_insts, si, s64, s32, true, sp);
 }
 
 // Captures the iteration loop of the current workspace into a graph with a WHILE node.

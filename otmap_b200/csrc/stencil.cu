@@ -218,15 +218,69 @@ enum {
   S_COUNT
 };
 
-__global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip_inst, double* partials) {
+// Last block of an instance in the sum sweep (thread 0): restores the factor (n/2)^2 / 2
+// of the line coefficients in the sums, then the early exit (otsolver_2dgrid.cpp:182),
+// beta (:248-261) and the step alpha of the quartic for d = d_hat + beta d_prev (:541-606).
+__device__ __forceinline__ void sums_step(Inst& I, double (&S)[S_COUNT], int n, int it) {
+  const double hw = 0.5 * (double)n;
+  const double h2 = 0.5 * hw * hw, h4 = h2 * h2;
+  S[S_JB] *= h2;
+  S[S_JA] *= h2;
+  S[S_B1R] *= h2;
+  S[S_B2R] *= h2;
+  S[S_A11R] *= h2;
+  S[S_A12R] *= h2;
+  S[S_A22R] *= h2;
+#pragma unroll
+  for (int k = S_B1B1; k <= S_B2B2; ++k) S[k] *= h4;
+#pragma unroll
+  for (int k = S_AB0; k < S_COUNT; ++k) S[k] *= h4;
+  if (sqrt(S[S_HH]) <= 2.0 * DBL_MIN) {  // otsolver_2dgrid.cpp:182
+    I.active = 0;
+    I.outcome = OTM_SMALL_STEP;
+    return;
+  }
+  const bool use_beta = it >= 1 && I.beta_cj;
+  I.use_beta = use_beta ? 1 : 0;
+  if (use_beta) {
+    const double alpha = I.alpha, eps = alpha / 2.0;
+    const double num = -eps * S[S_JB] + eps * eps * S[S_JA];
+    I.beta = std_max(-1.0, num / S[S_JJ] / eps * alpha);
+  }
+  const double B = use_beta ? I.beta : 0.0, B2 = B * B, B3 = B2 * B, B4 = B2 * B2;
+  const double sbr = S[S_B1R] + B * S[S_B2R];
+  const double sbb = S[S_B1B1] + 2.0 * B * S[S_B1B2] + B2 * S[S_B2B2];
+  const double sar = S[S_A11R] + B * S[S_A12R] + B2 * S[S_A22R];
+  const double sab = S[S_AB0] + B * S[S_AB1] + B2 * S[S_AB2] + B3 * S[S_AB3];
+  const double saa = S[S_AA0] + 2.0 * B * S[S_AA1] + B2 * S[S_AA2] + 2.0 * B3 * S[S_AA3] + B4 * S[S_AA4];
+  const double ea = 1.0 / ((double)n * (double)n);
+  double z[5] = {I.residual * ea, 2.0 * sbr, sbb + 2 * sar, 2.0 * sab, saa};
+  double alpha, rmin;
+  pick_step(z, &alpha, &rmin);
+  I.alpha = alpha;
+  I.residual = rmin / ea;
+  I.dnorm = sqrt(std_max(0.0, S[S_HH] + 2.0 * B * S[S_HQ] + B2 * S[S_QQ]));
+}
+
+// Last block of an instance in the update sweep (thread 0): the max residual, the
+// iteration count and the loop test (otsolver_2dgrid.cpp:160).
+__device__ __forceinline__ void update_step(Inst& I, double rmax, int n, int it) {
+  I.linf = rmax / (1.0 / ((double)n * (double)n));
+  I.it = it + 1;
+  I.active = (I.it < I.max_iter && I.residual > I.threshold) ? 1 : 0;
+  if (!I.active) stop_outcome(I);
+}
+
+__global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip_inst, int base, double* partials) {
   extern __shared__ __align__(16) double ring_smem[];
   __shared__ double red[32 * S_COUNT];
-  Inst& I = insts[strip_inst[blockIdx.x]];
+  const int blk = base + blockIdx.x;
+  Inst& I = insts[strip_inst[blk]];
   if (!I.active) return;
   const int n = I.n, it = I.it;
   // gradients are unscaled (vgrad): the shift e of the diagonals becomes e / (n/2)
   const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw;
-  const StripCoord sc = strip_coord(I, blockIdx.x);
+  const StripCoord sc = strip_coord(I, blk);
   const int j = sc.j0 + sc.lane;
   double acc[S_COUNT];
 #pragma unroll
@@ -300,63 +354,25 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
     }
     cp_async_wait<0>();
   }
-  write_partials<S_COUNT>(acc, red, partials, blockIdx.x);
+  write_partials<S_COUNT>(acc, red, partials, blk);
   if (last_block(&I.counter, I.nstrip)) {
     double S[S_COUNT];
     reduce_block_partials<S_COUNT>(partials, I.strip0, I.nstrip, S, red);
-    if (threadIdx.x == 0) {
-      // restore the factor (n/2)^2 / 2 of each line coefficient in the sums
-      const double h2 = 0.5 * hw * hw, h4 = h2 * h2;
-      S[S_JB] *= h2;
-      S[S_JA] *= h2;
-      S[S_B1R] *= h2;
-      S[S_B2R] *= h2;
-      S[S_A11R] *= h2;
-      S[S_A12R] *= h2;
-      S[S_A22R] *= h2;
-#pragma unroll
-      for (int k = S_B1B1; k <= S_B2B2; ++k) S[k] *= h4;
-#pragma unroll
-      for (int k = S_AB0; k < S_COUNT; ++k) S[k] *= h4;
-      if (sqrt(S[S_HH]) <= 2.0 * DBL_MIN) {  // otsolver_2dgrid.cpp:182
-        I.active = 0;
-        I.outcome = OTM_SMALL_STEP;
-      } else {
-        const bool use_beta = it >= 1 && I.beta_cj;
-        I.use_beta = use_beta ? 1 : 0;
-        if (use_beta) {
-          const double alpha = I.alpha, eps = alpha / 2.0;
-          const double num = -eps * S[S_JB] + eps * eps * S[S_JA];
-          I.beta = std_max(-1.0, num / S[S_JJ] / eps * alpha);
-        }
-        const double B = use_beta ? I.beta : 0.0, B2 = B * B, B3 = B2 * B, B4 = B2 * B2;
-        const double sbr = S[S_B1R] + B * S[S_B2R];
-        const double sbb = S[S_B1B1] + 2.0 * B * S[S_B1B2] + B2 * S[S_B2B2];
-        const double sar = S[S_A11R] + B * S[S_A12R] + B2 * S[S_A22R];
-        const double sab = S[S_AB0] + B * S[S_AB1] + B2 * S[S_AB2] + B3 * S[S_AB3];
-        const double saa = S[S_AA0] + 2.0 * B * S[S_AA1] + B2 * S[S_AA2] + 2.0 * B3 * S[S_AA3] + B4 * S[S_AA4];
-        const double ea = 1.0 / ((double)n * (double)n);
-        double z[5] = {I.residual * ea, 2.0 * sbr, sbb + 2 * sar, 2.0 * sab, saa};
-        double alpha, rmin;
-        pick_step(z, &alpha, &rmin);
-        I.alpha = alpha;
-        I.residual = rmin / ea;
-        I.dnorm = sqrt(std_max(0.0, S[S_HH] + 2.0 * B * S[S_HQ] + B2 * S[S_QQ]));
-      }
-    }
+    if (threadIdx.x == 0) sums_step(I, S, n, it);
   }
 }
 
-__global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* strip_inst, double* partials) {
+__global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* strip_inst, int base, double* partials) {
   extern __shared__ __align__(16) double ring_smem[];
   __shared__ double red[32];
-  Inst& I = insts[strip_inst[blockIdx.x]];
+  const int blk = base + blockIdx.x;
+  Inst& I = insts[strip_inst[blk]];
   if (!I.active) return;
   const int n = I.n, it = I.it;
   const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw, h2 = 0.5 * hw * hw, alpha = I.alpha;
   const bool use_beta = I.use_beta;
   const double beta = I.beta;
-  const StripCoord sc = strip_coord(I, blockIdx.x);
+  const StripCoord sc = strip_coord(I, blk);
   const int j = sc.j0 + sc.lane;
   double* dnew = I.d[it & 1];
   double* psin = I.psi[(it + 1) & 1];
@@ -424,18 +440,352 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
     cp_async_wait<0>();
   }
   mx = block_max(mx, red);
-  if (threadIdx.x == 0) partials[(size_t)blockIdx.x * KA] = mx;
+  if (threadIdx.x == 0) partials[(size_t)blk * KA] = mx;
   if (last_block(&I.counter, I.nstrip)) {
     double m = -INFINITY;
     for (int t = threadIdx.x; t < I.nstrip; t += blockDim.x)
       m = fmax(m, __ldcg(&partials[(size_t)(I.strip0 + t) * KA]));
     m = block_max(m, red);
-    if (threadIdx.x == 0) {
-      I.linf = m / (1.0 / ((double)n * (double)n));
-      I.it = it + 1;
-      I.active = (I.it < I.max_iter && I.residual > I.threshold) ? 1 : 0;
-      if (!I.active) stop_outcome(I);
+    if (threadIdx.x == 0) update_step(I, m, n, it);
+  }
+}
+
+// ---- split precision (OTM_PRECISION_SPLIT) ----
+//
+// psi stays FP64; r_k, r_{k-1}, d_hat and d are FP32 arrays. The sweeps form the
+// potential's vertex gradients and diagonals in FP64 (differences of neighbouring
+// potentials need its precision), the direction's and the per-cell line coefficients in
+// FP32, and take every product that enters a sum, the sums themselves, beta, the quartic
+// and its root in FP64: the tracked residual is the line search's own estimate
+// (otsolver_2dgrid.cpp:605), so the sums must keep FP64 accuracy. psi' = psi + alpha d is
+// formed in FP64, r' = r + alpha b + alpha^2 a in FP32. Algorithmic bytes per cell: sums
+// 24 (psi 8, d_hat, d_prev, r_k, r_{k-1} 4 each), update 36 (reads psi, d_hat, d_prev,
+// r_k; writes psi' 8, d 4, r' 4).
+
+struct RowF {
+  float c, l, r;
+};
+struct VGf {
+  float gx, gy, gxr, gyr;
+};
+struct Diagf {
+  float ax, ay, bx, by;
+};
+
+__device__ __forceinline__ VGf vgradf(const RowF& a, const RowF& b) {
+  VGf g;
+  const float sc = a.c + b.c;
+  g.gx = (b.l + b.c) - (a.l + a.c);
+  g.gy = sc - (a.l + b.l);
+  g.gxr = (b.c + b.r) - (a.c + a.r);
+  g.gyr = (a.r + b.r) - sc;
+  return g;
+}
+
+__device__ __forceinline__ Diagf diagf(const VGf& p, const VGf& q) {
+  Diagf d;
+  d.ax = q.gxr - p.gx;
+  d.ay = q.gyr - p.gy;
+  d.bx = p.gxr - q.gx;
+  d.by = p.gyr - q.gy;
+  return d;
+}
+
+// The potential's shifted diagonals (FP64 differences, then FP32): g.ax + e, g.ay + e,
+// g.bx - e, g.by + e of line_ab.
+__device__ __forceinline__ Diagf shifted(const Diag& g, double e) {
+  Diagf d;
+  d.ax = (float)(g.ax + e);
+  d.ay = (float)(g.ay + e);
+  d.bx = (float)(g.bx - e);
+  d.by = (float)(g.by + e);
+  return d;
+}
+
+__device__ __forceinline__ void line_abf(const Diagf& g0, const Diagf& h, float& a, float& b) {
+  a = h.ax * h.by - h.ay * h.bx;
+  b = h.ax * g0.by - h.ay * g0.bx + g0.ax * h.by - g0.ay * h.bx;
+}
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16v(void* dst, const void* src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+
+// Prefetch ring for one FP64 stencil field (the potential; 36 doubles as in Ring), NS
+// FP32 stencil fields (40 floats: columns j0-4 .. j0+35, slot 4 + lane is column j) and
+// NP FP32 pointwise fields (32 floats). Interior strips (j0 >= 4, j0 + 36 <= n, n a
+// multiple of 4) copy with 16-byte cp.async (18 lanes for the FP64 row, 10 per FP32
+// stencil row, 8 per pointwise row); edge strips copy element-wise with clamped columns.
+template <int NS, int NP>
+struct RingS {
+  static constexpr int PD = 36, FS = 40, FP = 32;
+  static constexpr int STAGE = PD * 8 + NS * FS * 4 + NP * FP * 4;  // bytes
+  static_assert(STAGE % 16 == 0, "stages stay 16-byte aligned");
+  unsigned char* buf;  // RD * STAGE bytes (this warp's)
+  const double* psi;
+  const float* sf[NS > 0 ? NS : 1];
+  const float* pf[NP > 0 ? NP : 1];
+  int n, j0, lane, rows_end;
+  bool interior;
+  int soff, gcol;  // this lane's FP64 slot and column (interior copies)
+
+  __device__ __forceinline__ void setup() {
+    interior = (j0 >= 4) && (j0 + 36 <= n) && ((n & 3) == 0);
+    soff = lane < 16 ? 2 + 2 * lane : (lane == 16 ? 0 : 34);
+    gcol = lane < 16 ? j0 + 2 * lane : (lane == 16 ? j0 - 2 : j0 + 32);
+  }
+  __device__ __forceinline__ unsigned char* stage(int row) {
+    return buf + ((unsigned)(row + RD) & (RD - 1u)) * STAGE;
+  }
+  __device__ __forceinline__ double* pstage(int row) { return reinterpret_cast<double*>(stage(row)); }
+  __device__ __forceinline__ float* fstage(int row, int k) {
+    return reinterpret_cast<float*>(stage(row) + PD * 8) + k * FS;
+  }
+  __device__ __forceinline__ float* ptstage(int row, int k) {
+    return reinterpret_cast<float*>(stage(row) + PD * 8 + NS * FS * 4) + k * FP;
+  }
+
+  __device__ __forceinline__ void issue(int row) {
+    if (row <= rows_end) {
+      double* sp = pstage(row);
+      const size_t base = (size_t)clampn(row, n) * n;
+      if (interior) {
+        if (lane < 18) cp_async16v(sp + soff, psi + base + gcol);
+        if (lane < 10) {
+#pragma unroll
+          for (int k = 0; k < NS; ++k) cp_async16v(fstage(row, k) + 4 * lane, sf[k] + base + j0 - 4 + 4 * lane);
+        }
+        if (lane < 8) {
+#pragma unroll
+          for (int k = 0; k < NP; ++k) cp_async16v(ptstage(row, k) + 4 * lane, pf[k] + base + j0 + 4 * lane);
+        }
+      } else {
+        const size_t cj = base + clampn(j0 + lane, n);
+        cp_async8(sp + 2 + lane, psi + cj);
+        if (lane == 0) cp_async8(sp + 1, psi + base + clampn(j0 - 1, n));
+        if (lane == 31) cp_async8(sp + 34, psi + base + clampn(j0 + 32, n));
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          float* d = fstage(row, k);
+          cp_async4(d + 4 + lane, sf[k] + cj);
+          if (lane == 0) cp_async4(d + 3, sf[k] + base + clampn(j0 - 1, n));
+          if (lane == 31) cp_async4(d + 36, sf[k] + base + clampn(j0 + 32, n));
+        }
+#pragma unroll
+        for (int k = 0; k < NP; ++k) cp_async4(ptstage(row, k) + lane, pf[k] + cj);
+      }
     }
+    cp_async_commit();
+  }
+  __device__ __forceinline__ Row prow(int row) {
+    const double* d = pstage(row);
+    Row r;
+    r.c = d[2 + lane];
+    r.l = d[1 + lane];
+    r.r = d[3 + lane];
+    return r;
+  }
+  __device__ __forceinline__ RowF frow(int row, int k) {
+    const float* d = fstage(row, k);
+    RowF r;
+    r.c = d[4 + lane];
+    r.l = d[3 + lane];
+    r.r = d[5 + lane];
+    return r;
+  }
+  __device__ __forceinline__ float point(int row, int k) { return ptstage(row, k)[lane]; }
+};
+
+// The split-precision form of k_sweep_sums (same sums, same last-block step).
+__global__ __launch_bounds__(ST) void k_sweep_sums_split(Inst* insts, const int* strip_inst, int base,
+                                                         double* partials) {
+  extern __shared__ __align__(16) unsigned char ring_raw[];
+  __shared__ double red[32 * S_COUNT];
+  const int blk = base + blockIdx.x;
+  Inst& I = insts[strip_inst[blk]];
+  if (!I.active) return;
+  const int n = I.n, it = I.it;
+  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw;
+  const StripCoord sc = strip_coord(I, blk);
+  const int j = sc.j0 + sc.lane;
+  double acc[S_COUNT];
+#pragma unroll
+  for (int k = 0; k < S_COUNT; ++k) acc[k] = 0.0;
+  if (sc.i0 < n) {
+    using RS = RingS<2, 2>;
+    RS R;
+    R.buf = ring_raw + (size_t)sc.warp * RD * RS::STAGE;
+    R.psi = I.psi[it & 1];
+    R.sf[0] = reinterpret_cast<const float*>(I.dhat);
+    R.sf[1] = reinterpret_cast<const float*>(I.d[(it + 1) & 1]);
+    R.pf[0] = reinterpret_cast<const float*>(I.r[it % 3]);
+    R.pf[1] = reinterpret_cast<const float*>(I.r[(it + 2) % 3]);
+    R.n = n;
+    R.j0 = sc.j0;
+    R.lane = sc.lane;
+    const int last = min(sc.i0 + I.srows, n);
+    R.rows_end = last;
+    R.setup();
+#pragma unroll
+    for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
+    VG gp;
+    VGf gh, gq;
+#pragma unroll 2
+    for (int row = sc.i0; row <= last; ++row) {
+      cp_async_wait<RD - 3>();
+      __syncwarp();
+      const Row ap = R.prow(row - 1), bp = R.prow(row);
+      const RowF ah = R.frow(row - 1, 0), aq = R.frow(row - 1, 1);
+      const RowF bh = R.frow(row, 0), bq = R.frow(row, 1);
+      VG np = vgrad(ap, bp);
+      VGf nh = vgradf(ah, bh);
+      VGf nq = vgradf(aq, bq);
+      if (row > sc.i0 && j < n) {
+        const int c = row - 1;
+        const Diagf G = shifted(diag(gp, np), es);
+        const Diagf Hd = diagf(gh, nh), Qd = diagf(gq, nq);
+        float a11f, b1f, a22f, b2f;
+        line_abf(G, Hd, a11f, b1f);
+        line_abf(G, Qd, a22f, b2f);
+        const float a12f = Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx;
+        const float rf = R.point(c, 0);
+        const double a11 = a11f, b1 = b1f, a22 = a22f, b2 = b2f, a12 = a12f;
+        const double r = rf, jd = (double)(rf - R.point(c, 1));
+        const double hv = ah.c, qv = aq.c;
+        acc[S_HH] = fma(hv, hv, acc[S_HH]);
+        acc[S_HQ] = fma(hv, qv, acc[S_HQ]);
+        acc[S_QQ] = fma(qv, qv, acc[S_QQ]);
+        acc[S_JB] = fma(jd, b1, acc[S_JB]);
+        acc[S_JA] = fma(jd, a11, acc[S_JA]);
+        acc[S_JJ] = fma(jd, jd, acc[S_JJ]);
+        acc[S_B1R] = fma(b1, r, acc[S_B1R]);
+        acc[S_B2R] = fma(b2, r, acc[S_B2R]);
+        acc[S_B1B1] = fma(b1, b1, acc[S_B1B1]);
+        acc[S_B1B2] = fma(b1, b2, acc[S_B1B2]);
+        acc[S_B2B2] = fma(b2, b2, acc[S_B2B2]);
+        acc[S_A11R] = fma(a11, r, acc[S_A11R]);
+        acc[S_A12R] = fma(a12, r, acc[S_A12R]);
+        acc[S_A22R] = fma(a22, r, acc[S_A22R]);
+        acc[S_AB0] = fma(a11, b1, acc[S_AB0]);
+        acc[S_AB1] = fma(a11, b2, fma(a12, b1, acc[S_AB1]));
+        acc[S_AB2] = fma(a12, b2, fma(a22, b1, acc[S_AB2]));
+        acc[S_AB3] = fma(a22, b2, acc[S_AB3]);
+        acc[S_AA0] = fma(a11, a11, acc[S_AA0]);
+        acc[S_AA1] = fma(a11, a12, acc[S_AA1]);
+        acc[S_AA2] = fma(a12, a12, fma(a11 + a11, a22, acc[S_AA2]));
+        acc[S_AA3] = fma(a12, a22, acc[S_AA3]);
+        acc[S_AA4] = fma(a22, a22, acc[S_AA4]);
+      }
+      gp = np;
+      gh = nh;
+      gq = nq;
+      __syncwarp();
+      R.issue(row - 2 + RD);
+    }
+    cp_async_wait<0>();
+  }
+  write_partials<S_COUNT>(acc, red, partials, blk);
+  if (last_block(&I.counter, I.nstrip)) {
+    double S[S_COUNT];
+    reduce_block_partials<S_COUNT>(partials, I.strip0, I.nstrip, S, red);
+    if (threadIdx.x == 0) sums_step(I, S, n, it);
+  }
+}
+
+// The split-precision form of k_sweep_update.
+__global__ __launch_bounds__(ST) void k_sweep_update_split(Inst* insts, const int* strip_inst, int base,
+                                                           double* partials) {
+  extern __shared__ __align__(16) unsigned char ring_raw[];
+  __shared__ double red[32];
+  const int blk = base + blockIdx.x;
+  Inst& I = insts[strip_inst[blk]];
+  if (!I.active) return;
+  const int n = I.n, it = I.it;
+  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw, alpha = I.alpha;
+  const float h2 = (float)(0.5 * hw * hw), af = (float)alpha, af2 = (float)(alpha * alpha);
+  const bool use_beta = I.use_beta;
+  const float beta = (float)I.beta;
+  const StripCoord sc = strip_coord(I, blk);
+  const int j = sc.j0 + sc.lane;
+  float* dnew = reinterpret_cast<float*>(I.d[it & 1]);
+  double* psin = I.psi[(it + 1) & 1];
+  float* rn = reinterpret_cast<float*>(I.r[(it + 1) % 3]);
+  float mx = -INFINITY;
+  if (sc.i0 < n) {
+    using RS = RingS<2, 1>;
+    RS R;
+    R.buf = ring_raw + (size_t)sc.warp * RD * RS::STAGE;
+    R.psi = I.psi[it & 1];
+    R.sf[0] = reinterpret_cast<const float*>(I.dhat);
+    R.sf[1] = reinterpret_cast<const float*>(I.d[(it + 1) & 1]);
+    R.pf[0] = reinterpret_cast<const float*>(I.r[it % 3]);
+    R.n = n;
+    R.j0 = sc.j0;
+    R.lane = sc.lane;
+    const int last = min(sc.i0 + I.srows, n);
+    R.rows_end = last;
+    R.setup();
+#pragma unroll
+    for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
+    auto drow = [&](int row) {
+      RowF h = R.frow(row, 0);
+      if (!use_beta) return h;
+      RowF q = R.frow(row, 1);
+      RowF d;
+      d.c = h.c + beta * q.c;
+      d.l = h.l + beta * q.l;
+      d.r = h.r + beta * q.r;
+      return d;
+    };
+    VG gp;
+    VGf gd;
+    Row pc;
+    RowF dc;
+#pragma unroll 4
+    for (int row = sc.i0; row <= last; ++row) {
+      cp_async_wait<RD - 3>();
+      __syncwarp();
+      if (row == sc.i0) {
+        pc = R.prow(row - 1);
+        dc = drow(row - 1);
+      }
+      const Row pb = R.prow(row);
+      const RowF db = drow(row);
+      VG np = vgrad(pc, pb);
+      VGf nd = vgradf(dc, db);
+      if (row > sc.i0 && j < n) {
+        const int c = row - 1;
+        const size_t f = (size_t)c * n + j;
+        float a, b;
+        line_abf(shifted(diag(gp, np), es), diagf(gd, nd), a, b);
+        dnew[f] = dc.c;
+        psin[f] = pc.c + alpha * (double)dc.c;
+        const float r = h2 * (a * af2 + b * af) + R.point(c, 0);
+        rn[f] = r;
+        mx = fmaxf(mx, r);
+      }
+      gp = np;
+      gd = nd;
+      pc = pb;
+      dc = db;
+      __syncwarp();
+      R.issue(row - 2 + RD);
+    }
+    cp_async_wait<0>();
+  }
+  double m64 = block_max((double)mx, red);
+  if (threadIdx.x == 0) partials[(size_t)blk * KA] = m64;
+  if (last_block(&I.counter, I.nstrip)) {
+    double m = -INFINITY;
+    for (int t = threadIdx.x; t < I.nstrip; t += blockDim.x)
+      m = fmax(m, __ldcg(&partials[(size_t)(I.strip0 + t) * KA]));
+    m = block_max(m, red);
+    if (threadIdx.x == 0) update_step(I, m, n, it);
   }
 }
 
@@ -451,19 +801,35 @@ void sweep_attrs(int device) {
                                 (int)(SWARPS * RD * Ring<3, 2>::STAGE * sizeof(double))));
   OTM_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(SWARPS * RD * Ring<3, 1>::STAGE * sizeof(double))));
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_sums_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(SWARPS * RD * RingS<2, 2>::STAGE)));
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_update_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(SWARPS * RD * RingS<2, 1>::STAGE)));
   if (device < 64) done[device] = true;
 }
 
-void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials) {
+void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int base, int nblocks, bool split,
+                double* partials) {
   sweep_attrs(ctx->device);
-  launch_smem(ctx, "sweep_sums", k_sweep_sums, nblocks, ST, SWARPS * RD * Ring<3, 2>::STAGE * sizeof(double),
-              d_insts, strip_inst, partials);
+  if (nblocks <= 0) return;
+  if (split)
+    launch_smem(ctx, "sweep32_sums", k_sweep_sums_split, nblocks, ST, SWARPS * RD * RingS<2, 2>::STAGE, d_insts,
+                strip_inst, base, partials);
+  else
+    launch_smem(ctx, "sweep_sums", k_sweep_sums, nblocks, ST, SWARPS * RD * Ring<3, 2>::STAGE * sizeof(double),
+                d_insts, strip_inst, base, partials);
 }
 
-void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int nblocks, double* partials) {
+void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int base, int nblocks, bool split,
+                  double* partials) {
   sweep_attrs(ctx->device);
-  launch_smem(ctx, "sweep_update", k_sweep_update, nblocks, ST, SWARPS * RD * Ring<3, 1>::STAGE * sizeof(double),
-              d_insts, strip_inst, partials);
+  if (nblocks <= 0) return;
+  if (split)
+    launch_smem(ctx, "sweep32_update", k_sweep_update_split, nblocks, ST, SWARPS * RD * RingS<2, 1>::STAGE, d_insts,
+                strip_inst, base, partials);
+  else
+    launch_smem(ctx, "sweep_update", k_sweep_update, nblocks, ST, SWARPS * RD * Ring<3, 1>::STAGE * sizeof(double),
+                d_insts, strip_inst, base, partials);
 }
 
 }  // namespace otm

@@ -27,6 +27,8 @@ OPT_POISSON = 1
 POISSON_AUTO, POISSON_DENSE, POISSON_FFT = 0, 1, 2
 OPT_LOOP = 2
 LOOP_GRAPH, LOOP_HOST = 0, 1
+OPT_PRECISION = 4
+PRECISION_FP64, PRECISION_SPLIT = 0, 1
 OPT_WAIT_TEST = 3
 RIO_PER_VERTEX, RIO_PER_FACE = 0, 1
 INV_DENSEST, INV_FIRST = 0, 1
@@ -188,6 +190,11 @@ class Context:
 
     def set_loop(self, mode: int):
         check(lib().otm_set_option(self._h, OPT_LOOP, int(mode)))
+
+    def set_precision(self, mode: int):
+        """PRECISION_FP64 (default) or PRECISION_SPLIT (FP32 residuals, directions and
+        transforms; FP64 potential, sums and line search)."""
+        check(lib().otm_set_option(self._h, OPT_PRECISION, int(mode)))
 
     def stream(self) -> int:
         s = C.c_void_p()

@@ -1,0 +1,124 @@
+"""The split-precision mode (OTM_PRECISION_SPLIT: FP32 residuals, directions and cosine
+transforms; FP64 potential, line-search sums, quartic, root and projection) against the
+FP64 reference solve (otsolver_2dgrid.cpp:106-245). Tolerances: vertex positions within
+1e-5 of the unit square, the reported residual <= the threshold, and the residual
+recomputed from the final forward mesh (quad areas against e^2 times the adjusted
+density, otsolver_2dgrid.cpp:425-465) within 2x the threshold: the FP32 residual update
+may drift from the areas only by rounding."""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+POS_TOL = 1e-5
+
+
+def mesh_residual(fwd, density, n):
+    """sum (A_f - e^2 rho_f)^2 / e^2 with A_f half the cross product of the diagonals of
+    face f = j + i n (vertices v = j + i (n+1))."""
+    P = np.asarray(fwd).reshape(n + 1, n + 1, 2)  # [i, j]
+    p00, p10, p01, p11 = P[:-1, :-1], P[1:, :-1], P[:-1, 1:], P[1:, 1:]
+    a = p11 - p00
+    b = p01 - p10
+    area = 0.5 * (a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0])  # [i, j]
+    e2 = 1.0 / (n * n)
+    r = area.ravel() - e2 * np.asarray(density)
+    return float((r * r).sum() / e2)
+
+
+def split_solver(ot):
+    from otmap_b200 import native
+
+    ctx = native.Context(0)
+    ctx.set_precision(native.PRECISION_SPLIT)
+    s = ot.GridBasedTransportSolver(ctx)
+    s.set_verbose_level(0)
+    return s, ctx
+
+
+@pytest.fixture(scope="module")
+def ot():
+    from otmap_b200 import otmap
+
+    return otmap
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_split_config1_256_vs_oracle(seed, ot, oracle_port):
+    from otmap_b200 import workloads as W
+
+    n = 256
+    d = W.to_cells(W.gaussian_mixture(n, seed))
+    o = oracle_port.solve(d, n)
+    s, _ = split_solver(ot)
+    s.init(n)
+    m = s.solve(d)
+    err = float(np.abs(m.fwd_mesh() - o.fwd).max())
+    assert err <= POS_TOL, err
+    assert m.stats.residual <= 1e-7
+    assert mesh_residual(m.fwd_mesh(), m.density(), n) <= 2e-7
+    assert abs(m.stats.iterations - o.iterations) <= 3
+
+
+def test_split_config2_1024_vs_reference(ot):
+    from oracle import ref
+    from otmap_b200 import workloads as W
+
+    if not ref.available():
+        pytest.skip("the reference library (oracle/_ref) is not built")
+    n = 1024
+    d = W.to_cells(W.blurred_shapes(n, 0, sigma_px=5.0))
+    rs = ref.RefSolver()
+    rs.init(n)
+    rm = rs.solve(d, threshold=1e-7)
+    s, _ = split_solver(ot)
+    s.init(n)
+    m = s.solve(d)
+    err = float(np.abs(m.fwd_mesh() - rm.fwd()).max())
+    assert err <= POS_TOL, err
+    assert m.stats.residual <= 1e-7
+    assert mesh_residual(m.fwd_mesh(), m.density(), n) <= 2e-7
+    assert abs(m.stats.iterations - rm.iterations) <= 5, (m.stats.iterations, rm.iterations)
+
+
+def test_split_batch_with_fp64_sizes(ot):
+    """A split-precision batch with sizes outside the FP32 transforms (48, 100 stay FP64):
+    both sweep forms in the same iterations; every instance equals its single solve in
+    the same mode, and the FP64 instances equal FP64-mode solves."""
+    from otmap_b200 import native
+    from otmap_b200 import workloads as W
+
+    sizes = [64, 48, 128, 100, 256, 1024]
+    imgs = [W.gaussian_mixture(n, 800 + k) for k, n in enumerate(sizes)]
+    ctx = native.Context(0)
+    ctx.set_precision(native.PRECISION_SPLIT)
+    maps = ot.solve_batch(imgs, context=ctx)
+    for img, m in zip(imgs, maps):
+        n = img.shape[0]
+        s, _ = split_solver(ot)
+        s.init(n)
+        single = s.solve(W.to_cells(img))
+        assert m.stats.iterations == single.stats.iterations
+        assert np.array_equal(m.fwd_mesh(), single.fwd_mesh())
+        if n in (48, 100):
+            f64 = ot.GridBasedTransportSolver()
+            f64.set_verbose_level(0)
+            f64.init(n)
+            assert np.array_equal(m.fwd_mesh(), f64.solve(W.to_cells(img)).fwd_mesh())
+
+
+def test_split_graph_and_host_loops_agree(ot):
+    from otmap_b200 import native
+    from otmap_b200 import workloads as W
+
+    imgs = [W.gaussian_mixture(n, 900 + k) for k, n in enumerate([64, 256, 512])]
+    out = {}
+    for loop in (native.LOOP_GRAPH, native.LOOP_HOST):
+        ctx = native.Context(0)
+        ctx.set_precision(native.PRECISION_SPLIT)
+        ctx.set_loop(loop)
+        out[loop] = ot.solve_batch(imgs, context=ctx)
+    for a, b in zip(out[native.LOOP_GRAPH], out[native.LOOP_HOST]):
+        assert a.stats.iterations == b.stats.iterations
+        assert np.array_equal(a.fwd_mesh(), b.fwd_mesh())
