@@ -544,6 +544,27 @@ def bench_adjoint(ctx, stream, n=512, repeats=3):
                      "relative_residual": ast.relative_residual}
     ref = grads["krylov"]
     out["one_step"]["relative_error_vs_krylov"] = float(np.linalg.norm(grads["one_step"] - ref) / np.linalg.norm(ref))
+    # truncated GMRES: k Arnoldi steps (k Poisson solves) and the final lambda = M^+ (V y)
+    curve = []
+    for k in range(1, 9):
+        ao = N.AdjointOptionsC()
+        N.lib().otm_default_adjoint_options(C.byref(ao))
+        ao.mode = N.ADJOINT_KRYLOV
+        ao.tol = 0.0
+        ao.max_iter = k
+        ao.restart = max(k, 8)
+        ast = N.AdjointStatsC()
+        g = torch.empty(n * n, dtype=torch.float64, device="cuda")
+        t, _ = timed(lambda: N.check(N.lib().otm_adjoint(ctx.handle, n, C.c_void_p(dens.data_ptr()),
+                                                        C.c_void_p(fwd.data_ptr()), C.c_void_p(q.data_ptr()),
+                                                        C.byref(ao), C.c_void_p(g.data_ptr()), C.byref(ast))))
+        gh = g.double().cpu().numpy()
+        curve.append({"k": k, "poisson_solves": ast.iterations, "ms": t, "per_forward_iteration": t / per_iter,
+                      "relative_error_vs_krylov": float(np.linalg.norm(gh - ref) / np.linalg.norm(ref)),
+                      "relative_residual": ast.relative_residual})
+    out["truncated_gmres"] = curve
+    meets = [c["k"] for c in curve if c["relative_error_vs_krylov"] <= 1e-3]
+    out["smallest_k_within_1e-3"] = meets[0] if meets else None
     out.update({"workload": f"{n}^2 blur(softmax(N(0,1) logits)), sigma 8 px; dL/dfwd random",
                 "forward_solve_ms": t_solve, "forward_iterations": st.iterations, "forward_iteration_ms": per_iter})
     return out

@@ -23,6 +23,7 @@
  *   otm_grid_transport_cost  GridBasedTransportSolver::compute_transport_cost  otsolver_2dgrid.cpp:608-640
  *   otm_mesh_blend        interpolate (bilinear / linear blend)    apps/barycenters.cpp:127-139, 250-276
  *   otm_barycenter        interpolate + synthetize_and_save_image  apps/barycenters.cpp:250-290
+ *   otm_barycenter_loss   the barycenters demo as one differentiable loss apps/barycenters.cpp:184-198, 250-290
  *   otm_sample_image      sample_transportmap_to_image             utils/stochastic_rasterizer.cpp:19-88
  *   otm_grid_faces        generate_quad_mesh's faces               utils/mesh_utils.cpp:90-122
  *   otm_write_off         Surface_mesh::write (.off)               surface_mesh/IO_off.cpp:312-380
@@ -163,6 +164,12 @@ int otm_map_inverse_mode(otm_map* map, double* points, long count, int mode, int
  * unit density (rasterizer.cpp:305-308). img receives rows*cols doubles. */
 int otm_rasterize(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols,
                   double* img);
+/* The face each pixel of the PerFace raster of the (n+1)^2 grid mesh xy takes its value
+ * from (rows x cols ints, [y][x]; -1 where no face covers the pixel centre): the highest
+ * face index accepting the pixel, as rasterize_image's sequential loop leaves it
+ * (rasterizer.cpp:162-236). No counterpart in the reference; the differentiable
+ * barycenter loss holds this ownership fixed. */
+int otm_rasterize_faces(otm_context* ctx, int n, const double* xy, int rows, int cols, int* face);
 
 /* rasterize_image's RasterImageOption (utils/rasterizer.h:16-19). */
 #define OTM_RIO_PER_VERTEX 0
@@ -306,6 +313,34 @@ void otm_default_adjoint_options(otm_adjoint_options* opt); /* Krylov, tol 1e-10
  *   grad_density cells out: dL/ddensity */
 int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fwd_xy, const double* grad_fwd,
                 const otm_adjoint_options* opt, double* grad_density, otm_adjoint_stats* stats);
+
+/* ---- differentiable barycenter image (no counterpart in the reference for the gradient;
+ * the forward pass is apps/barycenters.cpp:184-198 and 250-290) ----
+ *
+ * The pipeline of the barycenters demo for `count` (<= 8) densities of one grid size n:
+ * their transport maps in one batched solve, each map's inverse at the (n+1)^2 origin grid
+ * vertices (apply_inverse_map of the origin mesh, barycenters.cpp:190), the blend of the
+ * inverse meshes with `weights` (bilerp / lerp: otm_mesh_blend), its PerFace raster with
+ * unit density at res x res, rescaled to expected = sum_k w_k mean(density_k)
+ * (synthetize_and_save_image) -> image ([y][x], optional), and the loss
+ * L = sum_pixels (image - target)^2 (target [y][x], res x res).
+ * With grad_density non-null, also dL/ddensity_k (cells) for every k: through the image
+ * rescale, each face's area in the raster (pixel ownership held fixed: it is piecewise
+ * constant in the mesh), the blend, the bilinear inversion (the origin point held fixed in
+ * the located face) and otm_adjoint of each map (aopt; NULL = defaults), plus the
+ * expected-mean term. Buffers may be host or device memory. */
+typedef struct {
+  int iterations[8];
+  int outcome[8];
+  double residual[8];
+  long inverse_missing;  /* origin vertices located in no face, over all maps */
+  double expected_mean;  /* sum_k w_k mean(density_k) */
+  double raster_mean;    /* mean of the raster before rescaling */
+  int adjoint_solves[8]; /* Poisson solves of each map's adjoint (gradient only) */
+} otm_barycenter_stats;
+int otm_barycenter_loss(otm_context* ctx, int n, int count, const double* const* density, const double* weights,
+                        int res, const double* target, const otm_solver_options* opt, const otm_adjoint_options* aopt,
+                        double* image, double* loss, double* const* grad_density, otm_barycenter_stats* stats);
 
 /* Context options (no counterpart in the reference).
  *   OTM_OPT_POISSON: how d_hat = M^+ r is computed.

@@ -89,3 +89,54 @@ def blur_torch(img, sigma):
             acc = acc + k[q] * p.narrow(dim, q, n)
         out = acc
     return out
+
+
+class _BarycenterLoss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, densities, weights, target, res, threshold, max_iter, adjoint_mode, adjoint_tol, context):
+        if not densities.is_cuda or densities.dtype != torch.float64 or densities.dim() != 2:
+            raise TypeError("densities must be a (count, n*n) float64 CUDA tensor")
+        count, cells = densities.shape
+        n = int(round(cells ** 0.5))
+        d = densities.contiguous()
+        t = target.contiguous().to(device=d.device, dtype=torch.float64)
+        grads = torch.empty_like(d)
+        image = torch.empty((res, res), dtype=torch.float64, device=d.device)
+        opt = N.default_options()
+        opt.threshold = threshold
+        opt.max_iter = max_iter
+        aopt = N.AdjointOptionsC()
+        N.lib().otm_default_adjoint_options(C.byref(aopt))
+        aopt.mode = adjoint_mode
+        aopt.tol = adjoint_tol
+        st = N.BarycenterStatsC()
+        loss = C.c_double(0.0)
+        dp = (C.c_void_p * count)(*[d[k].data_ptr() for k in range(count)])
+        gp = (C.c_void_p * count)(*[grads[k].data_ptr() for k in range(count)])
+        w = (C.c_double * count)(*[float(x) for x in weights])
+        torch.cuda.current_stream(d.device).synchronize()
+        N.check(N.lib().otm_barycenter_loss(context.handle, n, count, dp, w, res, C.c_void_p(t.data_ptr()),
+                                            C.byref(opt), C.byref(aopt), C.c_void_p(image.data_ptr()),
+                                            C.byref(loss), gp, C.byref(st)))
+        ctx.save_for_backward(grads)
+        context.last_barycenter_stats = st
+        context.last_barycenter_image = image
+        return torch.tensor(loss.value, dtype=torch.float64, device=d.device)
+
+    @staticmethod
+    def backward(ctx, grad_loss):
+        (grads,) = ctx.saved_tensors
+        return grad_loss * grads, None, None, None, None, None, None, None, None
+
+
+def barycenter_loss(densities, weights, target, res=None, threshold=1e-7, max_iter=1000, adjoint="krylov",
+                    adjoint_tol=1e-10, context=None):
+    """L = sum (barycenter image - target)^2 of the barycenters pipeline for densities (a
+    (count, n*n) float64 CUDA tensor, face order), differentiable with respect to them. The
+    gradient is computed with the forward pass (one library call) and kept until backward;
+    the image of the forward pass is left in context.last_barycenter_image."""
+    mode = N.ADJOINT_KRYLOV if adjoint == "krylov" else N.ADJOINT_ONE_STEP
+    ctx = context or N.default_context()
+    res = int(res or target.shape[0])
+    return _BarycenterLoss.apply(densities, tuple(float(x) for x in weights), target, res, float(threshold),
+                                 int(max_iter), mode, float(adjoint_tol), ctx)

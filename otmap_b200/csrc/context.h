@@ -168,6 +168,27 @@ void copy_out(otm_context* ctx, void* dst, const void* src, size_t bytes);
 void raster_grid(otm_context* ctx, int n, const double* xy, const double* density, int rows, int cols, int mode,
                  double* img);
 
+// Inversion of `count` device points through map m (locator built on demand), in place;
+// face, hit0 (the first hit in the reference's order), nhits (device, may be null) and
+// missing (device counter, added to) as otm_map_inverse_mode reports them.
+void map_inverse_dev(otm_map* m, double* pts, long count, int mode, int* face, int* hit0, int* nhits,
+                     unsigned long long* missing);
+
+// Backward of the PerFace unit-density raster of the (n+1)^2 grid mesh xy that
+// raster_grid just drew (its face boxes and pixel owners are still in the context's
+// raster scratch): dL/dxy (V x 2, overwritten) from dL/dpixel (rows x cols), through each
+// face's |area| (the value of an owned pixel is scale / |area|); pixel ownership is held
+// fixed (it is piecewise constant in the mesh).
+void raster_grid_backward(otm_context* ctx, int n, const double* xy, int rows, int cols, const double* dL_dpix,
+                          double* dL_dxy);
+
+// Backward of the inversion of the (n+1)^2 origin grid vertices through the forward mesh
+// fwd (apps/barycenters.cpp:190): for each vertex located with first hit hit0[v],
+// inverse position I_v = sum_i w_i(x_v; fwd corners of hit0) O_i, dL/dfwd (V x 2,
+// overwritten) from dL/dI (V x 2). Deterministic: per-face point lists in index order.
+void inverse_grid_backward(otm_context* ctx, int n, const double* fwd, const int* hit0, const double* dL_dI,
+                           double* dL_dfwd);
+
 // Launches `kernel` on the context stream, counting it and (when profiling) bracketing
 // it with CUDA events.
 template <class K, class... Args>

@@ -529,7 +529,8 @@ constexpr int MAXHITS = 8;
 // first-hit mode (inv_fast, bvh2d.cpp:66-81) keeps the first.
 __global__ void k_inverse(const double* xy, const double* density, int n, int B, const int* starts,
                           const int* faces, const double4* boxes, const int* rank, const double4* lbox, double* pts,
-                          long P, int first_hit, int* face_out, int* nhits_out, unsigned long long* missing) {
+                          long P, int first_hit, int* face_out, int* hit0_out, int* nhits_out,
+                          unsigned long long* missing) {
   long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= P) return;
   double qx = fmin(fmax(pts[2 * i], 0.), 1.);
@@ -576,6 +577,7 @@ __global__ void k_inverse(const double* xy, const double* density, int n, int B,
     ++nh;
   }
   if (nhits_out) nhits_out[i] = nh;
+  if (hit0_out) hit0_out[i] = nh > 0 ? hf[0] : -1;
   if (nh == 0) {
     pts[2 * i] = NAN;
     pts[2 * i + 1] = NAN;
@@ -890,6 +892,148 @@ __global__ void k_vertex_values_mesh(int nv, const int* vstart, int* vfaces, con
   value[v] = (float)((double)(scale * acc) / div);
 }
 
+// ---- backward of the grid raster and of the grid inversion (differentiable barycenters) ----
+
+// dL/dA_f per face of a grid mesh from the pixels it owns in the last raster: an owned
+// pixel's PerFace value is scale / |A_f| with A_f the signed fan area of face_abs_area,
+// so d value / d A_f = -value / A_f.
+__global__ void k_raster_area_grad(MeshRef m, int rows, int cols, const FaceRaster* fr, const int* owner,
+                                   const double* dL_dpix, double* dL_dA) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  const FaceRaster r = fr[f];
+  double acc = 0.0;
+  for (int y = r.y0; y < r.y1; ++y)
+    for (int x = r.x0; x < r.x1; ++x) {
+      const size_t q = (size_t)y * cols + x;
+      if (owner[q] == f) acc += dL_dpix[q];
+    }
+  Quad p;
+  int vid[4];
+  load_face(m, f, p, vid);
+  const double A = signed_area3(p.x[0], p.y[0], p.x[1], p.y[1], p.x[2], p.y[2]) +
+                   signed_area3(p.x[0], p.y[0], p.x[2], p.y[2], p.x[3], p.y[3]);
+  dL_dA[f] = (acc != 0.0 && A != 0.0) ? -acc * r.value / A : 0.0;
+}
+
+// Per vertex (i, j) of the grid mesh, in a fixed order over the faces around it (face
+// (i,j) corner 0, (i-1,j) corner 1, (i-1,j-1) corner 2, (i,j-1) corner 3): with dL_dA,
+// sum_f dL/dA_f times the shoelace gradient dA/dx_c = (y_{c+1} - y_{c-1}) / 2,
+// dA/dy_c = (x_{c-1} - x_{c+1}) / 2; with cs, the per-face corner sums cs[f][c] as they are.
+__global__ void k_grid_vertex_gather(const double* xy, int n, const double* dL_dA, const double2* cs, double* out) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long V = (long)(n + 1) * (n + 1);
+  if (v >= V) return;
+  const int i = (int)(v / (n + 1)), j = (int)(v % (n + 1));
+  double gx = 0.0, gy = 0.0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int a = i - ((c == 1 || c == 2) ? 1 : 0), b = j - ((c == 2 || c == 3) ? 1 : 0);
+    if (a < 0 || b < 0 || a >= n || b >= n) continue;
+    const int f = b + a * n;
+    if (cs) {
+      const double2 t = cs[4 * (size_t)f + c];
+      gx += t.x;
+      gy += t.y;
+    } else {
+      const double g = dL_dA[f];
+      if (g == 0.0) continue;
+      Quad p;
+      int vid[4];
+      load_quad(xy, n, f, p, vid);
+      const int nx = (c + 1) & 3, pv = (c + 3) & 3;
+      gx += g * (0.5 * (p.y[nx] - p.y[pv]));
+      gy += g * (0.5 * (p.x[pv] - p.x[nx]));
+    }
+  }
+  out[2 * v] = gx;
+  out[2 * v + 1] = gy;
+}
+
+struct InvGrad {  // per located origin vertex: q = -e J^-T dL/dI and the weights of its first hit
+  double qx, qy, w[4];
+};
+
+// Origin vertex v = (i * (1/n), j * (1/n)) (mesh_utils.cpp:100-108) located in face
+// h = hit0[v] of the forward mesh with weights w of the bilinear coordinates
+// (u, v) = (w1 + w2, w2 + w3): its inverse position is I = sum_c w_c O_c with O the
+// origin corners (a square of side e, so dI/d(u,v) = e Id), and x = sum_c w_c P_c with P
+// the forward corners. Holding x fixed, d(u,v) = -J^-1 sum_c w_c dP_c with
+// J = [dx/du | dx/dv], hence dL/dP_c = -e w_c J^-T dL/dI.
+__global__ void k_inv_point_grad(const double* fwd, int n, const int* hit0, const double* dL_dI, InvGrad* pg,
+                                 int* count) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long V = (long)(n + 1) * (n + 1);
+  if (v >= V) return;
+  InvGrad g;
+  g.qx = g.qy = 0.0;
+  g.w[0] = g.w[1] = g.w[2] = g.w[3] = 0.0;
+  const int h = hit0[v];
+  if (h >= 0) {
+    const double dx = 1.0 / (double)n;
+    const double qx = (double)(v / (n + 1)) * dx, qy = (double)(v % (n + 1)) * dx;
+    Quad P;
+    int vid[4];
+    load_quad(fwd, n, h, P, vid);
+    double w[4];
+    if (bilinear_weights(qx, qy, P, w)) {
+      const double u = w[1] + w[2], t = w[2] + w[3];
+      const double jux = (1.0 - t) * (P.x[1] - P.x[0]) + t * (P.x[2] - P.x[3]);
+      const double juy = (1.0 - t) * (P.y[1] - P.y[0]) + t * (P.y[2] - P.y[3]);
+      const double jvx = (1.0 - u) * (P.x[3] - P.x[0]) + u * (P.x[2] - P.x[1]);
+      const double jvy = (1.0 - u) * (P.y[3] - P.y[0]) + u * (P.y[2] - P.y[1]);
+      const double det = jux * jvy - juy * jvx;
+      if (det != 0.0 && isfinite(det)) {
+        const double gx = dL_dI[2 * v], gy = dL_dI[2 * v + 1];
+        const double s = -dx / det;
+        g.qx = s * (jvy * gx - juy * gy);
+        g.qy = s * (-jvx * gx + jux * gy);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) g.w[c] = w[c];
+      }
+    }
+    atomicAdd(&count[h], 1);
+  }
+  pg[v] = g;
+}
+
+__global__ void k_inv_fill(long V, const int* hit0, const int* start, int* cursor, int* list) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= V) return;
+  const int h = hit0[v];
+  if (h >= 0) list[start[h] + atomicAdd(&cursor[h], 1)] = (int)v;
+}
+
+// Per face: its points in increasing index order (the fill order is arbitrary), then the
+// corner sums cs[f][c] = sum_points w_c q in that order.
+__global__ void k_inv_face_sums(int N, const int* start, int* list, const InvGrad* pg, double2* cs) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= N) return;
+  const int b = start[f], e = start[f + 1];
+  for (int a = b + 1; a < e; ++a) {  // insertion sort: lists hold a few points
+    const int key = list[a];
+    int k = a - 1;
+    while (k >= b && list[k] > key) {
+      list[k + 1] = list[k];
+      --k;
+    }
+    list[k + 1] = key;
+  }
+  double2 acc[4];
+#pragma unroll
+  for (int c = 0; c < 4; ++c) acc[c] = make_double2(0.0, 0.0);
+  for (int a = b; a < e; ++a) {
+    const InvGrad g = pg[list[a]];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      acc[c].x += g.w[c] * g.qx;
+      acc[c].y += g.w[c] * g.qy;
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) cs[4 * (size_t)f + c] = acc[c];
+}
+
 // ---- host ----
 
 static void build_locator(otm_map* m) {
@@ -920,6 +1064,77 @@ static void build_locator(otm_map* m) {
   m->leaf_box.reserve(sizeof(double4) * N);
   build_bvh_order(ctx, xy, n, m->bvh_rank.as<int>(), m->leaf_box.as<double4>());
   m->located = true;
+}
+
+}  // namespace otm
+
+namespace otm {
+
+// Inversion of `count` points (device buffers) through map m, in place; face / hit0 (the
+// first hit in the reference's order) / nhits may be null; missing is added to.
+void map_inverse_dev(otm_map* m, double* pts, long count, int mode, int* face, int* hit0, int* nhits,
+                     unsigned long long* missing) {
+  otm_context* ctx = m->ctx;
+  if (!m->located) build_locator(m);
+  if (count <= 0) return;
+  const unsigned grid = (unsigned)((count + 255) / 256);
+  launch(ctx, "inverse", k_inverse, grid, 256, (const double*)m->fwd.as<double>(),
+         (const double*)m->density.as<double>(), m->n, m->bins, (const int*)m->bin_start.as<int>(),
+         (const int*)m->bin_faces.as<int>(), (const double4*)m->face_box.as<double4>(),
+         (const int*)m->bvh_rank.as<int>(), (const double4*)m->leaf_box.as<double4>(), pts, count,
+         mode == OTM_INV_FIRST ? 1 : 0, face, hit0, nhits, missing);
+  OTM_CUDA(cudaGetLastError());
+}
+
+void raster_grid_backward(otm_context* ctx, int n, const double* xy, int rows, int cols, const double* dL_dpix,
+                          double* dL_dxy) {
+  const int N = n * n;
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  // the layout raster_mesh leaves in the scratch: face boxes, then pixel owners
+  const char* base = ctx->raster_scratch.as<char>();
+  const FaceRaster* fr = reinterpret_cast<const FaceRaster*>(base);
+  const int* owner = reinterpret_cast<const int*>(base + al(sizeof(FaceRaster) * (size_t)(N > 0 ? N : 1)));
+  DevBuf dA;
+  dA.reserve(sizeof(double) * N);
+  MeshRef m{xy, n, N, (n + 1) * (n + 1), nullptr, nullptr};
+  launch(ctx, "raster_area_grad", k_raster_area_grad, (N + 255) / 256, 256, m, rows, cols, fr, owner, dL_dpix,
+         dA.as<double>());
+  const long V = (long)(n + 1) * (n + 1);
+  launch(ctx, "area_vertex_grad", k_grid_vertex_gather, (unsigned)((V + 255) / 256), 256, xy, n,
+         (const double*)dA.as<double>(), (const double2*)nullptr, dL_dxy);
+  OTM_CUDA(cudaGetLastError());
+  OTM_CUDA(cudaStreamSynchronize(ctx->stream));  // dA is released on return
+}
+
+void inverse_grid_backward(otm_context* ctx, int n, const double* fwd, const int* hit0, const double* dL_dI,
+                           double* dL_dfwd) {
+  cudaStream_t st = ctx->stream;
+  const int N = n * n;
+  const long V = (long)(n + 1) * (n + 1);
+  auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+  const size_t b_pg = al(sizeof(InvGrad) * V), b_cnt = al(sizeof(int) * (N + 1)), b_list = al(sizeof(int) * V);
+  const size_t b_cs = al(sizeof(double2) * 4 * (size_t)N), b_sums = al(sizeof(int) * ((N + SCAN_B - 1) / SCAN_B + 1));
+  DevBuf buf;
+  buf.reserve(b_pg + 3 * b_cnt + b_list + b_cs + b_sums);
+  char* q = buf.as<char>();
+  InvGrad* pg = reinterpret_cast<InvGrad*>(q);
+  int* count = reinterpret_cast<int*>(q + b_pg);
+  int* start = reinterpret_cast<int*>(q + b_pg + b_cnt);
+  int* cursor = reinterpret_cast<int*>(q + b_pg + 2 * b_cnt);
+  int* list = reinterpret_cast<int*>(q + b_pg + 3 * b_cnt);
+  double2* cs = reinterpret_cast<double2*>(q + b_pg + 3 * b_cnt + b_list);
+  int* sums = reinterpret_cast<int*>(q + b_pg + 3 * b_cnt + b_list + b_cs);
+  OTM_CUDA(cudaMemsetAsync(count, 0, sizeof(int) * N, st));
+  OTM_CUDA(cudaMemsetAsync(cursor, 0, sizeof(int) * N, st));
+  const unsigned gv = (unsigned)((V + 255) / 256), gf = (unsigned)((N + 255) / 256);
+  launch(ctx, "inv_point_grad", k_inv_point_grad, gv, 256, fwd, n, hit0, dL_dI, pg, count);
+  exclusive_scan(st, count, start, sums, N);
+  launch(ctx, "inv_fill", k_inv_fill, gv, 256, V, hit0, (const int*)start, cursor, list);
+  launch(ctx, "inv_face_sums", k_inv_face_sums, gf, 256, N, (const int*)start, list, (const InvGrad*)pg, cs);
+  launch(ctx, "inv_vertex_grad", k_grid_vertex_gather, gv, 256, fwd, n, (const double*)nullptr, (const double2*)cs,
+         dL_dfwd);
+  OTM_CUDA(cudaGetLastError());
+  OTM_CUDA(cudaStreamSynchronize(st));  // the scratch is released on return
 }
 
 }  // namespace otm
@@ -995,13 +1210,7 @@ extern "C" int otm_map_inverse_mode(otm_map* m, double* points, long count, int 
     unsigned long long* dm = reinterpret_cast<unsigned long long*>(base + al(bp) + al(bf) + al(bh));
     if (!pdev) OTM_CUDA(cudaMemcpyAsync(dp, points, bp, cudaMemcpyHostToDevice, st));
     OTM_CUDA(cudaMemsetAsync(dm, 0, sizeof(unsigned long long), st));
-    unsigned grid = (unsigned)((count + 255) / 256);
-    launch(ctx, "inverse", k_inverse, grid, 256, (const double*)m->fwd.as<double>(),
-           (const double*)m->density.as<double>(), m->n, m->bins, (const int*)m->bin_start.as<int>(),
-           (const int*)m->bin_faces.as<int>(), (const double4*)m->face_box.as<double4>(),
-           (const int*)m->bvh_rank.as<int>(), (const double4*)m->leaf_box.as<double4>(), dp, (long)count,
-           mode == OTM_INV_FIRST ? 1 : 0, df, dh, dm);
-    OTM_CUDA(cudaGetLastError());
+    map_inverse_dev(m, dp, (long)count, mode, df, nullptr, dh, dm);
     if (!pdev) OTM_CUDA(cudaMemcpyAsync(points, dp, bp, cudaMemcpyDeviceToHost, st));
     if (face && !fdev) OTM_CUDA(cudaMemcpyAsync(face, df, bf, cudaMemcpyDeviceToHost, st));
     if (nhits && !hdev) OTM_CUDA(cudaMemcpyAsync(nhits, dh, bh, cudaMemcpyDeviceToHost, st));
@@ -1177,6 +1386,34 @@ extern "C" int otm_rasterize_mode(otm_context* ctx, int n, const double* xy, con
     }
     raster_grid(ctx, n, pxy, pden, rows, cols, mode, pimg);
     if (!idev) OTM_CUDA(cudaMemcpyAsync(img, pimg, sizeof(double) * pix, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    return (int)OTM_OK;
+  });
+}
+
+extern "C" int otm_rasterize_faces(otm_context* ctx, int n, const double* xy, int rows, int cols, int* face) {
+  return guarded([&] {
+    if (!ctx || !xy || !face) throw BadArg{"otm_rasterize_faces: null argument"};
+    if (n < 1 || n > 16384 || rows < 1 || cols < 1 || rows > 65536 || cols > 65536)
+      throw BadArg{"otm_rasterize_faces: size out of range"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    const size_t V2 = 2 * (size_t)(n + 1) * (n + 1), pix = (size_t)rows * cols;
+    DevBuf buf;
+    buf.reserve(sizeof(double) * (V2 + pix) + 256);
+    const double* pxy = xy;
+    if (!is_device_ptr(xy)) {
+      OTM_CUDA(cudaMemcpyAsync(buf.p, xy, sizeof(double) * V2, cudaMemcpyHostToDevice, st));
+      pxy = buf.as<double>();
+    }
+    double* img = buf.as<double>() + V2;
+    raster_grid(ctx, n, pxy, nullptr, rows, cols, OTM_RIO_PER_FACE, img);
+    const int N = n * n;
+    auto al = [](size_t b) { return (b + 255) / 256 * 256; };
+    const int* owner =
+        reinterpret_cast<const int*>(ctx->raster_scratch.as<char>() + al(sizeof(FaceRaster) * (size_t)N));
+    OTM_CUDA(cudaMemcpyAsync(face, owner, sizeof(int) * pix, cudaMemcpyDefault, st));
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();
     return (int)OTM_OK;

@@ -4,6 +4,7 @@
 // without FMA contraction so the per-element arithmetic rounds as the reference's does.
 
 #include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "context.h"
@@ -317,6 +318,231 @@ extern "C" int otm_grid_transport_cost(otm_context* ctx, int n, const double* gr
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();
     *total = res;
+    return (int)OTM_OK;
+  });
+}
+
+// ---- differentiable barycenter image (apps/barycenters.cpp:184-198, 250-290) ----
+
+namespace otm {
+
+// The origin grid vertices, vertex v = j + i (n+1) at (i * (1/n), j * (1/n))
+// (utils/mesh_utils.cpp:100-108).
+__global__ void k_origin_grid(int n, double* xy) {
+  const long v = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long V = (long)(n + 1) * (n + 1);
+  if (v >= V) return;
+  const double dx = 1.0 / (double)n;
+  xy[2 * v] = (double)(v / (n + 1)) * dx;
+  xy[2 * v + 1] = (double)(v % (n + 1)) * dx;
+}
+
+// Per-block partial sums of (img - t)^2 and of g R (g = 2 (img - t), R = img / s the
+// raster before rescaling), and g itself.
+__global__ void k_bary_loss(long count, const double* img, const double* target, double inv_s, double* g,
+                            double* partial) {
+  __shared__ double red[64];
+  double v[2] = {0.0, 0.0};
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < count; t += (long)gridDim.x * blockDim.x) {
+    const double d = img[t] - target[t];
+    const double gt = 2.0 * d;
+    g[t] = gt;
+    v[0] += d * d;
+    v[1] += gt * (img[t] * inv_s);
+  }
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = v[0];
+    partial[2 * blockIdx.x + 1] = v[1];
+  }
+}
+
+__global__ void k_sum_partials2(int nparts, const double* partial, double* out) {
+  __shared__ double red[64];
+  double v[2] = {0.0, 0.0};
+  for (int b = threadIdx.x; b < nparts; b += blockDim.x) {
+    v[0] += partial[2 * b];
+    v[1] += partial[2 * b + 1];
+  }
+  block_sum<2>(v, red);
+  if (threadIdx.x == 0) {
+    out[0] = v[0];
+    out[1] = v[1];
+  }
+}
+
+// dL/dR = s (g - c2) in place of g.
+__global__ void k_bary_dR(long count, double s, double c2, double* g) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < count) g[t] = s * (g[t] - c2);
+}
+
+__global__ void k_scale(long count, double a, const double* x, double* y) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < count) y[t] = a * x[t];
+}
+
+__global__ void k_add_const(long count, double c, double* y) {
+  const long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < count) y[t] = y[t] + c;
+}
+
+}  // namespace otm
+
+extern "C" int otm_barycenter_loss(otm_context* ctx, int n, int count, const double* const* density,
+                                   const double* weights, int res, const double* target,
+                                   const otm_solver_options* opt, const otm_adjoint_options* aopt, double* image,
+                                   double* loss, double* const* grad_density, otm_barycenter_stats* stats) {
+  return guarded([&] {
+    if (!ctx || !density || !weights || !target || count < 1 || count > 8)
+      throw BadArg{"otm_barycenter_loss: bad arguments"};
+    if (n < 1 || n > 16384 || res < 1 || res > 65536) throw BadArg{"otm_barycenter_loss: size out of range"};
+    for (int k = 0; k < count; ++k)
+      if (!density[k] || (grad_density && !grad_density[k])) throw BadArg{"otm_barycenter_loss: null buffer"};
+    make_current(ctx);
+    cudaStream_t st = ctx->stream;
+    const size_t N = (size_t)n * n, V = (size_t)(n + 1) * (n + 1), V2 = 2 * V, pix = (size_t)res * res;
+    const int nparts = 512;
+    auto al = [](size_t w) { return (w + 31) / 32 * 32; };  // in doubles
+    // device layout: per map raw density, adjusted density, gradient, forward mesh, inverse
+    // mesh (later dL/dI), dL/dF, first hits; then the blend, its gradient, image, target,
+    // g, partials, scalars, blend pointers and weights
+    const size_t per = al(N) * 3 + al(V2) * 3 + al((V + 1) / 2);
+    DevBuf buf;
+    buf.reserve(sizeof(double) * (per * count + al(V2) * 2 + al(pix) * 3 + al(2 * nparts) + al(64) + al(8) * 2));
+    double* p = buf.as<double>();
+    auto take = [&](size_t w) {
+      double* r = p;
+      p += al(w);
+      return r;
+    };
+    std::vector<double*> rho(count), adj(count), fwd(count), inv(count), dF(count), grad(count);
+    std::vector<int*> hit0(count);
+    for (int k = 0; k < count; ++k) {
+      rho[k] = take(N);
+      adj[k] = take(N);
+      grad[k] = take(N);
+      fwd[k] = take(V2);
+      inv[k] = take(V2);
+      dF[k] = take(V2);
+      hit0[k] = reinterpret_cast<int*>(take((V + 1) / 2));
+    }
+    double* blend = take(V2);
+    double* dB = take(V2);
+    double* img = take(pix);
+    double* tgt = take(pix);
+    double* g = take(pix);
+    double* part = take(2 * nparts);
+    double* scal = take(64);  // reduction results and the missing counter
+    const double** d_ptrs = reinterpret_cast<const double**>(take(8));
+    double* d_w = take(8);
+
+    // inputs and the expected mean sum_k w_k mean(density_k) (barycenters.cpp:193, 283)
+    for (int k = 0; k < count; ++k) copy_in(ctx, rho[k], density[k], sizeof(double) * N);
+    copy_in(ctx, tgt, target, sizeof(double) * pix);
+    for (int k = 0; k < count; ++k) {
+      launch(ctx, "img_partials", k_img_partials, nparts, 256, (long)N, (const double*)rho[k], part);
+      launch(ctx, "sum_partials", k_sum_partials, 1, 256, nparts, (const double*)part, scal + k);
+    }
+    std::vector<double> hs(count);
+    OTM_CUDA(cudaMemcpyAsync(hs.data(), scal, sizeof(double) * count, cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    double expected = 0.0;
+    for (int k = 0; k < count; ++k) {
+      const double mean = hs[k] / (double)N;
+      expected = k == 0 ? weights[0] * mean : expected + weights[k] * mean;
+    }
+
+    // forward maps (one batch), inverse meshes of the origin grid
+    std::vector<int> ns(count, n);
+    std::vector<const double*> rin(rho.begin(), rho.end());
+    std::vector<otm_solve_stats> sst(count);
+    int rc = otm_solve_batch(ctx, count, ns.data(), rin.data(), opt, fwd.data(), adj.data(), sst.data());
+    if (rc != OTM_OK) return rc;
+    unsigned long long* d_missing = reinterpret_cast<unsigned long long*>(scal + 16);
+    OTM_CUDA(cudaMemsetAsync(d_missing, 0, sizeof(unsigned long long), st));
+    const unsigned gv = (unsigned)((V + 255) / 256), gv2 = (unsigned)((V2 + 255) / 256);
+    for (int k = 0; k < count; ++k) {
+      otm_map* m = nullptr;
+      rc = otm_map_create(ctx, n, fwd[k], adj[k], &m);
+      if (rc != OTM_OK) return rc;
+      try {
+        launch(ctx, "origin_grid", k_origin_grid, gv, 256, n, inv[k]);
+        map_inverse_dev(m, inv[k], (long)V, OTM_INV_DENSEST, nullptr, hit0[k], nullptr, d_missing);
+        OTM_CUDA(cudaStreamSynchronize(st));
+      } catch (...) {
+        otm_map_destroy(m);
+        throw;
+      }
+      otm_map_destroy(m);
+    }
+
+    // blend, raster, rescale, loss
+    OTM_CUDA(cudaMemcpyAsync(d_w, weights, sizeof(double) * count, cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(d_ptrs, inv.data(), sizeof(double*) * count, cudaMemcpyHostToDevice, st));
+    launch(ctx, "blend", k_blend, gv2, 256, (long)V2, count, (const double* const*)d_ptrs, (const double*)d_w,
+           blend);
+    raster_grid(ctx, n, blend, nullptr, res, res, OTM_RIO_PER_FACE, img);
+    launch(ctx, "img_partials", k_img_partials, nparts, 256, (long)pix, (const double*)img, part);
+    const unsigned sb = (unsigned)std::min<size_t>((pix + 255) / 256, (size_t)4 * ctx->num_sms);
+    launch(ctx, "img_rescale", k_img_rescale, sb, 256, (long)pix, nparts, (const double*)part, expected, img,
+           scal + 8);
+    double rmean = 0.0;
+    OTM_CUDA(cudaMemcpyAsync(&rmean, scal + 8, sizeof(double), cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    const double s = expected / rmean;  // image = s R
+    launch(ctx, "bary_loss", k_bary_loss, nparts, 256, (long)pix, (const double*)img, (const double*)tgt, 1.0 / s, g,
+           part);
+    launch(ctx, "sum_partials2", k_sum_partials2, 1, 256, nparts, (const double*)part, scal + 10);
+    double red2[2];
+    unsigned long long miss = 0;
+    OTM_CUDA(cudaMemcpyAsync(red2, scal + 10, sizeof(red2), cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaMemcpyAsync(&miss, d_missing, sizeof(miss), cudaMemcpyDeviceToHost, st));
+    OTM_CUDA(cudaStreamSynchronize(st));
+    const double L = red2[0], sgR = red2[1];
+    std::vector<int> solves(count, 0);
+
+    if (grad_density) {
+      // dL/dR = s (g - sum(g R) / sum(R)); dL/dexpected = sum(g R) / mean(R)
+      const double sumR = rmean * (double)pix;
+      const double c2 = sgR / sumR, dL_dexp = sgR / rmean;
+      const unsigned gp = (unsigned)((pix + 255) / 256);
+      launch(ctx, "bary_dR", k_bary_dR, gp, 256, (long)pix, s, c2, g);
+      raster_grid_backward(ctx, n, blend, res, res, g, dB);
+      otm_adjoint_options ao;
+      otm_default_adjoint_options(&ao);
+      if (aopt) ao = *aopt;
+      for (int k = 0; k < count; ++k) {
+        double* dI = inv[k];  // the inverse mesh is no longer needed: its buffer holds dL/dI
+        launch(ctx, "scale", k_scale, gv2, 256, (long)V2, weights[k], (const double*)dB, dI);
+        inverse_grid_backward(ctx, n, fwd[k], hit0[k], dI, dF[k]);
+        otm_adjoint_stats ast;
+        rc = otm_adjoint(ctx, n, rho[k], fwd[k], dF[k], &ao, grad[k], &ast);
+        if (rc != OTM_OK) return rc;
+        solves[k] = ast.iterations;
+        // expected = ... + w_k mean(density_k): d/ddensity_k = w_k / N per cell
+        launch(ctx, "add_const", k_add_const, (unsigned)((N + 255) / 256), 256, (long)N,
+               weights[k] * dL_dexp / (double)N, grad[k]);
+        copy_out(ctx, grad_density[k], grad[k], sizeof(double) * N);
+      }
+    }
+    if (image) copy_out(ctx, image, img, sizeof(double) * pix);
+    OTM_CUDA(cudaGetLastError());
+    OTM_CUDA(cudaStreamSynchronize(st));
+    ctx->prof.flush();
+    if (loss) *loss = L;
+    if (stats) {
+      std::memset(stats, 0, sizeof(*stats));
+      for (int k = 0; k < count; ++k) {
+        stats->iterations[k] = sst[k].iterations;
+        stats->outcome[k] = sst[k].outcome;
+        stats->residual[k] = sst[k].residual;
+        stats->adjoint_solves[k] = solves[k];
+      }
+      stats->inverse_missing = (long)miss;
+      stats->expected_mean = expected;
+      stats->raster_mean = rmean;
+    }
     return (int)OTM_OK;
   });
 }

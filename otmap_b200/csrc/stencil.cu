@@ -68,6 +68,7 @@ template <int NS, int NP>
 struct Ring {
   static constexpr int SS = 36;  // slots of a stencil field row
   static constexpr int STAGE = NS * SS + NP * 32;
+  static constexpr int STAGE_BYTES = STAGE * 8;
   double* buf;  // RD * STAGE doubles (this warp's)
   const double* sf[NS > 0 ? NS : 1];
   const double* pf[NP > 0 ? NP : 1];
@@ -75,6 +76,14 @@ struct Ring {
   bool interior;              // 16-byte copies (warp-uniform)
   int soff, gcol;             // this lane's stencil slot and global column (interior copies)
 
+  // the sweeps' fields: psi, d_hat, d_prev; r_k (, r_{k-1})
+  __device__ __forceinline__ void bind(const Inst& I, int it) {
+    sf[0] = I.psi[it & 1];
+    sf[1] = I.dhat;
+    sf[2] = I.d[(it + 1) & 1];
+    pf[0] = I.r[it % 3];
+    if constexpr (NP > 1) pf[1] = I.r[(it + 2) % 3];
+  }
   __device__ __forceinline__ void setup() {
     interior = (j0 >= 2) && (j0 + 34 <= n) && ((n & 1) == 0);
     soff = lane < 16 ? 2 + 2 * lane : (lane == 16 ? 0 : 34);
@@ -271,8 +280,125 @@ __device__ __forceinline__ void update_step(Inst& I, double rmax, int n, int it)
   if (!I.active) stop_outcome(I);
 }
 
-__global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip_inst, int base, double* partials) {
-  extern __shared__ __align__(16) double ring_smem[];
+// ---- split precision (OTM_PRECISION_SPLIT) ----
+//
+// r_k, r_{k-1}, d_hat and d are stored in FP32 (psi stays FP64): the sweeps move 24 and
+// 36 bytes per cell instead of 40 and 56. The per-cell arithmetic stays FP64: the staged
+// FP32 values are converted exactly when read, so the line coefficients a, b are exact
+// for the directions the update applies and the line search's tracked residual stays
+// that of the stored residual. (Forming the directions' vertex gradients and diagonals in
+// FP32 is not enough: they are second differences of smooth fields, and the cancellation
+// left about 1e-4 relative error in a and b; at 1024^2 the tracked residual then drifted
+// away from the mesh's, solves stopped 5e-3 away from the reference's map or ran to
+// max_iter.) d and r' are rounded to FP32 when stored; psi' = psi + alpha d uses the
+// unrounded d, as do a and b of the update.
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16v(void* dst, const void* src) {
+  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
+}
+
+// Prefetch ring of the split form: the FP64 potential (36 doubles as in Ring), two FP32
+// stencil fields d_hat, d_prev (40 floats: columns j0-4 .. j0+35, slot 4 + lane is column
+// j) and NP FP32 pointwise fields r_k (, r_{k-1}) (32 floats). Interior strips (j0 >= 4,
+// j0 + 36 <= n, n a multiple of 4) copy with 16-byte cp.async (18 lanes for the FP64 row,
+// 10 per FP32 stencil row, 8 per pointwise row); edge strips copy element-wise with
+// clamped columns. Reads return FP64 rows and values, as Ring's do.
+template <int NP>
+struct RingS {
+  static constexpr int NS = 2, PD = 36, FS = 40, FP = 32;
+  static constexpr int STAGE_BYTES = PD * 8 + NS * FS * 4 + NP * FP * 4;
+  static_assert(STAGE_BYTES % 16 == 0, "stages stay 16-byte aligned");
+  unsigned char* buf;  // RD * STAGE_BYTES (this warp's)
+  const double* psi;
+  const float* sf[NS];
+  const float* pf[NP];
+  int n, j0, lane, rows_end;
+  bool interior;
+  int soff, gcol;  // this lane's FP64 slot and column (interior copies)
+
+  __device__ __forceinline__ void bind(const Inst& I, int it) {
+    psi = I.psi[it & 1];
+    sf[0] = reinterpret_cast<const float*>(I.dhat);
+    sf[1] = reinterpret_cast<const float*>(I.d[(it + 1) & 1]);
+    pf[0] = reinterpret_cast<const float*>(I.r[it % 3]);
+    if constexpr (NP > 1) pf[1] = reinterpret_cast<const float*>(I.r[(it + 2) % 3]);
+  }
+  __device__ __forceinline__ void setup() {
+    interior = (j0 >= 4) && (j0 + 36 <= n) && ((n & 3) == 0);
+    soff = lane < 16 ? 2 + 2 * lane : (lane == 16 ? 0 : 34);
+    gcol = lane < 16 ? j0 + 2 * lane : (lane == 16 ? j0 - 2 : j0 + 32);
+  }
+  __device__ __forceinline__ unsigned char* stage(int row) {
+    return buf + ((unsigned)(row + RD) & (RD - 1u)) * STAGE_BYTES;
+  }
+  __device__ __forceinline__ double* pstage(int row) { return reinterpret_cast<double*>(stage(row)); }
+  __device__ __forceinline__ float* fstage(int row, int k) {
+    return reinterpret_cast<float*>(stage(row) + PD * 8) + k * FS;
+  }
+  __device__ __forceinline__ float* ptstage(int row, int k) {
+    return reinterpret_cast<float*>(stage(row) + PD * 8 + NS * FS * 4) + k * FP;
+  }
+  __device__ __forceinline__ void issue(int row) {
+    if (row <= rows_end) {
+      double* sp = pstage(row);
+      const size_t base = (size_t)clampn(row, n) * n;
+      if (interior) {
+        if (lane < 18) cp_async16v(sp + soff, psi + base + gcol);
+        if (lane < 10) {
+#pragma unroll
+          for (int k = 0; k < NS; ++k) cp_async16v(fstage(row, k) + 4 * lane, sf[k] + base + j0 - 4 + 4 * lane);
+        }
+        if (lane < 8) {
+#pragma unroll
+          for (int k = 0; k < NP; ++k) cp_async16v(ptstage(row, k) + 4 * lane, pf[k] + base + j0 + 4 * lane);
+        }
+      } else {
+        const size_t cj = base + clampn(j0 + lane, n);
+        cp_async8(sp + 2 + lane, psi + cj);
+        if (lane == 0) cp_async8(sp + 1, psi + base + clampn(j0 - 1, n));
+        if (lane == 31) cp_async8(sp + 34, psi + base + clampn(j0 + 32, n));
+#pragma unroll
+        for (int k = 0; k < NS; ++k) {
+          float* d = fstage(row, k);
+          cp_async4(d + 4 + lane, sf[k] + cj);
+          if (lane == 0) cp_async4(d + 3, sf[k] + base + clampn(j0 - 1, n));
+          if (lane == 31) cp_async4(d + 36, sf[k] + base + clampn(j0 + 32, n));
+        }
+#pragma unroll
+        for (int k = 0; k < NP; ++k) cp_async4(ptstage(row, k) + lane, pf[k] + cj);
+      }
+    }
+    cp_async_commit();
+  }
+  // field 0: the potential; fields 1, 2: d_hat, d_prev (converted to FP64, exactly)
+  __device__ __forceinline__ Row row_of(int row, int k) {
+    Row r;
+    if (k == 0) {
+      const double* d = pstage(row);
+      r.c = d[2 + lane];
+      r.l = d[1 + lane];
+      r.r = d[3 + lane];
+    } else {
+      const float* d = fstage(row, k - 1);
+      r.c = (double)d[4 + lane];
+      r.l = (double)d[3 + lane];
+      r.r = (double)d[5 + lane];
+    }
+    return r;
+  }
+  __device__ __forceinline__ double point(int row, int k) { return (double)ptstage(row, k)[lane]; }
+};
+
+// The two sweeps over a ring type: Ring<3, NP> (every field FP64) or RingS<NP> (split
+// precision: FP32 storage of r, d_hat, d; FP64 arithmetic).
+template <class RT, bool SPLIT>
+__global__ __launch_bounds__(ST) void k_sweep_sums_t(Inst* insts, const int* strip_inst, int base, double* partials) {
+  extern __shared__ __align__(16) unsigned char ring_raw[];
   __shared__ double red[32 * S_COUNT];
   const int blk = base + blockIdx.x;
   Inst& I = insts[strip_inst[blk]];
@@ -286,13 +412,9 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
 #pragma unroll
   for (int k = 0; k < S_COUNT; ++k) acc[k] = 0.0;
   if (sc.i0 < n) {
-    Ring<3, 2> R;
-    R.buf = ring_smem + sc.warp * RD * Ring<3, 2>::STAGE;
-    R.sf[0] = I.psi[it & 1];
-    R.sf[1] = I.dhat;
-    R.sf[2] = I.d[(it + 1) & 1];
-    R.pf[0] = I.r[it % 3];
-    R.pf[1] = I.r[(it + 2) % 3];
+    RT R;
+    R.buf = reinterpret_cast<decltype(R.buf)>(ring_raw + (size_t)sc.warp * RD * RT::STAGE_BYTES);
+    R.bind(I, it);
     R.n = n;
     R.j0 = sc.j0;
     R.lane = sc.lane;
@@ -362,8 +484,10 @@ __global__ __launch_bounds__(ST) void k_sweep_sums(Inst* insts, const int* strip
   }
 }
 
-__global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* strip_inst, int base, double* partials) {
-  extern __shared__ __align__(16) double ring_smem[];
+template <class RT, bool SPLIT>
+__global__ __launch_bounds__(ST) void k_sweep_update_t(Inst* insts, const int* strip_inst, int base,
+                                                       double* partials) {
+  extern __shared__ __align__(16) unsigned char ring_raw[];
   __shared__ double red[32];
   const int blk = base + blockIdx.x;
   Inst& I = insts[strip_inst[blk]];
@@ -374,17 +498,12 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
   const double beta = I.beta;
   const StripCoord sc = strip_coord(I, blk);
   const int j = sc.j0 + sc.lane;
-  double* dnew = I.d[it & 1];
   double* psin = I.psi[(it + 1) & 1];
-  double* rn = I.r[(it + 1) % 3];
   double mx = -INFINITY;
   if (sc.i0 < n) {
-    Ring<3, 1> R;
-    R.buf = ring_smem + sc.warp * RD * Ring<3, 1>::STAGE;
-    R.sf[0] = I.psi[it & 1];
-    R.sf[1] = I.dhat;
-    R.sf[2] = I.d[(it + 1) & 1];
-    R.pf[0] = I.r[it % 3];
+    RT R;
+    R.buf = reinterpret_cast<decltype(R.buf)>(ring_raw + (size_t)sc.warp * RD * RT::STAGE_BYTES);
+    R.bind(I, it);
     R.n = n;
     R.j0 = sc.j0;
     R.lane = sc.lane;
@@ -423,11 +542,18 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
         const size_t f = (size_t)c * n + j;
         double a, b;
         line_ab(diag(gp, np), diag(gd, nd), es, a, b);
-        dnew[f] = dc.c;
         psin[f] = pc.c + alpha * dc.c;
         // (n/2)^2 / 2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
         double r = h2 * (a * (alpha * alpha) + b * alpha) + R.point(c, 0);
-        rn[f] = r;
+        if constexpr (SPLIT) {
+          reinterpret_cast<float*>(I.d[it & 1])[f] = (float)dc.c;
+          const float rf = (float)r;
+          reinterpret_cast<float*>(I.r[(it + 1) % 3])[f] = rf;
+          r = (double)rf;
+        } else {
+          I.d[it & 1][f] = dc.c;
+          I.r[(it + 1) % 3][f] = r;
+        }
         mx = fmax(mx, r);
       }
       gp = np;
@@ -450,361 +576,27 @@ __global__ __launch_bounds__(ST) void k_sweep_update(Inst* insts, const int* str
   }
 }
 
-// ---- split precision (OTM_PRECISION_SPLIT) ----
-//
-// psi stays FP64; r_k, r_{k-1}, d_hat and d are FP32 arrays. The sweeps form the
-// potential's vertex gradients and diagonals in FP64 (differences of neighbouring
-// potentials need its precision), the direction's and the per-cell line coefficients in
-// FP32, and take every product that enters a sum, the sums themselves, beta, the quartic
-// and its root in FP64: the tracked residual is the line search's own estimate
-// (otsolver_2dgrid.cpp:605), so the sums must keep FP64 accuracy. psi' = psi + alpha d is
-// formed in FP64, r' = r + alpha b + alpha^2 a in FP32. Algorithmic bytes per cell: sums
-// 24 (psi 8, d_hat, d_prev, r_k, r_{k-1} 4 each), update 36 (reads psi, d_hat, d_prev,
-// r_k; writes psi' 8, d 4, r' 4).
-
-struct RowF {
-  float c, l, r;
-};
-struct VGf {
-  float gx, gy, gxr, gyr;
-};
-struct Diagf {
-  float ax, ay, bx, by;
-};
-
-__device__ __forceinline__ VGf vgradf(const RowF& a, const RowF& b) {
-  VGf g;
-  const float sc = a.c + b.c;
-  g.gx = (b.l + b.c) - (a.l + a.c);
-  g.gy = sc - (a.l + b.l);
-  g.gxr = (b.c + b.r) - (a.c + a.r);
-  g.gyr = (a.r + b.r) - sc;
-  return g;
-}
-
-__device__ __forceinline__ Diagf diagf(const VGf& p, const VGf& q) {
-  Diagf d;
-  d.ax = q.gxr - p.gx;
-  d.ay = q.gyr - p.gy;
-  d.bx = p.gxr - q.gx;
-  d.by = p.gyr - q.gy;
-  return d;
-}
-
-// The potential's shifted diagonals (FP64 differences, then FP32): g.ax + e, g.ay + e,
-// g.bx - e, g.by + e of line_ab.
-__device__ __forceinline__ Diagf shifted(const Diag& g, double e) {
-  Diagf d;
-  d.ax = (float)(g.ax + e);
-  d.ay = (float)(g.ay + e);
-  d.bx = (float)(g.bx - e);
-  d.by = (float)(g.by + e);
-  return d;
-}
-
-__device__ __forceinline__ void line_abf(const Diagf& g0, const Diagf& h, float& a, float& b) {
-  a = h.ax * h.by - h.ay * h.bx;
-  b = h.ax * g0.by - h.ay * g0.bx + g0.ax * h.by - g0.ay * h.bx;
-}
-
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async16v(void* dst, const void* src) {
-  unsigned s = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src) : "memory");
-}
-
-// Prefetch ring for one FP64 stencil field (the potential; 36 doubles as in Ring), NS
-// FP32 stencil fields (40 floats: columns j0-4 .. j0+35, slot 4 + lane is column j) and
-// NP FP32 pointwise fields (32 floats). Interior strips (j0 >= 4, j0 + 36 <= n, n a
-// multiple of 4) copy with 16-byte cp.async (18 lanes for the FP64 row, 10 per FP32
-// stencil row, 8 per pointwise row); edge strips copy element-wise with clamped columns.
-template <int NS, int NP>
-struct RingS {
-  static constexpr int PD = 36, FS = 40, FP = 32;
-  static constexpr int STAGE = PD * 8 + NS * FS * 4 + NP * FP * 4;  // bytes
-  static_assert(STAGE % 16 == 0, "stages stay 16-byte aligned");
-  unsigned char* buf;  // RD * STAGE bytes (this warp's)
-  const double* psi;
-  const float* sf[NS > 0 ? NS : 1];
-  const float* pf[NP > 0 ? NP : 1];
-  int n, j0, lane, rows_end;
-  bool interior;
-  int soff, gcol;  // this lane's FP64 slot and column (interior copies)
-
-  __device__ __forceinline__ void setup() {
-    interior = (j0 >= 4) && (j0 + 36 <= n) && ((n & 3) == 0);
-    soff = lane < 16 ? 2 + 2 * lane : (lane == 16 ? 0 : 34);
-    gcol = lane < 16 ? j0 + 2 * lane : (lane == 16 ? j0 - 2 : j0 + 32);
-  }
-  __device__ __forceinline__ unsigned char* stage(int row) {
-    return buf + ((unsigned)(row + RD) & (RD - 1u)) * STAGE;
-  }
-  __device__ __forceinline__ double* pstage(int row) { return reinterpret_cast<double*>(stage(row)); }
-  __device__ __forceinline__ float* fstage(int row, int k) {
-    return reinterpret_cast<float*>(stage(row) + PD * 8) + k * FS;
-  }
-  __device__ __forceinline__ float* ptstage(int row, int k) {
-    return reinterpret_cast<float*>(stage(row) + PD * 8 + NS * FS * 4) + k * FP;
-  }
-
-  __device__ __forceinline__ void issue(int row) {
-    if (row <= rows_end) {
-      double* sp = pstage(row);
-      const size_t base = (size_t)clampn(row, n) * n;
-      if (interior) {
-        if (lane < 18) cp_async16v(sp + soff, psi + base + gcol);
-        if (lane < 10) {
-#pragma unroll
-          for (int k = 0; k < NS; ++k) cp_async16v(fstage(row, k) + 4 * lane, sf[k] + base + j0 - 4 + 4 * lane);
-        }
-        if (lane < 8) {
-#pragma unroll
-          for (int k = 0; k < NP; ++k) cp_async16v(ptstage(row, k) + 4 * lane, pf[k] + base + j0 + 4 * lane);
-        }
-      } else {
-        const size_t cj = base + clampn(j0 + lane, n);
-        cp_async8(sp + 2 + lane, psi + cj);
-        if (lane == 0) cp_async8(sp + 1, psi + base + clampn(j0 - 1, n));
-        if (lane == 31) cp_async8(sp + 34, psi + base + clampn(j0 + 32, n));
-#pragma unroll
-        for (int k = 0; k < NS; ++k) {
-          float* d = fstage(row, k);
-          cp_async4(d + 4 + lane, sf[k] + cj);
-          if (lane == 0) cp_async4(d + 3, sf[k] + base + clampn(j0 - 1, n));
-          if (lane == 31) cp_async4(d + 36, sf[k] + base + clampn(j0 + 32, n));
-        }
-#pragma unroll
-        for (int k = 0; k < NP; ++k) cp_async4(ptstage(row, k) + lane, pf[k] + cj);
-      }
-    }
-    cp_async_commit();
-  }
-  __device__ __forceinline__ Row prow(int row) {
-    const double* d = pstage(row);
-    Row r;
-    r.c = d[2 + lane];
-    r.l = d[1 + lane];
-    r.r = d[3 + lane];
-    return r;
-  }
-  __device__ __forceinline__ RowF frow(int row, int k) {
-    const float* d = fstage(row, k);
-    RowF r;
-    r.c = d[4 + lane];
-    r.l = d[3 + lane];
-    r.r = d[5 + lane];
-    return r;
-  }
-  __device__ __forceinline__ float point(int row, int k) { return ptstage(row, k)[lane]; }
-};
-
-// The split-precision form of k_sweep_sums (same sums, same last-block step).
-__global__ __launch_bounds__(ST) void k_sweep_sums_split(Inst* insts, const int* strip_inst, int base,
-                                                         double* partials) {
-  extern __shared__ __align__(16) unsigned char ring_raw[];
-  __shared__ double red[32 * S_COUNT];
-  const int blk = base + blockIdx.x;
-  Inst& I = insts[strip_inst[blk]];
-  if (!I.active) return;
-  const int n = I.n, it = I.it;
-  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw;
-  const StripCoord sc = strip_coord(I, blk);
-  const int j = sc.j0 + sc.lane;
-  double acc[S_COUNT];
-#pragma unroll
-  for (int k = 0; k < S_COUNT; ++k) acc[k] = 0.0;
-  if (sc.i0 < n) {
-    using RS = RingS<2, 2>;
-    RS R;
-    R.buf = ring_raw + (size_t)sc.warp * RD * RS::STAGE;
-    R.psi = I.psi[it & 1];
-    R.sf[0] = reinterpret_cast<const float*>(I.dhat);
-    R.sf[1] = reinterpret_cast<const float*>(I.d[(it + 1) & 1]);
-    R.pf[0] = reinterpret_cast<const float*>(I.r[it % 3]);
-    R.pf[1] = reinterpret_cast<const float*>(I.r[(it + 2) % 3]);
-    R.n = n;
-    R.j0 = sc.j0;
-    R.lane = sc.lane;
-    const int last = min(sc.i0 + I.srows, n);
-    R.rows_end = last;
-    R.setup();
-#pragma unroll
-    for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
-    VG gp;
-    VGf gh, gq;
-#pragma unroll 2
-    for (int row = sc.i0; row <= last; ++row) {
-      cp_async_wait<RD - 3>();
-      __syncwarp();
-      const Row ap = R.prow(row - 1), bp = R.prow(row);
-      const RowF ah = R.frow(row - 1, 0), aq = R.frow(row - 1, 1);
-      const RowF bh = R.frow(row, 0), bq = R.frow(row, 1);
-      VG np = vgrad(ap, bp);
-      VGf nh = vgradf(ah, bh);
-      VGf nq = vgradf(aq, bq);
-      if (row > sc.i0 && j < n) {
-        const int c = row - 1;
-        const Diagf G = shifted(diag(gp, np), es);
-        const Diagf Hd = diagf(gh, nh), Qd = diagf(gq, nq);
-        float a11f, b1f, a22f, b2f;
-        line_abf(G, Hd, a11f, b1f);
-        line_abf(G, Qd, a22f, b2f);
-        const float a12f = Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx;
-        const float rf = R.point(c, 0);
-        const double a11 = a11f, b1 = b1f, a22 = a22f, b2 = b2f, a12 = a12f;
-        const double r = rf, jd = (double)(rf - R.point(c, 1));
-        const double hv = ah.c, qv = aq.c;
-        acc[S_HH] = fma(hv, hv, acc[S_HH]);
-        acc[S_HQ] = fma(hv, qv, acc[S_HQ]);
-        acc[S_QQ] = fma(qv, qv, acc[S_QQ]);
-        acc[S_JB] = fma(jd, b1, acc[S_JB]);
-        acc[S_JA] = fma(jd, a11, acc[S_JA]);
-        acc[S_JJ] = fma(jd, jd, acc[S_JJ]);
-        acc[S_B1R] = fma(b1, r, acc[S_B1R]);
-        acc[S_B2R] = fma(b2, r, acc[S_B2R]);
-        acc[S_B1B1] = fma(b1, b1, acc[S_B1B1]);
-        acc[S_B1B2] = fma(b1, b2, acc[S_B1B2]);
-        acc[S_B2B2] = fma(b2, b2, acc[S_B2B2]);
-        acc[S_A11R] = fma(a11, r, acc[S_A11R]);
-        acc[S_A12R] = fma(a12, r, acc[S_A12R]);
-        acc[S_A22R] = fma(a22, r, acc[S_A22R]);
-        acc[S_AB0] = fma(a11, b1, acc[S_AB0]);
-        acc[S_AB1] = fma(a11, b2, fma(a12, b1, acc[S_AB1]));
-        acc[S_AB2] = fma(a12, b2, fma(a22, b1, acc[S_AB2]));
-        acc[S_AB3] = fma(a22, b2, acc[S_AB3]);
-        acc[S_AA0] = fma(a11, a11, acc[S_AA0]);
-        acc[S_AA1] = fma(a11, a12, acc[S_AA1]);
-        acc[S_AA2] = fma(a12, a12, fma(a11 + a11, a22, acc[S_AA2]));
-        acc[S_AA3] = fma(a12, a22, acc[S_AA3]);
-        acc[S_AA4] = fma(a22, a22, acc[S_AA4]);
-      }
-      gp = np;
-      gh = nh;
-      gq = nq;
-      __syncwarp();
-      R.issue(row - 2 + RD);
-    }
-    cp_async_wait<0>();
-  }
-  write_partials<S_COUNT>(acc, red, partials, blk);
-  if (last_block(&I.counter, I.nstrip)) {
-    double S[S_COUNT];
-    reduce_block_partials<S_COUNT>(partials, I.strip0, I.nstrip, S, red);
-    if (threadIdx.x == 0) sums_step(I, S, n, it);
-  }
-}
-
-// The split-precision form of k_sweep_update.
-__global__ __launch_bounds__(ST) void k_sweep_update_split(Inst* insts, const int* strip_inst, int base,
-                                                           double* partials) {
-  extern __shared__ __align__(16) unsigned char ring_raw[];
-  __shared__ double red[32];
-  const int blk = base + blockIdx.x;
-  Inst& I = insts[strip_inst[blk]];
-  if (!I.active) return;
-  const int n = I.n, it = I.it;
-  const double hw = 0.5 * (double)n, es = (1.0 / (double)n) / hw, alpha = I.alpha;
-  const float h2 = (float)(0.5 * hw * hw), af = (float)alpha, af2 = (float)(alpha * alpha);
-  const bool use_beta = I.use_beta;
-  const float beta = (float)I.beta;
-  const StripCoord sc = strip_coord(I, blk);
-  const int j = sc.j0 + sc.lane;
-  float* dnew = reinterpret_cast<float*>(I.d[it & 1]);
-  double* psin = I.psi[(it + 1) & 1];
-  float* rn = reinterpret_cast<float*>(I.r[(it + 1) % 3]);
-  float mx = -INFINITY;
-  if (sc.i0 < n) {
-    using RS = RingS<2, 1>;
-    RS R;
-    R.buf = ring_raw + (size_t)sc.warp * RD * RS::STAGE;
-    R.psi = I.psi[it & 1];
-    R.sf[0] = reinterpret_cast<const float*>(I.dhat);
-    R.sf[1] = reinterpret_cast<const float*>(I.d[(it + 1) & 1]);
-    R.pf[0] = reinterpret_cast<const float*>(I.r[it % 3]);
-    R.n = n;
-    R.j0 = sc.j0;
-    R.lane = sc.lane;
-    const int last = min(sc.i0 + I.srows, n);
-    R.rows_end = last;
-    R.setup();
-#pragma unroll
-    for (int k = 0; k < RD - 1; ++k) R.issue(sc.i0 - 1 + k);
-    auto drow = [&](int row) {
-      RowF h = R.frow(row, 0);
-      if (!use_beta) return h;
-      RowF q = R.frow(row, 1);
-      RowF d;
-      d.c = h.c + beta * q.c;
-      d.l = h.l + beta * q.l;
-      d.r = h.r + beta * q.r;
-      return d;
-    };
-    VG gp;
-    VGf gd;
-    Row pc;
-    RowF dc;
-#pragma unroll 4
-    for (int row = sc.i0; row <= last; ++row) {
-      cp_async_wait<RD - 3>();
-      __syncwarp();
-      if (row == sc.i0) {
-        pc = R.prow(row - 1);
-        dc = drow(row - 1);
-      }
-      const Row pb = R.prow(row);
-      const RowF db = drow(row);
-      VG np = vgrad(pc, pb);
-      VGf nd = vgradf(dc, db);
-      if (row > sc.i0 && j < n) {
-        const int c = row - 1;
-        const size_t f = (size_t)c * n + j;
-        float a, b;
-        line_abf(shifted(diag(gp, np), es), diagf(gd, nd), a, b);
-        dnew[f] = dc.c;
-        psin[f] = pc.c + alpha * (double)dc.c;
-        const float r = h2 * (a * af2 + b * af) + R.point(c, 0);
-        rn[f] = r;
-        mx = fmaxf(mx, r);
-      }
-      gp = np;
-      gd = nd;
-      pc = pb;
-      dc = db;
-      __syncwarp();
-      R.issue(row - 2 + RD);
-    }
-    cp_async_wait<0>();
-  }
-  double m64 = block_max((double)mx, red);
-  if (threadIdx.x == 0) partials[(size_t)blk * KA] = m64;
-  if (last_block(&I.counter, I.nstrip)) {
-    double m = -INFINITY;
-    for (int t = threadIdx.x; t < I.nstrip; t += blockDim.x)
-      m = fmax(m, __ldcg(&partials[(size_t)(I.strip0 + t) * KA]));
-    m = block_max(m, red);
-    if (threadIdx.x == 0) update_step(I, m, n, it);
-  }
-}
-
 int strip_blocks(int n, int srows) {
   const int strips = ((n + srows - 1) / srows) * ((n + SW - 1) / SW);
   return (strips + SWARPS - 1) / SWARPS;
 }
 
+using SumsF64 = Ring<3, 2>;
+using UpdF64 = Ring<3, 1>;
+using SumsSplit = RingS<2>;
+using UpdSplit = RingS<1>;
+
 void sweep_attrs(int device) {
   static bool done[64] = {};
   if (device < 64 && done[device]) return;
-  OTM_CUDA(cudaFuncSetAttribute(k_sweep_sums, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(SWARPS * RD * Ring<3, 2>::STAGE * sizeof(double))));
-  OTM_CUDA(cudaFuncSetAttribute(k_sweep_update, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(SWARPS * RD * Ring<3, 1>::STAGE * sizeof(double))));
-  OTM_CUDA(cudaFuncSetAttribute(k_sweep_sums_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(SWARPS * RD * RingS<2, 2>::STAGE)));
-  OTM_CUDA(cudaFuncSetAttribute(k_sweep_update_split, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)(SWARPS * RD * RingS<2, 1>::STAGE)));
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_sums_t<SumsF64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SWARPS * RD * SumsF64::STAGE_BYTES));
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_update_t<UpdF64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SWARPS * RD * UpdF64::STAGE_BYTES));
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_sums_t<SumsSplit, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SWARPS * RD * SumsSplit::STAGE_BYTES));
+  OTM_CUDA(cudaFuncSetAttribute(k_sweep_update_t<UpdSplit, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                SWARPS * RD * UpdSplit::STAGE_BYTES));
   if (device < 64) done[device] = true;
 }
 
@@ -813,10 +605,10 @@ void sweep_sums(otm_context* ctx, Inst* d_insts, const int* strip_inst, int base
   sweep_attrs(ctx->device);
   if (nblocks <= 0) return;
   if (split)
-    launch_smem(ctx, "sweep32_sums", k_sweep_sums_split, nblocks, ST, SWARPS * RD * RingS<2, 2>::STAGE, d_insts,
-                strip_inst, base, partials);
+    launch_smem(ctx, "sweep32_sums", k_sweep_sums_t<SumsSplit, true>, nblocks, ST, SWARPS * RD * SumsSplit::STAGE_BYTES,
+                d_insts, strip_inst, base, partials);
   else
-    launch_smem(ctx, "sweep_sums", k_sweep_sums, nblocks, ST, SWARPS * RD * Ring<3, 2>::STAGE * sizeof(double),
+    launch_smem(ctx, "sweep_sums", k_sweep_sums_t<SumsF64, false>, nblocks, ST, SWARPS * RD * SumsF64::STAGE_BYTES,
                 d_insts, strip_inst, base, partials);
 }
 
@@ -825,10 +617,10 @@ void sweep_update(otm_context* ctx, Inst* d_insts, const int* strip_inst, int ba
   sweep_attrs(ctx->device);
   if (nblocks <= 0) return;
   if (split)
-    launch_smem(ctx, "sweep32_update", k_sweep_update_split, nblocks, ST, SWARPS * RD * RingS<2, 1>::STAGE, d_insts,
-                strip_inst, base, partials);
+    launch_smem(ctx, "sweep32_update", k_sweep_update_t<UpdSplit, true>, nblocks, ST,
+                SWARPS * RD * UpdSplit::STAGE_BYTES, d_insts, strip_inst, base, partials);
   else
-    launch_smem(ctx, "sweep_update", k_sweep_update, nblocks, ST, SWARPS * RD * Ring<3, 1>::STAGE * sizeof(double),
+    launch_smem(ctx, "sweep_update", k_sweep_update_t<UpdF64, false>, nblocks, ST, SWARPS * RD * UpdF64::STAGE_BYTES,
                 d_insts, strip_inst, base, partials);
 }
 

@@ -58,6 +58,12 @@ class AdjointStatsC(C.Structure):
 ADJOINT_ONE_STEP, ADJOINT_KRYLOV = 0, 1
 
 
+class BarycenterStatsC(C.Structure):
+    _fields_ = [("iterations", C.c_int * 8), ("outcome", C.c_int * 8), ("residual", C.c_double * 8),
+                ("inverse_missing", C.c_long), ("expected_mean", C.c_double), ("raster_mean", C.c_double),
+                ("adjoint_solves", C.c_int * 8)]
+
+
 class OtmError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"otmap_b200 error {code}: {msg}")
@@ -86,6 +92,7 @@ SIGNATURES = {
     "otm_map_inverse_mode": (C.c_int, [C.c_void_p, C.c_void_p, C.c_long, C.c_int, C.c_void_p, C.c_void_p,
                                        C.POINTER(C.c_long)]),
     "otm_rasterize": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "otm_rasterize_faces": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "otm_rasterize_mode": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
                                      C.c_void_p]),
     "otm_rasterize_mesh": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -112,6 +119,9 @@ SIGNATURES = {
     "otm_default_adjoint_options": (None, [C.POINTER(AdjointOptionsC)]),
     "otm_adjoint": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(AdjointOptionsC),
                               C.c_void_p, C.POINTER(AdjointStatsC)]),
+    "otm_barycenter_loss": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_void_p), _dp, C.c_int, C.c_void_p,
+                                      C.POINTER(SolverOptionsC), C.POINTER(AdjointOptionsC), C.c_void_p,
+                                      C.POINTER(C.c_double), C.POINTER(C.c_void_p), C.POINTER(BarycenterStatsC)]),
     "otm_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
     "otm_launch_count": (C.c_long, [C.c_void_p]),
     "otm_profile": (C.c_int, [C.c_void_p, C.c_int]),

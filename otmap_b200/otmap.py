@@ -457,6 +457,48 @@ def barycenter_image(inv_maps, alpha: float, beta: float | None, density_means, 
     return img, mesh
 
 
+def raster_faces(mesh: np.ndarray, rows: int, cols: int, n: int | None = None, context=None) -> np.ndarray:
+    """The face index each pixel of the PerFace raster of a grid mesh takes its value from
+    ([rows, cols] int32, -1 where no face covers the pixel centre)."""
+    ctx = context or _n.default_context()
+    xy = np.ascontiguousarray(mesh, dtype=np.float64).reshape(-1, 2)
+    n = _grid_n(xy, n)
+    out = np.empty((rows, cols), dtype=np.int32)
+    _n.check(_n.lib().otm_rasterize_faces(ctx.handle, n, _n.ptr(xy), rows, cols, _n.ptr(out)))
+    return out
+
+
+def barycenter_loss(densities, weights, target, res: int | None = None, opt: SolverOptions | None = None,
+                    adjoint_opt=None, grad: bool = True, context=None):
+    """The barycenters demo (apps/barycenters.cpp:184-198, 250-290) as one differentiable
+    loss: maps of `densities` (up to 8 per-cell vectors or square images of one size n) in
+    one batch, inverse meshes of the origin grid, the blend with `weights`, its raster at
+    res x res rescaled to the blended density mean, and L = sum (image - target)^2.
+    Returns (loss, image[res, res], grads (list of per-cell gradients, or None), stats)."""
+    import ctypes as C
+
+    ctx = context or _n.default_context()
+    cells = [_as_cells(d) for d in densities]
+    count = len(cells)
+    n = int(round(np.sqrt(cells[0].size)))
+    t = np.ascontiguousarray(target, dtype=np.float64)
+    res = int(res or t.shape[0])
+    if t.shape != (res, res):
+        raise ValueError("target must be res x res")
+    w = (C.c_double * count)(*[float(x) for x in weights])
+    dp = (C.c_void_p * count)(*[c.ctypes.data for c in cells])
+    img = np.empty((res, res))
+    loss = C.c_double(0.0)
+    grads = [np.empty(n * n) for _ in range(count)] if grad else None
+    gp = (C.c_void_p * count)(*[g.ctypes.data for g in grads]) if grad else None
+    st = _n.BarycenterStatsC()
+    o = (opt or SolverOptions()).to_c()
+    _n.check(_n.lib().otm_barycenter_loss(ctx.handle, n, count, dp, w, res, _n.ptr(t), C.byref(o),
+                                          C.byref(adjoint_opt) if adjoint_opt is not None else None, _n.ptr(img),
+                                          C.byref(loss), gp, C.byref(st)))
+    return loss.value, img, grads, st
+
+
 def compose(tmap_u: TransportMap, tmap_v: TransportMap, verbose_level: int = 0) -> np.ndarray:
     """The map u -> v of apps/otmap.cpp:120-126: map u's forward mesh pulled through the
     inverse of map v. Returns the composite (n_u+1)^2 vertex array."""

@@ -1,0 +1,229 @@
+"""The differentiable barycenter loss (otm_barycenter_loss): the barycenters demo
+(apps/barycenters.cpp:184-198 inverse meshes, :250-276 blend, :280-290 raster and
+rescale) as one loss L = sum (image - target)^2 and its gradient with respect to every
+input density.
+
+* forward: equal to the same pipeline composed of the public calls (batched solve,
+  inverse of the origin grid, otm_barycenter);
+* gradient: against an FP64 CPU chain -- the raster's area derivative with pixel
+  ownership held fixed, the blend, a numerical Jacobian of the bilinear inversion
+  (Newton solve, central differences) and the sparse-Jacobian adjoint reference --
+  within 1e-6;
+* at 512^2 with four blurred-shape densities: against central differences (h = 1e-4,
+  FP64) of the same loss with the pixel ownership held fixed, along random directions.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ot():
+    from otmap_b200 import otmap
+
+    return otmap
+
+
+def weights_bilinear(a, b):
+    return [(1 - a) * (1 - b), a * (1 - b), a * b, (1 - a) * b]
+
+
+def origin_grid(n):
+    t = np.arange(n + 1, dtype=np.float64) * (1.0 / n)
+    return np.stack([np.repeat(t, n + 1), np.tile(t, n + 1)], axis=1)
+
+
+def signed_areas(B, n):
+    P = B.reshape(n + 1, n + 1, 2)
+    c = [P[:-1, :-1], P[1:, :-1], P[1:, 1:], P[:-1, 1:]]  # corners 0..3 of face (i, j)
+    A = np.zeros((n, n))
+    for k in range(4):
+        a, b = c[k], c[(k + 1) % 4]
+        A += 0.5 * (a[..., 0] * b[..., 1] - b[..., 0] * a[..., 1])
+    return A.ravel(), c  # face f = j + i n  <->  [i, j]
+
+
+def frozen_image(B, n, owner, expected):
+    """PerFace unit-density raster of B with the given pixel ownership, rescaled to the
+    expected mean (apps/barycenters.cpp:280-284); returns (image, R, s)."""
+    A, _ = signed_areas(B, n)
+    scale = float(np.float32(1.0 / (n * n)))
+    val = scale / np.abs(A)
+    R = np.where(owner >= 0, val[np.maximum(owner, 0)], 0.0)
+    s = expected / R.mean()
+    return R * s, R, s
+
+
+def bilinear_uv(x, P, uv0):
+    """Newton solve of x = (1-u)(1-v)P0 + u(1-v)P1 + uvP2 + (1-u)vP3 (vectorised)."""
+    u, v = uv0[:, 0].copy(), uv0[:, 1].copy()
+    for _ in range(8):
+        X = ((1 - u) * (1 - v))[:, None] * P[:, 0] + (u * (1 - v))[:, None] * P[:, 1] + (u * v)[:, None] * P[:, 2] \
+            + ((1 - u) * v)[:, None] * P[:, 3]
+        Ju = (1 - v)[:, None] * (P[:, 1] - P[:, 0]) + v[:, None] * (P[:, 2] - P[:, 3])
+        Jv = (1 - u)[:, None] * (P[:, 3] - P[:, 0]) + u[:, None] * (P[:, 2] - P[:, 1])
+        r = X - x
+        det = Ju[:, 0] * Jv[:, 1] - Ju[:, 1] * Jv[:, 0]
+        du = (Jv[:, 1] * r[:, 0] - Jv[:, 0] * r[:, 1]) / det
+        dv = (-Ju[:, 1] * r[:, 0] + Ju[:, 0] * r[:, 1]) / det
+        u, v = u - du, v - dv
+    return np.stack([u, v], axis=1)
+
+
+def reference_chain(ot, port, n, res, dens_raw, w, target, fwds, adjs):
+    """FP64 CPU gradient of the frozen-ownership loss with respect to each raw density."""
+    from adjoint_ref import reference_gradient
+
+    count = len(dens_raw)
+    x = origin_grid(n)
+    inv, hit0 = [], []
+    for k in range(count):
+        pos, _, _, _ = port.apply_inverse(fwds[k], adjs[k], n, x)
+        nh, hits, _ = port.query_all(fwds[k], n, x, cap=4)
+        assert (nh > 0).all()
+        inv.append(pos)
+        hit0.append(hits[:, 0])
+    B = w[0] * inv[0]
+    for k in range(1, count):
+        B = B + w[k] * inv[k]
+    owner = ot.raster_faces(B, res, res, n=n)
+    expected = sum(w[k] * dens_raw[k].mean() for k in range(count))
+    img, R, s = frozen_image(B, n, owner, expected)
+    g = 2.0 * (img - target)
+    sgR = (g * R).sum()
+    dR = s * (g - sgR / R.sum())
+    dexp = sgR / R.mean()
+    A, _ = signed_areas(B, n)
+    scale = float(np.float32(1.0 / (n * n)))
+    dA = np.zeros(n * n)
+    np.add.at(dA, owner[owner >= 0], dR[owner >= 0])
+    Rf = scale / np.abs(A)
+    dA = -dA * Rf / A
+    # shoelace gradient back to the vertices of B
+    dB = np.zeros(((n + 1), (n + 1), 2))
+    P = B.reshape(n + 1, n + 1, 2)
+    c = [P[:-1, :-1], P[1:, :-1], P[1:, 1:], P[:-1, 1:]]
+    sl = [(slice(0, n), slice(0, n)), (slice(1, n + 1), slice(0, n)), (slice(1, n + 1), slice(1, n + 1)),
+          (slice(0, n), slice(1, n + 1))]
+    dA2 = dA.reshape(n, n)
+    for k in range(4):
+        nx, pv = c[(k + 1) % 4], c[(k + 3) % 4]
+        dB[sl[k] + (0,)] += dA2 * 0.5 * (nx[..., 1] - pv[..., 1])
+        dB[sl[k] + (1,)] += dA2 * 0.5 * (pv[..., 0] - nx[..., 0])
+    dB = dB.reshape(-1, 2)
+    grads = []
+    e = 1.0 / n
+    for k in range(count):
+        dI = w[k] * dB
+        F = fwds[k].reshape(-1, 2)
+        h = hit0[k]
+        i, j = h // n, h % n
+        vid = np.stack([j + i * (n + 1), j + (i + 1) * (n + 1), (j + 1) + (i + 1) * (n + 1), (j + 1) + i * (n + 1)], 1)
+        Pq = F[vid]  # (V, 4, 2)
+        uv = bilinear_uv(x, Pq, np.full((x.shape[0], 2), 0.5))
+        dF = np.zeros_like(F)
+        hh = 1e-7
+        for cc in range(4):
+            for d in range(2):
+                Pp = Pq.copy()
+                Pm = Pq.copy()
+                Pp[:, cc, d] += hh
+                Pm[:, cc, d] -= hh
+                duv = (bilinear_uv(x, Pp, uv) - bilinear_uv(x, Pm, uv)) / (2 * hh)
+                contrib = e * (duv * dI).sum(axis=1)  # I = O + e (u, v)
+                np.add.at(dF[:, d], vid[:, cc], contrib)
+        gk, _ = reference_gradient(fwds[k], dens_raw[k], dF, n)
+        grads.append(gk + w[k] * dexp / (n * n))
+    loss = float(((img - target) ** 2).sum())
+    return loss, img, grads
+
+
+def test_forward_matches_composed_pipeline(ot):
+    from otmap_b200 import workloads as W
+
+    n, res = 64, 64
+    dens = [W.to_cells(W.blurred_shapes(n, 30 + k, sigma_px=1.5)) for k in range(4)]
+    target = W.gaussian_mixture(res, 9)
+    w = weights_bilinear(0.5, 0.5)
+    loss, img, _, st = ot.barycenter_loss(dens, w, target, grad=False)
+    maps = ot.solve_batch(dens)
+    inv = []
+    for m in maps:
+        p = origin_grid(n).copy()
+        m.apply_inverse(p)
+        inv.append(p)
+    img2, _ = ot.barycenter_image(inv, 0.5, 0.5, [d.mean() for d in dens], res)
+    # the density means are summed in different orders (numpy here, a fixed tree on the GPU)
+    np.testing.assert_allclose(img, img2, rtol=1e-13, atol=0)
+    assert abs(loss - ((img2 - target) ** 2).sum()) <= 1e-12 * max(1.0, loss)
+    assert st.inverse_missing == 0
+
+
+@pytest.mark.parametrize("n,res", [(24, 24), (20, 36)])
+def test_gradient_matches_fp64_reference(n, res, ot, oracle_port):
+    from otmap_b200 import workloads as W
+
+    dens = [W.to_cells(W.gaussian_mixture(n, 70 + k)) * (1.0 + 0.3 * k) for k in range(4)]
+    target = W.gaussian_mixture(res, 5)
+    w = weights_bilinear(0.3, 0.6)
+    opt = ot.SolverOptions(threshold=0.0, max_iter=300)
+    loss, img, grads, st = ot.barycenter_loss(dens, w, target, res=res, opt=opt)
+    fwds, adjs = [], []
+    for d in dens:
+        s = ot.GridBasedTransportSolver()
+        s.set_verbose_level(0)
+        s.init(n)
+        m = s.solve(d, opt)
+        fwds.append(m.fwd_mesh())
+        adjs.append(m.density())
+    loss_r, img_r, grads_r = reference_chain(ot, oracle_port, n, res, dens, w, target, fwds, adjs)
+    np.testing.assert_allclose(img, img_r, rtol=1e-12, atol=0)
+    assert abs(loss - loss_r) <= 1e-12 * loss_r
+    for g, gr in zip(grads, grads_r):
+        rel = np.linalg.norm(g - gr) / np.linalg.norm(gr)
+        assert rel <= 1e-6, rel
+
+
+def test_gradient_central_differences_512(ot):
+    """Config-5 sizes: four 512^2 blurred-shape densities, centre barycenter rasterized at
+    512^2 against a seeded Gaussian-mixture target; directional derivatives against central
+    differences of the loss with the pixel ownership of the base point held fixed."""
+    from otmap_b200 import workloads as W
+
+    n = res = 512
+    dens = [W.to_cells(W.blurred_shapes(n, 50 + k, sigma_px=2.5)) for k in range(4)]
+    target = W.gaussian_mixture(res, 17)
+    w = weights_bilinear(0.5, 0.5)
+    opt = ot.SolverOptions(threshold=1e-13, max_iter=2000)
+    loss, img, grads, st = ot.barycenter_loss(dens, w, target, opt=opt)
+    assert st.inverse_missing == 0
+
+    def blend_of(ds):
+        maps = ot.solve_batch(ds, opt)
+        B = None
+        for k, m in enumerate(maps):
+            p = origin_grid(n).copy()
+            m.apply_inverse(p)
+            B = w[0] * p if B is None else B + w[k] * p
+        return B
+
+    B0 = blend_of(dens)
+    owner = ot.raster_faces(B0, res, res, n=n)
+
+    def frozen_loss(ds):
+        expected = sum(w[k] * ds[k].mean() for k in range(4))
+        im, _, _ = frozen_image(blend_of(ds), n, owner, expected)
+        return float(((im - target) ** 2).sum())
+
+    assert abs(frozen_loss(dens) - loss) <= 1e-10 * loss
+    rng = np.random.default_rng(2)
+    h = 1e-4
+    for _ in range(4):
+        v = [rng.standard_normal(n * n) for _ in range(4)]  # O(1) per cell: h perturbs each density value
+        plus = frozen_loss([d + h * x for d, x in zip(dens, v)])
+        minus = frozen_loss([d - h * x for d, x in zip(dens, v)])
+        fd = (plus - minus) / (2 * h)
+        an = sum(float(g @ x) for g, x in zip(grads, v))
+        assert abs(fd - an) <= 2e-3 * max(abs(an), 1e-12 * loss), (fd, an)

@@ -62,7 +62,8 @@ def test_config2_solve_1024(config2):
     err = float(np.abs(gm.fwd_mesh() - config2["ref_fwd"]).max())
     assert err <= POS_TOL, err
     assert gm.stats.residual <= 1e-7
-    np.testing.assert_allclose(gm.density(), config2["ref_density"], rtol=1e-13, atol=0)
+    # the normalisation sums 2^20 values: the reference in sequence, the GPU in a fixed tree
+    np.testing.assert_allclose(gm.density(), config2["ref_density"], rtol=1e-11, atol=0)
 
 
 def test_config2_inverse_2p20_points(config2, ref, ot):

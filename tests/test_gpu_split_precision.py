@@ -84,8 +84,9 @@ def test_split_config2_1024_vs_reference(ot):
 
 def test_split_batch_with_fp64_sizes(ot):
     """A split-precision batch with sizes outside the FP32 transforms (48, 100 stay FP64):
-    both sweep forms in the same iterations; every instance equals its single solve in
-    the same mode, and the FP64 instances equal FP64-mode solves."""
+    both sweep forms in the same iterations; every instance agrees with its single solve
+    in the same mode (a batch may walk its sweeps in taller strips than a lone instance,
+    which changes the order of the sums, so to 1e-7 rather than bit for bit)."""
     from otmap_b200 import native
     from otmap_b200 import workloads as W
 
@@ -99,13 +100,14 @@ def test_split_batch_with_fp64_sizes(ot):
         s, _ = split_solver(ot)
         s.init(n)
         single = s.solve(W.to_cells(img))
-        assert m.stats.iterations == single.stats.iterations
-        assert np.array_equal(m.fwd_mesh(), single.fwd_mesh())
+        assert abs(m.stats.iterations - single.stats.iterations) <= 1
+        assert np.abs(m.fwd_mesh() - single.fwd_mesh()).max() <= 1e-7
+        assert m.stats.residual <= 1e-7
         if n in (48, 100):
             f64 = ot.GridBasedTransportSolver()
             f64.set_verbose_level(0)
             f64.init(n)
-            assert np.array_equal(m.fwd_mesh(), f64.solve(W.to_cells(img)).fwd_mesh())
+            assert np.abs(m.fwd_mesh() - f64.solve(W.to_cells(img)).fwd_mesh()).max() <= 1e-7
 
 
 def test_split_graph_and_host_loops_agree(ot):
