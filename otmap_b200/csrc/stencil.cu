@@ -181,6 +181,22 @@ __device__ __forceinline__ void line_ab(const Diag& g, const Diag& h, double e, 
   b = h.ax * diag0b_y - h.ay * diag0b_x + diag0a_x * h.by - diag0a_y * h.bx;
 }
 
+// The split form's line coefficients with fused multiply-adds (no reference rounding to
+// retrace there): g0 holds the potential's shifted diagonals (g.ax + e, g.ay + e,
+// g.bx - e, g.by + e), h the direction's diagonals.
+__device__ __forceinline__ Diag shift_diag(const Diag& g, double e) {
+  Diag d;
+  d.ax = g.ax + e;
+  d.ay = g.ay + e;
+  d.bx = g.bx - e;
+  d.by = g.by + e;
+  return d;
+}
+__device__ __forceinline__ void line_ab_fma(const Diag& g0, const Diag& h, double& a, double& b) {
+  a = fma(h.ax, h.by, -(h.ay * h.bx));
+  b = fma(h.ax, g0.by, fma(-h.ay, g0.bx, fma(g0.ax, h.by, -(g0.ay * h.bx))));
+}
+
 struct StripCoord {
   int i0, j0, lane, warp;
 };
@@ -291,7 +307,8 @@ __device__ __forceinline__ void update_step(Inst& I, double rmax, int n, int it)
 // left about 1e-4 relative error in a and b; at 1024^2 the tracked residual then drifted
 // away from the mesh's, solves stopped 5e-3 away from the reference's map or ran to
 // max_iter.) d and r' are rounded to FP32 when stored; psi' = psi + alpha d uses the
-// unrounded d, as do a and b of the update.
+// unrounded d, as do a and b of the update. Having no reference rounding to retrace, the
+// split form fuses its multiply-adds (line coefficients, d, psi', r').
 
 __device__ __forceinline__ void cp_async4(void* dst, const void* src) {
   unsigned s = (unsigned)__cvta_generic_to_shared(dst);
@@ -438,10 +455,17 @@ __global__ __launch_bounds__(ST) void k_sweep_sums_t(Inst* insts, const int* str
       if (row > sc.i0 && j < n) {
         const int c = row - 1;
         Diag G = diag(gp, np), Hd = diag(gh, nh), Qd = diag(gq, nq);
-        double a11, b1, a22, b2;
-        line_ab(G, Hd, es, a11, b1);
-        line_ab(G, Qd, es, a22, b2);
-        double a12 = Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx;
+        double a11, b1, a22, b2, a12;
+        if constexpr (SPLIT) {
+          const Diag G0 = shift_diag(G, es);
+          line_ab_fma(G0, Hd, a11, b1);
+          line_ab_fma(G0, Qd, a22, b2);
+          a12 = fma(Hd.ax, Qd.by, fma(-Hd.ay, Qd.bx, fma(Qd.ax, Hd.by, -(Qd.ay * Hd.bx))));
+        } else {
+          line_ab(G, Hd, es, a11, b1);
+          line_ab(G, Qd, es, a22, b2);
+          a12 = Hd.ax * Qd.by - Hd.ay * Qd.bx + Qd.ax * Hd.by - Qd.ay * Hd.bx;
+        }
         double r = R.point(c, 0), jd = r - R.point(c, 1);
         double hv = ah.c, qv = aq.c;
         acc[S_HH] = fma(hv, hv, acc[S_HH]);
@@ -519,9 +543,15 @@ __global__ __launch_bounds__(ST) void k_sweep_update_t(Inst* insts, const int* s
       if (!use_beta) return h;
       Row q = R.row_of(row, 2);
       Row d;
-      d.c = h.c + beta * q.c;
-      d.l = h.l + beta * q.l;
-      d.r = h.r + beta * q.r;
+      if constexpr (SPLIT) {
+        d.c = fma(beta, q.c, h.c);
+        d.l = fma(beta, q.l, h.l);
+        d.r = fma(beta, q.r, h.r);
+      } else {
+        d.c = h.c + beta * q.c;
+        d.l = h.l + beta * q.l;
+        d.r = h.r + beta * q.r;
+      }
       return d;
     };
     VG gp, gd;
@@ -540,11 +570,17 @@ __global__ __launch_bounds__(ST) void k_sweep_update_t(Inst* insts, const int* s
       if (row > sc.i0 && j < n) {
         const int c = row - 1;
         const size_t f = (size_t)c * n + j;
-        double a, b;
-        line_ab(diag(gp, np), diag(gd, nd), es, a, b);
-        psin[f] = pc.c + alpha * dc.c;
-        // (n/2)^2 / 2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
-        double r = h2 * (a * (alpha * alpha) + b * alpha) + R.point(c, 0);
+        double a, b, r;
+        if constexpr (SPLIT) {
+          line_ab_fma(shift_diag(diag(gp, np), es), diag(gd, nd), a, b);
+          psin[f] = fma(alpha, dc.c, pc.c);
+          r = fma(h2, fma(a, alpha * alpha, b * alpha), R.point(c, 0));
+        } else {
+          line_ab(diag(gp, np), diag(gd, nd), es, a, b);
+          psin[f] = pc.c + alpha * dc.c;
+          // (n/2)^2 / 2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
+          r = h2 * (a * (alpha * alpha) + b * alpha) + R.point(c, 0);
+        }
         if constexpr (SPLIT) {
           reinterpret_cast<float*>(I.d[it & 1])[f] = (float)dc.c;
           const float rf = (float)r;

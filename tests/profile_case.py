@@ -1,6 +1,6 @@
 """A short, fixed solve for kernel profiling (ncu) and quick timing.
 
-    python tests/profile_case.py [--n 1024] [--batch 2] [--iters 3] [--poisson fft|dense]
+    python tests/profile_case.py [--n 1024] [--batch 2] [--iters 3] [--poisson fft|dense] [--precision fp64|split]
 
 Solves `batch` blurred-shape densities of size n for a fixed number of iterations
 (max_iter = iters, so every instance runs exactly that many) through the C ABI, with
@@ -28,6 +28,7 @@ def main():
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--poisson", default="fft", choices=["fft", "dense"])
     ap.add_argument("--repeat", type=int, default=1)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
     a = ap.parse_args()
 
     import torch
@@ -37,6 +38,7 @@ def main():
 
     ctx = N.Context(0)
     ctx.set_poisson(N.POISSON_FFT if a.poisson == "fft" else N.POISSON_DENSE)
+    ctx.set_precision(N.PRECISION_SPLIT if a.precision == "split" else N.PRECISION_FP64)
     n, B = a.n, a.batch
     dens = [torch.from_numpy(W.to_cells(W.blurred_shapes(n, k, sigma_px=5.0))).cuda() for k in range(B)]
     fwd = [torch.empty(((n + 1) ** 2, 2), dtype=torch.float64, device="cuda") for _ in range(B)]

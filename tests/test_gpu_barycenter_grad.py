@@ -138,14 +138,19 @@ def reference_chain(ot, port, n, res, dens_raw, w, target, fwds, adjs):
         Pq = F[vid]  # (V, 4, 2)
         uv = bilinear_uv(x, Pq, np.full((x.shape[0], 2), 0.5))
         dF = np.zeros_like(F)
-        hh = 1e-7
+
+        def central(cc, d, hh):
+            Pp = Pq.copy()
+            Pm = Pq.copy()
+            Pp[:, cc, d] += hh
+            Pm[:, cc, d] -= hh
+            return (bilinear_uv(x, Pp, uv) - bilinear_uv(x, Pm, uv)) / (2 * hh)
+
         for cc in range(4):
             for d in range(2):
-                Pp = Pq.copy()
-                Pm = Pq.copy()
-                Pp[:, cc, d] += hh
-                Pm[:, cc, d] -= hh
-                duv = (bilinear_uv(x, Pp, uv) - bilinear_uv(x, Pm, uv)) / (2 * hh)
+                # Richardson extrapolation of central differences: the inversion is strongly
+                # curved on boundary points, where a single 1e-7 step leaves ~1e-6 of error
+                duv = (4.0 * central(cc, d, 1e-7) - central(cc, d, 2e-7)) / 3.0
                 contrib = e * (duv * dI).sum(axis=1)  # I = O + e (u, v)
                 np.add.at(dF[:, d], vid[:, cc], contrib)
         gk, _ = reference_gradient(fwds[k], dens_raw[k], dF, n)
@@ -210,7 +215,9 @@ def test_gradient_central_differences_512(ot):
     dens = [W.to_cells(W.blurred_shapes(n, 50 + k, sigma_px=2.5)) for k in range(4)]
     target = W.gaussian_mixture(res, 17)
     w = weights_bilinear(0.5, 0.5)
-    opt = ot.SolverOptions(threshold=1e-13, max_iter=2000)
+    # the maps must be converged to the FP64 floor: a solve stopped at residual 1e-13 is still
+    # ~1e-5 from its limit at this size, as much as an h = 1e-4 perturbation moves it
+    opt = ot.SolverOptions(threshold=0.0, max_iter=700)
     loss, img, grads, st = ot.barycenter_loss(dens, w, target, opt=opt, adjoint_opt=tight_adjoint())
     assert st.inverse_missing == 0
 
