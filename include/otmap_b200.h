@@ -347,11 +347,15 @@ int otm_barycenter_loss(otm_context* ctx, int n, int count, const double* const*
  *     OTM_POISSON_AUTO  (default) fast cosine transform for power-of-two n in [8, 4096],
  *                       dense products otherwise
  *     OTM_POISSON_DENSE C.X.C^T products with the cosine basis, any n
- *     OTM_POISSON_FFT   fast transform where possible (same as AUTO) */
+ *     OTM_POISSON_FFT   fast transform where possible (same as AUTO)
+ *     OTM_POISSON_TENSOR split-precision instances of n in {128, 256, 512, 1024}: the
+ *                       four products C.R.C^T and C^T.Y.C on the tensor cores (tcgen05,
+ *                       3xTF32 with FP32 accumulation); other instances as AUTO */
 #define OTM_OPT_POISSON 1
 #define OTM_POISSON_AUTO 0
 #define OTM_POISSON_DENSE 1
 #define OTM_POISSON_FFT 2
+#define OTM_POISSON_TENSOR 3
 /*   OTM_OPT_LOOP: how the iteration loop is driven.
  *     OTM_LOOP_GRAPH (default) one CUDA graph launch per solve: the iteration kernels sit
  *                    in the body of a device-side WHILE node that stops when no instance

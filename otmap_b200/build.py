@@ -22,7 +22,7 @@ LIB = os.path.join(LIBDIR, "libotmap_b200.so")
 INCLUDE = os.path.join(ROOT, "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["capi.cu", "solver.cu", "stencil.cu", "poisson.cu", "dct_reg.cu", "adjoint.cu", "locate.cu",
+SOURCES = ["capi.cu", "solver.cu", "stencil.cu", "poisson.cu", "dct_reg.cu", "dct_tc.cu", "adjoint.cu", "locate.cu",
            "pipeline.cu", "meshio.cu"]
 
 

@@ -178,7 +178,7 @@ extern "C" int otm_set_option(otm_context* ctx, int key, int value) {
     return OTM_ERR_BAD_ARG;
   }
   if (key == OTM_OPT_POISSON) {
-    if (value < OTM_POISSON_AUTO || value > OTM_POISSON_FFT) {
+    if (value < OTM_POISSON_AUTO || value > OTM_POISSON_TENSOR) {
       set_error("otm_set_option: unknown Poisson mode");
       return OTM_ERR_BAD_ARG;
     }

@@ -40,6 +40,8 @@ struct SizeTables {
   DevBuf cosk;  // n doubles
   DevBuf tw;    // n/2 double2, exp(-2 pi i k / n) (power-of-two n)
   DevBuf pt;    // n double2, (cos, sin)(pi k / 2n) (power-of-two n)
+  DevBuf Cf;    // n*n floats, C[k][i] (tensor-core transform sizes)
+  DevBuf CTf;   // n*n floats, C^T
   bool dct_ok = false;      // the assembled matrix is diagonalised by C (checked on the GPU)
   double dct_check_err = 0;  // relative error of that check
 };
@@ -52,6 +54,7 @@ struct Workspace {
   DevBuf insts;      // Inst[count]
   DevBuf tile_inst;  // int per stencil tile
   DevBuf gemm_inst;  // int per GEMM tile (instances on the dense-product transform)
+  DevBuf tc_inst;    // int per output tile of the tensor-core transform
   DevBuf strip_inst;  // int per sweep block
   DevBuf sweep_partials;  // double[sweep blocks * SWEEP_SLOTS]
   DevBuf row_inst;   // int per row block of the fast transform
@@ -61,7 +64,7 @@ struct Workspace {
   std::vector<unsigned char> h_insts;  // host mirror of Inst[count]
   void* h_pinned = nullptr;            // pinned staging for Inst readback
   size_t h_pinned_bytes = 0;
-  int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0, total_strips = 0;
+  int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0, total_strips = 0, total_tc = 0;
   int mode = -1;       // poisson mode the layout was built for
   int precision = -1;  // precision the layout was built for
   int split_strip0 = 0;  // strips of split-precision instances start here (FP64 ones before)

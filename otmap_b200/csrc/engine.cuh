@@ -34,6 +34,9 @@ struct Inst {
   const double2* pt;  // (cos, sin)(pi k / (2n)), k < n (fast transform)
   int fft, logn;      // fast transform used (n a power of two) / log2 n
   int split;          // split precision: r, d_hat, d, t1 hold FP32 values (psi, rho FP64)
+  int tc0, ntc;       // tensor-core transform (dct_tc.cu): first item and item count of its work list
+  const float* Cf;    // FP32 cosine basis C[k][i] and its transpose (tensor-core transform)
+  const float* CTf;
   int row0, nrow, col0, ncol;  // first item and item count in the row / column work lists
   int strip0, nstrip;          // first block and block count in the strip work list
   // loop state
@@ -139,6 +142,12 @@ int dct_reg_cols_per_block(int n);
 // fp32: the FP32 kernels (r_k, the transform temporary t1 and d_hat are FP32 arrays).
 void dct_reg_run(otm_context* ctx, int n, bool fp32, Inst* d_insts, const int* row_inst, int roff, int rcnt, const int* col_inst,
                  int coff, int ccnt);
+// Tensor-core transform (dct_tc.cu) for split-precision instances of n in {128, ..., 1024}:
+// d_hat = C^T ((C r C^T) / lambda) C as four tcgen05 products, 3xTF32 in FP32.
+bool dct_tc_supported(int n);
+int dct_tc_tiles(int n);  // 128 x 128 output tiles of one product
+void dct_tc_attrs(int device);
+void dct_tc_run(otm_context* ctx, Inst* d_insts, const int* tc_inst, int base, int count);
 // Dynamic shared-memory limits of the kernels of each family (set once per device,
 // before any stream capture).
 void sweep_attrs(int device);

@@ -545,7 +545,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
   const int count = (int)sizes.size();
   std::vector<Inst> h(count);
   size_t cells = 0;
-  int tiles = 0, gemm = 0, rows = 0, cols = 0, strips = 0, split_strip0 = 0;
+  int tiles = 0, gemm = 0, rows = 0, cols = 0, strips = 0, split_strip0 = 0, tcitems = 0;
   // Taller sweep strips halve the per-strip overhead (ring prologue, block reduction) when
   // the batch has blocks to spare; a batch that does not fill the GPU twice over keeps
   // 32-row strips for parallelism, and one with fewer 32-row blocks than SMs takes 16-row
@@ -571,7 +571,12 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.nstrip = strip_blocks(n, srows);
     I.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
     I.split = (ctx->precision == OTM_PRECISION_SPLIT && I.fft && dct_reg_supported(n)) ? 1 : 0;
-    if (I.fft) {
+    if (ctx->poisson_mode == OTM_POISSON_TENSOR && I.split && dct_tc_supported(n)) {
+      I.fft = 0;  // the tensor-core products instead of the FFT passes
+      I.tc0 = tcitems;
+      I.ntc = dct_tc_tiles(n);
+      tcitems += I.ntc;
+    } else if (I.fft) {
       int lg = 0;
       while ((1 << lg) < n) ++lg;
       I.logn = lg;
@@ -641,14 +646,16 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     ws.insts.reserve(sizeof(Inst) * count);
     ws.tile_inst.reserve(sizeof(int) * tiles);
     ws.gemm_inst.reserve(sizeof(int) * (gemm > 0 ? gemm : 1));
+    ws.tc_inst.reserve(sizeof(int) * (tcitems > 0 ? tcitems : 1));
     ws.row_inst.reserve(sizeof(int) * (rows > 0 ? rows : 1));
     ws.col_inst.reserve(sizeof(int) * (cols > 0 ? cols : 1));
     ws.partials.reserve(sizeof(double) * KP * (size_t)tiles);
     ws.strip_inst.reserve(sizeof(int) * strips);
     ws.sweep_partials.reserve(sizeof(double) * SWEEP_SLOTS * (size_t)strips);
     ws.arena.reserve(sizeof(double) * cells);
-    std::vector<int> ti(tiles), gi(gemm), ri(rows), ci(cols), si(strips);
+    std::vector<int> ti(tiles), gi(gemm), ri(rows), ci(cols), si(strips), tci(tcitems);
     for (int q = 0; q < count; ++q) {
+      for (int k = 0; k < h[q].ntc; ++k) tci[h[q].tc0 + k] = q;
       for (int k = 0; k < h[q].ntiles; ++k) ti[h[q].tile0 + k] = q;
       for (int k = 0; k < h[q].nstrip; ++k) si[h[q].strip0 + k] = q;
       for (int k = 0; k < h[q].ngemm; ++k) gi[h[q].gemm0 + k] = q;
@@ -659,6 +666,8 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     OTM_CUDA(cudaMemcpyAsync(ws.tile_inst.p, ti.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, st));
     OTM_CUDA(cudaMemcpyAsync(ws.strip_inst.p, si.data(), sizeof(int) * strips, cudaMemcpyHostToDevice, st));
     if (gemm) OTM_CUDA(cudaMemcpyAsync(ws.gemm_inst.p, gi.data(), sizeof(int) * gemm, cudaMemcpyHostToDevice, st));
+    if (tcitems)
+      OTM_CUDA(cudaMemcpyAsync(ws.tc_inst.p, tci.data(), sizeof(int) * tcitems, cudaMemcpyHostToDevice, st));
     if (rows) OTM_CUDA(cudaMemcpyAsync(ws.row_inst.p, ri.data(), sizeof(int) * rows, cudaMemcpyHostToDevice, st));
     if (cols) OTM_CUDA(cudaMemcpyAsync(ws.col_inst.p, ci.data(), sizeof(int) * cols, cudaMemcpyHostToDevice, st));
     OTM_CUDA(cudaStreamSynchronize(st));
@@ -668,6 +677,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     ws.split_strip0 = split_strip0;
     ws.total_tiles = tiles;
     ws.total_gemm = gemm;
+    ws.total_tc = tcitems;
     ws.total_rows = rows;
     ws.total_cols = cols;
     ws.total_strips = strips;
@@ -705,6 +715,8 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.cosk = T->cosk.as<double>();
     I.tw = T->tw.as<double2>();
     I.pt = T->pt.as<double2>();
+    I.Cf = T->Cf.as<float>();
+    I.CTf = T->CTf.as<float>();
   }
   return h;
 }
@@ -753,6 +765,7 @@ static void launch_iteration(otm_context* ctx, Inst* d_insts) {
     else
       poisson_fft(ctx, d_insts, ws.row_inst.as<int>(), sg.roff, sg.rcnt, ws.col_inst.as<int>(), sg.coff, sg.ccnt);
   }
+  if (ws.total_tc > 0) dct_tc_run(ctx, d_insts, ws.tc_inst.as<int>(), 0, ws.total_tc);
   const int* si = ws.strip_inst.as<int>();
   double* sp = ws.sweep_partials.as<double>();
   const int s64 = ws.split_strip0, s32 = ws.total_strips - ws.split_strip0;
@@ -768,6 +781,7 @@ static void build_loop_graph(otm_context* ctx, int count) {
   cudaStream_t st = ctx->stream;
   sweep_attrs(ctx->device);
   dct_reg_attrs(ctx->device);
+  dct_tc_attrs(ctx->device);
   poisson_fft_attrs(ctx->device);
   ws.loopctl.reserve(sizeof(LoopCtl));
   cudaGraph_t g = nullptr;
@@ -932,6 +946,19 @@ static SizeTables* init_size(otm_context* ctx, int n) {
     OTM_CUDA(cudaStreamSynchronize(st));
   }
   OTM_CUDA(cudaMemcpyAsync(T->C.p, C.data(), sizeof(double) * C.size(), cudaMemcpyHostToDevice, st));
+  if (dct_tc_supported(n)) {  // FP32 basis and its transpose for the tensor-core transform
+    std::vector<float> cf((size_t)n * n), ctf((size_t)n * n);
+    for (int k = 0; k < n; ++k)
+      for (int i = 0; i < n; ++i) {
+        cf[(size_t)k * n + i] = (float)C[(size_t)k * n + i];
+        ctf[(size_t)i * n + k] = (float)C[(size_t)k * n + i];
+      }
+    T->Cf.reserve(sizeof(float) * cf.size());
+    T->CTf.reserve(sizeof(float) * ctf.size());
+    OTM_CUDA(cudaMemcpyAsync(T->Cf.p, cf.data(), sizeof(float) * cf.size(), cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaMemcpyAsync(T->CTf.p, ctf.data(), sizeof(float) * ctf.size(), cudaMemcpyHostToDevice, st));
+    OTM_CUDA(cudaStreamSynchronize(st));  // the host vectors are released on return
+  }
   OTM_CUDA(cudaMemcpyAsync(T->cosk.p, ck.data(), sizeof(double) * n, cudaMemcpyHostToDevice, st));
 
   // Check M x == C^T (lambda o (C X C^T)) C on a random probe (otsolver_2dgrid.cpp:284-311).

@@ -24,7 +24,7 @@ ERR_NOT_INIT = -5
 
 CONVERGED, MAX_ITER, SMALL_STEP, NONFINITE = 0, 1, 2, 3
 OPT_POISSON = 1
-POISSON_AUTO, POISSON_DENSE, POISSON_FFT = 0, 1, 2
+POISSON_AUTO, POISSON_DENSE, POISSON_FFT, POISSON_TENSOR = 0, 1, 2, 3
 OPT_LOOP = 2
 LOOP_GRAPH, LOOP_HOST = 0, 1
 OPT_PRECISION = 4
