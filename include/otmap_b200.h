@@ -337,6 +337,7 @@ typedef struct {
   double expected_mean;  /* sum_k w_k mean(density_k) */
   double raster_mean;    /* mean of the raster before rescaling */
   int adjoint_solves[8]; /* Poisson solves of each map's adjoint (gradient only) */
+  double adjoint_residual[8]; /* final relative residual of each map's Krylov adjoint (-1: one-step) */
 } otm_barycenter_stats;
 int otm_barycenter_loss(otm_context* ctx, int n, int count, const double* const* density, const double* weights,
                         int res, const double* target, const otm_solver_options* opt, const otm_adjoint_options* aopt,

@@ -501,6 +501,7 @@ extern "C" int otm_barycenter_loss(otm_context* ctx, int n, int count, const dou
     OTM_CUDA(cudaStreamSynchronize(st));
     const double L = red2[0], sgR = red2[1];
     std::vector<int> solves(count, 0);
+    std::vector<double> ares(count, 0.0);
 
     if (grad_density) {
       // dL/dR = s (g - sum(g R) / sum(R)); dL/dexpected = sum(g R) / mean(R)
@@ -520,6 +521,7 @@ extern "C" int otm_barycenter_loss(otm_context* ctx, int n, int count, const dou
         rc = otm_adjoint(ctx, n, rho[k], fwd[k], dF[k], &ao, grad[k], &ast);
         if (rc != OTM_OK) return rc;
         solves[k] = ast.iterations;
+        ares[k] = ast.relative_residual;
         // expected = ... + w_k mean(density_k): d/ddensity_k = w_k / N per cell
         launch(ctx, "add_const", k_add_const, (unsigned)((N + 255) / 256), 256, (long)N,
                weights[k] * dL_dexp / (double)N, grad[k]);
@@ -538,6 +540,7 @@ extern "C" int otm_barycenter_loss(otm_context* ctx, int n, int count, const dou
         stats->outcome[k] = sst[k].outcome;
         stats->residual[k] = sst[k].residual;
         stats->adjoint_solves[k] = solves[k];
+        stats->adjoint_residual[k] = ares[k];
       }
       stats->inverse_missing = (long)miss;
       stats->expected_mean = expected;

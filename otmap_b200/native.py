@@ -61,7 +61,7 @@ ADJOINT_ONE_STEP, ADJOINT_KRYLOV = 0, 1
 class BarycenterStatsC(C.Structure):
     _fields_ = [("iterations", C.c_int * 8), ("outcome", C.c_int * 8), ("residual", C.c_double * 8),
                 ("inverse_missing", C.c_long), ("expected_mean", C.c_double), ("raster_mean", C.c_double),
-                ("adjoint_solves", C.c_int * 8)]
+                ("adjoint_solves", C.c_int * 8), ("adjoint_residual", C.c_double * 8)]
 
 
 class OtmError(RuntimeError):
