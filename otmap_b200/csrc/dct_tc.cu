@@ -11,8 +11,8 @@
 // store their results transposed. A CTA of 128 threads computes one 128 x 128 tile of D
 // in tensor memory (128 lanes x 128 FP32 columns): it stages 128 x 32 slices of A and B in
 // shared memory in the canonical no-swizzle K-major layout (8-row x 16-byte core
-// matrices), each value split into a TF32 high part (the top 10 mantissa bits) and the
-// FP32 remainder, and one thread issues tcgen05.mma kind::tf32 (M = 128, N = 128, K = 8)
+// matrices), each value split into its nearest TF32 value and the TF32-rounded remainder,
+// and one thread issues tcgen05.mma kind::tf32 (M = 128, N = 128, K = 8)
 // for the products hi*hi + hi*lo + lo*hi accumulated in FP32 ("3xTF32": about FP32
 // accuracy). Completion is signalled by tcgen05.commit on an mbarrier; every wait is
 // bounded and a wait that runs out flags the instance (Inst::fault) and stops it, frees
@@ -94,22 +94,30 @@ __device__ __forceinline__ void tmem_ld32(unsigned addr, float (&v)[32]) {
 // Offset of (row r, K chunk c of 4 values) in a staged slice.
 __device__ __forceinline__ int core_off(int r, int c) { return (r >> 3) * SBO + c * LBO + (r & 7) * 16; }
 
+// Nearest TF32 value of x (10 mantissa bits), as an FP32 bit pattern.
+__device__ __forceinline__ float to_tf32(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
 // Stages a 128 x 32 slice of the K-major operand M (row stride n) starting at (row0, k0):
-// high part = the top 10 mantissa bits, low part = the exact remainder.
+// high part = x rounded to TF32, low part = the remainder rounded to TF32 (|x - hi - lo|
+// <= 2^-22 |x|).
 __device__ __forceinline__ void stage_slice(const float* M, int n, int row0, int k0, unsigned char* hi,
                                             unsigned char* lo) {
   for (int e = threadIdx.x; e < TCM * (TCK / 4); e += blockDim.x) {
     const int r = e >> 3, c = e & 7;
     const float4 x = *reinterpret_cast<const float4*>(M + (size_t)(row0 + r) * n + k0 + 4 * c);
     float4 h, l;
-    h.x = __uint_as_float(__float_as_uint(x.x) & 0xFFFFE000u);
-    h.y = __uint_as_float(__float_as_uint(x.y) & 0xFFFFE000u);
-    h.z = __uint_as_float(__float_as_uint(x.z) & 0xFFFFE000u);
-    h.w = __uint_as_float(__float_as_uint(x.w) & 0xFFFFE000u);
-    l.x = x.x - h.x;
-    l.y = x.y - h.y;
-    l.z = x.z - h.z;
-    l.w = x.w - h.w;
+    h.x = to_tf32(x.x);
+    h.y = to_tf32(x.y);
+    h.z = to_tf32(x.z);
+    h.w = to_tf32(x.w);
+    l.x = to_tf32(x.x - h.x);
+    l.y = to_tf32(x.y - h.y);
+    l.z = to_tf32(x.z - h.z);
+    l.w = to_tf32(x.w - h.w);
     const int o = core_off(r, c);
     *reinterpret_cast<float4*>(hi + o) = h;
     *reinterpret_cast<float4*>(lo + o) = l;
