@@ -59,6 +59,8 @@ def parse():
                         "line search and potential; the single-solve workload's stated precision) or fp64")
     p.add_argument("--no-other-precision", action="store_true")
     p.add_argument("--no-locate", action="store_true")
+    p.add_argument("--no-barycenter", action="store_true")
+    p.add_argument("--no-tensor", action="store_true")
     p.add_argument("--mixed-count", type=int, default=64)
     p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations per warm-up step")
     return p.parse_args()
@@ -359,6 +361,9 @@ def run_ours(args):
 
     adjoint = None if args.no_adjoint else bench_adjoint(ctx, stream)
     locate = None if args.no_locate else bench_locate(ctx, stream, n, dev_in[0])
+    bary = None if args.no_barycenter else bench_barycenter(local, cpu=(rank == 0 and world == 1 and
+                                                                    not args.no_cpu_baseline))
+    tensor = None if args.no_tensor else bench_tensor(local, n, dev_in, opt, steps=min(args.steps, 5))
     mixed = None if args.no_mixed else bench_mixed(stream, args.mixed_count, precision=prec_of[args.precision])
 
     peaks = load_peaks()
@@ -392,7 +397,7 @@ def run_ours(args):
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
                 "precision": args.precision, "iterations": head["iterations"],
                 "final_residual_max": head["final_residual_max"], "gpu_launches": launches,
-                "e2e": e2e, "other_precision": other, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "e2e": e2e, "other_precision": other, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "barycenter": bary, "tensor_transform": tensor, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:
@@ -682,6 +687,143 @@ def bench_plain(device, n, dev_in, dev_out, opt, precision, steps=5):
 
 LOCATE_POINTS = 1 << 20
 LOCATE_SEED = 7
+
+
+def bench_barycenter(device, n=512, res=512, cpu=True):
+    """The bilinear barycenter pipeline at 512^2: four blurred-shape densities (the
+    single-solve generator at 512^2, blur sigma 2.5 px) solved in one batch, their inverse
+    meshes at the origin grid by GPU point location, the 5 x 5 grid of bilinear
+    barycenters rasterized at 512^2; then the gradient of the L2 loss between the centre
+    barycenter and a seeded Gaussian-mixture image with respect to the four densities
+    (otm_barycenter_loss, Krylov adjoint). Host buffers in and out, wall clock around each
+    whole phase after a warm-up. With cpu, the reference's forward pipeline on one core
+    (oracle/_ref: 4 solves, 4 inversions, 25 rasters)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from otmap_b200 import native as N
+    from otmap_b200 import otmap as ot
+    from otmap_b200 import workloads as W
+
+    ctx = N.Context(device)
+    dens = [W.to_cells(W.blurred_shapes(n, 100 + k, sigma_px=2.5)) for k in range(4)]
+    means = [d.mean() for d in dens]
+    target = W.gaussian_mixture(res, 17)
+    grid = ot.grid_vertices(n)
+    steps = [0.0, 0.25, 0.5, 0.75, 1.0]
+
+    def forward():
+        maps = ot.solve_batch(dens, context=ctx)
+        inv = []
+        for m in maps:
+            p = grid.copy()
+            m.apply_inverse(p)
+            inv.append(p)
+        imgs = [ot.barycenter_image(inv, a, b, means, res, context=ctx)[0] for a in steps for b in steps]
+        return maps, imgs
+
+    forward()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    maps, imgs = forward()
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    w = ot.bilinear_weights(0.5, 0.5)
+    ot.barycenter_loss(dens, w, target, context=ctx)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    loss, img, grads, st = ot.barycenter_loss(dens, w, target, context=ctx)
+    torch.cuda.synchronize()
+    t_grad = time.perf_counter() - t0
+    out = {"workload": f"4 blurred-shape densities {n}^2 (sigma 2.5 px), 5x5 bilinear barycenters rasterized at "
+                       f"{res}^2; gradient of sum (centre image - Gaussian-mixture target)^2 w.r.t. the 4 densities",
+           "forward_ms": 1e3 * t_fwd, "forward_iterations": [m.stats.iterations for m in maps],
+           "gradient_ms": 1e3 * t_grad, "loss": loss, "adjoint_solves": list(st.adjoint_solves)[:4],
+           "adjoint_residual": list(st.adjoint_residual)[:4],
+           "timing": "wall clock, host buffers in and out, after one warm-up of each phase"}
+    ctx.close()
+    if cpu:
+        from oracle import ref
+
+        if ref.available():
+            t0 = time.perf_counter()
+            rs = ref.RefSolver()
+            rs.init(n)
+            t_init = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            rmaps = [rs.solve(d) for d in dens]
+            inv = []
+            for m in rmaps:
+                p, _ = m.apply_inverse(grid)
+                inv.append(p)
+            for a in steps:
+                for b in steps:
+                    ref.barycenter(n, inv, a, b, means, res, res)
+            out["cpu_reference_forward_ms"] = 1e3 * (time.perf_counter() - t0)
+            out["cpu_reference_init_ms"] = 1e3 * t_init
+            out["cpu_reference_sample"] = "the same forward pipeline in the reference library on one core (init excluded)"
+    return out
+
+
+def bench_tensor(device, n, dev_in, opt, steps=5):
+    """The batch of the headline step in split precision with the tensor-core cosine
+    transform (OTM_POISSON_TENSOR): solves/s (device-resident, CUDA events, best step)
+    and the per-launch time of the tensor-core kernel from a profiled pass."""
+    import ctypes as C
+
+    import torch
+
+    from otmap_b200 import native as N
+
+    B = len(dev_in)
+    ctx = N.Context(device)
+    ctx.set_precision(N.PRECISION_SPLIT)
+    ctx.set_poisson(N.POISSON_TENSOR)
+    ctx.init(n)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", device))
+    V = (n + 1) ** 2
+    out = [torch.empty((V, 2), dtype=torch.float64, device="cuda") for _ in range(B)]
+    stats = (N.SolveStatsC * B)()
+    ns = (C.c_int * B)(*([n] * B))
+    dp = (C.c_void_p * B)(*[x.data_ptr() for x in dev_in])
+    fp = (C.c_void_p * B)(*[x.data_ptr() for x in out])
+    run = lambda: N.check(N.lib().otm_solve_batch(ctx.handle, B, ns, dp, C.byref(opt), fp, None, stats))
+    run()
+    times = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        run()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    ctx.profile(-1)
+    ctx.profile(1)
+    run()
+    prof = ctx.profile_totals()
+    ctx.profile(0)
+    ctx.close()
+    its = [stats[k].iterations for k in range(B)]
+    rec = {"value": B / (min(times) / 1e3), "unit": UNIT, "ms_per_step_best": min(times), "iterations": its,
+           "final_residual_max": max(stats[k].residual for k in range(B)),
+           "form": "split precision, OTM_POISSON_TENSOR (tcgen05 3xTF32 products), same batch as the headline"}
+    if prof and "dct_tc" in prof:
+        ms, cnt = prof["dct_tc"]
+        # four n x n x n products per instance-iteration: 8 n^3 algorithmic flops (the
+        # 3xTF32 split issues three MMAs per product, 24 n^3 on the tensor pipe)
+        flops = 8.0 * n ** 3 * sum(its)
+        peaks = load_peaks()
+        tf = flops / (ms / 1e3) / 1e12
+        rec["dct_tc"] = {"ms": ms, "launches": cnt, "avg_launch_us": 1e3 * ms / max(cnt, 1),
+                         "algorithmic_tflops": tf, "issued_tflops": 3 * tf,
+                         "frac_issued_of_tf32_peak": 3 * tf / (peaks["bf16_tflops"] / 2),
+                         "note": "one launch per product, four per iteration; tf32 peak taken as half the "
+                                 "measured bf16 GEMM rate (" + peaks["source"].split(":")[0] + ")"}
+    return rec
 
 
 def bench_locate(ctx, stream, n, dens_dev, repeats=5):

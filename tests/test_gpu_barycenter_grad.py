@@ -9,9 +9,9 @@ input density.
   ownership held fixed, the blend, a numerical Jacobian of the bilinear inversion
   (Newton solve, central differences) and the sparse-Jacobian adjoint reference --
   within 1e-5;
-* at 512^2 with four blurred-shape densities: against central differences (h = 1e-4
-  relative to each density value, FP64) of the same loss with the pixel ownership held
-  fixed, along the gradient's direction and smooth random directions, within 1e-2.
+* at 512^2 with four Gaussian-mixture densities: against central differences (h = 1e-3
+  .. 1e-5 relative to each density value, FP64) of the same loss with the pixel ownership
+  held fixed, along the gradient's direction and smooth random directions, within 1e-3.
 """
 
 import numpy as np
@@ -211,31 +211,38 @@ def test_gradient_matches_fp64_reference(n, res, ot, oracle_port):
 
 
 def test_gradient_central_differences_512(ot):
-    """Config-5 sizes: four 512^2 blurred-shape densities, centre barycenter rasterized at
-    512^2 against a seeded Gaussian-mixture target; directional derivatives against central
-    differences of the loss with the pixel ownership of the base point held fixed."""
+    """Config-5 sizes (four 512^2 densities, the centre barycenter rasterized at 512^2, a
+    seeded Gaussian-mixture target): directional derivatives against central differences
+    of the loss with the pixel ownership of the base point held fixed, along the gradient's
+    own direction and two smooth random directions, for h = 1e-3 .. 1e-5 relative to each
+    density value. Gaussian-mixture densities: their maps have no folded faces, so no
+    origin vertex lies in two faces and the loss is smooth (with the sharp blurred-shape
+    densities a few origin vertices fall in overlapping folded faces near the boundary,
+    where the reference's inversion rule -- first hit's weights, densest face -- jumps;
+    finite differences there pick up those jumps)."""
     from otmap_b200 import workloads as W
+    from otmap_b200.workloads import gaussian_blur
 
     n = res = 512
-    dens = [W.to_cells(W.blurred_shapes(n, 50 + k, sigma_px=2.5)) for k in range(4)]
+    dens = [W.to_cells(W.gaussian_mixture(n, 60 + k)) for k in range(4)]
     target = W.gaussian_mixture(res, 17)
     w = weights_bilinear(0.5, 0.5)
-    # the maps must be converged to the FP64 floor: a solve stopped at residual 1e-13 is still
-    # ~1e-5 from its limit at this size, as much as an h = 1e-4 perturbation moves it
-    opt = ot.SolverOptions(threshold=0.0, max_iter=2000)
-    # densities with a 1e3 background ratio: the adjoint takes hundreds of Poisson solves;
-    # a long restart keeps GMRES from stalling, and its residual is checked
+    # maps converged to the FP64 floor (threshold 0): a solve stopped at residual 1e-13 is
+    # still ~1e-5 from its limit at this size
+    opt = ot.SolverOptions(threshold=0.0, max_iter=3000)
     loss, img, grads, st = ot.barycenter_loss(dens, w, target, opt=opt,
-                                              adjoint_opt=tight_adjoint(1e-10, restart=200, max_iter=6000))
+                                              adjoint_opt=tight_adjoint(1e-12, restart=200, max_iter=8000))
     assert st.inverse_missing == 0
-    assert max(st.adjoint_residual[k] for k in range(4)) <= 1e-10, list(st.adjoint_residual)[:4]
+    assert max(st.adjoint_residual[k] for k in range(4)) <= 1e-11, list(st.adjoint_residual)[:4]
 
     def blend_of(ds):
         maps = ot.solve_batch(ds, opt)
         B = None
         for k, m in enumerate(maps):
             p = origin_grid(n).copy()
-            m.apply_inverse(p)
+            nh = np.zeros(len(p), dtype=np.int32)
+            m.apply_inverse(p, None, nh)
+            assert (nh == 1).all()  # no origin vertex in two faces: the loss is smooth here
             B = w[0] * p if B is None else B + w[k] * p
         return B
 
@@ -248,22 +255,16 @@ def test_gradient_central_differences_512(ot):
         return float(((im - target) ** 2).sum())
 
     assert abs(frozen_loss(dens) - loss) <= 1e-10 * loss
-    # Directions: the loss is ~1.5e6 and a white-noise perturbation of 1e-4 per cell moves
-    # it by ~1, below what the maps' residual error leaves; so the gradient's own direction
-    # (the largest first-order change per relative perturbation) and smooth random fields,
-    # each scaled so that no density value changes by more than h of itself.
-    from otmap_b200.workloads import gaussian_blur
-
     rng = np.random.default_rng(2)
-    h = 1e-4
     dirs = [[g * d * d for g, d in zip(grads, dens)]]
     for _ in range(2):
         dirs.append([W.to_cells(gaussian_blur(rng.standard_normal((n, n)), 16.0)) * d for d in dens])
     for v in dirs:
         scale = max(float(np.abs(x / d).max()) for x, d in zip(v, dens))
         v = [x / scale for x in v]
-        plus = frozen_loss([d + h * x for d, x in zip(dens, v)])
-        minus = frozen_loss([d - h * x for d, x in zip(dens, v)])
-        fd = (plus - minus) / (2 * h)
         an = sum(float(g @ x) for g, x in zip(grads, v))
-        assert abs(fd - an) <= 1e-2 * abs(an), (fd, an)
+        for h in (1e-3, 1e-4, 1e-5):
+            plus = frozen_loss([d + h * x for d, x in zip(dens, v)])
+            minus = frozen_loss([d - h * x for d, x in zip(dens, v)])
+            fd = (plus - minus) / (2 * h)
+            assert abs(fd - an) <= 1e-3 * abs(an), (h, fd, an)

