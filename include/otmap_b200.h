@@ -104,6 +104,8 @@ void otm_default_options(otm_solver_options* opt);
 
 /* Creates a context on CUDA device `device` (its own non-blocking stream). */
 int otm_create(int device, otm_context** ctx);
+/* Frees the context. Every otm_map created on it must be destroyed first: a map keeps
+ * using its context's device and stream, and destroying it afterwards is undefined. */
 int otm_destroy(otm_context* ctx);
 
 /* GridBasedTransportSolver::init (otsolver_2dgrid.cpp:75-104): prepares the size-n

@@ -12,12 +12,17 @@
 // in tensor memory (128 lanes x 128 FP32 columns): it stages 128 x 32 slices of A and B in
 // shared memory in the canonical no-swizzle K-major layout (8-row x 16-byte core
 // matrices), each value split into its nearest TF32 value and the TF32-rounded remainder,
-// and one thread issues tcgen05.mma kind::tf32 (M = 128, N = 128, K = 8)
-// for the products hi*hi + hi*lo + lo*hi accumulated in FP32 ("3xTF32": about FP32
-// accuracy). Completion is signalled by tcgen05.commit on an mbarrier; every wait is
-// bounded and a wait that runs out flags the instance (Inst::fault) and stops it, frees
-// the tensor memory and returns. The epilogue reads the accumulator with tcgen05.ld
-// (32 lanes x 32 columns per warp and step).
+// and one thread issues tcgen05.mma kind::tf32 (M = 128, N = 128, K = 8) for the products
+// hi*hi + hi*lo + lo*hi ("3xTF32": about FP32 accuracy). The tensor core rounds each
+// accumulation into its FP32 accumulator with a bias (the error of the first-step
+// transform grows linearly with the number of accumulations), so the two small correction
+// products go to a second accumulator (columns 128..255) and the large one takes one
+// accumulation per K = 8 only; the epilogue adds the two. Slices are double-buffered: the
+// threads stage slice s+1 while the products of slice s run. Completion is signalled by
+// tcgen05.commit on one mbarrier per buffer; every wait is bounded and a wait that runs
+// out (block-uniformly) flags the instance (Inst::fault) and stops it, waits for the
+// products in flight, frees the tensor memory and returns. The epilogue reads the
+// accumulators with tcgen05.ld (32 lanes x 32 columns per warp and step).
 
 #include <cmath>
 
@@ -31,7 +36,10 @@ constexpr int CORE = 128;                        // bytes of a core matrix (8 ro
 constexpr int LBO = CORE;                        // next core matrix along K
 constexpr int SBO = (TCK / 4) * CORE;            // next 8-row group
 constexpr int SLICE = TCM * TCK * 4;             // bytes of one operand slice (16 KB)
-constexpr int SMEM = 4 * SLICE + 64;             // A hi/lo, B hi/lo, mbarrier, tmem address
+constexpr int STAGES = 2;                        // slice buffers (A hi/lo, B hi/lo each)
+constexpr int BUF = 4 * SLICE;
+constexpr int SMEM = STAGES * BUF + 64;          // buffers, one mbarrier per buffer, tmem address
+constexpr int TMEM_COLS = 2 * TCN;               // main and correction accumulators
 constexpr long long kTcWait = 2000000000LL;      // ~1 s at the B200's clock
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -103,11 +111,13 @@ __device__ __forceinline__ float to_tf32(float x) {
 
 // Stages a 128 x 32 slice of the K-major operand M (row stride n) starting at (row0, k0):
 // high part = x rounded to TF32, low part = the remainder rounded to TF32 (|x - hi - lo|
-// <= 2^-22 |x|).
+// <= 2^-22 |x|). Thread e of a pass takes row (e>>6)*8 + (e&7), chunk (e>>3)&7: the 8
+// threads of a quarter-warp write 8 consecutive rows of one core matrix (128 contiguous
+// bytes, no bank conflict) and read 16 bytes each from 8 rows, 64 bytes per row per warp.
 __device__ __forceinline__ void stage_slice(const float* M, int n, int row0, int k0, unsigned char* hi,
                                             unsigned char* lo) {
   for (int e = threadIdx.x; e < TCM * (TCK / 4); e += blockDim.x) {
-    const int r = e >> 3, c = e & 7;
+    const int r = ((e >> 6) << 3) | (e & 7), c = (e >> 3) & 7;
     const float4 x = *reinterpret_cast<const float4*>(M + (size_t)(row0 + r) * n + k0 + 4 * c);
     float4 h, l;
     h.x = to_tf32(x.x);
@@ -144,30 +154,39 @@ __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_in
     case 2: A = I.CTf; B = T2; break;
     default: A = T1; B = I.CTf; break;
   }
-  unsigned char* a_hi = sm;
-  unsigned char* a_lo = sm + SLICE;
-  unsigned char* b_hi = sm + 2 * SLICE;
-  unsigned char* b_lo = sm + 3 * SLICE;
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sm + 4 * SLICE);
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + 4 * SLICE + 16);
+  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sm + STAGES * BUF);
+  unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + STAGES * BUF + 8 * STAGES);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(TCN)
+                 "r"(TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (threadIdx.x == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+    for (int b = 0; b < STAGES; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + b)) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const unsigned tmem = *tmem_slot;
+  const unsigned tmem = *tmem_slot, tmem_corr = tmem + (unsigned)TCN;
   bool ok = true;
-  unsigned phase = 0;
-  for (int k0 = 0; k0 < n && ok; k0 += TCK) {
+  unsigned phase[STAGES] = {};
+  bool pending[STAGES] = {};
+  for (int s = 0, k0 = 0; k0 < n; ++s, k0 += TCK) {
+    const int b = s % STAGES;
+    unsigned char* a_hi = sm + b * BUF;
+    unsigned char* a_lo = a_hi + SLICE;
+    unsigned char* b_hi = a_hi + 2 * SLICE;
+    unsigned char* b_lo = a_hi + 3 * SLICE;
+    if (pending[b]) {  // the buffer is reused: wait for the products that read it
+      ok = __syncthreads_and(bar_wait(bar + b, phase[b], limit) ? 1 : 0) != 0;
+      if (!ok) break;  // still pending: waited for once more below
+      phase[b] ^= 1u;
+      pending[b] = false;
+    }
     stage_slice(A, n, tm * TCM, k0, a_hi, a_lo);
     stage_slice(B, n, tn * TCN, k0, b_hi, b_lo);
     // generic-proxy writes to shared memory become visible to the tensor core's reads
@@ -176,37 +195,43 @@ __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_in
     if (threadIdx.x == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-      for (int s = 0; s < TCK / 8; ++s) {  // K = 8 per instruction: two core matrices along K
-        const unsigned off = (unsigned)(s * 2 * LBO);
+      for (int q = 0; q < TCK / 8; ++q) {  // K = 8 per instruction: two core matrices along K
+        const unsigned off = (unsigned)(q * 2 * LBO);
         const unsigned long long ah = smem_desc(smem_u32(a_hi) + off), al = smem_desc(smem_u32(a_lo) + off);
         const unsigned long long bh = smem_desc(smem_u32(b_hi) + off), bl = smem_desc(smem_u32(b_lo) + off);
-        mma_tf32(tmem, ah, bh, (k0 > 0 || s > 0) ? 1u : 0u);
-        mma_tf32(tmem, ah, bl, 1u);
-        mma_tf32(tmem, al, bh, 1u);
+        const unsigned first = (k0 > 0 || q > 0) ? 1u : 0u;
+        mma_tf32(tmem, ah, bh, first);
+        mma_tf32(tmem_corr, ah, bl, first);
+        mma_tf32(tmem_corr, al, bh, 1u);
       }
-      mma_commit(bar);
+      mma_commit(bar + b);
     }
-    // the slices are reused: wait for the products that read them
-    ok = bar_wait(bar, phase, limit);
-    phase ^= 1u;
-    __syncthreads();
+    pending[b] = true;
   }
+  // the products in flight (all of them once ok; after a timeout, one more bounded wait each)
+  for (int b = 0; b < STAGES; ++b)
+    if (pending[b]) {
+      const bool w = __syncthreads_and(bar_wait(bar + b, phase[b], limit) ? 1 : 0) != 0;
+      ok = ok && w;
+    }
   if (!ok) {
     if (threadIdx.x == 0) {
       atomicExch(&I.fault, 1);
       I.active = 0;
     }
-    bar_wait(bar, phase ^ 1u, limit);  // one more bounded wait for the products in flight
   } else {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int m = tm * TCM + warp * 32 + lane;  // this thread's output row
-    const unsigned row_addr = tmem + ((unsigned)(warp * 32) << 16);
+    const unsigned lane_off = (unsigned)(warp * 32) << 16;
     float ck = 0.f;
     if (stage == 1) ck = (float)I.cosk[m];
 #pragma unroll 1
     for (int c0 = 0; c0 < TCN; c0 += 32) {
-      float v[32];
-      tmem_ld32(row_addr + (unsigned)c0, v);
+      float v[32], w[32];
+      tmem_ld32(tmem + lane_off + (unsigned)c0, v);
+      tmem_ld32(tmem_corr + lane_off + (unsigned)c0, w);
+#pragma unroll
+      for (int q = 0; q < 32; ++q) v[q] += w[q];
       const int n0 = tn * TCN + c0;
       if (stage == 0 || stage == 1) {
         float* out = stage == 0 ? T1 : T2;
@@ -231,7 +256,7 @@ __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_in
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
 }  // namespace

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -176,6 +177,12 @@ class Context:
         check(lib().otm_create(int(device), C.byref(h)))
         self._h = h
         self.device = device
+        self._owners = weakref.WeakSet()
+
+    def track(self, owner):
+        """Registers an object holding device maps of this context (it has a release()
+        method): close() releases them before it frees the context."""
+        self._owners.add(owner)
 
     @property
     def handle(self):
@@ -183,6 +190,8 @@ class Context:
 
     def close(self):
         if getattr(self, "_h", None):
+            for o in list(getattr(self, "_owners", ())):
+                o.release()
             lib().otm_destroy(self._h)
             self._h = None
 

@@ -74,13 +74,18 @@ class TransportMap:
         self._map = None
         self.stats = stats
 
-    def __del__(self):
+    def release(self):
+        """Frees the device map (the point locator); it is rebuilt on the next inverse."""
         m = getattr(self, "_map", None)
+        self._map = None
         if m is not None:
-            try:
-                _n.lib().otm_map_destroy(m)
-            except Exception:
-                pass
+            _n.lib().otm_map_destroy(m)
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
 
     def origin_mesh(self) -> np.ndarray:
         return grid_vertices(self.n)
@@ -99,6 +104,7 @@ class TransportMap:
             _n.check(_n.lib().otm_map_create(self._ctx.handle, self.n, _n.ptr(self._fwd), _n.ptr(self._density),
                                              C.byref(h)))
             self._map = h
+            self._ctx.track(self)
         return self._map
 
     def init_inverse(self):

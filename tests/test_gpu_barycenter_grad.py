@@ -210,21 +210,42 @@ def test_gradient_matches_fp64_reference(n, res, ot, oracle_port):
         assert rel <= 1e-5, rel
 
 
+def folded_corners(fwd, n):
+    """Corners of the quads (v = j + i (n+1); corners (i,j), (i+1,j), (i+1,j+1), (i,j+1))
+    whose turn has the opposite sign to the undeformed grid's, or none."""
+    P = np.asarray(fwd).reshape(n + 1, n + 1, 2)
+    q = [P[:-1, :-1], P[1:, :-1], P[1:, 1:], P[:-1, 1:]]
+    G = origin_grid(n).reshape(n + 1, n + 1, 2)
+    g = [G[:-1, :-1], G[1:, :-1], G[1:, 1:], G[:-1, 1:]]
+    bad = 0
+    for c in range(4):
+        def turn(v):
+            a, b, p = v[c], v[(c + 1) % 4], v[(c + 3) % 4]
+            u, w_ = b - a, p - a
+            return u[..., 0] * w_[..., 1] - u[..., 1] * w_[..., 0]
+        bad += int((turn(q) * np.sign(turn(g)) <= 0).sum())
+    return bad
+
+
 def test_gradient_central_differences_512(ot):
     """Config-5 sizes (four 512^2 densities, the centre barycenter rasterized at 512^2, a
     seeded Gaussian-mixture target): directional derivatives against central differences
     of the loss with the pixel ownership of the base point held fixed, along the gradient's
     own direction and two smooth random directions, for h = 1e-3 .. 1e-5 relative to each
-    density value. Gaussian-mixture densities: their maps have no folded faces, so no
-    origin vertex lies in two faces and the loss is smooth (with the sharp blurred-shape
+    density value. Gaussian-mixture densities: their forward meshes have no folded faces
+    (every corner of every quad keeps the grid's orientation), so the inverse is a
+    continuous function of the mesh and the loss is smooth -- an origin vertex on an edge
+    shared by two faces gets the same position from either. With the sharp blurred-shape
     densities a few origin vertices fall in overlapping folded faces near the boundary,
-    where the reference's inversion rule -- first hit's weights, densest face -- jumps;
-    finite differences there pick up those jumps)."""
+    where the reference's inversion rule (first hit's weights, densest face) jumps, and
+    finite differences pick up those jumps."""
     from otmap_b200 import workloads as W
     from otmap_b200.workloads import gaussian_blur
 
     n = res = 512
-    dens = [W.to_cells(W.gaussian_mixture(n, 60 + k)) for k in range(4)]
+    # seeds whose maps are fold-free at 512^2 (seeds 60 and 62 have 448 and 866 folded
+    # corners in low-density regions)
+    dens = [W.to_cells(W.gaussian_mixture(n, 64 + k)) for k in range(4)]
     target = W.gaussian_mixture(res, 17)
     w = weights_bilinear(0.5, 0.5)
     # maps converged to the FP64 floor (threshold 0): a solve stopped at residual 1e-13 is
@@ -235,16 +256,20 @@ def test_gradient_central_differences_512(ot):
     assert st.inverse_missing == 0
     assert max(st.adjoint_residual[k] for k in range(4)) <= 1e-11, list(st.adjoint_residual)[:4]
 
-    def blend_of(ds):
+    def blend_of(ds, check_folds=False):
         maps = ot.solve_batch(ds, opt)
         B = None
         for k, m in enumerate(maps):
+            if check_folds:
+                assert folded_corners(m.fwd_mesh(), n) == 0
             p = origin_grid(n).copy()
             nh = np.zeros(len(p), dtype=np.int32)
             m.apply_inverse(p, None, nh)
-            assert (nh == 1).all()  # no origin vertex in two faces: the loss is smooth here
+            assert (nh >= 1).all()
             B = w[0] * p if B is None else B + w[k] * p
         return B
+
+    blend_of(dens, check_folds=True)
 
     B0 = blend_of(dens)
     owner = ot.raster_faces(B0, res, res, n=n)

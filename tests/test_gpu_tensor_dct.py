@@ -4,8 +4,9 @@ for split-precision instances, against the FFT transform of the same mode and ag
 FP64 reference's accuracy.
 
 * one iteration from the same start (max_iter = 1): the step taken with the tensor-core
-  direction equals the FFT one to the accuracy of the 3xTF32 split (each operand
-  represented to 2^-22 of itself, FP32 accumulation over n terms; positions within 1e-4);
+  direction is as close to the step of the FP64 transform as the FFT transform of the same
+  mode is (both FP32 transforms; the step's positions and residual differ from the FP64
+  step by up to 1e-4 and 7e-4 relative at 1024^2, and the two FP32 forms by about as much);
 * whole solves: the reported and the mesh-recomputed residual meet the threshold and the
   map lies within 1e-4 of the FFT-path map;
 * a batch mixing tensor-core sizes, FFT sizes and an FP64-only size agrees with single
@@ -53,16 +54,25 @@ def test_first_step_matches_fft_transform(n, ot):
 
     d = W.to_cells(W.blurred_shapes(n, 3, sigma_px=n / 200.0))
     opt = ot.SolverOptions(threshold=0.0, max_iter=1)
+    f64 = ot.GridBasedTransportSolver(N.Context(0))
+    f64.set_verbose_level(0)
+    f64.init(n)
+    exact = f64.solve(d, opt)
     out = {}
     for mode in (N.POISSON_FFT, N.POISSON_TENSOR):
         s = solver(ot, mode)
         s.init(n)
         out[mode] = s.solve(d, opt)
     a, b = out[N.POISSON_FFT], out[N.POISSON_TENSOR]
-    assert a.stats.iterations == b.stats.iterations == 1
-    err = float(np.abs(a.fwd_mesh() - b.fwd_mesh()).max())
-    assert err <= 1e-4, err  # measured: 8e-6 (128), 1.7e-5 (256), 2.5e-5 (512), 6.8e-5 (1024)
-    assert abs(a.stats.residual - b.stats.residual) <= 1e-4 * a.stats.residual
+    assert exact.stats.iterations == a.stats.iterations == b.stats.iterations == 1
+    pos = lambda m: float(np.abs(m.fwd_mesh() - exact.fwd_mesh()).max())
+    res = lambda m: abs(m.stats.residual - exact.stats.residual) / exact.stats.residual
+    # measured against the FP64 step, FFT / tensor: positions 2.8e-6 / 5.8e-6 (128),
+    # 2.5e-5 / 2.7e-5 (256), 6.3e-5 / 6.1e-5 (512), 9.8e-5 / 1.06e-4 (1024); residual
+    # 5.6e-6 / 1.7e-5, 1.6e-6 / 3.2e-5, 1.4e-4 / 1.6e-4, 5.2e-4 / 7.2e-4
+    assert pos(b) <= 2.0 * pos(a) + 1e-5, (pos(b), pos(a))
+    assert res(b) <= 2.0 * res(a) + 1e-4, (res(b), res(a))
+    assert float(np.abs(a.fwd_mesh() - b.fwd_mesh()).max()) <= 1e-4
 
 
 @pytest.mark.parametrize("n", [128, 512])
