@@ -40,8 +40,8 @@ struct SizeTables {
   DevBuf cosk;  // n doubles
   DevBuf tw;    // n/2 double2, exp(-2 pi i k / n) (power-of-two n)
   DevBuf pt;    // n double2, (cos, sin)(pi k / 2n) (power-of-two n)
-  DevBuf Cf;    // n*n floats, C[k][i] (tensor-core transform sizes)
-  DevBuf CTf;   // n*n floats, C^T
+  DevBuf Cf;    // C[k][i] as TF32 planes, hi then lo (2 n*n floats; tensor-core transform sizes)
+  DevBuf CTf;   // C^T, likewise
   bool dct_ok = false;      // the assembled matrix is diagonalised by C (checked on the GPU)
   double dct_check_err = 0;  // relative error of that check
 };
@@ -61,6 +61,8 @@ struct Workspace {
   DevBuf col_inst;   // int per column block of the fast transform
   DevBuf partials;   // double[total_tiles * 8]
   DevBuf arena;      // per-instance cell arrays
+  DevBuf tmaps;      // tensor maps of the tensor-core transform instances
+  std::vector<const void*> tmap_key;  // the buffers those maps were encoded for
   std::vector<unsigned char> h_insts;  // host mirror of Inst[count]
   void* h_pinned = nullptr;            // pinned staging for Inst readback
   size_t h_pinned_bytes = 0;

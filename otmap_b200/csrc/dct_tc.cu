@@ -5,60 +5,79 @@
 //   stage 0  U  = R C^T        A = R      B = C     stored transposed (T1[l][i] = U[i][l])
 //   stage 1  X  = C U          A = C      B = T1    Y = X / lambda, stored transposed (T2)
 //   stage 2  W  = C^T Y        A = C^T    B = T2    stored as is (T1)
-//   stage 3  d  = W C          A = T1     B = C^T   stored as is (d_hat)
+//   stage 3  d  = W C          A = T1     B = C^T   stored as is (d_hat, FP32)
 // Every product is D[m][n] = sum_k A[m][k] B[n][k] with both operands K-major (row m of A
 // and row n of B hold their k values contiguously), which is why the first two products
-// store their results transposed. A CTA of 128 threads computes one 128 x 128 tile of D
-// in tensor memory (128 lanes x 128 FP32 columns): it stages 128 x 32 slices of A and B in
-// shared memory in the canonical no-swizzle K-major layout (8-row x 16-byte core
-// matrices), each value split into its nearest TF32 value and the TF32-rounded remainder,
-// and one thread issues tcgen05.mma kind::tf32 (M = 128, N = 128, K = 8) for the products
-// hi*hi + hi*lo + lo*hi ("3xTF32": about FP32 accuracy). The tensor core rounds each
-// accumulation into its FP32 accumulator with a bias (the error of the first-step
-// transform grows linearly with the number of accumulations), so the two small correction
-// products go to a second accumulator (columns 128..255) and the large one takes one
-// accumulation per K = 8 only; the epilogue adds the two. Slices are double-buffered: the
-// threads stage slice s+1 while the products of slice s run. Completion is signalled by
-// tcgen05.commit on one mbarrier per buffer; every wait is bounded and a wait that runs
-// out (block-uniformly) flags the instance (Inst::fault) and stops it, waits for the
-// products in flight, frees the tensor memory and returns. The epilogue reads the
-// accumulators with tcgen05.ld (32 lanes x 32 columns per warp and step).
+// store their results transposed.
+//
+// 3xTF32: every operand value x is held as two TF32 planes, hi = x rounded to TF32 and
+// lo = (x - hi) rounded to TF32 (|x - hi - lo| <= 2^-22 |x|), and a product is
+// hi*hi + hi*lo + lo*hi accumulated in FP32. The planes are written once per value: the
+// basis C and C^T at init, R by k_tc_split before stage 0, the intermediates by the
+// epilogue of the stage that produces them. The tensor core rounds each accumulation into
+// its FP32 accumulator with a bias (the error of the first-step transform grows linearly
+// with the number of accumulations), so the two small correction products go to a second
+// accumulator and the large one takes one accumulation per K = 8 only; the epilogue adds
+// the two.
+//
+// A CTA of 128 threads computes one 128 x TN output tile (TN = 256, or 128 for n = 128) in
+// tensor memory: main accumulator in columns [0, TN), correction in [256, 256 + TN).
+// Thread 0 is the producer: it streams 128 x 32 slices of A and TN x 32 slices of B (hi
+// and lo planes) into a two-stage shared-memory ring with TMA (2-D tiled loads, 128-byte
+// rows, 128-byte swizzle, no multicast), each stage completing an mbarrier with its
+// transaction bytes. Thread 32 issues tcgen05.mma kind::tf32 (M = 128, N = TN, K = 8) on
+// the swizzled K-major layout (8-row groups 1024 bytes apart; the K offset within the
+// 128-byte row advances the start address by 32 bytes) and frees each stage with
+// tcgen05.commit on its "empty" mbarrier, then commits the last products to "done". All
+// four warps run the epilogue: tcgen05.ld of 32 lanes x 32 columns per warp and step.
+// Every wait is bounded; a wait that runs out flags the instance (Inst::fault) and stops
+// it, the CTA waits (again bounded) for the loads and products in flight, frees the
+// tensor memory and returns.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <vector>
 
 #include "engine.cuh"
 
 namespace otm {
 namespace {
 
-constexpr int TCM = 128, TCN = 128, TCK = 32;   // CTA tile and K slice
-constexpr int CORE = 128;                        // bytes of a core matrix (8 rows x 16 bytes)
-constexpr int LBO = CORE;                        // next core matrix along K
-constexpr int SBO = (TCK / 4) * CORE;            // next 8-row group
-constexpr int SLICE = TCM * TCK * 4;             // bytes of one operand slice (16 KB)
-constexpr int STAGES = 2;                        // slice buffers (A hi/lo, B hi/lo each)
-constexpr int BUF = 4 * SLICE;
-constexpr int SMEM = STAGES * BUF + 64;          // buffers, one mbarrier per buffer, tmem address
-constexpr int TMEM_COLS = 2 * TCN;               // main and correction accumulators
+constexpr int TM = 128, TK = 32, TN_MAX = 256;   // CTA tile (TN runtime: 256 or 128), K slice
+constexpr int STAGES = 2;
+constexpr int A_BYTES = TM * TK * 4;             // one plane of an A slice (16 KB)
+constexpr int B_BYTES = TN_MAX * TK * 4;         // one plane of a B slice (32 KB)
+constexpr int STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+constexpr int CTL_BYTES = 128;                   // mbarriers and control words
+constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + CTL_BYTES;  // + alignment slack
+constexpr int TMEM_COLS = 512, CORR_COL = 256;
 constexpr long long kTcWait = 2000000000LL;      // ~1 s at the B200's clock
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
-// Shared-memory matrix descriptor: start address, leading (K) and stride (M/N) byte
-// offsets in 16-byte units, descriptor version 1, no swizzle.
-__device__ __forceinline__ unsigned long long smem_desc(unsigned addr) {
-  return (unsigned long long)((addr >> 4) & 0x3FFFu) | ((unsigned long long)((LBO >> 4) & 0x3FFF) << 16) |
-         ((unsigned long long)((SBO >> 4) & 0x3FFF) << 32) | (1ull << 46);
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte swizzled layout:
+// start address, leading offset 16 bytes (unused for this layout), stride offset 1024
+// bytes between 8-row groups, descriptor version 1, layout type SWIZZLE_128B (2).
+__device__ __forceinline__ unsigned long long smem_desc_sw128(unsigned addr) {
+  return (unsigned long long)((addr >> 4) & 0x3FFFu) | (1ull << 16) | ((unsigned long long)(1024 >> 4) << 32) |
+         (1ull << 46) | (2ull << 61);
 }
 
-// Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major, N = 128, M = 128.
-constexpr unsigned kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(TCN >> 3) << 17) | ((unsigned)(TCM >> 4) << 24);
+// Instruction descriptor: FP32 accumulator, TF32 A and B, both K-major, M = 128, N = tn.
+__device__ __forceinline__ unsigned idesc_tf32(int tn) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((unsigned)(tn >> 3) << 17) | ((unsigned)(TM >> 4) << 24);
+}
 
-__device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long da, unsigned long long db, unsigned acc) {
+__device__ __forceinline__ void mma_tf32(unsigned tmem_d, unsigned long long da, unsigned long long db, unsigned idesc,
+                                         unsigned acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(kIdesc), "r"(acc)
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
       : "memory");
 }
 
@@ -82,6 +101,19 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, unsigned parit
   }
 }
 
+__device__ __forceinline__ void bar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+// 2-D tiled TMA load of the box at (x, y) = (column, row) of the map into shared memory,
+// completing its bytes on the mbarrier's transaction count.
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // 32 consecutive FP32 columns of this thread's accumulator row (warp w reads lanes
 // 32w .. 32w+31).
 __device__ __forceinline__ void tmem_ld32(unsigned addr, float (&v)[32]) {
@@ -99,9 +131,6 @@ __device__ __forceinline__ void tmem_ld32(unsigned addr, float (&v)[32]) {
   for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-// Offset of (row r, K chunk c of 4 values) in a staged slice.
-__device__ __forceinline__ int core_off(int r, int c) { return (r >> 3) * SBO + c * LBO + (r & 7) * 16; }
-
 // Nearest TF32 value of x (10 mantissa bits), as an FP32 bit pattern.
 __device__ __forceinline__ float to_tf32(float x) {
   unsigned r;
@@ -109,16 +138,18 @@ __device__ __forceinline__ float to_tf32(float x) {
   return __uint_as_float(r);
 }
 
-// Stages a 128 x 32 slice of the K-major operand M (row stride n) starting at (row0, k0):
-// high part = x rounded to TF32, low part = the remainder rounded to TF32 (|x - hi - lo|
-// <= 2^-22 |x|). Thread e of a pass takes row (e>>6)*8 + (e&7), chunk (e>>3)&7: the 8
-// threads of a quarter-warp write 8 consecutive rows of one core matrix (128 contiguous
-// bytes, no bank conflict) and read 16 bytes each from 8 rows, 64 bytes per row per warp.
-__device__ __forceinline__ void stage_slice(const float* M, int n, int row0, int k0, unsigned char* hi,
-                                            unsigned char* lo) {
-  for (int e = threadIdx.x; e < TCM * (TCK / 4); e += blockDim.x) {
-    const int r = ((e >> 6) << 3) | (e & 7), c = (e >> 3) & 7;
-    const float4 x = *reinterpret_cast<const float4*>(M + (size_t)(row0 + r) * n + k0 + 4 * c);
+// The hi and lo TF32 planes of the residual R (FP32, from the sweep) for stage 0. Work
+// item t of an instance splits cells [t E, (t+1) E), E = n^2 / items.
+__global__ __launch_bounds__(256) void k_tc_split(Inst* insts, const int* tc_inst, int base) {
+  const int item = base + blockIdx.x;
+  const Inst& I = insts[tc_inst[item]];
+  if (!I.active) return;
+  const size_t nn = (size_t)I.n * I.n, E = nn / I.ntc, e0 = (size_t)(item - I.tc0) * E;
+  const float4* r = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(I.r[I.it % 3]) + e0);
+  float4* hi = reinterpret_cast<float4*>(I.rs + e0);
+  float4* lo = reinterpret_cast<float4*>(I.rs + nn + e0);
+  for (size_t k = threadIdx.x; k < E / 4; k += blockDim.x) {
+    const float4 x = r[k];
     float4 h, l;
     h.x = to_tf32(x.x);
     h.y = to_tf32(x.y);
@@ -128,92 +159,111 @@ __device__ __forceinline__ void stage_slice(const float* M, int n, int row0, int
     l.y = to_tf32(x.y - h.y);
     l.z = to_tf32(x.z - h.z);
     l.w = to_tf32(x.w - h.w);
-    const int o = core_off(r, c);
-    *reinterpret_cast<float4*>(hi + o) = h;
-    *reinterpret_cast<float4*>(lo + o) = l;
+    hi[k] = h;
+    lo[k] = l;
   }
 }
 
-// One 128 x 128 output tile of stage `stage` for the instance owning work item blockIdx.x.
+// One 128 x TN output tile of stage `stage` for the instance owning work item blockIdx.x.
 __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_inst, int base, int stage,
                                                    long long limit) {
-  extern __shared__ __align__(128) unsigned char sm[];
+  extern __shared__ unsigned char sm_raw[];
   const int item = base + blockIdx.x;
   Inst& I = insts[tc_inst[item]];
   if (!I.active) return;
-  const int n = I.n, tiles = n / TCM;
-  const int t = item - I.tc0, tm = t / tiles, tn = t - (t / tiles) * tiles;
-  const float* R = reinterpret_cast<const float*>(I.r[I.it % 3]);
-  float* T1 = reinterpret_cast<float*>(I.t1);
-  float* T2 = reinterpret_cast<float*>(I.t2);
-  const float* A;
-  const float* B;
-  switch (stage) {
-    case 0: A = R; B = I.Cf; break;
-    case 1: A = I.Cf; B = T1; break;
-    case 2: A = I.CTf; B = T2; break;
-    default: A = T1; B = I.CTf; break;
-  }
-  unsigned long long* bar = reinterpret_cast<unsigned long long*>(sm + STAGES * BUF);
-  unsigned* tmem_slot = reinterpret_cast<unsigned*>(sm + STAGES * BUF + 8 * STAGES);
+  const int n = I.n, TN = I.tcn, tiles_n = n / TN;
+  const int t = item - I.tc0, tm = t / tiles_n, tn = t - tm * tiles_n;
+  const size_t nn = (size_t)n * n;
+  // 1024-byte aligned stages (the 128-byte swizzle repeats every 8 rows of 128 bytes)
+  const unsigned raw = smem_u32(sm_raw), sbase = (raw + 1023u) & ~1023u;
+  unsigned char* ctl_p = sm_raw + (sbase - raw) + STAGES * STAGE_BYTES;
+  unsigned long long* full = reinterpret_cast<unsigned long long*>(ctl_p);
+  unsigned long long* empty = full + STAGES;
+  unsigned long long* done = empty + STAGES;
+  volatile int* ctl = reinterpret_cast<volatile int*>(done + 1);  // tmem, fault, issued, consumed
+  const CUtensorMap* maps = reinterpret_cast<const CUtensorMap*>(I.tmaps) + 4 * stage;  // A hi, A lo, B hi, B lo
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32((const void*)ctl)),
                  "r"(TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (threadIdx.x == 0) {
-    for (int b = 0; b < STAGES; ++b)
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + b)) : "memory");
+  if (threadIdx.x == 32) {
+    for (int s = 0; s < STAGES; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + s)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(empty + s)) : "memory");
+    }
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(done)) : "memory");
+    ctl[1] = 0;
+    ctl[2] = 0;
+    ctl[3] = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const unsigned tmem = *tmem_slot, tmem_corr = tmem + (unsigned)TCN;
-  bool ok = true;
-  unsigned phase[STAGES] = {};
-  bool pending[STAGES] = {};
-  for (int s = 0, k0 = 0; k0 < n; ++s, k0 += TCK) {
-    const int b = s % STAGES;
-    unsigned char* a_hi = sm + b * BUF;
-    unsigned char* a_lo = a_hi + SLICE;
-    unsigned char* b_hi = a_hi + 2 * SLICE;
-    unsigned char* b_lo = a_hi + 3 * SLICE;
-    if (pending[b]) {  // the buffer is reused: wait for the products that read it
-      ok = __syncthreads_and(bar_wait(bar + b, phase[b], limit) ? 1 : 0) != 0;
-      if (!ok) break;  // still pending: waited for once more below
-      phase[b] ^= 1u;
-      pending[b] = false;
-    }
-    stage_slice(A, n, tm * TCM, k0, a_hi, a_lo);
-    stage_slice(B, n, tn * TCN, k0, b_hi, b_lo);
-    // generic-proxy writes to shared memory become visible to the tensor core's reads
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-#pragma unroll
-      for (int q = 0; q < TCK / 8; ++q) {  // K = 8 per instruction: two core matrices along K
-        const unsigned off = (unsigned)(q * 2 * LBO);
-        const unsigned long long ah = smem_desc(smem_u32(a_hi) + off), al = smem_desc(smem_u32(a_lo) + off);
-        const unsigned long long bh = smem_desc(smem_u32(b_hi) + off), bl = smem_desc(smem_u32(b_lo) + off);
-        const unsigned first = (k0 > 0 || q > 0) ? 1u : 0u;
-        mma_tf32(tmem, ah, bh, first);
-        mma_tf32(tmem_corr, ah, bl, first);
-        mma_tf32(tmem_corr, al, bh, 1u);
+  const unsigned tmem = (unsigned)ctl[0], tmem_corr = tmem + (unsigned)CORR_COL;
+  const int slices = n / TK;
+
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      const unsigned tx = 2u * (unsigned)(A_BYTES + TN * TK * 4);
+      int i = 0;
+      for (; i < slices; ++i) {
+        const int s = i % STAGES;
+        if (i >= STAGES && !bar_wait(empty + s, (unsigned)((i / STAGES - 1) & 1), limit)) {
+          ctl[1] = 1;
+          break;
+        }
+        const unsigned st = sbase + (unsigned)(s * STAGE_BYTES);
+        bar_expect_tx(full + s, tx);
+        tma_load_2d(st, maps + 0, i * TK, tm * TM, full + s);
+        tma_load_2d(st + A_BYTES, maps + 1, i * TK, tm * TM, full + s);
+        tma_load_2d(st + 2 * A_BYTES, maps + 2, i * TK, tn * TN, full + s);
+        tma_load_2d(st + 2 * A_BYTES + B_BYTES, maps + 3, i * TK, tn * TN, full + s);
       }
-      mma_commit(bar + b);
+      ctl[2] = i;
     }
-    pending[b] = true;
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      const unsigned idesc = idesc_tf32(TN);
+      int i = 0;
+      for (; i < slices; ++i) {
+        const int s = i % STAGES;
+        if (!bar_wait(full + s, (unsigned)((i / STAGES) & 1), limit)) {
+          ctl[1] = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned st = sbase + (unsigned)(s * STAGE_BYTES);
+#pragma unroll
+        for (int q = 0; q < TK / 8; ++q) {  // K = 8 TF32 = 32 bytes of each 128-byte row
+          const unsigned off = (unsigned)(q * 32);
+          const unsigned long long ah = smem_desc_sw128(st + off), al = smem_desc_sw128(st + A_BYTES + off);
+          const unsigned long long bh = smem_desc_sw128(st + 2 * A_BYTES + off);
+          const unsigned long long bl = smem_desc_sw128(st + 2 * A_BYTES + B_BYTES + off);
+          const unsigned acc = (i > 0 || q > 0) ? 1u : 0u;
+          mma_tf32(tmem, ah, bh, idesc, acc);
+          mma_tf32(tmem_corr, ah, bl, idesc, acc);
+          mma_tf32(tmem_corr, al, bh, idesc, 1u);
+        }
+        mma_commit(empty + s);  // the stage is free once these products have read it
+      }
+      ctl[3] = i;
+      mma_commit(done);  // completes once every product issued above has
+    }
+    __syncwarp();
   }
-  // the products in flight (all of them once ok; after a timeout, one more bounded wait each)
-  for (int b = 0; b < STAGES; ++b)
-    if (pending[b]) {
-      const bool w = __syncthreads_and(bar_wait(bar + b, phase[b], limit) ? 1 : 0) != 0;
-      ok = ok && w;
-    }
+  __syncthreads();
+  // loads issued but not consumed (after a timeout): wait for them before the CTA exits
+  if (threadIdx.x == 0)
+    for (int i = ctl[3]; i < ctl[2]; ++i)
+      if (!bar_wait(full + (i % STAGES), (unsigned)((i / STAGES) & 1), limit)) ctl[1] = 1;
+  const bool fin = bar_wait(done, 0u, limit);
+  const bool ok = __syncthreads_and(fin && ctl[1] == 0) != 0;
   if (!ok) {
     if (threadIdx.x == 0) {
       atomicExch(&I.fault, 1);
@@ -221,20 +271,22 @@ __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_in
     }
   } else {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const int m = tm * TCM + warp * 32 + lane;  // this thread's output row
+    const int m = tm * TM + warp * 32 + lane;  // this thread's output row
     const unsigned lane_off = (unsigned)(warp * 32) << 16;
-    float ck = 0.f;
-    if (stage == 1) ck = (float)I.cosk[m];
+    float* T1 = reinterpret_cast<float*>(I.t1);
+    float* T2 = reinterpret_cast<float*>(I.t2);
+    const float ck = stage == 1 ? (float)I.cosk[m] : 0.f;
 #pragma unroll 1
-    for (int c0 = 0; c0 < TCN; c0 += 32) {
+    for (int c0 = 0; c0 < TN; c0 += 32) {
       float v[32], w[32];
       tmem_ld32(tmem + lane_off + (unsigned)c0, v);
       tmem_ld32(tmem_corr + lane_off + (unsigned)c0, w);
 #pragma unroll
       for (int q = 0; q < 32; ++q) v[q] += w[q];
-      const int n0 = tn * TCN + c0;
+      const int n0 = tn * TN + c0;
       if (stage == 0 || stage == 1) {
-        float* out = stage == 0 ? T1 : T2;
+        float* hi = stage == 0 ? T1 : T2;
+        float* lo = hi + nn;
 #pragma unroll
         for (int q = 0; q < 32; ++q) {
           float x = v[q];
@@ -243,13 +295,33 @@ __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_in
             const float lam = 2.0f - 2.0f * ck * (float)I.cosk[l];
             x = (m == 0 && l == 0) ? 0.0f : x / lam;
           }
-          out[(size_t)(n0 + q) * n + m] = x;  // transposed: the warp's 32 rows are 32 consecutive floats
+          const float h = to_tf32(x);
+          // transposed: the warp's 32 rows are 32 consecutive floats of row n0 + q
+          hi[(size_t)(n0 + q) * n + m] = h;
+          lo[(size_t)(n0 + q) * n + m] = to_tf32(x - h);
+        }
+      } else if (stage == 2) {
+        float* hi = T1 + (size_t)m * n + n0;
+        float* lo = hi + nn;
+#pragma unroll
+        for (int q = 0; q < 32; q += 4) {
+          float4 h, l;
+          h.x = to_tf32(v[q]);
+          h.y = to_tf32(v[q + 1]);
+          h.z = to_tf32(v[q + 2]);
+          h.w = to_tf32(v[q + 3]);
+          l.x = to_tf32(v[q] - h.x);
+          l.y = to_tf32(v[q + 1] - h.y);
+          l.z = to_tf32(v[q + 2] - h.z);
+          l.w = to_tf32(v[q + 3] - h.w);
+          *reinterpret_cast<float4*>(hi + q) = h;
+          *reinterpret_cast<float4*>(lo + q) = l;
         }
       } else {
-        float* out = stage == 2 ? T1 : reinterpret_cast<float*>(I.dhat);
+        float* out = reinterpret_cast<float*>(I.dhat) + (size_t)m * n + n0;
 #pragma unroll
         for (int q = 0; q < 32; q += 4)
-          *reinterpret_cast<float4*>(out + (size_t)m * n + n0 + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
+          *reinterpret_cast<float4*>(out + q) = make_float4(v[q], v[q + 1], v[q + 2], v[q + 3]);
       }
     }
   }
@@ -259,11 +331,81 @@ __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_in
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    OTM_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+    if (q != cudaDriverEntryPointSuccess || !p) throw std::runtime_error("cuTensorMapEncodeTiled is not available");
+    fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// Map of one n x n FP32 plane (row-major) read in boxes of 32 columns (128 bytes) x rows.
+void encode_plane(CUtensorMap* m, const float* plane, int n, int rows) {
+  const cuuint64_t dim[2] = {(cuuint64_t)n, (cuuint64_t)n};
+  const cuuint64_t stride[1] = {(cuuint64_t)n * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)TK, (cuuint32_t)rows};
+  const cuuint32_t es[2] = {1, 1};
+  const CUresult r = encode_fn()(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(plane), dim, stride, box, es,
+                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed for a transform plane");
+}
+
 }  // namespace
 
 bool dct_tc_supported(int n) { return n == 128 || n == 256 || n == 512 || n == 1024; }
 
-int dct_tc_tiles(int n) { return (n / TCM) * (n / TCM); }
+int dct_tc_tn(int n) { return n >= TN_MAX ? TN_MAX : 128; }
+
+int dct_tc_tiles(int n) { return (n / TM) * (n / dct_tc_tn(n)); }
+
+size_t dct_tc_map_bytes() { return 16 * sizeof(CUtensorMap); }
+
+void dct_tc_encode(const Inst& I, void* host_maps) {
+  CUtensorMap m[16];  // 64-byte aligned for the encoder; copied out below
+  const int n = I.n, TN = I.tcn;
+  const size_t nn = (size_t)n * n;
+  const float* T1 = reinterpret_cast<const float*>(I.t1);
+  const float* T2 = reinterpret_cast<const float*>(I.t2);
+  const float* A[4] = {I.rs, I.Cf, I.CTf, T1};  // hi planes; the lo plane follows at + n^2
+  const float* B[4] = {I.Cf, T1, T2, I.CTf};
+  for (int s = 0; s < 4; ++s) {
+    encode_plane(m + 4 * s + 0, A[s], n, TM);
+    encode_plane(m + 4 * s + 1, A[s] + nn, n, TM);
+    encode_plane(m + 4 * s + 2, B[s], n, TN);
+    encode_plane(m + 4 * s + 3, B[s] + nn, n, TN);
+  }
+  std::memcpy(host_maps, m, sizeof(m));
+}
+
+void dct_tc_split_basis(const double* C, int n, std::vector<float>& cs, std::vector<float>& cts) {
+  // nearest TF32 value, ties away from zero (as cvt.rna), of a finite float below 2^127
+  auto tf32 = [](float x) {
+    unsigned u;
+    std::memcpy(&u, &x, 4);
+    u = (u + 0x1000u) & 0xFFFFE000u;
+    float y;
+    std::memcpy(&y, &u, 4);
+    return y;
+  };
+  const size_t nn = (size_t)n * n;
+  cs.assign(2 * nn, 0.f);
+  cts.assign(2 * nn, 0.f);
+  for (int k = 0; k < n; ++k)
+    for (int i = 0; i < n; ++i) {
+      const double c = C[(size_t)k * n + i];
+      const float h = tf32((float)c);
+      const float l = tf32((float)(c - (double)h));
+      cs[(size_t)k * n + i] = h;
+      cs[nn + (size_t)k * n + i] = l;
+      cts[(size_t)i * n + k] = h;
+      cts[nn + (size_t)i * n + k] = l;
+    }
+}
 
 void dct_tc_attrs(int device) {
   static bool done[64] = {};
@@ -275,6 +417,7 @@ void dct_tc_attrs(int device) {
 void dct_tc_run(otm_context* ctx, Inst* d_insts, const int* tc_inst, int base, int count) {
   dct_tc_attrs(ctx->device);
   if (count <= 0) return;
+  launch(ctx, "dct_tc_split", k_tc_split, count, 256, d_insts, tc_inst, base);
   for (int s = 0; s < 4; ++s)
     launch_smem(ctx, "dct_tc", k_dct_tc, count, 128, SMEM, d_insts, tc_inst, base, s, kTcWait);
 }

@@ -35,8 +35,11 @@ struct Inst {
   int fft, logn;      // fast transform used (n a power of two) / log2 n
   int split;          // split precision: r, d_hat, d, t1 hold FP32 values (psi, rho FP64)
   int tc0, ntc;       // tensor-core transform (dct_tc.cu): first item and item count of its work list
-  const float* Cf;    // FP32 cosine basis C[k][i] and its transpose (tensor-core transform)
+  int tcn;            // its output tile width (256, or 128 for n = 128)
+  const float* Cf;    // C[k][i] and C^T as TF32 planes: hi (n^2 floats) then lo (n^2 floats)
   const float* CTf;
+  float* rs;          // the residual's TF32 planes (hi, lo) for the first product
+  const void* tmaps;  // 16 TMA tensor maps of the four products (device memory)
   int row0, nrow, col0, ncol;  // first item and item count in the row / column work lists
   int strip0, nstrip;          // first block and block count in the strip work list
   // loop state
@@ -144,8 +147,15 @@ void dct_reg_run(otm_context* ctx, int n, bool fp32, Inst* d_insts, const int* r
                  int coff, int ccnt);
 // Tensor-core transform (dct_tc.cu) for split-precision instances of n in {128, ..., 1024}:
 // d_hat = C^T ((C r C^T) / lambda) C as four tcgen05 products, 3xTF32 in FP32.
+// The TF32 planes (hi then lo, n^2 floats each) of t1, t2 and rs hold every operand; the
+// 16 tensor maps of an instance are encoded on the host (dct_tc_encode) once its buffers
+// are laid out.
 bool dct_tc_supported(int n);
-int dct_tc_tiles(int n);  // 128 x 128 output tiles of one product
+int dct_tc_tn(int n);     // output tile width
+int dct_tc_tiles(int n);  // 128 x dct_tc_tn(n) output tiles of one product
+size_t dct_tc_map_bytes();  // bytes of one instance's tensor maps
+void dct_tc_encode(const Inst& I, void* host_maps);
+void dct_tc_split_basis(const double* C, int n, std::vector<float>& cs, std::vector<float>& cts);
 void dct_tc_attrs(int device);
 void dct_tc_run(otm_context* ctx, Inst* d_insts, const int* tc_inst, int base, int count);
 // Dynamic shared-memory limits of the kernels of each family (set once per device,

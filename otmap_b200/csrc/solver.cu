@@ -575,6 +575,7 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
       I.fft = 0;  // the tensor-core products instead of the FFT passes
       I.tc0 = tcitems;
       I.ntc = dct_tc_tiles(n);
+      I.tcn = dct_tc_tn(n);
       tcitems += I.ntc;
     } else if (I.fft) {
       int lg = 0;
@@ -585,8 +586,9 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
       I.ngemm = gemm_tiles_of(n);
       gemm += I.ngemm;
     }
-    // 11 cell arrays per instance, each padded to 32 doubles (256 bytes)
-    cells += 11 * (((size_t)n * n + 31) / 32 * 32);
+    // 11 cell arrays per instance (12 on the tensor-core transform: the residual's TF32
+    // planes), each padded to 32 doubles (256 bytes)
+    cells += (11 + (I.ntc > 0 ? 1 : 0)) * (((size_t)n * n + 31) / 32 * 32);
   }
   // sweep work list: the FP64 instances' strips, then the split-precision ones' (two
   // launches of each sweep when a batch has both)
@@ -694,8 +696,8 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
   for (int q = 0; q < count; ++q) {
     Inst& I = h[q];
     size_t N = (((size_t)I.n * I.n + 31) / 32) * 32;
-    double* arr[11];
-    for (int k = 0; k < 11; ++k) {
+    double* arr[12] = {};
+    for (int k = 0; k < 11 + (I.ntc > 0 ? 1 : 0); ++k) {
       arr[k] = base;
       base += N;
     }
@@ -717,6 +719,30 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.pt = T->pt.as<double2>();
     I.Cf = T->Cf.as<float>();
     I.CTf = T->CTf.as<float>();
+    I.rs = reinterpret_cast<float*>(arr[11]);
+  }
+  if (tcitems > 0) {
+    // tensor maps of the tensor-core instances, encoded again only when their buffers moved
+    std::vector<const void*> key;
+    for (const Inst& I : h)
+      if (I.ntc > 0) key.insert(key.end(), {(const void*)I.rs, I.t1, I.t2, I.Cf, I.CTf, (const void*)(size_t)I.n});
+    const size_t mb = dct_tc_map_bytes();
+    if (key != ws.tmap_key) {
+      ws.tmap_key.clear();
+      std::vector<unsigned char> maps;
+      for (const Inst& I : h)
+        if (I.ntc > 0) {
+          maps.resize(maps.size() + mb);
+          dct_tc_encode(I, maps.data() + maps.size() - mb);
+        }
+      ws.tmaps.reserve(maps.size());
+      OTM_CUDA(cudaMemcpyAsync(ws.tmaps.p, maps.data(), maps.size(), cudaMemcpyHostToDevice, ctx->stream));
+      OTM_CUDA(cudaStreamSynchronize(ctx->stream));
+      ws.tmap_key = key;
+    }
+    size_t k = 0;
+    for (Inst& I : h)
+      if (I.ntc > 0) I.tmaps = ws.tmaps.as<unsigned char>() + mb * k++;
   }
   return h;
 }
@@ -946,13 +972,9 @@ static SizeTables* init_size(otm_context* ctx, int n) {
     OTM_CUDA(cudaStreamSynchronize(st));
   }
   OTM_CUDA(cudaMemcpyAsync(T->C.p, C.data(), sizeof(double) * C.size(), cudaMemcpyHostToDevice, st));
-  if (dct_tc_supported(n)) {  // FP32 basis and its transpose for the tensor-core transform
-    std::vector<float> cf((size_t)n * n), ctf((size_t)n * n);
-    for (int k = 0; k < n; ++k)
-      for (int i = 0; i < n; ++i) {
-        cf[(size_t)k * n + i] = (float)C[(size_t)k * n + i];
-        ctf[(size_t)i * n + k] = (float)C[(size_t)k * n + i];
-      }
+  if (dct_tc_supported(n)) {  // TF32 planes of the basis and its transpose (tensor-core transform)
+    std::vector<float> cf, ctf;
+    dct_tc_split_basis(C.data(), n, cf, ctf);
     T->Cf.reserve(sizeof(float) * cf.size());
     T->CTf.reserve(sizeof(float) * ctf.size());
     OTM_CUDA(cudaMemcpyAsync(T->Cf.p, cf.data(), sizeof(float) * cf.size(), cudaMemcpyHostToDevice, st));
