@@ -1,6 +1,6 @@
 """A short, fixed solve for kernel profiling (ncu) and quick timing.
 
-    python tests/profile_case.py [--n 1024] [--batch 2] [--iters 3] [--poisson fft|dense] [--precision fp64|split]
+    python tests/profile_case.py [--n 1024] [--batch 2] [--iters 3] [--poisson fft|dense|tensor] [--precision fp64|split]
 
 Solves `batch` blurred-shape densities of size n for a fixed number of iterations
 (max_iter = iters, so every instance runs exactly that many) through the C ABI, with
@@ -26,7 +26,7 @@ def main():
     ap.add_argument("--n", type=int, default=1024)
     ap.add_argument("--batch", type=int, default=2)
     ap.add_argument("--iters", type=int, default=3)
-    ap.add_argument("--poisson", default="fft", choices=["fft", "dense"])
+    ap.add_argument("--poisson", default="fft", choices=["fft", "dense", "tensor"])
     ap.add_argument("--repeat", type=int, default=1)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
     a = ap.parse_args()
@@ -37,7 +37,7 @@ def main():
     from otmap_b200 import workloads as W
 
     ctx = N.Context(0)
-    ctx.set_poisson(N.POISSON_FFT if a.poisson == "fft" else N.POISSON_DENSE)
+    ctx.set_poisson({"fft": N.POISSON_FFT, "dense": N.POISSON_DENSE, "tensor": N.POISSON_TENSOR}[a.poisson])
     ctx.set_precision(N.PRECISION_SPLIT if a.precision == "split" else N.PRECISION_FP64)
     n, B = a.n, a.batch
     dens = [torch.from_numpy(W.to_cells(W.blurred_shapes(n, k, sigma_px=5.0))).cuda() for k in range(B)]
