@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--no-locate", action="store_true")
     p.add_argument("--no-barycenter", action="store_true")
     p.add_argument("--no-tensor", action="store_true")
+    p.add_argument("--no-config1", action="store_true")
     p.add_argument("--mixed-count", type=int, default=64)
     p.add_argument("--sample-iters", type=int, default=10, help="reference arm: iterations per warm-up step")
     return p.parse_args()
@@ -364,6 +365,7 @@ def run_ours(args):
     bary = None if args.no_barycenter else bench_barycenter(local, cpu=(rank == 0 and world == 1 and
                                                                     not args.no_cpu_baseline))
     tensor = None if args.no_tensor else bench_tensor(local, n, dev_in, opt, steps=min(args.steps, 5))
+    cfg1 = None if args.no_config1 else bench_config1(local, cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
     mixed = None if args.no_mixed else bench_mixed(stream, args.mixed_count, precision=prec_of[args.precision])
 
     peaks = load_peaks()
@@ -397,7 +399,7 @@ def run_ours(args):
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
                 "precision": args.precision, "iterations": head["iterations"],
                 "final_residual_max": head["final_residual_max"], "gpu_launches": launches,
-                "e2e": e2e, "other_precision": other, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "barycenter": bary, "tensor_transform": tensor, "roofline": roof, "kernels": kernels, "clocks": clk,
+                "e2e": e2e, "other_precision": other, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "barycenter": bary, "tensor_transform": tensor, "config1": cfg1, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}
         print(json.dumps(line))
     if world > 1:
@@ -765,6 +767,80 @@ def bench_barycenter(device, n=512, res=512, cpu=True):
             out["cpu_reference_init_ms"] = 1e3 * t_init
             out["cpu_reference_sample"] = "the same forward pipeline in the reference library on one core (init excluded)"
     return out
+
+
+def bench_config1(device, cpu=True, n=256, seed=0, repeats=5):
+    """The reference's own CPU-sized case: one 256^2 Gaussian-mixture solve (8 Gaussians +
+    floor 1e-3, residual <= 1e-7, FP64 mode) and the inversion of its 257^2 grid vertices
+    (locator build included), device-resident buffers, CUDA events around the whole unit,
+    median of `repeats` after a warm-up. With cpu, the same unit in the reference library on
+    one core (init, the per-size factorisation, excluded as the reference caches it)."""
+    import ctypes as C
+
+    import torch
+
+    from otmap_b200 import native as N
+    from otmap_b200 import otmap as ot
+    from otmap_b200 import workloads as W
+
+    ctx = N.Context(device)
+    ctx.init(n)
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", device))
+    dens_h = W.to_cells(W.gaussian_mixture(n, seed))
+    dens = torch.from_numpy(dens_h).cuda()
+    V = (n + 1) ** 2
+    fwd = torch.empty((V, 2), dtype=torch.float64, device="cuda")
+    adj = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    grid = torch.from_numpy(ot.grid_vertices(n)).cuda()
+    pts = torch.empty_like(grid)
+    opt = N.default_options()
+    opt.threshold = THRESHOLD
+    st = N.SolveStatsC()
+    missing = C.c_long(0)
+
+    def unit():
+        N.check(N.lib().otm_solve(ctx.handle, n, C.c_void_p(dens.data_ptr()), C.byref(opt), C.c_void_p(fwd.data_ptr()),
+                                  C.c_void_p(adj.data_ptr()), C.byref(st)))
+        h = C.c_void_p()
+        N.check(N.lib().otm_map_create(ctx.handle, n, C.c_void_p(fwd.data_ptr()), C.c_void_p(adj.data_ptr()),
+                                       C.byref(h)))
+        pts.copy_(grid)
+        N.check(N.lib().otm_map_inverse(h, C.c_void_p(pts.data_ptr()), V, None, None, C.byref(missing)))
+        N.lib().otm_map_destroy(h)
+
+    unit()
+    times = []
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        unit()
+        b.record(stream)
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    med = sorted(times)[len(times) // 2]
+    rec = {"workload": f"{n}^2 Gaussian mixture (8 Gaussians, floor 1e-3, seed {seed}), residual <= {THRESHOLD}, FP64; "
+                       f"inversion of the {n + 1}^2 grid vertices (locator build included)",
+           "ms": med, "units_per_s": 1e3 / med, "iterations": int(st.iterations), "residual": float(st.residual),
+           "inverse_missing": int(missing.value),
+           "timing": "CUDA events around solve + map + inversion, device-resident buffers, median of %d" % repeats}
+    ctx.close()
+    if cpu:
+        from oracle import ref
+
+        if ref.available():
+            rs = ref.RefSolver()
+            rs.init(n)
+            m = rs.solve(dens_h, threshold=THRESHOLD)
+            _, t_inv = m.apply_inverse(ot.grid_vertices(n))
+            rec["cpu_reference"] = {"seconds": m.seconds + t_inv, "solve_seconds": m.seconds,
+                                    "inverse_seconds": t_inv, "iterations": int(m.iterations), "cores": 1,
+                                    "units_per_s": 1.0 / (m.seconds + t_inv)}
+            import numpy as np
+
+            rec["max_vertex_err_vs_reference"] = float(np.abs(fwd.cpu().numpy() - m.fwd()).max())
+    return rec
 
 
 def bench_tensor(device, n, dev_in, opt, steps=5):
