@@ -137,6 +137,23 @@ struct otm_context {
   void* h_poll = nullptr;
   size_t h_poll_bytes = 0;
   otm::DevBuf raster_scratch;  // rasterizer face boxes, pixel owners, vertex values (grow-only)
+  // point-locator builds (locate.cu, grow-only): bin counts and scan sums; the BVH-order
+  // build's per-position arrays and node lists. Builds are ordered on the context stream.
+  otm::DevBuf locate_scratch, bvh_scratch;
+  // the BVH-order build of a grid size as a graph over bvh_scratch (rebuilt when the
+  // scratch moves)
+  struct GraphExec {
+    cudaGraphExec_t exec = nullptr;
+    void* base = nullptr;
+    long kernels = 0;
+    GraphExec() = default;
+    GraphExec(const GraphExec&) = delete;
+    GraphExec& operator=(const GraphExec&) = delete;
+    ~GraphExec() {
+      if (exec) cudaGraphExecDestroy(exec);
+    }
+  };
+  std::map<int, std::unique_ptr<GraphExec>> bvh_graphs;
   // adjoint workspaces per grid size (adjoint.cu); type-erased to keep this header small
   struct Erased {
     virtual ~Erased() = default;

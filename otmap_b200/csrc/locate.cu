@@ -230,10 +230,14 @@ __device__ __forceinline__ void bvh_node_init(BvhNode& b, int start, int end) {
 // Face centroids (bvh2d.cpp:44-58: zero + the corners in circulator order, / 4), face
 // boxes, identity permutation, every position in the root node.
 __global__ void k_bvh_init(const double* xy, int n, int* fac, double2* cen, double4* fbox, int* node_of,
-                           BvhNode* root) {
+                           BvhNode* root, int* counts) {
   const int N = n * n;
   int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f == 0) bvh_node_init(*root, 0, N);
+  if (f == 0) {
+    bvh_node_init(*root, 0, N);
+    counts[0] = 1;  // one node in the first level's list
+    counts[1] = 0;
+  }
   if (f >= N) return;
   Quad p;
   int vid[4];
@@ -254,13 +258,37 @@ __global__ void k_bvh_init(const double* xy, int n, int* fac, double2* cen, doub
 }
 
 // Node boxes: per position its face box folded into its node's with 64-bit atomics on
-// order-preserving keys; a warp whose positions share one node reduces first.
-__global__ void k_bvh_bbox(int N, const int* node_of, const double4* fbox, BvhNode* nodes) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+// order-preserving keys. A node's positions are contiguous, so a block whose 256
+// positions all belong to one node (the upper levels) reduces them first and issues one
+// set of atomics; otherwise every warp reduces each run of equal nodes with a segmented
+// shuffle scan and the last lane of a run issues its atomics.
+__device__ __forceinline__ double4 box_join(double4 a, double4 b) {
+  return make_double4(fmin(a.x, b.x), fmin(a.y, b.y), fmax(a.z, b.z), fmax(a.w, b.w));
+}
+__device__ __forceinline__ double4 box_shfl_up(double4 b, int o) {
+  return make_double4(__shfl_up_sync(0xffffffffu, b.x, o), __shfl_up_sync(0xffffffffu, b.y, o),
+                      __shfl_up_sync(0xffffffffu, b.z, o), __shfl_up_sync(0xffffffffu, b.w, o));
+}
+__device__ __forceinline__ void box_atomic(BvhNode& nd, const double4& b) {
+  atomicMin(&nd.kmin[0], dkey(b.x));
+  atomicMin(&nd.kmin[1], dkey(b.y));
+  atomicMax(&nd.kmax[0], dkey(b.z));
+  atomicMax(&nd.kmax[1], dkey(b.w));
+}
+
+constexpr int BBOX_T = 256;
+
+__global__ __launch_bounds__(BBOX_T) void k_bvh_bbox(int N, const int* node_of, const double4* fbox, BvhNode* nodes) {
+  __shared__ int s_first;
+  __shared__ double4 s_box[BBOX_T / 32];
+  const int p = blockIdx.x * BBOX_T + threadIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int k = p < N ? node_of[p] : -1;
   double4 b = k >= 0 ? fbox[p] : make_double4(0, 0, 0, 0);
-  const int k0 = __shfl_sync(0xffffffffu, k, 0);
-  if (__all_sync(0xffffffffu, k == k0) && k0 >= 0) {
+  if (threadIdx.x == 0) s_first = k;
+  __syncthreads();
+  const int first = s_first;
+  if (__syncthreads_and(k == first)) {  // one node (or only finished positions) in the block
+    if (first < 0) return;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       b.x = fmin(b.x, __shfl_xor_sync(0xffffffffu, b.x, o));
@@ -268,15 +296,25 @@ __global__ void k_bvh_bbox(int N, const int* node_of, const double4* fbox, BvhNo
       b.z = fmax(b.z, __shfl_xor_sync(0xffffffffu, b.z, o));
       b.w = fmax(b.w, __shfl_xor_sync(0xffffffffu, b.w, o));
     }
-    if ((threadIdx.x & 31) != 0) return;
-  } else if (k < 0) {
+    if (lane == 0) s_box[warp] = b;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double4 t = s_box[0];
+#pragma unroll
+      for (int w = 1; w < BBOX_T / 32; ++w) t = box_join(t, s_box[w]);
+      box_atomic(nodes[first], t);
+    }
     return;
   }
-  BvhNode& nd = nodes[k];
-  atomicMin(&nd.kmin[0], dkey(b.x));
-  atomicMin(&nd.kmin[1], dkey(b.y));
-  atomicMax(&nd.kmax[0], dkey(b.z));
-  atomicMax(&nd.kmax[1], dkey(b.w));
+  // runs of equal node ids are contiguous: inclusive segmented scan over each run
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double4 u = box_shfl_up(b, o);
+    const int ku = __shfl_up_sync(0xffffffffu, k, o);
+    if (lane >= o && ku == k) b = box_join(b, u);
+  }
+  const int kn = __shfl_down_sync(0xffffffffu, k, 1);
+  if (k >= 0 && (lane == 31 || kn != k)) box_atomic(nodes[k], b);
 }
 
 // Enlarged box, leaf test by size and depth, split dimension and value (bvh2d.cpp:178-212).
@@ -408,7 +446,12 @@ __global__ void k_bvh_assign(int N, int* node_of, const BvhNode* nodes, const in
   }
 }
 
-// rank[f] and the leaf box of f for the n^2 quads of the forward mesh xy (device).
+// rank[f] and the leaf box of f for the n^2 quads of the forward mesh xy (device). The
+// levels are a fixed sequence of ~250 small launches for a given n: they run as one CUDA
+// graph per size (captured on first use, kept in the context), on the context's grow-only
+// scratch, with the mesh copied in and the results copied out around it -- a host that
+// enqueues launches slowly then costs one launch instead of ~250. With profiling on, the
+// same launches are issued one by one so that each is timed.
 static void build_bvh_order(otm_context* ctx, const double* xy, int n, int* rank, double4* lbox) {
   cudaStream_t st = ctx->stream;
   const int N = n * n;
@@ -417,8 +460,9 @@ static void build_bvh_order(otm_context* ctx, const double* xy, int n, int* rank
   const int nsums = (N + 1 + SCAN_B - 1) / SCAN_B + 1;
   const size_t b_fac = al(sizeof(int) * N), b_cen = al(sizeof(double2) * N), b_box = al(sizeof(double4) * N);
   const size_t b_int = al(sizeof(int) * (N + 1)), b_nodes = al(sizeof(BvhNode) * cap), b_sums = al(sizeof(int) * nsums);
-  DevBuf buf;
-  buf.reserve(b_fac + b_cen + b_box + 5 * b_int + 2 * b_nodes + b_sums + 256);
+  const size_t b_xy = al(sizeof(double) * 2 * (size_t)(n + 1) * (n + 1));
+  DevBuf& buf = ctx->bvh_scratch;  // grow-only: no allocation once a size has been built
+  buf.reserve(b_fac + b_cen + 2 * b_box + 5 * b_int + 2 * b_nodes + b_sums + b_xy + b_fac + 256);
   char* q = buf.as<char>();
   auto take = [&](size_t b) {
     char* r = q;
@@ -436,34 +480,69 @@ static void build_bvh_order(otm_context* ctx, const double* xy, int n, int* rank
   BvhNode* lists[2] = {reinterpret_cast<BvhNode*>(take(b_nodes)), reinterpret_cast<BvhNode*>(take(b_nodes))};
   int* sums = reinterpret_cast<int*>(take(b_sums));
   int* counts = reinterpret_cast<int*>(take(256));  // node count of the current and next list
-  const int one = 1;
-  OTM_CUDA(cudaMemcpyAsync(counts, &one, sizeof(int), cudaMemcpyHostToDevice, st));
-  const unsigned ge = (unsigned)((N + 255) / 256);
-  launch(ctx, "bvh_init", k_bvh_init, ge, 256, xy, n, fac, cen, fbox, node_of, lists[0]);
-  for (int level = 0; level <= BVH_DEPTH; ++level) {
-    BvhNode* cur = lists[level & 1];
-    BvhNode* nxt = lists[(level + 1) & 1];
-    int* ccount = counts + (level & 1);
-    int* ncount = counts + ((level + 1) & 1);
-    const int ncap = std::min(level < 30 ? (1 << level) : cap, cap);
-    const unsigned gn = (unsigned)((ncap + 255) / 256);
-    OTM_CUDA(cudaMemsetAsync(ncount, 0, sizeof(int), st));
-    launch(ctx, "bvh_bbox", k_bvh_bbox, ge, 256, N, (const int*)node_of, (const double4*)fbox, cur);
-    launch(ctx, "bvh_decide", k_bvh_decide, gn, 256, cur, (const int*)ccount, level);
-    launch(ctx, "bvh_classify", k_bvh_classify, ge, 256, N, (const int*)node_of, (const double2*)cen,
-           (const BvhNode*)cur, small);
-    exclusive_scan(st, small, spre, sums, N);
-    ctx->launches += 3;
-    launch(ctx, "bvh_slots", k_bvh_slots, ge, 256, N, (const int*)node_of, (const BvhNode*)cur, (const int*)small,
-           (const int*)spre, slot_big, slot_small);
-    launch(ctx, "bvh_swap", k_bvh_swap, ge, 256, N, (const int*)node_of, (const BvhNode*)cur, (const int*)small,
-           (const int*)spre, (const int*)slot_small, fac, cen, fbox);
-    launch(ctx, "bvh_children", k_bvh_children, gn, 256, cur, (const int*)ccount, (const int*)spre,
-           (const int*)slot_big, (const int*)slot_small, (const double2*)cen, nxt, ncount);
-    launch(ctx, "bvh_assign", k_bvh_assign, ge, 256, N, node_of, (const BvhNode*)cur, (const int*)fac, rank, lbox);
+  double* sxy = reinterpret_cast<double*>(take(b_xy));
+  int* srank = reinterpret_cast<int*>(take(b_fac));
+  double4* slbox = reinterpret_cast<double4*>(take(b_box));
+  auto levels = [&]() {
+    const unsigned ge = (unsigned)((N + 255) / 256);
+    launch(ctx, "bvh_init", k_bvh_init, ge, 256, (const double*)sxy, n, fac, cen, fbox, node_of, lists[0], counts);
+    for (int level = 0; level <= BVH_DEPTH; ++level) {
+      BvhNode* cur = lists[level & 1];
+      BvhNode* nxt = lists[(level + 1) & 1];
+      int* ccount = counts + (level & 1);
+      int* ncount = counts + ((level + 1) & 1);
+      const int ncap = std::min(level < 30 ? (1 << level) : cap, cap);
+      const unsigned gn = (unsigned)((ncap + 255) / 256);
+      OTM_CUDA(cudaMemsetAsync(ncount, 0, sizeof(int), st));
+      launch(ctx, "bvh_bbox", k_bvh_bbox, (unsigned)((N + BBOX_T - 1) / BBOX_T), BBOX_T, N, (const int*)node_of,
+             (const double4*)fbox, cur);
+      launch(ctx, "bvh_decide", k_bvh_decide, gn, 256, cur, (const int*)ccount, level);
+      launch(ctx, "bvh_classify", k_bvh_classify, ge, 256, N, (const int*)node_of, (const double2*)cen,
+             (const BvhNode*)cur, small);
+      exclusive_scan(st, small, spre, sums, N);
+      ctx->launches += 3;
+      launch(ctx, "bvh_slots", k_bvh_slots, ge, 256, N, (const int*)node_of, (const BvhNode*)cur, (const int*)small,
+             (const int*)spre, slot_big, slot_small);
+      launch(ctx, "bvh_swap", k_bvh_swap, ge, 256, N, (const int*)node_of, (const BvhNode*)cur, (const int*)small,
+             (const int*)spre, (const int*)slot_small, fac, cen, fbox);
+      launch(ctx, "bvh_children", k_bvh_children, gn, 256, cur, (const int*)ccount, (const int*)spre,
+             (const int*)slot_big, (const int*)slot_small, (const double2*)cen, nxt, ncount);
+      launch(ctx, "bvh_assign", k_bvh_assign, ge, 256, N, node_of, (const BvhNode*)cur, (const int*)fac, srank,
+             slbox);
+    }
+  };
+  OTM_CUDA(cudaMemcpyAsync(sxy, xy, sizeof(double) * 2 * (size_t)(n + 1) * (n + 1), cudaMemcpyDeviceToDevice, st));
+  if (ctx->prof.on) {
+    levels();
+  } else {
+    auto& slot = ctx->bvh_graphs[n];
+    if (!slot || slot->base != buf.p) {
+      slot.reset(new otm_context::GraphExec());
+      slot->base = buf.p;
+      cudaGraph_t g = nullptr;
+      const long before = ctx->launches;
+      OTM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        levels();
+      } catch (...) {
+        cudaGraph_t dummy;
+        cudaStreamEndCapture(st, &dummy);
+        if (dummy) cudaGraphDestroy(dummy);
+        throw;
+      }
+      OTM_CUDA(cudaStreamEndCapture(st, &g));
+      slot->kernels = ctx->launches - before;
+      ctx->launches = before;  // captured, not executed
+      const cudaError_t e = cudaGraphInstantiate(&slot->exec, g, 0);
+      cudaGraphDestroy(g);
+      OTM_CUDA(e);
+    }
+    OTM_CUDA(cudaGraphLaunch(slot->exec, st));
+    ctx->launches += slot->kernels;
   }
+  OTM_CUDA(cudaMemcpyAsync(rank, srank, sizeof(int) * N, cudaMemcpyDeviceToDevice, st));
+  OTM_CUDA(cudaMemcpyAsync(lbox, slbox, sizeof(double4) * N, cudaMemcpyDeviceToDevice, st));
   OTM_CUDA(cudaGetLastError());
-  OTM_CUDA(cudaStreamSynchronize(st));  // the scratch is released on return
 }
 
 // ---- point location (TransportMap::init_inverse / inv_impl) ----
@@ -1045,20 +1124,22 @@ static void build_locator(otm_map* m) {
   m->bins = B;
   m->bin_start.reserve(sizeof(int) * (nb + 1));
   m->face_box.reserve(sizeof(double4) * N);
-  DevBuf counts, sums;
-  counts.reserve(sizeof(int) * nb);
-  sums.reserve(sizeof(int) * ((nb + SCAN_B - 1) / SCAN_B + 1));
-  OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
+  // bin counts and scan sums in the context's grow-only scratch
+  const size_t b_counts = (sizeof(int) * nb + 255) / 256 * 256;
+  ctx->locate_scratch.reserve(b_counts + sizeof(int) * ((nb + SCAN_B - 1) / SCAN_B + 1));
+  int* counts = ctx->locate_scratch.as<int>();
+  int* sums = reinterpret_cast<int*>(ctx->locate_scratch.as<char>() + b_counts);
+  OTM_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * nb, st));
   const double* xy = m->fwd.as<double>();
-  launch(ctx, "bin_count", k_bin_count, (N + 255) / 256, 256, xy, n, B, counts.as<int>(), m->face_box.as<double4>());
-  exclusive_scan(st, counts.as<int>(), m->bin_start.as<int>(), sums.as<int>(), nb);
+  launch(ctx, "bin_count", k_bin_count, (N + 255) / 256, 256, xy, n, B, counts, m->face_box.as<double4>());
+  exclusive_scan(st, counts, m->bin_start.as<int>(), sums, nb);
   int total = 0;
   OTM_CUDA(cudaMemcpyAsync(&total, m->bin_start.as<int>() + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
   OTM_CUDA(cudaStreamSynchronize(st));
   m->bin_faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1));
-  OTM_CUDA(cudaMemsetAsync(counts.p, 0, sizeof(int) * nb, st));
-  launch(ctx, "bin_fill", k_bin_fill, (N + 255) / 256, 256, xy, n, B, (const int*)m->bin_start.as<int>(),
-         counts.as<int>(), m->bin_faces.as<int>());
+  OTM_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * nb, st));
+  launch(ctx, "bin_fill", k_bin_fill, (N + 255) / 256, 256, xy, n, B, (const int*)m->bin_start.as<int>(), counts,
+         m->bin_faces.as<int>());
   OTM_CUDA(cudaGetLastError());
   m->bvh_rank.reserve(sizeof(int) * N);
   m->leaf_box.reserve(sizeof(double4) * N);
@@ -1134,7 +1215,6 @@ void inverse_grid_backward(otm_context* ctx, int n, const double* fwd, const int
   launch(ctx, "inv_vertex_grad", k_grid_vertex_gather, gv, 256, fwd, n, (const double*)nullptr, (const double2*)cs,
          dL_dfwd);
   OTM_CUDA(cudaGetLastError());
-  OTM_CUDA(cudaStreamSynchronize(st));  // the scratch is released on return
 }
 
 }  // namespace otm
