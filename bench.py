@@ -279,6 +279,7 @@ def run_ours(args):
         pass (host loop, per-kernel events) and the end-to-end pass (pinned host buffers)."""
         ctx = N.Context(local)
         ctx.set_precision(prec_of[precision])
+        ctx.set_autotune(True)  # the sweeps' strip height timed on the first call
         stream = torch.cuda.ExternalStream(ctx.stream(), device=torch.device("cuda", local))
         dev_out = [torch.empty((V, 2), dtype=torch.float64, device="cuda") for _ in range(B)]
         stats = (N.SolveStatsC * B)()
@@ -330,6 +331,7 @@ def run_ours(args):
         t_ms = max_over_ranks(t_ms, world)
         ms_step = t_ms / args.steps
         rec = {"precision": precision, "value": job_value(B, world, ms_step), "ms_per_step": ms_step,
+               "strip_rows": ctx.strip_rows(),
                "iterations": [s.iterations for s in st_list],
                "final_residual_max": max(s.residual for s in st_list), "gpu_launches": launches}
         if with_e2e:
@@ -431,6 +433,7 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6, precision=0):
     opt.threshold = threshold
     ctx = N.Context(torch.cuda.current_device())
     ctx.set_precision(precision)
+    ctx.set_autotune(True)
     stream = torch.cuda.ExternalStream(ctx.stream())
     for n in sorted(set(ns)):
         ctx.init(n)
@@ -454,7 +457,8 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6, precision=0):
         return best
 
     batch = lambda: N.check(N.lib().otm_solve_batch(ctx.handle, count, ns_c, dp, C.byref(opt), fp, None, stats))
-    batch()  # warm-up: builds the graph
+    batch()  # warm-up: builds the graph (and tunes the strip height)
+    rows_batched = ctx.strip_rows()
     l0 = ctx.launch_count()
     t_batch = timed(batch, repeats)
     launches = (ctx.launch_count() - l0) // repeats
@@ -463,6 +467,7 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6, precision=0):
     # workspace cache keeps one workspace and captured graph per size), warmed up first
     ctx_plain = N.Context(torch.cuda.current_device())
     ctx_plain.set_precision(precision)
+    ctx_plain.set_autotune(True)
     for n in sorted(set(ns)):
         ctx_plain.init(n)
     stream_p = torch.cuda.ExternalStream(ctx_plain.stream())
@@ -494,7 +499,8 @@ def bench_mixed(stream, count=64, repeats=2, threshold=1e-6, precision=0):
             "unit": "1024^2-equivalent solves/s", "batched_over_plain": t_plain / t_batch,
             "plain_timing": f"CUDA events around {count} sequential otm_solve calls on a separate warmed-up context "
                             "(device-side graph loop, one cached workspace per size), best of %d" % repeats,
-            "iterations_min_max": [min(iters), max(iters)]}
+            "iterations_min_max": [min(iters), max(iters)], "strip_rows_batched": rows_batched,
+            "autotune": "strip height of the sweeps timed on each context's first call of a configuration"}
 
 
 def bench_adjoint(ctx, stream, n=512, repeats=3):

@@ -388,7 +388,22 @@ int otm_barycenter_loss(otm_context* ctx, int n, int count, const double* const*
 #define OTM_OPT_PRECISION 4
 #define OTM_PRECISION_FP64 0
 #define OTM_PRECISION_SPLIT 1
+/* Strip height of the two stencil sweeps of a batch configuration (its list of sizes,
+ * Poisson mode and precision): OTM_AUTOTUNE_OFF (default) takes it from a fixed rule (64
+ * rows when the batch has many 32-row blocks per SM, 16 when it has fewer than the SMs,
+ * else 32); OTM_AUTOTUNE_ON times a few iterations of the first call's own densities at
+ * each of 16, 32 and 64 rows (host-driven loop, CUDA events) and keeps the fastest for
+ * that configuration (the real solve then starts from the same initial state). The strip
+ * height changes the order of the partial sums, so results can differ from the untuned
+ * configuration's at the last bits. */
+#define OTM_OPT_AUTOTUNE 5
+#define OTM_AUTOTUNE_OFF 0
+#define OTM_AUTOTUNE_ON 1
+/* Read-only: the strip height used by the context's last solve call. */
+#define OTM_INFO_STRIP_ROWS 6
 int otm_set_option(otm_context* ctx, int key, int value);
+/* Current value of an option, or OTM_INFO_STRIP_ROWS. */
+int otm_get_option(otm_context* ctx, int key, int* value);
 
 /* ---- allocation-free solve (no counterpart in the reference) ----
  *

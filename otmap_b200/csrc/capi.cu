@@ -214,6 +214,30 @@ extern "C" int otm_set_option(otm_context* ctx, int key, int value) {
     ctx->precision = value;
     return OTM_OK;
   }
+  if (key == OTM_OPT_AUTOTUNE) {
+    if (value != OTM_AUTOTUNE_OFF && value != OTM_AUTOTUNE_ON) {
+      set_error("otm_set_option: OTM_OPT_AUTOTUNE takes 0 or 1");
+      return OTM_ERR_BAD_ARG;
+    }
+    ctx->autotune = value;
+    return OTM_OK;
+  }
   set_error("otm_set_option: unknown option");
   return OTM_ERR_BAD_ARG;
+}
+
+extern "C" int otm_get_option(otm_context* ctx, int key, int* value) {
+  if (!ctx || !value) {
+    set_error("otm_get_option: null argument");
+    return OTM_ERR_BAD_ARG;
+  }
+  switch (key) {
+    case OTM_OPT_POISSON: *value = ctx->poisson_mode; return OTM_OK;
+    case OTM_OPT_LOOP: *value = ctx->loop_mode; return OTM_OK;
+    case OTM_OPT_WAIT_TEST: *value = ctx->wait_test; return OTM_OK;
+    case OTM_OPT_PRECISION: *value = ctx->precision; return OTM_OK;
+    case OTM_OPT_AUTOTUNE: *value = ctx->autotune; return OTM_OK;
+    case OTM_INFO_STRIP_ROWS: *value = ctx->last_srows; return OTM_OK;
+    default: set_error("otm_get_option: unknown key"); return OTM_ERR_BAD_ARG;
+  }
 }

@@ -69,6 +69,8 @@ struct Workspace {
   int total_tiles = 0, total_gemm = 0, total_rows = 0, total_cols = 0, total_strips = 0, total_tc = 0;
   int mode = -1;       // poisson mode the layout was built for
   int precision = -1;  // precision the layout was built for
+  int srows = 0;       // strip height of the sweeps (rule or autotuned)
+  bool tuned = false;  // srows was chosen by timing (OTM_OPT_AUTOTUNE)
   int split_strip0 = 0;  // strips of split-precision instances start here (FP64 ones before)
   struct Segment {  // instances of one size on one transform kernel family
     int n, reg, split, roff, rcnt, coff, ccnt;
@@ -119,6 +121,8 @@ struct otm_context {
   int loop_mode = 0;     // OTM_LOOP_GRAPH (0) / OTM_LOOP_HOST (1)
   int wait_test = 0;     // OTM_OPT_WAIT_TEST: bounded waits made to run out
   int precision = 0;     // OTM_PRECISION_FP64 / _SPLIT
+  int autotune = 0;      // OTM_AUTOTUNE_OFF / _ON (sweep strip height per batch configuration)
+  int last_srows = 0;    // strip height of the last solve call (OTM_INFO_STRIP_ROWS)
   otm::Profiler prof;
   std::map<int, std::unique_ptr<otm::SizeTables>> tables;
   // Workspaces of the most recent batch configurations (size list + Poisson mode), most

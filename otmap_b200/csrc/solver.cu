@@ -539,13 +539,50 @@ static int gemm_tiles_of(int n) {
   return t * t;
 }
 
+// Strip height srows for every instance of h: its sweep blocks and their place in the
+// work list (FP64 instances first, then the split-precision ones: two launches of each
+// sweep when a batch has both). Returns the list length; *split0 = first split block.
+static int assign_strips(std::vector<Inst>& h, int srows, int* split0 = nullptr) {
+  int strips = 0;
+  for (auto& I : h) {
+    I.srows = srows;
+    I.nstrip = strip_blocks(I.n, srows);
+  }
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1 && split0) *split0 = strips;
+    for (auto& I : h)
+      if (I.split == pass) {
+        I.strip0 = strips;
+        strips += I.nstrip;
+      }
+  }
+  return strips;
+}
+
+// assign_strips, then the workspace's sweep work list (block -> instance) on the device
+// and its partial-sum slots.
+static void set_strips(otm_context* ctx, Workspace& ws, std::vector<Inst>& h, int srows) {
+  int split0 = 0;
+  const int strips = assign_strips(h, srows, &split0);
+  std::vector<int> si(strips);
+  for (size_t q = 0; q < h.size(); ++q)
+    for (int k = 0; k < h[q].nstrip; ++k) si[h[q].strip0 + k] = (int)q;
+  ws.strip_inst.reserve(sizeof(int) * strips);
+  ws.sweep_partials.reserve(sizeof(double) * SWEEP_SLOTS * (size_t)strips);
+  OTM_CUDA(cudaMemcpyAsync(ws.strip_inst.p, si.data(), sizeof(int) * strips, cudaMemcpyHostToDevice, ctx->stream));
+  OTM_CUDA(cudaStreamSynchronize(ctx->stream));  // the host list is released on return
+  ws.split_strip0 = split0;
+  ws.total_strips = strips;
+  ws.srows = srows;
+}
+
 // Lays out (or reuses) the workspace for a list of sizes and returns host copies of
 // the instance records with buffer pointers filled in.
 static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<int>& sizes) {
   const int count = (int)sizes.size();
   std::vector<Inst> h(count);
   size_t cells = 0;
-  int tiles = 0, gemm = 0, rows = 0, cols = 0, strips = 0, split_strip0 = 0, tcitems = 0;
+  int tiles = 0, gemm = 0, rows = 0, cols = 0, tcitems = 0;
   // Taller sweep strips halve the per-strip overhead (ring prologue, block reduction) when
   // the batch has blocks to spare; a batch that does not fill the GPU twice over keeps
   // 32-row strips for parallelism, and one with fewer 32-row blocks than SMs takes 16-row
@@ -567,8 +604,6 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     I.tile0 = tiles;
     I.ntiles = tiles_of(n);
     tiles += I.ntiles;
-    I.srows = srows;
-    I.nstrip = strip_blocks(n, srows);
     I.fft = (ctx->poisson_mode != OTM_POISSON_DENSE && fft_eligible(n)) ? 1 : 0;
     I.split = (ctx->precision == OTM_PRECISION_SPLIT && I.fft && dct_reg_supported(n)) ? 1 : 0;
     if (ctx->poisson_mode == OTM_POISSON_TENSOR && I.split && dct_tc_supported(n)) {
@@ -589,16 +624,6 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     // 11 cell arrays per instance (12 on the tensor-core transform: the residual's TF32
     // planes), each padded to 32 doubles (256 bytes)
     cells += (11 + (I.ntc > 0 ? 1 : 0)) * (((size_t)n * n + 31) / 32 * 32);
-  }
-  // sweep work list: the FP64 instances' strips, then the split-precision ones' (two
-  // launches of each sweep when a batch has both)
-  for (int pass = 0; pass < 2; ++pass) {
-    if (pass == 1) split_strip0 = strips;
-    for (int q = 0; q < count; ++q)
-      if (h[q].split == pass) {
-        h[q].strip0 = strips;
-        strips += h[q].nstrip;
-      }
   }
   // fast-transform work lists, grouped into one segment per (kernel family, size)
   std::vector<Workspace::Segment> segs;
@@ -652,21 +677,17 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     ws.row_inst.reserve(sizeof(int) * (rows > 0 ? rows : 1));
     ws.col_inst.reserve(sizeof(int) * (cols > 0 ? cols : 1));
     ws.partials.reserve(sizeof(double) * KP * (size_t)tiles);
-    ws.strip_inst.reserve(sizeof(int) * strips);
-    ws.sweep_partials.reserve(sizeof(double) * SWEEP_SLOTS * (size_t)strips);
     ws.arena.reserve(sizeof(double) * cells);
-    std::vector<int> ti(tiles), gi(gemm), ri(rows), ci(cols), si(strips), tci(tcitems);
+    std::vector<int> ti(tiles), gi(gemm), ri(rows), ci(cols), tci(tcitems);
     for (int q = 0; q < count; ++q) {
       for (int k = 0; k < h[q].ntc; ++k) tci[h[q].tc0 + k] = q;
       for (int k = 0; k < h[q].ntiles; ++k) ti[h[q].tile0 + k] = q;
-      for (int k = 0; k < h[q].nstrip; ++k) si[h[q].strip0 + k] = q;
       for (int k = 0; k < h[q].ngemm; ++k) gi[h[q].gemm0 + k] = q;
       for (int k = 0; k < h[q].nrow; ++k) ri[h[q].row0 + k] = q;
       for (int k = 0; k < h[q].ncol; ++k) ci[h[q].col0 + k] = q;
     }
     cudaStream_t st = ctx->stream;
     OTM_CUDA(cudaMemcpyAsync(ws.tile_inst.p, ti.data(), sizeof(int) * tiles, cudaMemcpyHostToDevice, st));
-    OTM_CUDA(cudaMemcpyAsync(ws.strip_inst.p, si.data(), sizeof(int) * strips, cudaMemcpyHostToDevice, st));
     if (gemm) OTM_CUDA(cudaMemcpyAsync(ws.gemm_inst.p, gi.data(), sizeof(int) * gemm, cudaMemcpyHostToDevice, st));
     if (tcitems)
       OTM_CUDA(cudaMemcpyAsync(ws.tc_inst.p, tci.data(), sizeof(int) * tcitems, cudaMemcpyHostToDevice, st));
@@ -676,13 +697,11 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
     ws.sizes = sizes;
     ws.mode = ctx->poisson_mode;
     ws.precision = ctx->precision;
-    ws.split_strip0 = split_strip0;
     ws.total_tiles = tiles;
     ws.total_gemm = gemm;
     ws.total_tc = tcitems;
     ws.total_rows = rows;
     ws.total_cols = cols;
-    ws.total_strips = strips;
     ws.segments = segs;
     size_t need = sizeof(Inst) * count;
     if (ws.h_pinned_bytes < need) {
@@ -692,6 +711,12 @@ static std::vector<Inst> layout_workspace(otm_context* ctx, const std::vector<in
       ws.h_pinned_bytes = need;
     }
   }
+  // sweep strips: a new layout takes the rule's height, a cached one keeps its own
+  // (possibly autotuned) height and work list
+  if (!same)
+    set_strips(ctx, ws, h, srows);
+  else
+    assign_strips(h, ws.srows);
   double* base = ws.arena.as<double>();
   for (int q = 0; q < count; ++q) {
     Inst& I = h[q];
@@ -934,6 +959,61 @@ static std::vector<Inst> run_solver(otm_context* ctx, std::vector<Inst>& h, cons
   return out;
 }
 
+// OTM_AUTOTUNE_ON, first call of a batch configuration: K iterations of the call's own
+// densities at each candidate strip height (host-driven loop, CUDA events on the context
+// stream, the second of two runs), the fastest kept for the configuration. Every run
+// starts from the raw densities (the set-up normalises them in place), and so does the
+// real solve afterwards.
+static void tune_strips(otm_context* ctx, std::vector<Inst>& h, const otm_solver_options& o,
+                        const double* const* density) {
+  Workspace& ws = ctx->ws();
+  const int K = 4;
+  ws.tuned = true;
+  if (o.max_iter < K) return;  // nothing worth timing
+  auto reload = [&] {
+    for (size_t q = 0; q < h.size(); ++q)
+      copy_in(ctx, h[q].rho, density[q], sizeof(double) * (size_t)h[q].n * h[q].n);
+  };
+  otm_solver_options t = o;
+  t.max_iter = K;
+  const int loop = ctx->loop_mode, rule = ws.srows;
+  cudaEvent_t a = nullptr, b = nullptr;
+  int best = rule;
+  double best_ms = 0.0;
+  try {
+    ctx->loop_mode = OTM_LOOP_HOST;
+    OTM_CUDA(cudaEventCreate(&a));
+    OTM_CUDA(cudaEventCreate(&b));
+    for (int c : {16, 32, 64}) {
+      set_strips(ctx, ws, h, c);
+      float ms = 0.f;
+      for (int rep = 0; rep < 2; ++rep) {
+        reload();
+        OTM_CUDA(cudaEventRecord(a, ctx->stream));
+        run_solver(ctx, h, t);
+        OTM_CUDA(cudaEventRecord(b, ctx->stream));
+        OTM_CUDA(cudaEventSynchronize(b));
+        OTM_CUDA(cudaEventElapsedTime(&ms, a, b));
+      }
+      if (best_ms == 0.0 || ms < best_ms) {
+        best_ms = ms;
+        best = c;
+      }
+    }
+  } catch (...) {
+    ctx->loop_mode = loop;
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    throw;
+  }
+  ctx->loop_mode = loop;
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  set_strips(ctx, ws, h, best);
+  ws.drop_graph();  // captured with another work list
+  reload();
+}
+
 static void fill_stats(const Inst& I, otm_solve_stats* s) {
   if (!s) return;
   s->iterations = I.it;
@@ -1079,6 +1159,8 @@ extern "C" int otm_solve_batch(otm_context* ctx, int count, const int* ns, const
     std::vector<Inst> h = layout_workspace(ctx, sizes);
     for (int q = 0; q < count; ++q)
       copy_in(ctx, h[q].rho, density[q], sizeof(double) * (size_t)sizes[q] * sizes[q]);
+    if (ctx->autotune == OTM_AUTOTUNE_ON && !ctx->ws().tuned && !ctx->prof.on) tune_strips(ctx, h, o, density);
+    ctx->last_srows = ctx->ws().srows;
     Inst* d_insts = ctx->ws().insts.as<Inst>();
     // Host outputs of a batch on the device loop: the mesh of an instance that has stopped
     // is formed and copied out on a second stream while the others still iterate.

@@ -30,6 +30,7 @@ OPT_LOOP = 2
 LOOP_GRAPH, LOOP_HOST = 0, 1
 OPT_PRECISION = 4
 PRECISION_FP64, PRECISION_SPLIT = 0, 1
+OPT_AUTOTUNE, AUTOTUNE_OFF, AUTOTUNE_ON, INFO_STRIP_ROWS = 5, 0, 1, 6
 OPT_WAIT_TEST = 3
 RIO_PER_VERTEX, RIO_PER_FACE = 0, 1
 INV_DENSEST, INV_FIRST = 0, 1
@@ -124,6 +125,7 @@ SIGNATURES = {
                                       C.POINTER(SolverOptionsC), C.POINTER(AdjointOptionsC), C.c_void_p,
                                       C.POINTER(C.c_double), C.POINTER(C.c_void_p), C.POINTER(BarycenterStatsC)]),
     "otm_stream": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    "otm_get_option": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "otm_launch_count": (C.c_long, [C.c_void_p]),
     "otm_profile": (C.c_int, [C.c_void_p, C.c_int]),
     "otm_profile_entry": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_double),
@@ -214,6 +216,20 @@ class Context:
         """PRECISION_FP64 (default) or PRECISION_SPLIT (FP32 residuals, directions and
         transforms; FP64 potential, sums and line search)."""
         check(lib().otm_set_option(self._h, OPT_PRECISION, int(mode)))
+
+    def set_autotune(self, on: bool):
+        """AUTOTUNE_ON: the sweeps' strip height of a batch configuration is timed on its
+        first call (16, 32, 64 rows) and the fastest kept; AUTOTUNE_OFF (default): a fixed rule."""
+        check(lib().otm_set_option(self._h, OPT_AUTOTUNE, AUTOTUNE_ON if on else AUTOTUNE_OFF))
+
+    def get_option(self, key: int) -> int:
+        v = C.c_int(0)
+        check(lib().otm_get_option(self._h, int(key), C.byref(v)))
+        return v.value
+
+    def strip_rows(self) -> int:
+        """Strip height of the sweeps in the last solve call."""
+        return self.get_option(INFO_STRIP_ROWS)
 
     def stream(self) -> int:
         s = C.c_void_p()
