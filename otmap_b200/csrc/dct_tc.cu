@@ -32,7 +32,8 @@
 // four warps run the epilogue: tcgen05.ld of 32 lanes x 32 columns per warp and step.
 // Every wait is bounded; a wait that runs out flags the instance (Inst::fault) and stops
 // it, the CTA waits (again bounded) for the loads and products in flight, frees the
-// tensor memory and returns.
+// tensor memory and returns. OTM_OPT_WAIT_TEST makes the stage barriers expect bytes that
+// never arrive, so that this path runs without any fault.
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -56,6 +57,7 @@ constexpr int CTL_BYTES = 128;                   // mbarriers and control words
 constexpr int SMEM = 1024 + STAGES * STAGE_BYTES + CTL_BYTES;  // + alignment slack
 constexpr int TMEM_COLS = 512, CORR_COL = 256;
 constexpr long long kTcWait = 2000000000LL;      // ~1 s at the B200's clock
+constexpr long long kTcTestWait = 2000000LL;     // ~1 ms (OTM_OPT_WAIT_TEST)
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -165,8 +167,11 @@ __global__ __launch_bounds__(256) void k_tc_split(Inst* insts, const int* tc_ins
 }
 
 // One 128 x TN output tile of stage `stage` for the instance owning work item blockIdx.x.
+// extra: bytes added to every stage's expected transaction count (0; 16 under
+// OTM_OPT_WAIT_TEST, so that no stage ever completes and every wait runs out after
+// `limit`, by which time the real copies have landed: nothing is in flight at exit).
 __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_inst, int base, int stage,
-                                                   long long limit) {
+                                                   unsigned extra, long long limit) {
   extern __shared__ unsigned char sm_raw[];
   const int item = base + blockIdx.x;
   Inst& I = insts[tc_inst[item]];
@@ -209,7 +214,7 @@ __global__ __launch_bounds__(128, 1) void k_dct_tc(Inst* insts, const int* tc_in
 
   if (warp == 0) {
     if (lane == 0) {  // producer
-      const unsigned tx = 2u * (unsigned)(A_BYTES + TN * TK * 4);
+      const unsigned tx = 2u * (unsigned)(A_BYTES + TN * TK * 4) + extra;
       int i = 0;
       for (; i < slices; ++i) {
         const int s = i % STAGES;
@@ -418,8 +423,10 @@ void dct_tc_run(otm_context* ctx, Inst* d_insts, const int* tc_inst, int base, i
   dct_tc_attrs(ctx->device);
   if (count <= 0) return;
   launch(ctx, "dct_tc_split", k_tc_split, count, 256, d_insts, tc_inst, base);
+  const unsigned extra = ctx->wait_test ? 16u : 0u;
+  const long long limit = ctx->wait_test ? kTcTestWait : kTcWait;
   for (int s = 0; s < 4; ++s)
-    launch_smem(ctx, "dct_tc", k_dct_tc, count, 128, SMEM, d_insts, tc_inst, base, s, kTcWait);
+    launch_smem(ctx, "dct_tc", k_dct_tc, count, 128, SMEM, d_insts, tc_inst, base, s, extra, limit);
 }
 
 }  // namespace otm

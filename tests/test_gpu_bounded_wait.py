@@ -42,3 +42,32 @@ def test_wait_runs_out_and_the_context_recovers():
     maps = ot.solve_batch(batch, context=ctx)
     assert all(m.stats.outcome == N.CONVERGED for m in maps)
     ctx.close()
+
+
+def test_tensor_transform_wait_runs_out_and_the_context_recovers():
+    """The tensor-core transform's stage barriers (TMA transaction counts): under
+    OTM_OPT_WAIT_TEST they expect 16 bytes more than the copies bring, every wait gives up
+    after about 1 ms with the copies landed, the instance is flagged and the call returns
+    OTM_ERR_TIMEOUT; afterwards the same context solves as before."""
+    from otmap_b200 import native as N
+    from otmap_b200 import otmap as ot
+    from otmap_b200 import workloads as W
+
+    ctx = N.Context(0)
+    ctx.set_precision(N.PRECISION_SPLIT)
+    ctx.set_poisson(N.POISSON_TENSOR)
+    n = 256
+    d = W.to_cells(W.gaussian_mixture(n, 5))
+    s = ot.GridBasedTransportSolver(ctx)
+    s.set_verbose_level(0)
+    s.init(n)
+    good = s.solve(d)
+    N.check(N.lib().otm_set_option(ctx.handle, N.OPT_WAIT_TEST, 1))
+    with pytest.raises(N.OtmError) as e:
+        s.solve(d)
+    assert e.value.code == N.ERR_TIMEOUT
+    N.check(N.lib().otm_set_option(ctx.handle, N.OPT_WAIT_TEST, 0))
+    again = s.solve(d)
+    assert again.stats.iterations == good.stats.iterations
+    assert np.array_equal(again.fwd_mesh(), good.fwd_mesh())
+    ctx.close()
