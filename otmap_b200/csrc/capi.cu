@@ -108,6 +108,15 @@ extern "C" int otm_create(int device, otm_context** out) {
       OTM_CUDA(cudaSetDevice(device));
       OTM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       OTM_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
+      // the per-map buffers come from the device's default memory pool (stream-ordered
+      // allocation): let the pool keep freed memory for the next map instead of returning
+      // it to the driver at every synchronisation (a property of this process's pool)
+      cudaMemPool_t pool;
+      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+      }
+      cudaGetLastError();
     } catch (...) {
       delete ctx;
       throw;

@@ -33,6 +33,31 @@ struct DevBuf {
   }
 };
 
+// Device buffer from the stream-ordered allocator (cudaMallocAsync / cudaFreeAsync on the
+// stream it was reserved on): freeing it does not synchronise the device, and the device's
+// memory pool hands the memory to the next allocation. Used for the per-map buffers, which
+// live and die with each TransportMap.
+struct AsyncBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  AsyncBuf() = default;
+  AsyncBuf(const AsyncBuf&) = delete;
+  AsyncBuf& operator=(const AsyncBuf&) = delete;
+  ~AsyncBuf() { release(); }
+  void release() {
+    if (p) cudaFreeAsync(p, st);
+    p = nullptr;
+    bytes = 0;
+  }
+  // Grows (never shrinks) to at least `b` bytes on stream s; contents are not preserved.
+  void reserve(size_t b, cudaStream_t s);
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
 // Per grid size: the orthonormal DCT-II basis and cos(pi k / n), built by otm_init.
 struct SizeTables {
   int n = 0;
@@ -168,17 +193,19 @@ struct otm_context {
 struct otm_map {
   otm_context* ctx = nullptr;
   int n = 0;
-  otm::DevBuf fwd;      // V*2 doubles
-  otm::DevBuf density;  // N doubles
+  // buffers on the context stream's stream-ordered allocator (destroying a map does not
+  // synchronise the device)
+  otm::AsyncBuf fwd;      // V*2 doubles
+  otm::AsyncBuf density;  // N doubles
   // point-location structure (built lazily)
   bool located = false;
   int bins = 0;
-  otm::DevBuf bin_start;  // int[bins*bins + 1]
-  otm::DevBuf bin_faces;  // int[entries]
-  otm::DevBuf face_box;   // double4 per face (min x, min y, max x, max y)
-  otm::DevBuf bvh_rank;   // int per face: its position in the reference's BVH face array
-  otm::DevBuf leaf_box;   // double4 per face: the enlarged box of its BVH leaf
-  otm::DevBuf scratch;
+  otm::AsyncBuf bin_start;  // int[bins*bins + 1]
+  otm::AsyncBuf bin_faces;  // int[entries]
+  otm::AsyncBuf face_box;   // double4 per face (min x, min y, max x, max y)
+  otm::AsyncBuf bvh_rank;   // int per face: its position in the reference's BVH face array
+  otm::AsyncBuf leaf_box;   // double4 per face: the enlarged box of its BVH leaf
+  otm::AsyncBuf scratch;
 };
 
 namespace otm {

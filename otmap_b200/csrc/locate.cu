@@ -852,18 +852,40 @@ __device__ __forceinline__ int pixel_weights(const MeshRef& m, int rows, int col
   return c;
 }
 
-// One thread per face: every pixel centre of its box that the face accepts records the
-// face index with atomicMax, so each pixel ends with the highest accepting index -- the
-// face the reference's sequential loop writes last (rasterizer.cpp:162-236).
-__global__ void k_raster_owner(MeshRef m, int rows, int cols, const FaceRaster* fr, int* owner) {
+// Box rows per face (0 for an empty box): the work list of k_raster_owner_rows.
+__global__ void k_box_rows(int nf, const FaceRaster* fr, int* rows_of) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= m.nf) return;
+  if (f >= nf) return;
   const FaceRaster r = fr[f];
-  if (r.x0 >= r.x1 || r.y0 >= r.y1) return;
-  Quad p;
-  int vid[4];
-  const int c = load_face(m, f, p, vid);
-  for (int y = r.y0; y < r.y1; ++y) {
+  rows_of[f] = (r.x0 < r.x1 && r.y0 < r.y1) ? r.y1 - r.y0 : 0;
+}
+
+// The owner pass: every pixel centre of a face's box that the face accepts records the
+// face index with atomicMax, so each pixel ends with the highest accepting index -- the
+// face the reference's sequential loop writes last (rasterizer.cpp:162-236). One thread
+// per (face, box row) rather than per face: a stretched face
+// (the inverse maps of sharp densities have some that span much of the image) spreads over
+// as many threads as its box has rows, instead of holding one thread for its whole box
+// while the rest of the grid idles. Work item t belongs to the last face f with
+// row_start[f] <= t (row_start: exclusive prefix of the box rows, total at [nf]); grid-
+// stride over the total, which is read on the device. Same atomicMax of the face index,
+// so the owners are those of the per-face pass.
+__global__ void k_raster_owner_rows(MeshRef m, int rows, int cols, const FaceRaster* fr, const int* row_start,
+                                    int* owner) {
+  const int nf = m.nf;
+  const int total = row_start[nf];
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    int lo = 0, hi = nf;  // row_start[lo] <= t < row_start[hi]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (row_start[mid] <= t) lo = mid; else hi = mid;
+    }
+    const int f = lo;
+    const FaceRaster r = fr[f];
+    const int y = r.y0 + (t - row_start[f]);
+    Quad p;
+    int vid[4];
+    const int c = load_face(m, f, p, vid);
     const double qy = ((double)y + 0.5) / (double)rows;
     for (int x = r.x0; x < r.x1; ++x) {
       const double qx = ((double)x + 0.5) / (double)cols;
@@ -1122,8 +1144,8 @@ static void build_locator(otm_map* m) {
   const int B = n;
   const int nb = B * B;
   m->bins = B;
-  m->bin_start.reserve(sizeof(int) * (nb + 1));
-  m->face_box.reserve(sizeof(double4) * N);
+  m->bin_start.reserve(sizeof(int) * (nb + 1), ctx->stream);
+  m->face_box.reserve(sizeof(double4) * N, ctx->stream);
   // bin counts and scan sums in the context's grow-only scratch
   const size_t b_counts = (sizeof(int) * nb + 255) / 256 * 256;
   ctx->locate_scratch.reserve(b_counts + sizeof(int) * ((nb + SCAN_B - 1) / SCAN_B + 1));
@@ -1136,13 +1158,13 @@ static void build_locator(otm_map* m) {
   int total = 0;
   OTM_CUDA(cudaMemcpyAsync(&total, m->bin_start.as<int>() + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
   OTM_CUDA(cudaStreamSynchronize(st));
-  m->bin_faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1));
+  m->bin_faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1), ctx->stream);
   OTM_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * nb, st));
   launch(ctx, "bin_fill", k_bin_fill, (N + 255) / 256, 256, xy, n, B, (const int*)m->bin_start.as<int>(), counts,
          m->bin_faces.as<int>());
   OTM_CUDA(cudaGetLastError());
-  m->bvh_rank.reserve(sizeof(int) * N);
-  m->leaf_box.reserve(sizeof(double4) * N);
+  m->bvh_rank.reserve(sizeof(int) * N, ctx->stream);
+  m->leaf_box.reserve(sizeof(double4) * N, ctx->stream);
   build_bvh_order(ctx, xy, n, m->bvh_rank.as<int>(), m->leaf_box.as<double4>());
   m->located = true;
 }
@@ -1231,8 +1253,8 @@ extern "C" int otm_map_create(otm_context* ctx, int n, const double* fwd_xy, con
     m->n = n;
     try {
       size_t V = (size_t)(n + 1) * (n + 1), N = (size_t)n * n;
-      m->fwd.reserve(sizeof(double) * 2 * V);
-      m->density.reserve(sizeof(double) * N);
+      m->fwd.reserve(sizeof(double) * 2 * V, ctx->stream);
+      m->density.reserve(sizeof(double) * N, ctx->stream);
       copy_in(ctx, m->fwd.p, fwd_xy, sizeof(double) * 2 * V);
       copy_in(ctx, m->density.p, density, sizeof(double) * N);
       OTM_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1248,8 +1270,7 @@ extern "C" int otm_map_create(otm_context* ctx, int n, const double* fwd_xy, con
 extern "C" int otm_map_destroy(otm_map* m) {
   if (!m) return OTM_OK;
   cudaSetDevice(m->ctx->device);
-  cudaStreamSynchronize(m->ctx->stream);
-  delete m;
+  delete m;  // the buffers are freed in stream order, after the work queued on them
   return OTM_OK;
 }
 
@@ -1282,7 +1303,7 @@ extern "C" int otm_map_inverse_mode(otm_map* m, double* points, long count, int 
     size_t bf = (face && !fdev) ? sizeof(int) * (size_t)count : 0;
     size_t bh = (nhits && !hdev) ? sizeof(int) * (size_t)count : 0;
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    m->scratch.reserve(al(bp) + al(bf) + al(bh) + 256);
+    m->scratch.reserve(al(bp) + al(bf) + al(bh) + 256, ctx->stream);
     char* base = m->scratch.as<char>();
     double* dp = pdev ? points : reinterpret_cast<double*>(base);
     int* df = face ? (fdev ? face : reinterpret_cast<int*>(base + al(bp))) : nullptr;
@@ -1369,17 +1390,27 @@ static void raster_mesh(otm_context* ctx, const MeshRef& m, const double* densit
   auto al = [](size_t b) { return (b + 255) / 256 * 256; };
   const size_t b_fr = al(sizeof(FaceRaster) * (size_t)(nf > 0 ? nf : 1)), b_own = al(sizeof(int) * pix);
   const size_t b_vv = al(sizeof(float) * (size_t)(m.nv > 0 ? m.nv : 1));
-  ctx->raster_scratch.reserve(b_fr + b_own + b_vv);  // grows, kept for the next call
+  const size_t b_rows = al(sizeof(int) * (size_t)(nf + 1)), b_rs = al(sizeof(int) * ((nf + SCAN_B) / SCAN_B + 1));
+  ctx->raster_scratch.reserve(b_fr + b_own + b_vv + 2 * b_rows + b_rs);  // grows, kept for the next call
   char* base = ctx->raster_scratch.as<char>();
   FaceRaster* fr = reinterpret_cast<FaceRaster*>(base);
   int* owner = reinterpret_cast<int*>(base + b_fr);
   float* vval = reinterpret_cast<float*>(base + b_fr + b_own);
+  int* rows_of = reinterpret_cast<int*>(base + b_fr + b_own + b_vv);
+  int* row_start = reinterpret_cast<int*>(base + b_fr + b_own + b_vv + b_rows);
+  int* row_sums = reinterpret_cast<int*>(base + b_fr + b_own + b_vv + 2 * b_rows);
   OTM_CUDA(cudaMemsetAsync(owner, 0xff, sizeof(int) * pix, st));  // -1: no face
   // rasterizer.cpp:193 keeps 1/density.size() in a float
   const float scale = (float)(1. / (double)(density ? cells : nf));
   const int fblocks = nf > 0 ? (nf + 255) / 256 : 1;
   launch(ctx, "face_boxes", k_face_boxes, fblocks, 256, m, density, scale, rows, cols, fr);
-  launch(ctx, "raster_owner", k_raster_owner, fblocks, 256, m, rows, cols, (const FaceRaster*)fr, owner);
+  if (nf > 0) {
+    launch(ctx, "box_rows", k_box_rows, fblocks, 256, nf, (const FaceRaster*)fr, rows_of);
+    exclusive_scan(st, rows_of, row_start, row_sums, nf);
+    ctx->launches += 3;
+    launch(ctx, "raster_owner", k_raster_owner_rows, ctx->num_sms * 8, 256, m, rows, cols, (const FaceRaster*)fr,
+           (const int*)row_start, owner);
+  }
   const float* pv = nullptr;
   DevBuf vcount, vstart, vsums, vfaces, inv_area;  // indexed PerVertex temporaries
   if (mode == OTM_RIO_PER_VERTEX) {

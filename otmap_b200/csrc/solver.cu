@@ -533,6 +533,14 @@ void DevBuf::reserve(size_t b) {
   bytes = b;
 }
 
+void AsyncBuf::reserve(size_t b, cudaStream_t s) {
+  if (b <= bytes) return;
+  release();
+  st = s;
+  OTM_CUDA(cudaMallocAsync(&p, b, s));
+  bytes = b;
+}
+
 static int tiles_of(int n) { return ((n + TI - 1) / TI) * ((n + TJ - 1) / TJ); }
 static int gemm_tiles_of(int n) {
   int t = (n + GB - 1) / GB;

@@ -123,12 +123,18 @@ class TransportMap:
         self.apply_inverse(q, fast=True)
         return q[0]
 
-    def apply_inverse(self, points: np.ndarray, face=None, nhits=None, fast: bool = False) -> int:
-        """In place on a (P, 2) float64 array; returns the number of points with no face.
-        fast=False chooses faces as inv does, fast=True as inv_fast."""
+    def apply_inverse(self, points, face=None, nhits=None, fast: bool = False) -> int:
+        """In place on a (P, 2) float64 array -- a numpy array or a CUDA tensor, which then
+        stays on the device; returns the number of points with no face. fast=False chooses
+        faces as inv does, fast=True as inv_fast."""
         import ctypes as C
 
-        if points.dtype != np.float64 or not points.flags["C_CONTIGUOUS"]:
+        if hasattr(points, "data_ptr"):
+            import torch
+
+            if points.dtype != torch.float64 or not points.is_contiguous() or points.dim() != 2 or points.shape[1] != 2:
+                raise TypeError("points must be a contiguous float64 (P, 2) tensor")
+        elif points.dtype != np.float64 or not points.flags["C_CONTIGUOUS"]:
             raise TypeError("points must be a C-contiguous float64 (P, 2) array")
         missing = C.c_long(0)
         mode = _n.INV_FIRST if fast else _n.INV_DENSEST
@@ -412,8 +418,15 @@ def linear_weights(alpha: float):
     return [1. - a, a]
 
 
+def _as_mesh(m):
+    """(V, 2) float64 vertex array: a CUDA tensor is passed through (device pointer)."""
+    if hasattr(m, "data_ptr"):
+        return m.reshape(-1, 2).contiguous()
+    return np.ascontiguousarray(m, dtype=np.float64).reshape(-1, 2)
+
+
 def _blend_args(inv_maps, alpha, beta):
-    ms = [np.ascontiguousarray(m, dtype=np.float64).reshape(-1, 2) for m in inv_maps]
+    ms = [_as_mesh(m) for m in inv_maps]
     if len(ms) == 4 and beta is not None:
         w = bilinear_weights(alpha, beta)
     elif len(ms) == 2:
@@ -431,17 +444,19 @@ def interpolate(inv_maps, alpha: float, beta: float | None = None, context=None)
     ctx = context or _n.default_context()
     ms, w = _blend_args(inv_maps, alpha, beta)
     n = _grid_n(ms[0], None)
-    out = np.empty_like(ms[0])
-    arr = (C.c_void_p * len(ms))(*[m.ctypes.data for m in ms])
+    out = np.empty((ms[0].shape[0], 2))
+    arr = (C.c_void_p * len(ms))(*[_n.ptr(m).value for m in ms])
     wc = (C.c_double * len(w))(*w)
     _n.check(_n.lib().otm_mesh_blend(ctx.handle, n, len(ms), arr, wc, _n.ptr(out)))
     return out
 
 
-def barycenter_image(inv_maps, alpha: float, beta: float | None, density_means, res: int, context=None):
+def barycenter_image(inv_maps, alpha: float, beta: float | None, density_means, res: int, context=None,
+                     want_mesh: bool = True):
     """One image of the barycenters demo (apps/barycenters.cpp:250-290): interpolate the
-    inverse meshes, rasterize with unit density at res x res, rescale to the blended
-    mean of the input densities. Returns (image[res, res], blended mesh)."""
+    inverse meshes (numpy arrays, or CUDA tensors that stay on the device), rasterize with
+    unit density at res x res, rescale to the blended mean of the input densities. Returns
+    (image[res, res], blended mesh, or None when want_mesh is False)."""
     import ctypes as C
 
     ctx = context or _n.default_context()
@@ -455,8 +470,8 @@ def barycenter_image(inv_maps, alpha: float, beta: float | None, density_means, 
         expected = (1. - a) * m[0] + a * m[1]
     n = _grid_n(ms[0], None)
     img = np.empty((res, res))
-    mesh = np.empty_like(ms[0])
-    arr = (C.c_void_p * len(ms))(*[x.ctypes.data for x in ms])
+    mesh = np.empty((ms[0].shape[0], 2)) if want_mesh else None
+    arr = (C.c_void_p * len(ms))(*[_n.ptr(x).value for x in ms])
     wc = (C.c_double * len(w))(*w)
     _n.check(_n.lib().otm_barycenter(ctx.handle, n, len(ms), arr, wc, expected, res, res, _n.ptr(mesh), _n.ptr(img),
                                      None))
