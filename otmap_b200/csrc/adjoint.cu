@@ -113,19 +113,61 @@ __global__ void k_adj_cells(int n, const double* h, double scale, const double* 
 }
 
 // partial[b * (m+1) + i] = sum over this block's cells of w . V_i, i < m (basis vectors
-// stored contiguously with stride `ld`), and partial[b * (m+1) + m] = w . w.
+// stored contiguously with stride `ld`), and partial[b * (m+1) + m] = w . w. The dot
+// products are formed DOT_CHUNK at a time in one pass over the cells (w read once per
+// chunk), each a per-thread FMA chain over the grid-stride cells, then reduced together.
+constexpr int DOT_CHUNK = 8;
 __global__ void k_adj_multidot(long N, const double* w, const double* V, long ld, int m, double* partial) {
-  __shared__ double red[32];
+  __shared__ double red[32 * DOT_CHUNK];
   const int P = m + 1;
-  for (int i = 0; i < P; ++i) {
-    const double* vi = i < m ? V + (size_t)i * ld : w;
-    double s = 0.0;
-    for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x)
-      s = fma(w[f], vi[f], s);
-    double v[1] = {s};
-    block_sum<1>(v, red);
-    if (threadIdx.x == 0) partial[(size_t)blockIdx.x * P + i] = v[0];
+  for (int i0 = 0; i0 < P; i0 += DOT_CHUNK) {
+    double s[DOT_CHUNK];
+#pragma unroll
+    for (int c = 0; c < DOT_CHUNK; ++c) s[c] = 0.0;
+    for (long f = (long)blockIdx.x * blockDim.x + threadIdx.x; f < N; f += (long)gridDim.x * blockDim.x) {
+      const double wf = w[f];
+#pragma unroll
+      for (int c = 0; c < DOT_CHUNK; ++c) {
+        const int i = i0 + c;
+        if (i < P) s[c] = fma(wf, i < m ? V[(size_t)i * ld + f] : wf, s[c]);
+      }
+    }
+    block_sum<DOT_CHUNK>(s, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+      for (int c = 0; c < DOT_CHUNK; ++c)
+        if (i0 + c < P) partial[(size_t)blockIdx.x * P + i0 + c] = s[c];
   }
+}
+
+// The block partials of k_adj_multidot summed in block order (thread i: entry i).
+__device__ __forceinline__ double sum_partials(const double* partial, int nblocks, int P, int i) {
+  double t = 0.0;
+  for (int b = 0; b < nblocks; ++b) t += partial[(size_t)b * P + i];
+  return t;
+}
+
+// Gram-Schmidt pass over basis vectors 0..j: c_i = <w, v_i> (for the combine) and the
+// Hessenberg column entry H_ij accumulated over the two passes (pass 0 sets it).
+__global__ void k_adj_orth_reduce(const double* partial, int nblocks, int j, int pass, double* hcol, double* c) {
+  const int i = threadIdx.x;
+  if (i > j) return;
+  const double d = sum_partials(partial, nblocks, j + 2, i);
+  c[i] = d;
+  hcol[i] = (pass ? hcol[i] : 0.0) + d;
+}
+
+// |w| after the passes: H_{j+1,j} and the factor that normalises w (0 when |w| = 0).
+__global__ void k_adj_norm_reduce(const double* partial, int nblocks, int j, double* hcol, double* inv) {
+  if (threadIdx.x != 0) return;
+  const double hn = sqrt(sum_partials(partial, nblocks, 1, 0));
+  hcol[j + 1] = hn;
+  *inv = hn > 0 ? 1.0 / hn : 1.0;
+}
+
+__global__ void k_adj_scale_by(long N, double* v, const double* a) {
+  const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (f < N) v[f] *= *a;
 }
 
 // w = a * w - sum_i c_i V_i (i < m); c in device memory
@@ -207,7 +249,7 @@ struct AdjointWs : otm_context::Erased {
   int n = 0, m = 0;
   size_t N = 0, V = 0, ld = 0;
   DevBuf buf, recs, lists;
-  double *b, *lam, *z, *h, *t1, *t2, *Vb, *c, *part, *sums;
+  double *b, *lam, *z, *h, *t1, *t2, *Vb, *c, *part, *sums, *hcol, *inv;
   int G = 0, rows = 0, cols = 0, reg = 0, fft = 0;
   // record k: src = basis vector k (k < m+1); record m+1: src = b; record m+2: src = h; dst = z
   Inst* rec(int k) { return recs.as<Inst>() + k; }
@@ -223,7 +265,7 @@ static AdjointWs* adjoint_ws(otm_context* ctx, int n, int m) {
   W->V = (size_t)(n + 1) * (n + 1);
   W->ld = (W->N + 31) / 32 * 32;
   const int nred = 256;
-  const size_t words = W->ld * 6 + 2 * W->V + (size_t)(m + 1) * W->ld + (m + 2) + (size_t)nred * (m + 2) + 64;
+  const size_t words = W->ld * 6 + 2 * W->V + (size_t)(m + 1) * W->ld + (m + 2) + (size_t)nred * (m + 2) + (m + 3) + 64;
   W->buf.reserve(sizeof(double) * words);
   double* p = W->buf.as<double>();
   W->b = p; p += W->ld;
@@ -235,7 +277,9 @@ static AdjointWs* adjoint_ws(otm_context* ctx, int n, int m) {
   W->Vb = p; p += (size_t)(m + 1) * W->ld;
   W->c = p; p += m + 2;
   W->sums = p; p += 2;
-  W->part = p;
+  W->part = p; p += (size_t)nred * (m + 2);
+  W->hcol = p; p += m + 2;  // the current Hessenberg column
+  W->inv = p;
   SizeTables* T = ctx->tables.at(n).get();
   Inst base;
   std::memset(&base, 0, sizeof(base));
@@ -375,7 +419,7 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
       OTM_CUDA(cudaMemcpyAsync(d_V, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
       multidot(d_V, 0, dots);
       const double bnorm = std::sqrt(dots[0]);
-      std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m);
+      std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m), hcol_h(m + 2);
       auto Hs = [&](int i, int j) -> double& { return H[(size_t)i * m + j]; };
       rel = bnorm > 0 ? 1.0 : 0.0;
       bool first = true;
@@ -402,17 +446,24 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
           poisson_rec(ctx, W, j);  // z = M^+ v_j
           ++solves;
           apply_jt(d_z, w);
+          // two Gram-Schmidt passes and the normalisation with the reductions on the
+          // device (partials summed in block order); one read-back of the column per step
+          const unsigned rt = (unsigned)((j + 1 + 31) / 32 * 32);
           for (int pass = 0; pass < 2; ++pass) {
-            multidot(w, j + 1, dots);
-            for (int i = 0; i <= j; ++i) Hs(i, j) = (pass ? Hs(i, j) : 0.0) + dots[i];
-            OTM_CUDA(cudaMemcpyAsync(d_c, dots.data(), sizeof(double) * (j + 1), cudaMemcpyHostToDevice, st));
+            launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, (const double*)w, (const double*)d_V, (long)ld,
+                   j + 1, d_part);
+            launch(ctx, "adj_reduce", k_adj_orth_reduce, 1, rt, (const double*)d_part, nred, j, pass, W->hcol, d_c);
             launch(ctx, "adj_combine", k_adj_combine, gN, RB, (long)N, w, 1.0, (const double*)d_V, (long)ld, j + 1,
                    (const double*)d_c);
           }
-          multidot(w, 0, dots);
-          const double hn = std::sqrt(dots[0]);
-          Hs(j + 1, j) = hn;
-          if (hn > 0) launch(ctx, "adj_scale", k_adj_scale, gN, RB, (long)N, w, 1.0 / hn);
+          launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, (const double*)w, (const double*)d_V, (long)ld, 0,
+                 d_part);
+          launch(ctx, "adj_reduce", k_adj_norm_reduce, 1, 32, (const double*)d_part, nred, j, W->hcol, W->inv);
+          launch(ctx, "adj_scale", k_adj_scale_by, gN, RB, (long)N, w, (const double*)W->inv);
+          OTM_CUDA(cudaMemcpyAsync(hcol_h.data(), W->hcol, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, st));
+          OTM_CUDA(cudaStreamSynchronize(st));
+          for (int i = 0; i <= j + 1; ++i) Hs(i, j) = hcol_h[i];
+          const double hn = hcol_h[j + 1];
           for (int i = 0; i < j; ++i) {  // previous rotations
             const double t = cs[i] * Hs(i, j) + sn[i] * Hs(i + 1, j);
             Hs(i + 1, j) = -sn[i] * Hs(i, j) + cs[i] * Hs(i + 1, j);
