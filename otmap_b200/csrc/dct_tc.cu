@@ -142,14 +142,19 @@ __device__ __forceinline__ float to_tf32(float x) {
 
 // The hi and lo TF32 planes of the residual R (FP32, from the sweep) for stage 0. Work
 // item t of an instance splits cells [t E, (t+1) E), E = n^2 / items.
+// Each work item is split by SPLIT_PARTS blocks; the loop keeps four loads in flight per
+// thread.
+constexpr int SPLIT_PARTS = 2;
 __global__ __launch_bounds__(256) void k_tc_split(Inst* insts, const int* tc_inst, int base) {
-  const int item = base + blockIdx.x;
+  const int item = base + blockIdx.x / SPLIT_PARTS, part = blockIdx.x % SPLIT_PARTS;
   const Inst& I = insts[tc_inst[item]];
   if (!I.active) return;
-  const size_t nn = (size_t)I.n * I.n, E = nn / I.ntc, e0 = (size_t)(item - I.tc0) * E;
+  const size_t nn = (size_t)I.n * I.n, E = nn / I.ntc / SPLIT_PARTS;
+  const size_t e0 = (size_t)(item - I.tc0) * E * SPLIT_PARTS + (size_t)part * E;
   const float4* r = reinterpret_cast<const float4*>(reinterpret_cast<const float*>(I.r[I.it % 3]) + e0);
   float4* hi = reinterpret_cast<float4*>(I.rs + e0);
   float4* lo = reinterpret_cast<float4*>(I.rs + nn + e0);
+#pragma unroll 4
   for (size_t k = threadIdx.x; k < E / 4; k += blockDim.x) {
     const float4 x = r[k];
     float4 h, l;
@@ -423,7 +428,7 @@ void dct_tc_attrs(int device) {
 void dct_tc_run(otm_context* ctx, Inst* d_insts, const int* tc_inst, int base, int count) {
   dct_tc_attrs(ctx->device);
   if (count <= 0) return;
-  launch(ctx, "dct_tc_split", k_tc_split, count, 256, d_insts, tc_inst, base);
+  launch(ctx, "dct_tc_split", k_tc_split, count * SPLIT_PARTS, 256, d_insts, tc_inst, base);
   const unsigned extra = ctx->wait_test ? 16u : 0u;
   const long long limit = ctx->wait_test ? kTcTestWait : kTcWait;
   for (int s = 0; s < 4; ++s)
