@@ -210,6 +210,15 @@ def kernel_rates(prof, cell_iters, peaks):
     return out
 
 
+def load_pipes():
+    """FP64 pipe and occupancy figures of the iteration kernels from one ncu capture
+    (profiles/pipe_utilisation.json)."""
+    p = os.path.join(ROOT, "profiles", "pipe_utilisation.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return {}
+
+
 def roofline(prof, cell_iters, steps, peaks):
     """Dominant kernel: algorithmic bytes per launch / its average CUDA-event launch time."""
     if not prof:
@@ -227,7 +236,19 @@ def roofline(prof, cell_iters, steps, peaks):
             "traffic": traffic * cells_per_launch if traffic is not None else None,
             "alg_bytes_per_launch": per_launch_bytes, "avg_launch_us": avg_s * 1e6, "launches": cnt,
             "peak_source": peaks["source"],
-            "traffic_source": "profiles/traffic_per_cell.json (ncu dram__bytes_read+write per cell, scaled)"}
+            "traffic_source": "profiles/traffic_per_cell.json (ncu dram__bytes_read+write per cell, scaled)",
+            **pipe_note(name)}
+
+
+def pipe_note(name):
+    """What bounds a kernel that sits below the HBM roofline while moving only its
+    algorithmic bytes: its FP64 pipe share and occupancy from the committed ncu capture."""
+    rec = load_pipes().get(name)
+    if not rec:
+        return {}
+    return {"fp64_pipe_busy": rec["fp64_pipe"], "warps_active": rec["warps_active"], "registers": rec["registers"],
+            "limiter": "latency of dependent FP64 operations at the occupancy the registers allow "
+                       "(ncu: traffic equals the algorithmic bytes; see profiles/pipe_utilisation.json)"}
 
 
 def load_peaks():
@@ -399,7 +420,7 @@ def run_ours(args):
                 "dtype": "f32 cells / f64 sums" if args.precision == "split" else "f64",
                 "data": "synthetic (seeded blurred-shape densities, generated on the host in FP64)",
                 "config": config(args, world, {"l2": "256 MiB write between steps; working set > L2"}),
-                "precision": args.precision, "iterations": head["iterations"],
+                "precision": args.precision, "strip_rows": head["strip_rows"], "iterations": head["iterations"],
                 "final_residual_max": head["final_residual_max"], "gpu_launches": launches,
                 "e2e": e2e, "other_precision": other, "plain": plain, "parity": parity, "adjoint": adjoint, "batched_mixed": mixed, "locate": locate, "barycenter": bary, "tensor_transform": tensor, "config1": cfg1, "roofline": roof, "kernels": kernels, "clocks": clk,
                 "cpu_baseline": cpu}

@@ -108,15 +108,17 @@ extern "C" int otm_create(int device, otm_context** out) {
       OTM_CUDA(cudaSetDevice(device));
       OTM_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       OTM_CUDA(cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device));
-      // the per-map buffers come from the device's default memory pool (stream-ordered
-      // allocation): let the pool keep freed memory for the next map instead of returning
-      // it to the driver at every synchronisation (a property of this process's pool)
-      cudaMemPool_t pool;
-      if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
-        uint64_t keep = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-      }
-      cudaGetLastError();
+      // the per-map buffers come from this context's own memory pool (stream-ordered
+      // allocation), which keeps freed memory for the next map instead of returning it to
+      // the driver at every synchronisation; the device's default pool is left as it is
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.handleTypes = cudaMemHandleTypeNone;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = device;
+      OTM_CUDA(cudaMemPoolCreate(&ctx->pool, &props));
+      uint64_t keep = UINT64_MAX;
+      OTM_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep));
     } catch (...) {
       delete ctx;
       throw;
@@ -134,8 +136,12 @@ extern "C" int otm_destroy(otm_context* ctx) {
   cudaStream_t st = ctx->stream, side = ctx->side;
   cudaEvent_t ready = ctx->side_ready;
   void* poll = ctx->h_poll;
+  cudaMemPool_t pool = ctx->pool;
   delete ctx;
   if (st) cudaStreamDestroy(st);
+  // maps are destroyed before their context; memory a map still held would go back to
+  // the driver when that map frees it
+  if (pool) cudaMemPoolDestroy(pool);
   if (side) cudaStreamDestroy(side);
   if (ready) cudaEventDestroy(ready);
   if (poll) cudaFreeHost(poll);

@@ -33,10 +33,10 @@ struct DevBuf {
   }
 };
 
-// Device buffer from the stream-ordered allocator (cudaMallocAsync / cudaFreeAsync on the
-// stream it was reserved on): freeing it does not synchronise the device, and the device's
-// memory pool hands the memory to the next allocation. Used for the per-map buffers, which
-// live and die with each TransportMap.
+// Device buffer from the stream-ordered allocator (cudaMallocFromPoolAsync / cudaFreeAsync
+// on the stream it was reserved on, from the context's memory pool): freeing it does not
+// synchronise the device, and the pool hands the memory to the next allocation. Used for
+// the per-map buffers, which live and die with each TransportMap.
 struct AsyncBuf {
   void* p = nullptr;
   size_t bytes = 0;
@@ -50,8 +50,9 @@ struct AsyncBuf {
     p = nullptr;
     bytes = 0;
   }
-  // Grows (never shrinks) to at least `b` bytes on stream s; contents are not preserved.
-  void reserve(size_t b, cudaStream_t s);
+  // Grows (never shrinks) to at least `b` bytes on stream s from `pool`; contents are not
+  // preserved.
+  void reserve(size_t b, cudaStream_t s, cudaMemPool_t pool);
   template <class T>
   T* as() const {
     return static_cast<T*>(p);
@@ -140,6 +141,7 @@ struct Profiler {
 struct otm_context {
   int device = 0;
   cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;  // stream-ordered allocations of the per-map buffers
   int num_sms = 0;
   long launches = 0;  // kernels launched by this context since creation
   int poisson_mode = 0;  // OTM_POISSON_AUTO / _DENSE / _FFT

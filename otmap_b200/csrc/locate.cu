@@ -1144,8 +1144,8 @@ static void build_locator(otm_map* m) {
   const int B = n;
   const int nb = B * B;
   m->bins = B;
-  m->bin_start.reserve(sizeof(int) * (nb + 1), ctx->stream);
-  m->face_box.reserve(sizeof(double4) * N, ctx->stream);
+  m->bin_start.reserve(sizeof(int) * (nb + 1), ctx->stream, ctx->pool);
+  m->face_box.reserve(sizeof(double4) * N, ctx->stream, ctx->pool);
   // bin counts and scan sums in the context's grow-only scratch
   const size_t b_counts = (sizeof(int) * nb + 255) / 256 * 256;
   ctx->locate_scratch.reserve(b_counts + sizeof(int) * ((nb + SCAN_B - 1) / SCAN_B + 1));
@@ -1158,13 +1158,13 @@ static void build_locator(otm_map* m) {
   int total = 0;
   OTM_CUDA(cudaMemcpyAsync(&total, m->bin_start.as<int>() + nb, sizeof(int), cudaMemcpyDeviceToHost, st));
   OTM_CUDA(cudaStreamSynchronize(st));
-  m->bin_faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1), ctx->stream);
+  m->bin_faces.reserve(sizeof(int) * (size_t)(total > 0 ? total : 1), ctx->stream, ctx->pool);
   OTM_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * nb, st));
   launch(ctx, "bin_fill", k_bin_fill, (N + 255) / 256, 256, xy, n, B, (const int*)m->bin_start.as<int>(), counts,
          m->bin_faces.as<int>());
   OTM_CUDA(cudaGetLastError());
-  m->bvh_rank.reserve(sizeof(int) * N, ctx->stream);
-  m->leaf_box.reserve(sizeof(double4) * N, ctx->stream);
+  m->bvh_rank.reserve(sizeof(int) * N, ctx->stream, ctx->pool);
+  m->leaf_box.reserve(sizeof(double4) * N, ctx->stream, ctx->pool);
   build_bvh_order(ctx, xy, n, m->bvh_rank.as<int>(), m->leaf_box.as<double4>());
   m->located = true;
 }
@@ -1253,8 +1253,8 @@ extern "C" int otm_map_create(otm_context* ctx, int n, const double* fwd_xy, con
     m->n = n;
     try {
       size_t V = (size_t)(n + 1) * (n + 1), N = (size_t)n * n;
-      m->fwd.reserve(sizeof(double) * 2 * V, ctx->stream);
-      m->density.reserve(sizeof(double) * N, ctx->stream);
+      m->fwd.reserve(sizeof(double) * 2 * V, ctx->stream, ctx->pool);
+      m->density.reserve(sizeof(double) * N, ctx->stream, ctx->pool);
       copy_in(ctx, m->fwd.p, fwd_xy, sizeof(double) * 2 * V);
       copy_in(ctx, m->density.p, density, sizeof(double) * N);
       OTM_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -1303,7 +1303,7 @@ extern "C" int otm_map_inverse_mode(otm_map* m, double* points, long count, int 
     size_t bf = (face && !fdev) ? sizeof(int) * (size_t)count : 0;
     size_t bh = (nhits && !hdev) ? sizeof(int) * (size_t)count : 0;
     auto al = [](size_t b) { return (b + 255) / 256 * 256; };
-    m->scratch.reserve(al(bp) + al(bf) + al(bh) + 256, ctx->stream);
+    m->scratch.reserve(al(bp) + al(bf) + al(bh) + 256, ctx->stream, ctx->pool);
     char* base = m->scratch.as<char>();
     double* dp = pdev ? points : reinterpret_cast<double*>(base);
     int* df = face ? (fdev ? face : reinterpret_cast<int*>(base + al(bp))) : nullptr;

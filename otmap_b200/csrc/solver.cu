@@ -533,11 +533,11 @@ void DevBuf::reserve(size_t b) {
   bytes = b;
 }
 
-void AsyncBuf::reserve(size_t b, cudaStream_t s) {
+void AsyncBuf::reserve(size_t b, cudaStream_t s, cudaMemPool_t pool) {
   if (b <= bytes) return;
   release();
   st = s;
-  OTM_CUDA(cudaMallocAsync(&p, b, s));
+  OTM_CUDA(cudaMallocFromPoolAsync(&p, b, pool, s));
   bytes = b;
 }
 

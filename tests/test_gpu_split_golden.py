@@ -1,0 +1,125 @@
+"""The split-precision mode (OTM_PRECISION_SPLIT) on the reference's own solve goldens and
+on the solver options at the sizes the FP32 transforms take (64 .. 1024, powers of two).
+
+* Sizes outside the FP32 transforms run the FP64 path inside a split-mode context: the
+  goldens' FP64 criteria hold unchanged (identical iteration counts, positions within
+  1e-6, adjusted density to 1e-13).
+* Sizes inside: iteration counts within 3, the reported residual at or below the
+  threshold and the residual recomputed from the mesh within 2x of it, the FP64 density
+  adjustment unchanged (otsolver_2dgrid.cpp:47-63, 106-245). A solve stopped at the
+  threshold lies inside a ball around the converged map whose radius is the reference's
+  own distance to it (1.2e-3 .. 2.3e-3 for these goldens); the split mode is held to at
+  most 1.25 x that distance (+1e-5) and to positions within max(1e-4, a tenth of it) of
+  the reference's. The converged map is the C oracle's solve to residual 1e-13.
+* BetaOpt::Zero, the max_ratio clamp, a max_iter cap and a loose threshold at 64^2 and
+  128^2 against the C oracle: the same bars; a capped run stops at the cap exactly, with
+  positions within 1e-4 of the oracle's after the same iterations.
+"""
+
+import numpy as np
+import pytest
+
+from conftest import golden_names, load_golden, mesh_residual
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-6
+SPLIT_TOL = 1e-4
+
+
+def fp32_transform_size(n):
+    return n in (64, 128, 256, 512, 1024)
+
+
+@pytest.fixture(scope="module")
+def ot():
+    from otmap_b200 import otmap
+
+    return otmap
+
+
+@pytest.fixture(scope="module")
+def split_ctx():
+    from otmap_b200 import native
+
+    ctx = native.Context(0)
+    ctx.set_precision(native.PRECISION_SPLIT)
+    yield ctx
+    ctx.close()
+
+
+def split_solve(ot, ctx, density, n, beta_cj=True, max_iter=1000, threshold=1e-7, max_ratio=None):
+    s = ot.GridBasedTransportSolver(ctx)
+    s.set_verbose_level(0)
+    s.init(n)
+    kw = dict(beta=ot.BetaOpt(int(beta_cj)), max_iter=int(max_iter), threshold=float(threshold))
+    if max_ratio is not None:
+        kw["max_ratio"] = float(max_ratio)
+    return s.solve(density, ot.SolverOptions(**kw))
+
+
+def check_split(m, ref_fwd, converged_fwd, n, threshold):
+    err = float(np.abs(m.fwd_mesh() - ref_fwd).max())
+    own = float(np.abs(ref_fwd - converged_fwd).max())
+    ours = float(np.abs(m.fwd_mesh() - converged_fwd).max())
+    assert err <= max(SPLIT_TOL, 0.1 * own), (err, own)
+    assert ours <= 1.25 * own + 1e-5, (ours, own)
+    assert m.stats.residual <= threshold
+    assert mesh_residual(m.fwd_mesh(), m.density(), n) <= 2 * threshold
+
+
+def converged(oracle_port, d, n, beta_cj=True, max_ratio=None):
+    kw = {} if max_ratio is None else {"max_ratio": max_ratio}
+    return oracle_port.solve(d, n, beta_cj=bool(beta_cj), max_iter=5000, threshold=1e-13, trace=False, **kw).fwd
+
+
+@pytest.mark.parametrize("name", golden_names("solve_"))
+def test_split_mode_on_solve_goldens(name, ot, split_ctx, oracle_port):
+    g = load_golden(name)
+    n = int(g["n"])
+    m = split_solve(ot, split_ctx, g["density"], n, beta_cj=int(g["beta_cj"]), max_iter=int(g["max_iter"]),
+                    threshold=float(g["threshold"]), max_ratio=float(g["max_ratio"]))
+    np.testing.assert_allclose(m.density(), g["adjusted"], rtol=1e-13, atol=0)
+    err = float(np.abs(m.fwd_mesh() - g["fwd"]).max())
+    if not fp32_transform_size(n):
+        assert m.stats.iterations == int(g["iterations"])
+        assert err <= FP64_TOL, err
+        return
+    assert abs(m.stats.iterations - int(g["iterations"])) <= 3, (m.stats.iterations, int(g["iterations"]))
+    if int(g["iterations"]) >= int(g["max_iter"]):
+        assert err <= SPLIT_TOL, err
+        return
+    conv = converged(oracle_port, g["density"], n, beta_cj=int(g["beta_cj"]), max_ratio=float(g["max_ratio"]))
+    check_split(m, g["fwd"], conv, n, float(g["threshold"]))
+
+
+CASES = [
+    # (n, seed, beta_cj, max_iter, threshold, max_ratio)
+    (64, 11, 0, 1000, 1e-7, None),
+    (128, 12, 0, 1000, 1e-7, None),
+    (64, 13, 1, 1000, 1e-7, 20.0),
+    (128, 14, 1, 1000, 1e-7, 5.0),
+    (64, 15, 1, 5, 1e-7, None),
+    (128, 16, 1, 7, 1e-7, None),
+    (128, 17, 1, 1000, 1e-4, None),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"n{c[0]}_s{c[1]}_b{c[2]}_it{c[3]}_th{c[4]:g}_r{c[5]}" for c in CASES])
+def test_split_options_vs_oracle(case, ot, split_ctx, oracle_port):
+    from otmap_b200 import workloads as W
+
+    n, seed, beta_cj, max_iter, threshold, max_ratio = case
+    d = W.to_cells(W.gaussian_mixture(n, seed))
+    kw = {} if max_ratio is None else {"max_ratio": max_ratio}
+    o = oracle_port.solve(d, n, beta_cj=bool(beta_cj), max_iter=max_iter, threshold=threshold, **kw)
+    m = split_solve(ot, split_ctx, d, n, beta_cj=beta_cj, max_iter=max_iter, threshold=threshold,
+                    max_ratio=max_ratio)
+    np.testing.assert_allclose(m.density(), o.density, rtol=1e-13, atol=0)
+    if o.iterations >= max_iter:
+        assert m.stats.iterations == max_iter
+        err = float(np.abs(m.fwd_mesh() - o.fwd).max())
+        assert err <= SPLIT_TOL, err
+    else:
+        assert abs(m.stats.iterations - o.iterations) <= 3, (m.stats.iterations, o.iterations)
+        check_split(m, o.fwd, converged(oracle_port, d, n, beta_cj, max_ratio), n, threshold)

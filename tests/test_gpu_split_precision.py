@@ -21,22 +21,11 @@ test_gpu_parity*.py). The split mode is held to:
 import numpy as np
 import pytest
 
+from conftest import mesh_residual
+
 pytestmark = pytest.mark.gpu
 
 POS_TOL = 1e-4
-
-
-def mesh_residual(fwd, density, n):
-    """sum (A_f - e^2 rho_f)^2 / e^2 with A_f half the cross product of the diagonals of
-    face f = j + i n (vertices v = j + i (n+1))."""
-    P = np.asarray(fwd).reshape(n + 1, n + 1, 2)  # [i, j]
-    p00, p10, p01, p11 = P[:-1, :-1], P[1:, :-1], P[:-1, 1:], P[1:, 1:]
-    a = p11 - p00
-    b = p01 - p10
-    area = 0.5 * (a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0])  # [i, j]
-    e2 = 1.0 / (n * n)
-    r = area.ravel() - e2 * np.asarray(density)
-    return float((r * r).sum() / e2)
 
 
 def split_solver(ot):

@@ -16,6 +16,8 @@ FP64 reference's accuracy.
 import numpy as np
 import pytest
 
+from conftest import mesh_residual
+
 pytestmark = pytest.mark.gpu
 
 
@@ -35,16 +37,6 @@ def solver(ot, poisson):
     s = ot.GridBasedTransportSolver(ctx)
     s.set_verbose_level(0)
     return s
-
-
-def mesh_residual(fwd, density, n):
-    P = np.asarray(fwd).reshape(n + 1, n + 1, 2)
-    a = P[1:, 1:] - P[:-1, :-1]
-    b = P[:-1, 1:] - P[1:, :-1]
-    area = 0.5 * (a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0])
-    e2 = 1.0 / (n * n)
-    r = area.ravel() - e2 * np.asarray(density)
-    return float((r * r).sum() / e2)
 
 
 @pytest.mark.parametrize("n", [128, 256, 512, 1024])
