@@ -554,10 +554,65 @@ __global__ __launch_bounds__(ST) void k_sweep_update_t(Inst* insts, const int* s
       }
       return d;
     };
+    // cell row c between vertex rows with gradients (pp, pd) and (qp, qd); pr, dr: grid
+    // row c of psi and of d
+    auto cell = [&](const VG& pp, const VG& pd, const VG& qp, const VG& qd, const Row& pr, const Row& dr, int c) {
+      const size_t f = (size_t)c * n + j;
+      double a, b, r;
+      if constexpr (SPLIT) {
+        line_ab_fma(shift_diag(diag(pp, qp), es), diag(pd, qd), a, b);
+        psin[f] = fma(alpha, dr.c, pr.c);
+        r = fma(h2, fma(a, alpha * alpha, b * alpha), R.point(c, 0));
+      } else {
+        line_ab(diag(pp, qp), diag(pd, qd), es, a, b);
+        psin[f] = pr.c + alpha * dr.c;
+        // (n/2)^2 / 2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
+        r = h2 * (a * (alpha * alpha) + b * alpha) + R.point(c, 0);
+      }
+      if constexpr (SPLIT) {
+        reinterpret_cast<float*>(I.d[it & 1])[f] = (float)dr.c;
+        const float rf = (float)r;
+        reinterpret_cast<float*>(I.r[(it + 1) % 3])[f] = rf;
+        r = (double)rf;
+      } else {
+        I.d[it & 1][f] = dr.c;
+        I.r[(it + 1) % 3][f] = r;
+      }
+      mx = fmax(mx, r);
+    };
     VG gp, gd;
     Row pc, dc;  // grid row row-1 of psi and of d, carried from the previous step
-#pragma unroll 4
-    for (int row = sc.i0; row <= last; ++row) {
+    int row = sc.i0;
+    // split form: two vertex rows per step, their gradients and cells independent chains
+    // issued after one wait (grid rows row-1 .. row+1 staged); 128 registers, four blocks
+    // per SM (one row per step with the loop unrolled: 142, three blocks; 102 -> 85 us at
+    // 8 x 1024^2). The FP64 form keeps one row per step (its two-row form measured slower).
+#pragma unroll 1
+    for (; SPLIT && row + 1 <= last; row += 2) {
+      cp_async_wait<RD - 4>();
+      __syncwarp();
+      if (row == sc.i0) {
+        pc = R.row_of(row - 1, 0);
+        dc = drow(row - 1);
+      }
+      const Row pb = R.row_of(row, 0), db = drow(row);
+      const Row pn = R.row_of(row + 1, 0), dn = drow(row + 1);
+      const VG mp = vgrad(pc, pb), md = vgrad(dc, db);
+      const VG np = vgrad(pb, pn), nd = vgrad(db, dn);
+      if (j < n) {
+        if (row > sc.i0) cell(gp, gd, mp, md, pc, dc, row - 1);
+        cell(mp, md, np, nd, pb, db, row);
+      }
+      gp = np;
+      gd = nd;
+      pc = pn;
+      dc = dn;
+      __syncwarp();
+      R.issue(row - 2 + RD);
+      R.issue(row - 1 + RD);
+    }
+    // one row per step: every row of the FP64 form, the odd last row of the split form
+    auto one_row = [&](int row) {
       cp_async_wait<RD - 3>();
       __syncwarp();
       if (row == sc.i0) {
@@ -565,39 +620,20 @@ __global__ __launch_bounds__(ST) void k_sweep_update_t(Inst* insts, const int* s
         dc = drow(row - 1);
       }
       const Row pb = R.row_of(row, 0), db = drow(row);
-      VG np = vgrad(pc, pb);
-      VG nd = vgrad(dc, db);
-      if (row > sc.i0 && j < n) {
-        const int c = row - 1;
-        const size_t f = (size_t)c * n + j;
-        double a, b, r;
-        if constexpr (SPLIT) {
-          line_ab_fma(shift_diag(diag(gp, np), es), diag(gd, nd), a, b);
-          psin[f] = fma(alpha, dc.c, pc.c);
-          r = fma(h2, fma(a, alpha * alpha, b * alpha), R.point(c, 0));
-        } else {
-          line_ab(diag(gp, np), diag(gd, nd), es, a, b);
-          psin[f] = pc.c + alpha * dc.c;
-          // (n/2)^2 / 2 (a alpha^2 + b alpha) = a_ref alpha^2 + b_ref alpha, exactly for power-of-two n
-          r = h2 * (a * (alpha * alpha) + b * alpha) + R.point(c, 0);
-        }
-        if constexpr (SPLIT) {
-          reinterpret_cast<float*>(I.d[it & 1])[f] = (float)dc.c;
-          const float rf = (float)r;
-          reinterpret_cast<float*>(I.r[(it + 1) % 3])[f] = rf;
-          r = (double)rf;
-        } else {
-          I.d[it & 1][f] = dc.c;
-          I.r[(it + 1) % 3][f] = r;
-        }
-        mx = fmax(mx, r);
-      }
+      const VG np = vgrad(pc, pb), nd = vgrad(dc, db);
+      if (row > sc.i0 && j < n) cell(gp, gd, np, nd, pc, dc, row - 1);
       gp = np;
       gd = nd;
       pc = pb;
       dc = db;
       __syncwarp();
       R.issue(row - 2 + RD);
+    };
+    if constexpr (SPLIT) {
+      if (row <= last) one_row(row);
+    } else {
+#pragma unroll 4
+      for (; row <= last; ++row) one_row(row);
     }
     cp_async_wait<0>();
   }
