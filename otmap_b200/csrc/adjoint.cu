@@ -31,6 +31,18 @@ namespace otm {
 
 __device__ __forceinline__ int clampv(int v, int n) { return v < 0 ? 0 : (v >= n ? n - 1 : v); }
 
+// Device state of one restart cycle of the Krylov solve. The cycle's Arnoldi steps run on
+// the device (a CUDA graph with a WHILE node, or the same kernels launched one step at a
+// time): every step kernel reads the step index j here instead of taking it as a launch
+// argument, and the Givens kernel advances it and decides whether the cycle goes on.
+struct AdjCtl {
+  int j;       // the step being taken: basis vectors 0..j are orthonormal
+  int go;      // the cycle takes another step
+  int m;       // restart length
+  int budget;  // steps allowed in this cycle (the call's cap on Poisson solves)
+  double bnorm, tol;
+};
+
 // Displacement g of vertex (i, j) from the forward mesh.
 __device__ __forceinline__ double2 disp(const double* fwd, int n, int i, int j) {
   const size_t v = (size_t)j + (size_t)i * (n + 1);
@@ -87,7 +99,9 @@ __global__ void k_adj_vertex(int n, const double* fwd, const double* lambda, dou
 // with gx coefficient (2a-1) n/2 and gy coefficient (2b-1) n/2
 // (otsolver_2dgrid.cpp:379-422 with clamped indices). Cell (i, j) collects every
 // (vertex, a, b) whose clamped position is (i, j); out = scale * G^T h (+ add).
-__global__ void k_adj_cells(int n, const double* h, double scale, const double* add, double* out) {
+__global__ void k_adj_cells(int n, const double* h, double scale, const double* add, double* out,
+                            const AdjCtl* ctl, long ld) {
+  if (ctl) out += (size_t)(ctl->j + 1) * ld;  // the new basis vector of the step
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= (long)n * n) return;
   const int i = (int)(f / n), j = (int)(f % n);
@@ -116,9 +130,15 @@ __global__ void k_adj_cells(int n, const double* h, double scale, const double* 
 // stored contiguously with stride `ld`), and partial[b * (m+1) + m] = w . w. The dot
 // products are formed DOT_CHUNK at a time in one pass over the cells (w read once per
 // chunk), each a per-thread FMA chain over the grid-stride cells, then reduced together.
+// With ctl: w is basis vector j + 1 and m = j + 1 (or 0: w . w alone, for norm_only).
 constexpr int DOT_CHUNK = 8;
-__global__ void k_adj_multidot(long N, const double* w, const double* V, long ld, int m, double* partial) {
+__global__ void k_adj_multidot(long N, const double* w, const double* V, long ld, int m, double* partial,
+                               const AdjCtl* ctl, int norm_only) {
   __shared__ double red[32 * DOT_CHUNK];
+  if (ctl) {
+    w = V + (size_t)(ctl->j + 1) * ld;
+    m = norm_only ? 0 : ctl->j + 1;
+  }
   const int P = m + 1;
   for (int i0 = 0; i0 < P; i0 += DOT_CHUNK) {
     double s[DOT_CHUNK];
@@ -149,7 +169,9 @@ __device__ __forceinline__ double sum_partials(const double* partial, int nblock
 
 // Gram-Schmidt pass over basis vectors 0..j: c_i = <w, v_i> (for the combine) and the
 // Hessenberg column entry H_ij accumulated over the two passes (pass 0 sets it).
-__global__ void k_adj_orth_reduce(const double* partial, int nblocks, int j, int pass, double* hcol, double* c) {
+__global__ void k_adj_orth_reduce(const double* partial, int nblocks, int j, int pass, double* hcol, double* c,
+                                  const AdjCtl* ctl) {
+  if (ctl) j = ctl->j;
   const int i = threadIdx.x;
   if (i > j) return;
   const double d = sum_partials(partial, nblocks, j + 2, i);
@@ -158,20 +180,28 @@ __global__ void k_adj_orth_reduce(const double* partial, int nblocks, int j, int
 }
 
 // |w| after the passes: H_{j+1,j} and the factor that normalises w (0 when |w| = 0).
-__global__ void k_adj_norm_reduce(const double* partial, int nblocks, int j, double* hcol, double* inv) {
+__global__ void k_adj_norm_reduce(const double* partial, int nblocks, int j, double* hcol, double* inv,
+                                  const AdjCtl* ctl) {
   if (threadIdx.x != 0) return;
+  if (ctl) j = ctl->j;
   const double hn = sqrt(sum_partials(partial, nblocks, 1, 0));
   hcol[j + 1] = hn;
   *inv = hn > 0 ? 1.0 / hn : 1.0;
 }
 
-__global__ void k_adj_scale_by(long N, double* v, const double* a) {
+__global__ void k_adj_scale_by(long N, double* v, const double* a, const AdjCtl* ctl, long ld) {
+  if (ctl) v += (size_t)(ctl->j + 1) * ld;
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f < N) v[f] *= *a;
 }
 
-// w = a * w - sum_i c_i V_i (i < m); c in device memory
-__global__ void k_adj_combine(long N, double* w, double a, const double* V, long ld, int m, const double* c) {
+// w = a * w - sum_i c_i V_i (i < m); c in device memory; with ctl, w = V_{j+1} and m = j + 1
+__global__ void k_adj_combine(long N, double* w, double a, const double* V, long ld, int m, const double* c,
+                              const AdjCtl* ctl) {
+  if (ctl) {
+    w = const_cast<double*>(V) + (size_t)(ctl->j + 1) * ld;
+    m = ctl->j + 1;
+  }
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= N) return;
   double x = a * w[f];
@@ -179,8 +209,69 @@ __global__ void k_adj_combine(long N, double* w, double a, const double* V, long
   w[f] = x;
 }
 
-// out = sum_i c_i V_i
-__global__ void k_adj_span(long N, double* out, const double* V, long ld, int m, const double* c) {
+// The Poisson record of the step reads basis vector j.
+__global__ void k_adj_set_src(Inst* rec, double* V, long ld, const AdjCtl* ctl) {
+  if (threadIdx.x == 0) rec->r[0] = V + (size_t)ctl->j * ld;
+}
+
+// Start of a restart cycle: residual norm rnorm in g_0.
+__global__ void k_adj_cycle_init(AdjCtl* ctl, double* gv, int m, double rnorm, double bnorm, double tol, int budget) {
+  if (threadIdx.x != 0) return;
+  ctl->j = 0;
+  ctl->go = budget > 0 ? 1 : 0;
+  ctl->m = m;
+  ctl->budget = budget;
+  ctl->bnorm = bnorm;
+  ctl->tol = tol;
+  gv[0] = rnorm;
+  for (int i = 1; i <= m; ++i) gv[i] = 0.0;
+}
+
+// End of Arnoldi step j (one thread): the new Hessenberg column, the previous Givens
+// rotations applied to it, the rotation that zeroes H_{j+1,j}, the updated residual
+// estimate |g_{j+1}|, and the loop test: go on while it is above tol * |b|, the new basis
+// vector is non-zero, the cycle has room and the call's budget is not spent. H is
+// (m+1) x m, row-major.
+__global__ void k_adj_givens(AdjCtl* ctl, const double* hcol, double* H, double* cs, double* sn, double* gv,
+                             cudaGraphConditionalHandle handle, int in_graph) {
+  if (threadIdx.x != 0) return;
+  const int j = ctl->j, m = ctl->m;
+  auto Hs = [&](int i, int c) -> double& { return H[(size_t)i * m + c]; };
+  for (int i = 0; i <= j + 1; ++i) Hs(i, j) = hcol[i];
+  const double hn = hcol[j + 1];
+  for (int i = 0; i < j; ++i) {
+    const double t = cs[i] * Hs(i, j) + sn[i] * Hs(i + 1, j);
+    Hs(i + 1, j) = -sn[i] * Hs(i, j) + cs[i] * Hs(i + 1, j);
+    Hs(i, j) = t;
+  }
+  const double den = hypot(Hs(j, j), Hs(j + 1, j));
+  cs[j] = den > 0 ? Hs(j, j) / den : 1.0;
+  sn[j] = den > 0 ? Hs(j + 1, j) / den : 0.0;
+  Hs(j, j) = den;
+  Hs(j + 1, j) = 0.0;
+  gv[j + 1] = -sn[j] * gv[j];
+  gv[j] = cs[j] * gv[j];
+  const int k = j + 1;
+  const int go = (fabs(gv[k]) / ctl->bnorm > ctl->tol) && hn != 0 && k < m && k < ctl->budget;
+  ctl->j = k;
+  ctl->go = go;
+  if (in_graph) cudaGraphSetConditional(handle, go ? 1u : 0u);
+}
+
+// H y = g for the k = j steps of the cycle (back substitution, one thread): y into c.
+__global__ void k_adj_trisolve(const AdjCtl* ctl, const double* H, const double* gv, double* y) {
+  if (threadIdx.x != 0) return;
+  const int k = ctl->j, m = ctl->m;
+  for (int i = k - 1; i >= 0; --i) {
+    double t = gv[i];
+    for (int l = i + 1; l < k; ++l) t -= H[(size_t)i * m + l] * y[l];
+    y[i] = t / H[(size_t)i * m + i];
+  }
+}
+
+// out = sum_i c_i V_i (i < m; with ctl, the cycle's step count)
+__global__ void k_adj_span(long N, double* out, const double* V, long ld, int m, const double* c, const AdjCtl* ctl) {
+  if (ctl) m = ctl->j;
   const long f = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= N) return;
   double x = 0.0;
@@ -250,8 +341,17 @@ struct AdjointWs : otm_context::Erased {
   size_t N = 0, V = 0, ld = 0;
   DevBuf buf, recs, lists;
   double *b, *lam, *z, *h, *t1, *t2, *Vb, *c, *part, *sums, *hcol, *inv;
+  double *fwdc, *H, *cs, *sn, *gv;  // the forward mesh of the call; the cycle's Hessenberg state
+  AdjCtl* ctl = nullptr;
   int G = 0, rows = 0, cols = 0, reg = 0, fft = 0;
-  // record k: src = basis vector k (k < m+1); record m+1: src = b; record m+2: src = h; dst = z
+  // the Arnoldi step as a graph with a WHILE node (built on first use) and its kernel count
+  cudaGraphExec_t step_graph = nullptr;
+  long step_kernels = 0;
+  ~AdjointWs() override {
+    if (step_graph) cudaGraphExecDestroy(step_graph);
+  }
+  // record k: src = basis vector k (k < m+1); record m+1: src = b; record m+2: src = h;
+  // record m+3: src = the basis vector of the current step (set on the device); dst = z
   Inst* rec(int k) { return recs.as<Inst>() + k; }
 };
 
@@ -265,7 +365,8 @@ static AdjointWs* adjoint_ws(otm_context* ctx, int n, int m) {
   W->V = (size_t)(n + 1) * (n + 1);
   W->ld = (W->N + 31) / 32 * 32;
   const int nred = 256;
-  const size_t words = W->ld * 6 + 2 * W->V + (size_t)(m + 1) * W->ld + (m + 2) + (size_t)nred * (m + 2) + (m + 3) + 64;
+  const size_t words = W->ld * 6 + 2 * W->V + (size_t)(m + 1) * W->ld + (m + 2) + (size_t)nred * (m + 2) + (m + 3) + 64 +
+                       16 + 2 * W->V + (size_t)(m + 1) * m + 3 * (size_t)m + 1;
   W->buf.reserve(sizeof(double) * words);
   double* p = W->buf.as<double>();
   W->b = p; p += W->ld;
@@ -279,7 +380,13 @@ static AdjointWs* adjoint_ws(otm_context* ctx, int n, int m) {
   W->sums = p; p += 2;
   W->part = p; p += (size_t)nred * (m + 2);
   W->hcol = p; p += m + 2;  // the current Hessenberg column
-  W->inv = p;
+  W->inv = p; p += 8;
+  W->ctl = reinterpret_cast<AdjCtl*>(p); p += 8;
+  W->fwdc = p; p += 2 * W->V;
+  W->H = p; p += (size_t)(m + 1) * m;
+  W->cs = p; p += m;
+  W->sn = p; p += m;
+  W->gv = p;
   SizeTables* T = ctx->tables.at(n).get();
   Inst base;
   std::memset(&base, 0, sizeof(base));
@@ -310,10 +417,11 @@ static AdjointWs* adjoint_ws(otm_context* ctx, int n, int m) {
     int t = (n + 63) / 64;
     base.ngemm = W->G = items = t * t;
   }
-  std::vector<Inst> recs(m + 3, base);
+  std::vector<Inst> recs(m + 4, base);
   for (int k = 0; k <= m; ++k) recs[k].r[0] = W->Vb + (size_t)k * W->ld;
   recs[m + 1].r[0] = W->b;
   recs[m + 2].r[0] = W->h;
+  recs[m + 3].r[0] = W->Vb;
   for (auto& r : recs) r.dhat = W->z;
   W->recs.reserve(sizeof(Inst) * recs.size());
   W->lists.reserve(sizeof(int) * items);
@@ -337,6 +445,73 @@ static void poisson_rec(otm_context* ctx, AdjointWs* W, int k) {
   } else {
     dense_poisson(ctx, d, L, W->G);
   }
+}
+
+// One Arnoldi step j of the cycle (j read on the device): z = M^+ v_j, w = J^T z into
+// v_{j+1}, two classical Gram-Schmidt passes and the normalisation (reductions in block
+// order on the device), then the Givens kernel, which advances j and sets the loop test.
+static void arnoldi_step(otm_context* ctx, AdjointWs* W, int n, cudaGraphConditionalHandle handle, int in_graph) {
+  const long N = (long)W->N, ld = (long)W->ld;
+  const int RB = 256, nred = 256;
+  const unsigned gN = (unsigned)((W->N + RB - 1) / RB), gV = (unsigned)((W->V + RB - 1) / RB);
+  const AdjCtl* ctl = W->ctl;
+  launch(ctx, "adj_set_src", k_adj_set_src, 1, 32, W->rec(W->m + 3), W->Vb, ld, ctl);
+  poisson_rec(ctx, W, W->m + 3);
+  launch(ctx, "adj_vertex", k_adj_vertex, gV, RB, n, (const double*)W->fwdc, (const double*)W->z, W->h);
+  launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)W->h, 1.0, (const double*)nullptr, W->Vb, ctl, ld);
+  const unsigned rt = (unsigned)((W->m + 1 + 31) / 32 * 32);
+  for (int pass = 0; pass < 2; ++pass) {
+    launch(ctx, "adj_dot", k_adj_multidot, nred, RB, N, (const double*)nullptr, (const double*)W->Vb, ld, 0, W->part,
+           ctl, 0);
+    launch(ctx, "adj_reduce", k_adj_orth_reduce, 1, rt, (const double*)W->part, nred, 0, pass, W->hcol, W->c, ctl);
+    launch(ctx, "adj_combine", k_adj_combine, gN, RB, N, W->Vb, 1.0, (const double*)W->Vb, ld, 0, (const double*)W->c,
+           ctl);
+  }
+  launch(ctx, "adj_dot", k_adj_multidot, nred, RB, N, (const double*)nullptr, (const double*)W->Vb, ld, 0, W->part, ctl,
+         1);
+  launch(ctx, "adj_reduce", k_adj_norm_reduce, 1, 32, (const double*)W->part, nred, 0, W->hcol, W->inv, ctl);
+  launch(ctx, "adj_scale", k_adj_scale_by, gN, RB, N, W->Vb, (const double*)W->inv, ctl, ld);
+  launch(ctx, "adj_givens", k_adj_givens, 1, 32, W->ctl, (const double*)W->hcol, W->H, W->cs, W->sn, W->gv, handle,
+         in_graph);
+}
+
+// The cycle's steps as a graph: a WHILE node whose body is one Arnoldi step, its condition
+// set by the Givens kernel (at most m bodies per launch).
+static void build_step_graph(otm_context* ctx, AdjointWs* W, int n) {
+  cudaStream_t st = ctx->stream;
+  dct_reg_attrs(ctx->device);
+  poisson_fft_attrs(ctx->device);
+  cudaGraph_t g = nullptr;
+  OTM_CUDA(cudaGraphCreate(&g, 0));
+  try {
+    cudaGraphConditionalHandle handle;
+    OTM_CUDA(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    cudaGraphNode_t node;
+    OTM_CUDA(cudaGraphAddNode(&node, g, nullptr, 0, &params));
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    const long before = ctx->launches;
+    OTM_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    try {
+      arnoldi_step(ctx, W, n, handle, 1);
+    } catch (...) {
+      cudaGraph_t dummy;
+      cudaStreamEndCapture(st, &dummy);
+      throw;
+    }
+    OTM_CUDA(cudaStreamEndCapture(st, &body));
+    W->step_kernels = ctx->launches - before;
+    ctx->launches = before;  // captured, not executed
+    OTM_CUDA(cudaGraphInstantiate(&W->step_graph, g, 0));
+  } catch (...) {
+    cudaGraphDestroy(g);
+    throw;
+  }
+  cudaGraphDestroy(g);
 }
 
 }  // namespace otm
@@ -388,10 +563,11 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     double* d_c = W->c;
     double* d_part = W->part;
     // b = G^T q
-    launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, d_q, 1.0, (const double*)nullptr, d_b);
+    launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, d_q, 1.0, (const double*)nullptr, d_b, (const AdjCtl*)nullptr, 0L);
     std::vector<double> hp;
     auto multidot = [&](const double* w, int k, std::vector<double>& out) {
-      launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, w, (const double*)d_V, (long)ld, k, d_part);
+      launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, w, (const double*)d_V, (long)ld, k, d_part,
+             (const AdjCtl*)nullptr, 0);
       hp.resize((size_t)nred * (k + 1));
       OTM_CUDA(cudaMemcpyAsync(hp.data(), d_part, sizeof(double) * hp.size(), cudaMemcpyDeviceToHost, st));
       OTM_CUDA(cudaStreamSynchronize(st));
@@ -401,7 +577,8 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     };
     auto apply_jt = [&](const double* x, double* out) {
       launch(ctx, "adj_vertex", k_adj_vertex, gV, RB, n, d_fwd, x, d_h);
-      launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_h, 1.0, (const double*)nullptr, out);
+      launch(ctx, "adj_cells", k_adj_cells, gN, RB, n, (const double*)d_h, 1.0, (const double*)nullptr, out,
+             (const AdjCtl*)nullptr, 0L);
     };
     int solves = 0;
     double rel = -1.0;
@@ -413,14 +590,17 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     } else {
       OTM_CUDA(cudaMemsetAsync(d_lam, 0, sizeof(double) * N, st));
       // Restarted GMRES(m) on J^T lambda = b, right-preconditioned: J^T M^+ y = b, lambda = M^+ y.
-      // Classical Gram-Schmidt applied twice; Givens rotations and the small triangular
-      // solve on the host.
+      // A cycle's Arnoldi steps run on the device (classical Gram-Schmidt applied twice,
+      // Givens rotations and the loop test in one-thread kernels) as one graph launch with a
+      // WHILE node -- or, in the host-driven loop mode and under the profiler, the same
+      // kernels one step at a time; the host reads the cycle's step count once per restart,
+      // forms the true residual and decides whether to restart.
       std::vector<double> dots;
       OTM_CUDA(cudaMemcpyAsync(d_V, d_b, sizeof(double) * N, cudaMemcpyDeviceToDevice, st));
+      OTM_CUDA(cudaMemcpyAsync(W->fwdc, d_fwd, sizeof(double) * 2 * V, cudaMemcpyDeviceToDevice, st));
       multidot(d_V, 0, dots);
       const double bnorm = std::sqrt(dots[0]);
-      std::vector<double> H((size_t)(m + 1) * m, 0.0), cs(m), sn(m), gv(m + 1), y(m), hcol_h(m + 2);
-      auto Hs = [&](int i, int j) -> double& { return H[(size_t)i * m + j]; };
+      const bool graph = ctx->loop_mode == OTM_LOOP_GRAPH && !ctx->prof.on;
       rel = bnorm > 0 ? 1.0 : 0.0;
       bool first = true;
       while (bnorm > 0) {
@@ -438,59 +618,32 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
         rel = rnorm / bnorm;
         if (!(rel > o.tol) || solves >= o.max_iter) break;
         launch(ctx, "adj_scale", k_adj_scale, gN, RB, (long)N, v0, 1.0 / rnorm);
-        std::fill(gv.begin(), gv.end(), 0.0);
-        gv[0] = rnorm;
-        int k = 0;
-        for (int j = 0; j < m && solves < o.max_iter; ++j) {
-          double* w = d_V + (size_t)(j + 1) * ld;
-          poisson_rec(ctx, W, j);  // z = M^+ v_j
-          ++solves;
-          apply_jt(d_z, w);
-          // two Gram-Schmidt passes and the normalisation with the reductions on the
-          // device (partials summed in block order); one read-back of the column per step
-          const unsigned rt = (unsigned)((j + 1 + 31) / 32 * 32);
-          for (int pass = 0; pass < 2; ++pass) {
-            launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, (const double*)w, (const double*)d_V, (long)ld,
-                   j + 1, d_part);
-            launch(ctx, "adj_reduce", k_adj_orth_reduce, 1, rt, (const double*)d_part, nred, j, pass, W->hcol, d_c);
-            launch(ctx, "adj_combine", k_adj_combine, gN, RB, (long)N, w, 1.0, (const double*)d_V, (long)ld, j + 1,
-                   (const double*)d_c);
-          }
-          launch(ctx, "adj_dot", k_adj_multidot, nred, RB, (long)N, (const double*)w, (const double*)d_V, (long)ld, 0,
-                 d_part);
-          launch(ctx, "adj_reduce", k_adj_norm_reduce, 1, 32, (const double*)d_part, nred, j, W->hcol, W->inv);
-          launch(ctx, "adj_scale", k_adj_scale_by, gN, RB, (long)N, w, (const double*)W->inv);
-          OTM_CUDA(cudaMemcpyAsync(hcol_h.data(), W->hcol, sizeof(double) * (j + 2), cudaMemcpyDeviceToHost, st));
-          OTM_CUDA(cudaStreamSynchronize(st));
-          for (int i = 0; i <= j + 1; ++i) Hs(i, j) = hcol_h[i];
-          const double hn = hcol_h[j + 1];
-          for (int i = 0; i < j; ++i) {  // previous rotations
-            const double t = cs[i] * Hs(i, j) + sn[i] * Hs(i + 1, j);
-            Hs(i + 1, j) = -sn[i] * Hs(i, j) + cs[i] * Hs(i + 1, j);
-            Hs(i, j) = t;
-          }
-          const double den = std::hypot(Hs(j, j), Hs(j + 1, j));
-          cs[j] = den > 0 ? Hs(j, j) / den : 1.0;
-          sn[j] = den > 0 ? Hs(j + 1, j) / den : 0.0;
-          Hs(j, j) = den;
-          Hs(j + 1, j) = 0.0;
-          gv[j + 1] = -sn[j] * gv[j];
-          gv[j] = cs[j] * gv[j];
-          k = j + 1;
-          if (!(std::fabs(gv[j + 1]) / bnorm > o.tol) || hn == 0) break;
+        launch(ctx, "adj_cycle", k_adj_cycle_init, 1, 32, W->ctl, W->gv, m, rnorm, bnorm, o.tol, o.max_iter - solves);
+        if (graph) {
+          if (!W->step_graph) build_step_graph(ctx, W, n);
+          OTM_CUDA(cudaGraphLaunch(W->step_graph, st));
+        } else {
+          AdjCtl hc;
+          do {
+            arnoldi_step(ctx, W, n, (cudaGraphConditionalHandle)0, 0);
+            OTM_CUDA(cudaMemcpyAsync(&hc, W->ctl, sizeof(hc), cudaMemcpyDeviceToHost, st));
+            OTM_CUDA(cudaStreamSynchronize(st));
+            ctx->prof.flush();
+          } while (hc.go);
         }
-        for (int i = k - 1; i >= 0; --i) {  // H y = g
-          double t = gv[i];
-          for (int l = i + 1; l < k; ++l) t -= Hs(i, l) * y[l];
-          y[i] = t / Hs(i, i);
-        }
-        // lambda += M^+ (V y)
-        OTM_CUDA(cudaMemcpyAsync(d_c, y.data(), sizeof(double) * k, cudaMemcpyHostToDevice, st));
-        launch(ctx, "adj_span", k_adj_span, gN, RB, (long)N, d_h, (const double*)d_V, (long)ld, k,
-               (const double*)d_c);
+        // lambda += M^+ (V y), H y = g solved on the device
+        launch(ctx, "adj_trisolve", k_adj_trisolve, 1, 32, (const AdjCtl*)W->ctl, (const double*)W->H,
+               (const double*)W->gv, d_c);
+        launch(ctx, "adj_span", k_adj_span, gN, RB, (long)N, d_h, (const double*)d_V, (long)ld, 0, (const double*)d_c,
+               (const AdjCtl*)W->ctl);
         poisson_rec(ctx, W, W->m + 2);  // z = M^+ h
-        ++solves;
         launch(ctx, "adj_add", k_adj_add, gN, RB, (long)N, (const double*)d_z, d_lam);
+        AdjCtl hc;
+        OTM_CUDA(cudaMemcpyAsync(&hc, W->ctl, sizeof(hc), cudaMemcpyDeviceToHost, st));
+        OTM_CUDA(cudaStreamSynchronize(st));
+        if (graph) ctx->launches += W->step_kernels * (long)hc.j;
+        solves += hc.j + 1;
+        if (hc.j == 0) break;  // no step was possible: nothing changes by restarting
       }
     }
     // chain through the density normalisation, reduced and applied on the device
@@ -501,7 +654,7 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     OTM_CUDA(cudaGetLastError());
     if (!odev) copy_out(ctx, grad_density, out, sizeof(double) * N);
     // a bounded wait inside a transform that gave up flags its record
-    std::vector<Inst> recs_h((size_t)W->m + 3);
+    std::vector<Inst> recs_h((size_t)W->m + 4);
     OTM_CUDA(cudaMemcpyAsync(recs_h.data(), W->rec(0), sizeof(Inst) * recs_h.size(), cudaMemcpyDeviceToHost, st));
     OTM_CUDA(cudaStreamSynchronize(st));
     ctx->prof.flush();

@@ -145,3 +145,36 @@ def test_logit_gradient_512_softmax_blur():
     print("logit FD errors / |grad|:", sorted(abs_errs))
     assert np.median(errs) <= 5e-3, errs
     assert max(abs_errs) <= 1e-3, abs_errs
+
+
+@pytest.mark.parametrize("n,restart", [(64, 40), (128, 8)])
+def test_krylov_graph_and_host_loops_agree(n, restart):
+    """The Krylov adjoint's Arnoldi cycles run as one graph launch per restart (WHILE node,
+    Givens rotations and the loop test on the device) or, in the host-driven loop mode,
+    as the same kernels one step at a time: the gradients and step counts are identical.
+    restart 8 at 128^2 takes several restarts."""
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    dens = W.to_cells(W.gaussian_mixture(n, 300 + n))
+    q = np.random.default_rng(n).standard_normal(((n + 1) ** 2, 2))
+    out = []
+    for loop in (N.LOOP_GRAPH, N.LOOP_HOST):
+        ctx = N.Context(0)
+        ctx.set_loop(loop)
+        fwd, _ = _solve(N, ctx, n, dens)
+        g = np.empty(n * n)
+        opt = N.AdjointOptionsC()
+        N.lib().otm_default_adjoint_options(C.byref(opt))
+        opt.mode = N.ADJOINT_KRYLOV
+        opt.tol = 1e-12
+        opt.restart = restart
+        st = N.AdjointStatsC()
+        N.check(N.lib().otm_adjoint(ctx.handle, n, N.ptr(dens), N.ptr(fwd), N.ptr(q), C.byref(opt), N.ptr(g),
+                                    C.byref(st)))
+        out.append((g, st.iterations, st.relative_residual))
+        ctx.close()
+    (g0, it0, r0), (g1, it1, r1) = out
+    assert it0 == it1 and r0 == r1
+    assert np.array_equal(g0, g1)
+    assert r0 <= 1e-12
