@@ -130,6 +130,8 @@ extern "C" int otm_create(int device, otm_context** out) {
 
 extern "C" int otm_destroy(otm_context* ctx) {
   if (!ctx) return OTM_OK;
+  for (otm_context* h : ctx->helpers) otm_destroy(h);
+  ctx->helpers.clear();
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->side) cudaStreamSynchronize(ctx->side);

@@ -190,6 +190,9 @@ struct otm_context {
     virtual ~Erased() = default;
   };
   std::map<int, std::unique_ptr<Erased>> adjoint;
+  // contexts of the same device on which otm_barycenter_loss runs the adjoints of its maps
+  // concurrently, one host thread each (created on first use, destroyed by otm_destroy)
+  std::vector<otm_context*> helpers;
 };
 
 struct otm_map {

@@ -5,11 +5,16 @@
 
 #include <algorithm>
 #include <cstring>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "context.h"
 
 namespace otm {
+
+void dct_reg_attrs(int device);      // dct_reg.cu
+void poisson_fft_attrs(int device);  // poisson.cu
 
 // out = sum_k w_k mesh_k, left to right (bilerp / lerp of apps/barycenters.cpp:127-139).
 __global__ void k_blend(long V2, int count, const double* const* meshes, const double* w, double* out) {
@@ -517,11 +522,50 @@ extern "C" int otm_barycenter_loss(otm_context* ctx, int n, int count, const dou
         double* dI = inv[k];  // the inverse mesh is no longer needed: its buffer holds dL/dI
         launch(ctx, "scale", k_scale, gv2, 256, (long)V2, weights[k], (const double*)dB, dI);
         inverse_grid_backward(ctx, n, fwd[k], hit0[k], dI, dF[k]);
-        otm_adjoint_stats ast;
-        rc = otm_adjoint(ctx, n, rho[k], fwd[k], dF[k], &ao, grad[k], &ast);
-        if (rc != OTM_OK) return rc;
-        solves[k] = ast.iterations;
-        ares[k] = ast.relative_residual;
+      }
+      // the maps' adjoints are independent: each runs on its own context (this one for map
+      // 0, cached helpers of the same device for the others) from its own host thread, so
+      // their kernels -- a 512^2 Poisson solve fills a fraction of the GPU -- overlap
+      OTM_CUDA(cudaStreamSynchronize(st));
+      dct_reg_attrs(ctx->device);  // device-wide set-up done once, before the threads
+      poisson_fft_attrs(ctx->device);
+      while ((int)ctx->helpers.size() < count - 1) {
+        otm_context* h = nullptr;
+        const int hrc = otm_create(ctx->device, &h);
+        if (hrc != OTM_OK) return hrc;
+        ctx->helpers.push_back(h);
+      }
+      std::vector<int> rcs(count, OTM_OK);
+      std::vector<otm_adjoint_stats> asts(count);
+      std::vector<std::string> errs(count);
+      std::vector<long> launches0(count, 0);
+      auto run = [&](int k) {
+        otm_context* c = k == 0 ? ctx : ctx->helpers[k - 1];
+        if (k > 0) {
+          c->poisson_mode = ctx->poisson_mode;
+          c->loop_mode = ctx->loop_mode;
+          c->wait_test = ctx->wait_test;
+          launches0[k] = c->launches;
+        }
+        rcs[k] = otm_adjoint(c, n, rho[k], fwd[k], dF[k], &ao, grad[k], &asts[k]);
+        if (rcs[k] != OTM_OK) errs[k] = otm_last_error();
+      };
+      {
+        std::vector<std::thread> threads;
+        for (int k = 1; k < count; ++k) threads.emplace_back(run, k);
+        run(0);
+        for (auto& t : threads) t.join();
+      }
+      make_current(ctx);
+      for (int k = 0; k < count; ++k)
+        if (rcs[k] != OTM_OK) {
+          set_error(errs[k]);
+          return rcs[k];
+        }
+      for (int k = 0; k < count; ++k) {
+        if (k > 0) ctx->launches += ctx->helpers[k - 1]->launches - launches0[k];
+        solves[k] = asts[k].iterations;
+        ares[k] = asts[k].relative_residual;
         // expected = ... + w_k mean(density_k): d/ddensity_k = w_k / N per cell
         launch(ctx, "add_const", k_add_const, (unsigned)((N + 255) / 256), 256, (long)N,
                weights[k] * dL_dexp / (double)N, grad[k]);
