@@ -330,7 +330,11 @@ int otm_adjoint(otm_context* ctx, int n, const double* density, const double* fw
  * rescale, each face's area in the raster (pixel ownership held fixed: it is piecewise
  * constant in the mesh), the blend, the bilinear inversion (the origin point held fixed in
  * the located face) and otm_adjoint of each map (aopt; NULL = defaults), plus the
- * expected-mean term. Buffers may be host or device memory. */
+ * expected-mean term. Buffers may be host or device memory. The maps' adjoints run
+ * concurrently: map 0 on ctx, the others on helper contexts of the same device that ctx
+ * creates on first use (count - 1 of them, each with its own stream, adjoint workspace and
+ * size tables) and keeps until otm_destroy, one host thread per map for the call's
+ * duration. */
 typedef struct {
   int iterations[8];
   int outcome[8];
