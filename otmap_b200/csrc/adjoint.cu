@@ -209,6 +209,16 @@ __global__ void k_adj_combine(long N, double* w, double a, const double* V, long
   w[f] = x;
 }
 
+// Every Poisson record of the workspace ready for a new call: a bounded wait that gave up in
+// an earlier call stopped its record and flagged it.
+__global__ void k_adj_reset_recs(Inst* recs, int count) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < count) {
+    recs[k].active = 1;
+    recs[k].fault = 0;
+  }
+}
+
 // The Poisson record of the step reads basis vector j.
 __global__ void k_adj_set_src(Inst* rec, double* V, long ld, const AdjCtl* ctl) {
   if (threadIdx.x == 0) rec->r[0] = V + (size_t)ctl->j * ld;
@@ -539,6 +549,7 @@ extern "C" int otm_adjoint(otm_context* ctx, int n, const double* density, const
     cudaStream_t st = ctx->stream;
     const int m = o.mode == OTM_ADJOINT_KRYLOV ? std::max(1, std::min(o.restart, 200)) : 1;
     AdjointWs* W = adjoint_ws(ctx, n, m);
+    launch(ctx, "adj_reset", k_adj_reset_recs, 1, 256, W->rec(0), W->m + 4);
     const size_t N = W->N, V = W->V, ld = W->ld;
     const int RB = 256, nred = 256;
     // inputs: used in place when they are device memory, else staged into the workspace

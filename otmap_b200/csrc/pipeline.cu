@@ -552,7 +552,12 @@ extern "C" int otm_barycenter_loss(otm_context* ctx, int n, int count, const dou
       };
       {
         std::vector<std::thread> threads;
-        for (int k = 1; k < count; ++k) threads.emplace_back(run, k);
+        try {
+          for (int k = 1; k < count; ++k) threads.emplace_back(run, k);
+        } catch (...) {  // a thread could not start: join those that did, then report
+          for (auto& t : threads) t.join();
+          throw;
+        }
         run(0);
         for (auto& t : threads) t.join();
       }

@@ -71,3 +71,56 @@ def test_tensor_transform_wait_runs_out_and_the_context_recovers():
     assert again.stats.iterations == good.stats.iterations
     assert np.array_equal(again.fwd_mesh(), good.fwd_mesh())
     ctx.close()
+
+
+@pytest.mark.parametrize("loop", ["graph", "host"])
+def test_adjoint_wait_runs_out_and_the_context_recovers(loop):
+    """The adjoint's Poisson solves use the same row transforms: under OTM_OPT_WAIT_TEST the
+    Krylov adjoint (its Arnoldi cycles as a graph launch, or step by step in the host loop)
+    returns OTM_ERR_TIMEOUT after a bounded number of steps; with the option off, the same
+    context's next adjoint equals that of a context that never saw the fault."""
+    import ctypes as C
+
+    from otmap_b200 import native as N
+    from otmap_b200 import workloads as W
+
+    n = 64
+    d = W.to_cells(W.gaussian_mixture(n, 7))
+    q = np.random.default_rng(3).standard_normal(((n + 1) ** 2, 2))
+
+    def adjoint(ctx, fwd):
+        g = np.empty(n * n)
+        opt = N.AdjointOptionsC()
+        N.lib().otm_default_adjoint_options(C.byref(opt))
+        opt.mode = N.ADJOINT_KRYLOV
+        opt.max_iter = 60
+        st = N.AdjointStatsC()
+        N.check(N.lib().otm_adjoint(ctx.handle, n, N.ptr(d), N.ptr(fwd), N.ptr(q), C.byref(opt), N.ptr(g),
+                                    C.byref(st)))
+        return g
+
+    def forward(ctx):
+        fwd = np.empty(((n + 1) ** 2, 2))
+        opt = N.default_options()
+        opt.threshold = 1e-13
+        opt.max_iter = 300
+        st = N.SolveStatsC()
+        N.check(N.lib().otm_solve(ctx.handle, n, N.ptr(d), C.byref(opt), N.ptr(fwd), None, C.byref(st)))
+        return fwd
+
+    clean = N.Context(0)
+    fwd = forward(clean)
+    good = adjoint(clean, fwd)
+    clean.close()
+
+    ctx = N.Context(0)
+    ctx.set_loop(N.LOOP_GRAPH if loop == "graph" else N.LOOP_HOST)
+    adjoint(ctx, fwd)  # workspace and step graph built before the fault
+    N.check(N.lib().otm_set_option(ctx.handle, N.OPT_WAIT_TEST, 1))
+    with pytest.raises(N.OtmError) as e:
+        adjoint(ctx, fwd)
+    assert e.value.code == N.ERR_TIMEOUT
+    N.check(N.lib().otm_set_option(ctx.handle, N.OPT_WAIT_TEST, 0))
+    again = adjoint(ctx, fwd)
+    assert np.array_equal(again, good)
+    ctx.close()
