@@ -195,7 +195,7 @@ def test_bad_arguments_raise(ot):
         ot.GridBasedTransportSolver().solve(np.ones(16))
 
 
-@pytest.mark.parametrize("n", [8, 16, 64, 128, 256, 512, 1024])
+@pytest.mark.parametrize("n", [8, 16, 64, 128, 256, 512, 1024, 2048])
 def test_fast_and_dense_transforms_agree(n, ot):
     """The fast cosine transform (power-of-two n) and the dense products give the same
     solve: same iterations, positions within 1e-9."""
@@ -214,6 +214,28 @@ def test_fast_and_dense_transforms_agree(n, ot):
     a, b = out[native.POISSON_DENSE], out[native.POISSON_FFT]
     assert a.stats.iterations == b.stats.iterations
     assert np.abs(a.fwd_mesh() - b.fwd_mesh()).max() <= 1e-9
+
+
+@pytest.mark.parametrize("n", [2048, 4096])
+def test_large_grids_converge(n, ot):
+    """Grids above the register transforms' 1024 (the shared-memory FFT of poisson.cu, the
+    largest fast-transform sizes): the solve reaches the threshold, the residual recomputed
+    from the final mesh (quad areas against e^2 times the adjusted density) is within 2x of
+    it, and the map keeps the unit square."""
+    from conftest import mesh_residual
+    from otmap_b200 import native
+    from otmap_b200 import workloads as W
+
+    d = W.to_cells(W.gaussian_mixture(n, 11))
+    s = ot.GridBasedTransportSolver()
+    s.set_verbose_level(0)
+    s.init(n)
+    m = s.solve(d)
+    assert m.stats.outcome == native.CONVERGED
+    assert m.stats.residual <= 1e-7
+    fwd = m.fwd_mesh()
+    assert mesh_residual(fwd, m.density(), n) <= 2e-7
+    assert fwd.min() >= -1e-9 and fwd.max() <= 1 + 1e-9
 
 
 def test_mixed_batch_uses_both_transforms(ot):
