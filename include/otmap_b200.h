@@ -295,7 +295,10 @@ int otm_prune_empty_faces(int nv, const double* xy, int nf, const int* face_star
  *   OTM_ADJOINT_ONE_STEP  lambda = -M^+ G^T dL/dfwd: one cosine-transform Poisson solve
  *                         (M the reference's pseudo-Laplacian, J = -M at psi = 0)
  *   OTM_ADJOINT_KRYLOV    restarted GMRES on J^T, right-preconditioned by M^+, until the
- *                         relative residual is <= tol (or max_iter Poisson solves) */
+ *                         relative residual is <= tol (or max_iter Poisson solves); each
+ *                         restart cycle runs on the device (one graph launch under
+ *                         OTM_LOOP_GRAPH, the same kernels step by step under
+ *                         OTM_LOOP_HOST, with identical results) */
 #define OTM_ADJOINT_ONE_STEP 0
 #define OTM_ADJOINT_KRYLOV 1
 typedef struct {
