@@ -330,3 +330,41 @@ def test_batch_outputs_host_and_device_mixed(ot):
         assert np.array_equal(got, m.fwd_mesh())
         assert np.array_equal(adj_host[k], m.density())
     ctx.close()
+
+
+def test_inverse_and_raster_2048(ot, oracle_port):
+    """Above the benchmarked size: a GPU-solved 2048^2 map (4.2 M faces), 2^18 FP32-drawn
+    query points and the 2048^2 raster. Hit counts and first hits against the reference's
+    own BVH (oracle/_ref), positions against the C oracle's apply_inverse_map (pinned to the
+    reference's goldens), the raster against the reference's rasterize_image: all
+    bit-exact (transport_map.cpp:50-128, rasterizer.cpp:188-236)."""
+    from oracle import ref
+    from otmap_b200 import workloads as W
+
+    if not ref.available():
+        pytest.skip("the reference library (oracle/_ref) is not built")
+    n = 2048
+    s = ot.GridBasedTransportSolver()
+    s.set_verbose_level(0)
+    s.init(n)
+    m = s.solve(W.to_cells(W.gaussian_mixture(n, 21)))
+    fwd, dens = m.fwd_mesh(), m.density()
+    pts = W.random_points(1 << 18, 9)
+    nh_ref, faces_ref, _ = ref.query_all(fwd, n, pts)
+    pos_port, face_port, nh_port, missing_port = oracle_port.apply_inverse(fwd, dens, n, pts)
+    assert np.array_equal(nh_port, nh_ref)
+    tm = ot.TransportMap(n, fwd, dens)
+    p = np.ascontiguousarray(pts.copy())
+    face = np.zeros(p.shape[0], dtype=np.int32)
+    nh = np.zeros(p.shape[0], dtype=np.int32)
+    missing = tm.apply_inverse(p, face, nh)
+    assert missing == missing_port == int((nh_ref == 0).sum())
+    assert np.array_equal(nh, nh_ref)
+    one = nh_ref == 1
+    assert np.array_equal(face[one], faces_ref[one, 0])
+    assert np.array_equal(face, face_port)
+    assert np.array_equal(p, pos_port), int((p != pos_port).any(axis=1).sum())
+    img_ref, _ = ref.rasterize(fwd, n, dens, n, n)
+    img = np.empty((n, n))
+    ot.rasterize_image(fwd, dens, img, n=n)
+    assert np.array_equal(img, img_ref), int((img != img_ref).sum())

@@ -123,3 +123,22 @@ def test_split_options_vs_oracle(case, ot, split_ctx, oracle_port):
     else:
         assert abs(m.stats.iterations - o.iterations) <= 3, (m.stats.iterations, o.iterations)
         check_split(m, o.fwd, converged(oracle_port, d, n, beta_cj, max_ratio), n, threshold)
+
+
+def test_tensor_transform_on_the_128_golden(ot, oracle_port):
+    """The tensor-core transform (OTM_POISSON_TENSOR, split precision) on the reference's
+    128^2 golden: the same bars as the FP32 FFT form."""
+    from otmap_b200 import native
+
+    g = load_golden("solve_mix_n128_s2.npz")
+    n = int(g["n"])
+    ctx = native.Context(0)
+    ctx.set_precision(native.PRECISION_SPLIT)
+    ctx.set_poisson(native.POISSON_TENSOR)
+    m = split_solve(ot, ctx, g["density"], n, beta_cj=int(g["beta_cj"]), max_iter=int(g["max_iter"]),
+                    threshold=float(g["threshold"]), max_ratio=float(g["max_ratio"]))
+    np.testing.assert_allclose(m.density(), g["adjusted"], rtol=1e-13, atol=0)
+    assert abs(m.stats.iterations - int(g["iterations"])) <= 3, (m.stats.iterations, int(g["iterations"]))
+    conv = converged(oracle_port, g["density"], n, beta_cj=int(g["beta_cj"]), max_ratio=float(g["max_ratio"]))
+    check_split(m, g["fwd"], conv, n, float(g["threshold"]))
+    ctx.close()
